@@ -1,0 +1,335 @@
+"""Benchmark of the splat render path on B200.
+
+Headline workload ("frame"): 1M splats, SH degree 3 (16 coefficients per
+channel), means from 8 Gaussian clusters, 1920x1080, cameras on a 30-view
+radius-4 orbit. A step renders one frame through the reference-facing API
+(Splats::render_with: project, onesweep depth sort, look-back scan, emit,
+tile sort, rasterize, with its one host sync for the intersection total).
+
+  value   frames/s, all ranks, device-timed with CUDA events on the launch
+          stream, inputs resident in HBM (236 MB of splat planes > 126 MB L2,
+          so no L2 flush is needed between frames);
+  e2e     the same frames through sf_render_to_host: the camera goes in from
+          host memory and each frame's RGBA8 image comes back into pinned
+          host memory inside the timed region (wall clock);
+  roofline the rasterizer (the dominant kernel) against the FP32 pipe: 24
+          FP32 operations per visited (pixel, splat) pair, pairs counted by
+          the kernel itself;
+  cpu_baseline the CPU oracle (a C++/OpenMP restatement of the reference's
+          kernels) on one frame of the same workload on this host's cores.
+
+--impl reference runs that CPU implementation alone as the reference arm (the
+reference itself is Rust on wgpu and cannot run on this machine).
+Multi-GPU: replicas only (each rank renders its share of the orbit); rank 0
+prints the one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import signal
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_SPLATS, SH_PER_CH, WIDTH, HEIGHT, N_CAMS, RADIUS = 1_000_000, 16, 1920, 1080, 30, 4.0
+WORKLOAD = ("frame: 1M splats SH3 (8 Gaussian clusters sigma 0.3 in [-2,2]^3), 1920x1080, "
+            "30-camera radius-4 orbit")
+METRIC = "1080p frames/s @1M splats"
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 lanes x FMA x 1.965 GHz
+RASTER_FLOPS_PER_PAIR = 24
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples taken while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)], stdout=self.out, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.send_signal(signal.SIGTERM)
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_scene():
+    from splatfield_b200 import synth
+
+    return synth.scene_clustered(N_SPLATS, SH_PER_CH, seed=0)
+
+
+def orbit(make_look_at):
+    from splatfield_b200 import synth
+
+    return synth.orbit_cameras(N_CAMS, RADIUS, WIDTH, HEIGHT, make_look_at)
+
+
+def cpu_frame_time(attr, sh, max_frames=3, budget_s=30.0):
+    """Seconds per frame of the CPU oracle on this host (all OpenMP threads)."""
+    import oracle as O
+
+    cams = orbit(O.look_at)
+    times = []
+    t_total = 0.0
+    for i in range(max_frames):
+        t0 = time.perf_counter()
+        prep = O.prepare(cams[i % len(cams)], WIDTH, HEIGHT, attr, sh, SH_PER_CH)
+        O.rasterize(prep, 0, want_float=False)
+        dt = time.perf_counter() - t0
+        times.append(dt)
+        t_total += dt
+        if t_total > budget_s:
+            break
+    return float(np.median(times)), len(times), O.num_threads()
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the CPU implementation of the path on this host."""
+    if rank != 0:
+        return
+    import oracle as O
+
+    attr, sh = make_scene()
+    cams = orbit(O.look_at)
+    for i in range(args.warmup):
+        prep = O.prepare(cams[i % N_CAMS], WIDTH, HEIGHT, attr, sh, SH_PER_CH)
+        O.rasterize(prep, 0, want_float=False)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        prep = O.prepare(cams[i % N_CAMS], WIDTH, HEIGHT, attr, sh, SH_PER_CH)
+        O.rasterize(prep, 0, want_float=False)
+    dt = time.perf_counter() - t0
+    fps = args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "host cores"},
+        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": O.num_threads(), "kind": "port",
+                         "sample": f"{args.steps} full frames of the workload"},
+        "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "suous/splatfield runs only on wgpu (no Rust toolchain and no graphics stack here); "
+                "its kernels are timed as the C++/OpenMP restatement used as the parity oracle",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world):
+    import torch
+
+    import splatfield_b200 as sf
+    from splatfield_b200 import _lib
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+    ctx = sf.Context(local)
+    attr, sh = make_scene()
+    splats = sf.Splats(attr, sh, ctx)
+    scratch = sf.RenderScratch(N_SPLATS, (WIDTH, HEIGHT), ctx)
+    cams = orbit(sf.look_at)
+    my_cams = [cams[(rank + world * i) % N_CAMS] for i in range(N_CAMS)]
+    stream = torch.cuda.current_stream()
+    size = (WIDTH, HEIGHT)
+
+    for i in range(max(args.warmup, 3)):
+        splats.render_with(scratch, my_cams[i % N_CAMS], size, stream=stream)
+    torch.cuda.synchronize()
+
+    # ---- device-timed frames
+    launches0 = _lib.lib().sf_kernel_launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for i in range(args.steps):
+            splats.render_with(scratch, my_cams[i % N_CAMS], size, stream=stream)
+        end.record(stream)
+        torch.cuda.synchronize()
+    launches = _lib.lib().sf_kernel_launches() - launches0
+    ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    fps = world * args.steps / (ms / 1e3)
+
+    # ---- per-stage split: prepare (everything before the rasterizer) vs rasterizer
+    prep_ms, rast_ms, stats = [], [], None
+    for i in range(min(args.steps, 10)):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        isects = splats.prepare_isects(scratch, my_cams[i % N_CAMS], size, stream=stream)
+        e1.record(stream)
+        splats.finalize_rgb(scratch, isects, size, stream=stream)
+        e2.record(stream)
+        torch.cuda.synchronize()
+        prep_ms.append(e0.elapsed_time(e1))
+        rast_ms.append(e1.elapsed_time(e2))
+        st = scratch.stats(stream)
+        stats = st if stats is None else {k: stats[k] + st[k] for k in st}
+    n_split = min(args.steps, 10)
+    raster_ms = float(np.mean(rast_ms))
+    pairs = stats["pairs_visited"] / n_split
+    achieved = pairs * RASTER_FLOPS_PER_PAIR / (raster_ms / 1e3) / 1e12
+
+    # ---- end to end through the host-facing call
+    host_out = np.empty((HEIGHT, WIDTH), np.uint32)
+    pin = None
+    try:
+        import ctypes as C
+
+        p = C.c_void_p()
+        if _lib.lib().sf_host_alloc(HEIGHT * WIDTH * 4, C.byref(p)) == 0:
+            pin = p
+            host_out = np.ctypeslib.as_array((C.c_uint32 * (HEIGHT * WIDTH)).from_address(p.value)).reshape(HEIGHT, WIDTH)
+    except Exception:
+        pin = None
+    for i in range(2):
+        splats.render_to_host(scratch, my_cams[i], size, out=host_out, stream=stream)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        splats.render_to_host(scratch, my_cams[i % N_CAMS], size, out=host_out, stream=stream)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    if pin is not None:
+        _lib.lib().sf_host_free(pin)
+    e2e_fps = world * args.steps / e2e_s
+
+    if rank != 0:
+        return
+    cpu_s, cpu_frames, cores = cpu_frame_time(attr, sh)
+    clk = clocks.summary()
+    peaks, which = measured_peaks()
+    line = {
+        "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "splats": N_SPLATS, "sh_per_ch": SH_PER_CH, "width": WIDTH,
+                   "height": HEIGHT, "cameras": N_CAMS,
+                   "l2": "inputs larger than L2: 236 MB of splat planes read per frame vs 126 MB L2",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": 36,
+                "d2h_bytes_per_step": WIDTH * HEIGHT * 4,
+                "path": "sf_render_to_host (camera by value, RGBA8 image to pinned host memory)"},
+        "roofline": {"kernel": "raster_kernel<RGB>", "bound": "fp32", "achieved": achieved,
+                     "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS,
+                     "traffic": None, "pairs_per_frame": pairs,
+                     "flops_per_pair": RASTER_FLOPS_PER_PAIR,
+                     "peak_source": "derived: 148 SMs x 128 FP32 lanes x 2 x 1.965 GHz (no measured FP32 peak)"},
+        "stages_ms": {"prepare": float(np.mean(prep_ms)), "raster": raster_ms},
+        "raster_stats": {k: v / n_split for k, v in stats.items()},
+        "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "frames/s", "cores": cores, "kind": "port",
+                         "sample": f"{cpu_frames} full frame(s) of the workload, median"},
+        "clocks": clk,
+        "gpu_launches": int(launches),
+        "peaks": {"source": which, "hbm_gbs": peaks.get("hbm_gbs")},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,281 @@
+/* splatfield_cuda.h — C ABI of the B200 (sm_100a) splat render +
+ * segmentation-evidence path.
+ *
+ * Drop-in for the GPU path of suous/splatfield v0.2.0 (Rust crate API; the
+ * reference has no FFI, so each entry point below names the Rust item it
+ * replaces, as path:line in that project). A Rust caller binds these through a
+ * thin `extern "C"` crate; the Python package `splatfield_b200` binds them
+ * with ctypes.
+ *
+ * Conventions
+ *  - Every call returns an int status: SF_OK (0) or an SF_ERR_* code; the
+ *    message of the last failure on the calling thread is sf_last_error().
+ *    No exception crosses the ABI.
+ *  - `sf_stream` is a cudaStream_t (NULL = the legacy default stream). Work is
+ *    ordered on that stream; a call returns after enqueuing unless noted
+ *    ("syncs") — the reference likewise blocks once per frame on its counters
+ *    readback (src/render.rs:308).
+ *  - Handles are not thread-safe: serialise each handle on one stream, as the
+ *    reference serialises everything on one ordered stream (src/lib.rs:20-27).
+ *  - Device pointers returned by a handle alias that handle's storage and stay
+ *    valid until the handle's next call of the same kind or its destruction
+ *    (the reference's returned tensors alias scratch the same way,
+ *    src/render.rs:366-368, crates/sort/src/sort.rs:278-281).
+ *  - Layouts are the reference's: attributes field-major, plane k of splat i
+ *    at k*n+i, planes [x,y,z,qw,qx,qy,qz,sx,sy,sz,opacity] (src/layout.rs:44-58);
+ *    SH coefficient k, channel c of splat i at (k*3+c)*n+i (src/project.rs:344-388);
+ *    RGBA8 pixels r|g<<8|b<<16|a<<24 with row_stride words per row
+ *    (src/raster.rs:223-229, src/render.rs:150); masks bit-packed LSB-first,
+ *    ceil(w/32) words per row (src/seg/mod.rs:105-143).
+ */
+#ifndef SPLATFIELD_CUDA_H
+#define SPLATFIELD_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SF_ABI_VERSION 1
+
+enum {
+    SF_OK = 0,
+    SF_ERR_ARG = 1,       /* null handle/pointer, bad enum */
+    SF_ERR_SHAPE = 2,     /* sizes inconsistent (e.g. zero splats, n > capacity) */
+    SF_ERR_CAPACITY = 3,  /* intersections exceed a fixed capacity (graph rounds) */
+    SF_ERR_TIMEOUT = 4,   /* a bounded device spin-wait gave up */
+    SF_ERR_CUDA = 5,      /* CUDA runtime error */
+    SF_ERR_NOMEM = 6      /* device allocation failed */
+};
+
+typedef void* sf_stream; /* cudaStream_t */
+typedef struct sf_ctx_t* sf_ctx;
+typedef struct sf_splats_t* sf_splats;
+typedef struct sf_scratch_t* sf_scratch;
+typedef struct sf_accum_t* sf_accum;
+typedef struct sf_mask_t* sf_mask;
+typedef struct sf_beta_t* sf_beta;
+typedef struct sf_radix_t* sf_radix;
+typedef struct sf_scan_t* sf_scan;
+
+/* Camera{fov, position, rotation} (src/camera.rs:5-9); rotation is a unit
+ * quaternion stored x, y, z, w (glam order). */
+typedef struct {
+    float fov[2];
+    float position[3];
+    float rotation[4];
+} sf_camera;
+
+/* CameraView kernel scalars (src/project.rs:63-74), built by
+ * CameraViewLaunch::for_camera (src/project.rs:76-96). */
+typedef struct {
+    float rot0[3], rot1[3], rot2[3];
+    float trans[3];
+    float focal[2];
+    float world_pos[3];
+    float img[2];
+    float tile_bounds[2];
+} sf_view;
+
+/* TileIsects (src/render.rs:463-471), device pointers into the scratch. */
+typedef struct {
+    const uint32_t* tile_ids;     /* sorted tile id per intersection [num_isects] */
+    const uint32_t* gaussian_ids; /* splat id per intersection, tile-major depth-minor */
+    const uint32_t* tile_start;   /* [tiles+1]: tile t's run is [start[t], start[t+1]) */
+    uint32_t num_isects;
+    uint32_t num_visible;
+    uint32_t tile_bounds[2];
+    uint32_t row_stride;
+} sf_isects;
+
+/* ---------------------------------------------------------------- runtime */
+const char* sf_last_error(void);
+int sf_abi_version(void);
+/* Number of kernels this library has launched in this process (all
+ * devices, all handles); a diagnostic for launch accounting. */
+uint64_t sf_kernel_launches(void);
+/* Context on one CUDA device; holds the entropy LUT and device properties. */
+int sf_ctx_create(int device, sf_ctx* out);
+int sf_ctx_destroy(sf_ctx ctx);
+/* Plain device buffers for callers without CUDA bindings of their own. */
+int sf_buffer_alloc(sf_ctx ctx, size_t bytes, void** dptr);
+int sf_buffer_free(sf_ctx ctx, void* dptr);
+int sf_memcpy_htod(void* dst_dev, const void* src_host, size_t bytes, sf_stream stream);
+int sf_memcpy_dtoh(void* dst_host, const void* src_dev, size_t bytes, sf_stream stream);
+int sf_memset(void* dst_dev, int value, size_t bytes, sf_stream stream);
+int sf_stream_sync(sf_stream stream);
+/* Page-locked host memory, for overlapped copies. */
+int sf_host_alloc(size_t bytes, void** hptr);
+int sf_host_free(void* hptr);
+
+/* ----------------------------------------------------------- camera math */
+/* Camera::look_at (src/camera.rs:57-63): minimal arc from +Z, fov 0.8 rad. */
+int sf_camera_look_at(const float position[3], const float target[3], sf_camera* out);
+/* Camera::focal (src/camera.rs:38-40). */
+int sf_camera_focal(const sf_camera* cam, uint32_t w, uint32_t h, float out[2]);
+/* CameraViewLaunch::for_camera (src/project.rs:76-96). */
+int sf_view_for_camera(const sf_camera* cam, uint32_t w, uint32_t h, sf_view* out);
+
+/* ---------------------------------------------------------------- splats */
+/* Splats::new / CpuSplats::upload (src/render.rs:31-33, 242-269): uploads
+ * field-major attributes [11*n] and SH [3*sh_per_ch*n] from host memory;
+ * n must be > 0 (the reference asserts it) and sh_per_ch one of 1, 4, 9, 16. */
+int sf_splats_create(sf_ctx ctx, const float* attributes, const float* sh, uint32_t n,
+                     uint32_t sh_per_ch, sf_splats* out);
+int sf_splats_destroy(sf_splats s);
+/* Splat count, SH coefficients per channel, bounds (min xyz, max xyz) and the
+ * device planes. */
+int sf_splats_info(sf_splats s, uint32_t* n, uint32_t* sh_per_ch, float bounds[6],
+                   const float** attributes_dev, const float** sh_dev);
+
+/* --------------------------------------------------------------- scratch */
+/* RenderScratch::new (src/render.rs:144-167): per-frame buffers for `total`
+ * splats at w x h, reused across frames; rebuilt in place when a frame's shape
+ * differs (src/render.rs:171-197). Intersection capacity grows to the exact
+ * scan total before emission, so nothing is truncated. */
+int sf_scratch_create(sf_ctx ctx, uint32_t total, uint32_t w, uint32_t h, sf_scratch* out);
+int sf_scratch_destroy(sf_scratch s);
+/* Current intersection capacity (entries). */
+int sf_scratch_capacity(sf_scratch s, uint64_t* capacity);
+
+/* ---------------------------------------------------------------- render */
+/* Splats::render_with (src/render.rs:371-380): one RGBA8 frame. Syncs once
+ * (intersection total). *bitmap receives a device pointer [h][row_stride]
+ * aliasing the scratch, valid until the next render on it. */
+int sf_render_with(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                   sf_stream stream, const uint32_t** bitmap, uint32_t* row_stride);
+/* The same frame with a float RGBA plane [h][w][4] (r, g, b, 1-T before
+ * quantisation) in addition to the RGBA8 bitmap. */
+int sf_render_float(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                    sf_stream stream, const float** rgba);
+/* render_with plus the read-back: packed RGBA8 rows [h][w] (stride removed)
+ * written to host memory `out`; syncs. */
+int sf_render_to_host(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w,
+                      uint32_t h, sf_stream stream, uint32_t* out);
+/* Splats::prepare_isects (src/render.rs:274-364): project, depth sort, gather
+ * scan, emit, stable tile sort, tile ranges. Syncs once. */
+int sf_prepare_isects(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                      sf_stream stream, sf_isects* out);
+/* Splats::finalize(Finalize::Rgb) (src/render.rs:387-460) over prepared
+ * intersections; optionally also the float plane. */
+int sf_finalize_rgb(sf_splats s, sf_scratch scratch, const sf_isects* isects, uint32_t w,
+                    uint32_t h, int want_float, sf_stream stream);
+
+/* The scratch's frame outputs (device pointers; rgba is NULL until a float
+ * render ran). */
+int sf_scratch_buffers(sf_scratch s, const uint32_t** bitmap, const float** rgba,
+                       uint32_t* row_stride);
+
+/* Pair statistics of the scratch's last rasterization (syncs): out[0] =
+ * (pixel, splat) pairs visited (256 per tile-list entry walked before the
+ * tile's early exit), out[1] = exponentials evaluated, out[2] = contributing
+ * pairs (alpha >= 1/255), out[3] = 0. */
+int sf_scratch_stats(sf_scratch s, uint64_t out[4], sf_stream stream);
+
+/* Intermediates of the last prepare, copied to host (syncs), for parity
+ * checks and debugging. `what`: */
+enum {
+    SF_READ_DEPTH_KEYS = 0,  /* u32 [total]: f32 bits of camera z, 0xFFFFFFFF culled */
+    SF_READ_TILE_COUNTS = 1, /* u32 [total] */
+    SF_READ_BBOX = 2,        /* u32 [2*total] packed min/max */
+    SF_READ_PROJECTED = 3,   /* f32 [9*total] reference row [mean.xy, conic.xyz, rgb, opacity] */
+    SF_READ_ORDER = 4,       /* u32 [num_visible] depth order */
+    SF_READ_OFFSETS = 5,     /* u32 [num_visible] gather-scan offsets */
+    SF_READ_TILE_IDS = 6,    /* u32 [num_isects] sorted */
+    SF_READ_GAUSSIAN_IDS = 7,/* u32 [num_isects] sorted */
+    SF_READ_TILE_START = 8,  /* u32 [tiles+1] */
+    SF_READ_BITMAP = 9,      /* u32 [h*row_stride] */
+    SF_READ_RGBA = 10,       /* f32 [h*w*4] */
+    SF_READ_FINAL_T = 11,    /* f32 [h*w] */
+    SF_READ_N_CONTRIB = 12   /* u32 [h*w] */
+};
+int sf_scratch_read(sf_scratch s, int what, void* host, size_t bytes, sf_stream stream);
+
+/* ------------------------------------------------------ responsibility / evidence */
+/* Accumulators::new (src/seg/mod.rs:62-69): u32 fixed-point resp/fg/bg [total]. */
+int sf_accum_create(sf_ctx ctx, uint32_t total, sf_accum* out);
+int sf_accum_destroy(sf_accum a);
+/* The current fixed-point scale and the device arrays. */
+int sf_accum_info(sf_accum a, float* scale, const uint32_t** resp, const uint32_t** fg,
+                  const uint32_t** bg);
+/* Set the fixed-point scale (the render paths set it from the frame size;
+ * the reference's tests build accumulators with an explicit scale,
+ * src/seg/beta.rs:351-359). */
+int sf_accum_set_scale(sf_accum a, float scale);
+/* Mask::from_bytes (src/seg/mod.rs:118-143): one byte per pixel, nonzero =
+ * foreground; packs and uploads. *fg_pixels gets the foreground count. */
+int sf_mask_create(sf_ctx ctx, uint32_t w, uint32_t h, const uint8_t* bytes, sf_mask* out,
+                   uint32_t* fg_pixels);
+/* A mask already packed (u32 words [h*ceil(w/32)], host memory). */
+int sf_mask_create_packed(sf_ctx ctx, uint32_t w, uint32_t h, const uint32_t* words, sf_mask* out);
+int sf_mask_destroy(sf_mask m);
+/* Splats::render_responsibility (src/seg/mod.rs:150-159): clears resp and
+ * accumulates eps_i = sum_p trunc(alpha*T*scale). Syncs once. */
+int sf_render_responsibility(sf_splats s, sf_scratch scratch, sf_accum acc, const sf_camera* cam,
+                             uint32_t w, uint32_t h, sf_stream stream);
+/* Splats::accumulate_prepared (src/seg/mod.rs:170-210): over intersections
+ * already prepared for this camera and size; mask NULL = total
+ * responsibility, else the fg/bg evidence split. */
+int sf_accumulate_prepared(sf_splats s, sf_scratch scratch, const sf_isects* isects, uint32_t w,
+                           uint32_t h, sf_accum acc, sf_mask mask, sf_stream stream);
+/* fractional_bits (src/seg/mod.rs:31-34) and the scale 2^bits. */
+uint32_t sf_fractional_bits(uint32_t w, uint32_t h);
+
+/* ------------------------------------------------------------ Beta / EIG */
+enum { SF_EIG_LUT_F32 = 0, SF_EIG_FP64 = 1 };
+/* BetaState::new_uniform (src/seg/beta.rs:230-238): a = b = 1. */
+int sf_beta_create_uniform(sf_ctx ctx, uint32_t total, sf_beta* out);
+/* A posterior from host arrays (the reference's test `state`, beta.rs:302-310). */
+int sf_beta_create(sf_ctx ctx, const float* a, const float* b, uint32_t n, sf_beta* out);
+int sf_beta_destroy(sf_beta beta);
+int sf_beta_read(sf_beta beta, float* a, float* b, sf_stream stream);
+int sf_beta_info(sf_beta beta, uint32_t* n, float** a_dev, float** b_dev);
+/* BetaState::eig (src/seg/beta.rs:241-268): EIG = sum_i dH_i for the accumulator's
+ * responsibility. mode SF_EIG_LUT_F32 reads the f32 445x445 log-spaced LUT
+ * (beta.rs:128-201); SF_EIG_FP64 evaluates the f64 lgamma/digamma entropy on
+ * the GPU. Reduced on the device in f64 (no partials read-back); syncs. */
+int sf_beta_eig(sf_beta beta, sf_accum acc, int mode, sf_stream stream, double* eig);
+/* Asynchronous form: the EIG lands in device memory `eig_dev` (one double). */
+int sf_beta_eig_async(sf_beta beta, sf_accum acc, int mode, double* eig_dev, sf_stream stream);
+/* BetaState::update (src/seg/beta.rs:273-286): a += fg/scale, b += bg/scale. */
+int sf_beta_update(sf_beta beta, sf_accum acc, sf_stream stream);
+/* map_labels (src/seg/beta.rs:294-297): out[i] = a[i] > b[i]. Host arrays. */
+int sf_map_labels(const float* a, const float* b, uint32_t n, uint8_t* out);
+/* The f32 entropy LUT the EIG kernel reads (445*445 floats, host copy). */
+int sf_entropy_table(float* out);
+/* table_entropy probe (beta.rs:336-342): out[i] = H_LUT(a[i], b[i]), device arrays. */
+int sf_table_entropy(sf_ctx ctx, const float* a, const float* b, uint32_t n, float* out,
+                     sf_stream stream);
+
+/* ------------------------------------------------------- sort / scan */
+/* bits_for (crates/sort/src/sort.rs:259-261). */
+uint32_t sf_bits_for(uint32_t max_exclusive);
+/* RadixScratch::new (crates/sort/src/sort.rs:291-300). */
+int sf_radix_create(sf_ctx ctx, uint32_t max_elems, sf_radix* out);
+int sf_radix_destroy(sf_radix r);
+/* RadixScratch::argsort (crates/sort/src/sort.rs:311-380): stable LSD sort of
+ * keys[0..n) by their low `bits` bits, carrying vals. Inputs are only read.
+ * Outputs are device pointers into the scratch (or the inputs themselves when
+ * n <= 1 or bits == 0, as the reference returns). write_keys = 0 leaves the
+ * returned keys stale (values are always sorted). Onesweep: 8-bit digits, one
+ * upfront histogram, one decoupled-look-back pass per digit. */
+int sf_radix_argsort(sf_radix r, const uint32_t* keys, const uint32_t* vals, uint32_t n,
+                     uint32_t bits, int write_keys, sf_stream stream, const uint32_t** keys_out,
+                     const uint32_t** vals_out);
+/* ScanScratch::new (crates/sort/src/scan.rs:54-59). */
+int sf_scan_create(sf_ctx ctx, uint32_t max_elems, sf_scan* out);
+int sf_scan_destroy(sf_scan s);
+/* exclusive_scan_gather (crates/sort/src/scan.rs:219-255):
+ * offsets[i] = sum_{j<i} counts[gids[j]], single-pass decoupled look-back;
+ * n = 0 writes nothing. */
+int sf_exclusive_scan_gather(sf_scan s, const uint32_t* gids, const uint32_t* counts,
+                             uint32_t* offsets, uint32_t n, sf_stream stream);
+/* exclusive_scan_buf (crates/sort/src/scan.rs:185-213): in place. */
+int sf_exclusive_scan(sf_scan s, uint32_t* buf, uint32_t n, sf_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPLATFIELD_CUDA_H */

@@ -1,0 +1,622 @@
+"""Host-side mirror of the reference's Rust API over the C ABI.
+
+Names follow suous/splatfield v0.2.0: ``CpuSplats.upload`` / ``Splats``
+(src/render.rs:25-269), ``RenderScratch`` (:116-198), ``Splats.render_with``
+(:371-380), ``prepare_isects`` / ``finalize`` (:274-460), ``Camera``
+(src/camera.rs:5-63), ``Accumulators`` / ``Mask`` / ``render_responsibility``
+/ ``accumulate_prepared`` (src/seg/mod.rs:52-210), ``BetaState`` /
+``map_labels`` (src/seg/beta.rs:215-297), ``RadixScratch`` / ``bits_for``
+(crates/sort/src/sort.rs:259-381), ``ScanScratch`` / ``exclusive_scan_gather``
+(crates/sort/src/scan.rs:49-255). Errors the reference raises by panicking
+(zero splats, undersized scratch) raise ``SplatfieldError`` here.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import Camera, Isects, SplatfieldError, View, check, lib
+
+__all__ = [
+    "Camera", "View", "Isects", "SplatfieldError", "Context", "default_context", "DeviceBuffer",
+    "DeviceView", "camera_default", "look_at", "focal", "view_for_camera", "CpuSplats", "Splats",
+    "RenderScratch", "TileIsects", "Accumulators", "Mask", "BetaState", "map_labels", "bits_for",
+    "RadixScratch", "ScanScratch", "exclusive_scan_gather", "exclusive_scan_buf", "entropy_table",
+    "table_entropy", "fractional_bits", "row_stride_for", "EIG_LUT_F32", "EIG_FP64",
+]
+
+EIG_LUT_F32, EIG_FP64 = L.EIG_LUT_F32, L.EIG_FP64
+BASE_FOV = 0.8  # Camera::BASE_FOV (src/camera.rs:86)
+
+
+def _vp(x) -> C.c_void_p:
+    if x is None:
+        return None
+    if isinstance(x, (DeviceBuffer, DeviceView)):
+        return C.c_void_p(x.ptr)
+    if isinstance(x, int):
+        return C.c_void_p(x)
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data_as(C.c_void_p)
+    raise TypeError(type(x))
+
+
+def _stream(stream) -> C.c_void_p:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    # torch.cuda.Stream and friends
+    return C.c_void_p(int(getattr(stream, "cuda_stream")))
+
+
+class Context:
+    """One CUDA device; owns the entropy LUT."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().sf_ctx_create(device, C.byref(h)))
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            lib().sf_ctx_destroy(self.handle)
+            self.handle = None
+
+
+_DEFAULT: Context | None = None
+
+
+def default_context() -> Context:
+    global _DEFAULT
+    if _DEFAULT is None:
+        _DEFAULT = Context(0)
+    return _DEFAULT
+
+
+class DeviceView:
+    """A non-owning view of device memory returned by the library (it aliases
+    a handle's storage, like the reference's returned GpuTensors)."""
+
+    def __init__(self, ptr: int, dtype, shape, keepalive=None):
+        self.ptr = int(ptr or 0)
+        self.dtype = np.dtype(dtype)
+        self.shape = tuple(shape)
+        self._keep = keepalive
+
+    @property
+    def nbytes(self) -> int:
+        return int(np.prod(self.shape)) * self.dtype.itemsize
+
+    def read(self, stream=None) -> np.ndarray:
+        """Blocking read-back (GpuTensor::read_vec)."""
+        out = np.empty(self.shape, self.dtype)
+        if out.nbytes:
+            check(lib().sf_memcpy_dtoh(_vp(out), C.c_void_p(self.ptr), out.nbytes, _stream(stream)))
+        return out
+
+
+class DeviceBuffer(DeviceView):
+    """An owned device allocation."""
+
+    def __init__(self, nbytes_or_array, dtype=np.uint32, ctx: Context | None = None, shape=None):
+        self.ctx = ctx or default_context()
+        if isinstance(nbytes_or_array, np.ndarray):
+            arr = np.ascontiguousarray(nbytes_or_array)
+            dtype, shape, nbytes = arr.dtype, arr.shape, arr.nbytes
+        else:
+            nbytes = int(nbytes_or_array)
+            arr = None
+            dtype = np.dtype(dtype)
+            shape = shape or (nbytes // dtype.itemsize,)
+        p = C.c_void_p()
+        check(lib().sf_buffer_alloc(self.ctx.handle, max(nbytes, 1), C.byref(p)))
+        super().__init__(p.value, dtype, shape)
+        if arr is not None and arr.nbytes:
+            self.write(arr)
+
+    @classmethod
+    def from_array(cls, arr, ctx: Context | None = None) -> "DeviceBuffer":
+        return cls(np.ascontiguousarray(arr), ctx=ctx)
+
+    @classmethod
+    def empty(cls, count: int, dtype=np.uint32, ctx: Context | None = None) -> "DeviceBuffer":
+        dt = np.dtype(dtype)
+        return cls(count * dt.itemsize, dt, ctx, shape=(count,))
+
+    def write(self, arr: np.ndarray, stream=None) -> None:
+        arr = np.ascontiguousarray(arr)
+        check(lib().sf_memcpy_htod(C.c_void_p(self.ptr), _vp(arr), arr.nbytes, _stream(stream)))
+        check(lib().sf_stream_sync(_stream(stream)))
+
+    def fill_zero(self, stream=None) -> None:
+        check(lib().sf_memset(C.c_void_p(self.ptr), 0, self.nbytes, _stream(stream)))
+
+    def free(self):
+        if self.ptr:
+            lib().sf_buffer_free(self.ctx.handle, C.c_void_p(self.ptr))
+            self.ptr = 0
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ camera
+
+def camera_default() -> Camera:
+    """Camera::default (src/camera.rs:72-80)."""
+    return make_camera()
+
+
+def make_camera(fov=(BASE_FOV, BASE_FOV), position=(0.0, 0.0, 0.0), rotation=(0.0, 0.0, 0.0, 1.0)) -> Camera:
+    c = Camera()
+    c.fov[:] = [float(v) for v in fov]
+    c.position[:] = [float(v) for v in position]
+    c.rotation[:] = [float(v) for v in rotation]
+    return c
+
+
+def quat_from_rotation_y(angle: float):
+    h = np.float32(angle) * np.float32(0.5)
+    return (0.0, float(np.sin(h, dtype=np.float32)), 0.0, float(np.cos(h, dtype=np.float32)))
+
+
+def look_at(position, target) -> Camera:
+    """Camera::look_at (src/camera.rs:57-63)."""
+    out = Camera()
+    p = np.ascontiguousarray(position, np.float32)
+    t = np.ascontiguousarray(target, np.float32)
+    check(lib().sf_camera_look_at(_vp(p), _vp(t), C.byref(out)))
+    return out
+
+
+def focal(cam: Camera, w: int, h: int):
+    out = np.empty(2, np.float32)
+    check(lib().sf_camera_focal(C.byref(cam), w, h, _vp(out)))
+    return out
+
+
+def view_for_camera(cam: Camera, w: int, h: int) -> View:
+    v = View()
+    check(lib().sf_view_for_camera(C.byref(cam), w, h, C.byref(v)))
+    return v
+
+
+def row_stride_for(w: int) -> int:
+    return ((4 * w + 255) // 256 * 256) // 4
+
+
+# ------------------------------------------------------------------ splats
+
+class CpuSplats:
+    """Host splat payload, field-major (src/render.rs:20-28)."""
+
+    def __init__(self, attributes, sh_coeffs):
+        self.attributes = np.ascontiguousarray(attributes, np.float32).reshape(-1)
+        self.sh_coeffs = np.ascontiguousarray(sh_coeffs, np.float32).reshape(-1)
+
+    def count(self) -> int:
+        return self.attributes.size // 11
+
+    def upload(self, ctx: Context | None = None) -> "Splats":
+        return Splats(self.attributes, self.sh_coeffs, ctx)
+
+
+class Splats:
+    """GPU splats (Splats::new, src/render.rs:242-269)."""
+
+    def __init__(self, attributes, sh_coeffs, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        attributes = np.ascontiguousarray(attributes, np.float32).reshape(-1)
+        sh_coeffs = np.ascontiguousarray(sh_coeffs, np.float32).reshape(-1)
+        n = attributes.size // 11
+        k = sh_coeffs.size // max(3 * n, 1) if n else 1
+        h = C.c_void_p()
+        check(lib().sf_splats_create(self.ctx.handle, _vp(attributes), _vp(sh_coeffs), n, k, C.byref(h)))
+        self.handle = h
+        self.n = n
+        self.sh_per_ch = k
+        b = np.empty(6, np.float32)
+        check(lib().sf_splats_info(h, None, None, _vp(b), None, None))
+        self.bounds = (b[:3].copy(), b[3:].copy())
+        self.positions = attributes[: 3 * n].copy()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sf_splats_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- render paths
+    def render_with(self, scratch: "RenderScratch", camera: Camera, img_size, stream=None) -> DeviceView:
+        w, h = img_size
+        ptr = C.c_void_p()
+        rs = C.c_uint32()
+        check(lib().sf_render_with(self.handle, scratch.handle, C.byref(camera), w, h, _stream(stream),
+                                   C.byref(ptr), C.byref(rs)))
+        return DeviceView(ptr.value, np.uint32, (h, rs.value), scratch)
+
+    def render_float(self, scratch: "RenderScratch", camera: Camera, img_size, stream=None) -> DeviceView:
+        w, h = img_size
+        ptr = C.c_void_p()
+        check(lib().sf_render_float(self.handle, scratch.handle, C.byref(camera), w, h, _stream(stream),
+                                    C.byref(ptr)))
+        return DeviceView(ptr.value, np.float32, (h, w, 4), scratch)
+
+    def render_to_host(self, scratch: "RenderScratch", camera: Camera, img_size, out=None, stream=None):
+        w, h = img_size
+        if out is None:
+            out = np.empty((h, w), np.uint32)
+        check(lib().sf_render_to_host(self.handle, scratch.handle, C.byref(camera), w, h, _stream(stream),
+                                      _vp(out)))
+        return out
+
+    def prepare_isects(self, scratch: "RenderScratch", camera: Camera, img_size, stream=None) -> "TileIsects":
+        w, h = img_size
+        out = Isects()
+        check(lib().sf_prepare_isects(self.handle, scratch.handle, C.byref(camera), w, h, _stream(stream),
+                                      C.byref(out)))
+        return TileIsects(out, scratch)
+
+    def finalize_rgb(self, scratch: "RenderScratch", isects: "TileIsects", img_size, want_float=False,
+                     stream=None) -> DeviceView:
+        w, h = img_size
+        check(lib().sf_finalize_rgb(self.handle, scratch.handle, C.byref(isects.raw), w, h,
+                                    1 if want_float else 0, _stream(stream)))
+        return DeviceView(scratch.bitmap_ptr(), np.uint32, (h, isects.raw.row_stride), scratch)
+
+    def render_responsibility(self, scratch: "RenderScratch", acc: "Accumulators", camera: Camera, img_size,
+                              stream=None) -> None:
+        w, h = img_size
+        check(lib().sf_render_responsibility(self.handle, scratch.handle, acc.handle, C.byref(camera), w, h,
+                                             _stream(stream)))
+        acc._sync_scale()
+
+    def accumulate_prepared(self, scratch: "RenderScratch", isects: "TileIsects", img_size,
+                            acc: "Accumulators", mask: "Mask | None" = None, stream=None) -> None:
+        w, h = img_size
+        check(lib().sf_accumulate_prepared(self.handle, scratch.handle, C.byref(isects.raw), w, h,
+                                           acc.handle, mask.handle if mask else None, _stream(stream)))
+        acc._sync_scale()
+
+
+class TileIsects:
+    def __init__(self, raw: Isects, scratch):
+        self.raw = raw
+        self._scratch = scratch
+
+    @property
+    def num_isects(self) -> int:
+        return int(self.raw.num_isects)
+
+    @property
+    def num_visible(self) -> int:
+        return int(self.raw.num_visible)
+
+    @property
+    def tile_bounds(self):
+        return (int(self.raw.tile_bounds[0]), int(self.raw.tile_bounds[1]))
+
+    def tile_ids(self) -> DeviceView:
+        return DeviceView(self.raw.tile_ids, np.uint32, (self.num_isects,), self._scratch)
+
+    def gaussian_ids(self) -> DeviceView:
+        return DeviceView(self.raw.gaussian_ids, np.uint32, (self.num_isects,), self._scratch)
+
+
+class RenderScratch:
+    """Per-frame buffers (RenderScratch::new, src/render.rs:144-167)."""
+
+    def __init__(self, total: int, img_size, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        w, h = img_size
+        hd = C.c_void_p()
+        check(lib().sf_scratch_create(self.ctx.handle, total, w, h, C.byref(hd)))
+        self.handle = hd
+
+    def capacity(self) -> int:
+        c = C.c_uint64()
+        check(lib().sf_scratch_capacity(self.handle, C.byref(c)))
+        return int(c.value)
+
+    def read(self, what: int, count: int, dtype=np.uint32, stream=None) -> np.ndarray:
+        out = np.empty(count, dtype)
+        check(lib().sf_scratch_read(self.handle, what, _vp(out), out.nbytes, _stream(stream)))
+        return out
+
+    def stats(self, stream=None) -> dict:
+        """Pair statistics of the last rasterization on this scratch."""
+        out = np.zeros(4, np.uint64)
+        check(lib().sf_scratch_stats(self.handle, _vp(out), _stream(stream)))
+        return dict(pairs_visited=int(out[0]), exp_evaluated=int(out[1]), contributing=int(out[2]))
+
+    def bitmap_ptr(self) -> int:
+        b = C.c_void_p()
+        check(lib().sf_scratch_buffers(self.handle, C.byref(b), None, None))
+        return b.value
+
+    def rgba_ptr(self) -> int:
+        r = C.c_void_p()
+        check(lib().sf_scratch_buffers(self.handle, None, C.byref(r), None))
+        return r.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sf_scratch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------ segmentation
+
+def fractional_bits(w: int, h: int) -> int:
+    return int(lib().sf_fractional_bits(w, h))
+
+
+class Accumulators:
+    """u32 fixed-point eps / fg / bg per splat (src/seg/mod.rs:52-85)."""
+
+    def __init__(self, total: int, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        check(lib().sf_accum_create(self.ctx.handle, total, C.byref(h)))
+        self.handle = h
+        self.total = total
+        self.scale = 1.0
+        self._ptrs()
+
+    def _ptrs(self):
+        s = C.c_float()
+        r, f, b = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(lib().sf_accum_info(self.handle, C.byref(s), C.byref(r), C.byref(f), C.byref(b)))
+        self.scale = float(s.value)
+        self.bits = DeviceView(r.value, np.uint32, (self.total,), self)
+        self.fg = DeviceView(f.value, np.uint32, (self.total,), self)
+        self.bg = DeviceView(b.value, np.uint32, (self.total,), self)
+
+    def _sync_scale(self):
+        s = C.c_float()
+        check(lib().sf_accum_info(self.handle, C.byref(s), None, None, None))
+        self.scale = float(s.value)
+
+    def set_scale(self, scale: float) -> None:
+        check(lib().sf_accum_set_scale(self.handle, float(scale)))
+        self.scale = float(scale)
+
+    def write_bits(self, bits) -> None:
+        """Overwrite the total-responsibility words (host array of total u32)."""
+        b = np.ascontiguousarray(bits, np.uint32)
+        if b.size != self.total:
+            raise SplatfieldError(L.SF_ERR_SHAPE, "bits length must equal the accumulator size")
+        check(lib().sf_memcpy_htod(C.c_void_p(self.bits.ptr), _vp(b), b.nbytes, None))
+        check(lib().sf_stream_sync(None))
+
+    @classmethod
+    def from_eps(cls, eps, scale: float, ctx: "Context | None" = None) -> "Accumulators":
+        """An accumulator holding trunc(eps * scale) at `scale` (the reference
+        tests' eps_acc, src/seg/beta.rs:351-359)."""
+        bits = (np.asarray(eps, np.float32) * np.float32(scale)).astype(np.uint32)
+        acc = cls(bits.size, ctx)
+        acc.write_bits(bits)
+        acc.set_scale(scale)
+        return acc
+
+    def read_f32(self) -> np.ndarray:
+        return self.bits.read().astype(np.float32) / np.float32(self.scale)
+
+    def read_evidence_f32(self):
+        s = np.float32(self.scale)
+        return self.fg.read().astype(np.float32) / s, self.bg.read().astype(np.float32) / s
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sf_accum_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Mask:
+    """Bit-packed binary mask (src/seg/mod.rs:105-144)."""
+
+    def __init__(self, handle, size, fg_pixels: int):
+        self.handle = handle
+        self.size = tuple(size)
+        self.words_per_row = (size[0] + 31) // 32
+        self.fg_pixels = fg_pixels
+
+    @classmethod
+    def from_bytes(cls, size, data, ctx: Context | None = None) -> "Mask":
+        ctx = ctx or default_context()
+        w, h = size
+        b = np.ascontiguousarray(data, np.uint8).reshape(-1)
+        if b.size != w * h:
+            raise SplatfieldError(L.SF_ERR_SHAPE, "mask bytes must be one per pixel")
+        hd = C.c_void_p()
+        fg = C.c_uint32()
+        check(lib().sf_mask_create(ctx.handle, w, h, _vp(b), C.byref(hd), C.byref(fg)))
+        return cls(hd, size, int(fg.value))
+
+    @classmethod
+    def from_words(cls, size, words, ctx: Context | None = None) -> "Mask":
+        ctx = ctx or default_context()
+        w, h = size
+        wd = np.ascontiguousarray(words, np.uint32).reshape(-1)
+        hd = C.c_void_p()
+        check(lib().sf_mask_create_packed(ctx.handle, w, h, _vp(wd), C.byref(hd)))
+        return cls(hd, size, int(sum(bin(int(x)).count("1") for x in wd)))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sf_mask_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BetaState:
+    """Per-splat Beta(a, b) posteriors (src/seg/beta.rs:215-287)."""
+
+    def __init__(self, handle, n: int, ctx: Context):
+        self.handle = handle
+        self.n = n
+        self.ctx = ctx
+
+    @classmethod
+    def new_uniform(cls, total: int, ctx: Context | None = None) -> "BetaState":
+        ctx = ctx or default_context()
+        h = C.c_void_p()
+        check(lib().sf_beta_create_uniform(ctx.handle, total, C.byref(h)))
+        return cls(h, total, ctx)
+
+    @classmethod
+    def from_host(cls, a, b, ctx: Context | None = None) -> "BetaState":
+        ctx = ctx or default_context()
+        a = np.ascontiguousarray(a, np.float32)
+        b = np.ascontiguousarray(b, np.float32)
+        h = C.c_void_p()
+        check(lib().sf_beta_create(ctx.handle, _vp(a), _vp(b), a.size, C.byref(h)))
+        return cls(h, a.size, ctx)
+
+    def eig(self, acc: Accumulators, mode: int = EIG_LUT_F32, stream=None) -> float:
+        out = C.c_double()
+        check(lib().sf_beta_eig(self.handle, acc.handle, mode, _stream(stream), C.byref(out)))
+        return float(out.value)
+
+    def update(self, acc: Accumulators, stream=None) -> None:
+        check(lib().sf_beta_update(self.handle, acc.handle, _stream(stream)))
+
+    def read(self, stream=None):
+        a = np.empty(self.n, np.float32)
+        b = np.empty(self.n, np.float32)
+        check(lib().sf_beta_read(self.handle, _vp(a), _vp(b), _stream(stream)))
+        return a, b
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sf_beta_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def map_labels(a, b) -> np.ndarray:
+    """MAP foreground labels a > b (src/seg/beta.rs:294-297)."""
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    if a.size != b.size:
+        raise SplatfieldError(L.SF_ERR_SHAPE, "posterior length mismatch")
+    out = np.empty(a.size, np.uint8)
+    check(lib().sf_map_labels(_vp(a), _vp(b), a.size, _vp(out)))
+    return out.astype(bool)
+
+
+def entropy_table() -> np.ndarray:
+    t = np.empty(445 * 445, np.float32)
+    check(lib().sf_entropy_table(_vp(t)))
+    return t
+
+
+def table_entropy(a, b, ctx: Context | None = None) -> np.ndarray:
+    """The probe of the LUT lookup the EIG kernel uses (src/seg/beta.rs:336-342)."""
+    ctx = ctx or default_context()
+    da = DeviceBuffer.from_array(np.asarray(a, np.float32), ctx)
+    db = DeviceBuffer.from_array(np.asarray(b, np.float32), ctx)
+    out = DeviceBuffer.empty(da.shape[0], np.float32, ctx)
+    check(lib().sf_table_entropy(ctx.handle, _vp(da), _vp(db), da.shape[0], _vp(out), None))
+    return out.read()
+
+
+# ------------------------------------------------------------- sort / scan
+
+def bits_for(max_exclusive: int) -> int:
+    """bits_for (crates/sort/src/sort.rs:259-261)."""
+    return int(lib().sf_bits_for(int(max_exclusive) & 0xFFFFFFFF))
+
+
+class RadixScratch:
+    """Onesweep radix scratch (RadixScratch, crates/sort/src/sort.rs:282-381)."""
+
+    def __init__(self, max_elems: int, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        check(lib().sf_radix_create(self.ctx.handle, max_elems, C.byref(h)))
+        self.handle = h
+        self.max = max_elems
+
+    def argsort(self, keys, vals, n: int, bits: int, write_keys: bool = True, stream=None):
+        ko, vo = C.c_void_p(), C.c_void_p()
+        check(lib().sf_radix_argsort(self.handle, _vp(keys), _vp(vals), n, bits, 1 if write_keys else 0,
+                                     _stream(stream), C.byref(ko), C.byref(vo)))
+        return DeviceView(ko.value, np.uint32, (n,), self), DeviceView(vo.value, np.uint32, (n,), self)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sf_radix_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ScanScratch:
+    """Decoupled look-back scan scratch (ScanScratch, crates/sort/src/scan.rs:49-60)."""
+
+    def __init__(self, max_elems: int, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        check(lib().sf_scan_create(self.ctx.handle, max_elems, C.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sf_scan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def exclusive_scan_gather(gids, counts, offsets, n: int, scratch: ScanScratch, stream=None) -> None:
+    """offsets[i] = sum_{j<i} counts[gids[j]] (crates/sort/src/scan.rs:219-255)."""
+    check(lib().sf_exclusive_scan_gather(scratch.handle, _vp(gids), _vp(counts), _vp(offsets), n,
+                                         _stream(stream)))
+
+
+def exclusive_scan_buf(buf, n: int, scratch: ScanScratch, stream=None) -> None:
+    check(lib().sf_exclusive_scan(scratch.handle, _vp(buf), n, _stream(stream)))

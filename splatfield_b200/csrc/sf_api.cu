@@ -1,0 +1,1081 @@
+// C ABI of the splat path: handles, buffer ownership, capacity management and
+// the per-frame orchestration of the kernels (see include/splatfield_cuda.h).
+//
+// Frame = project -> depth sort (onesweep, 32-bit keys, values = splat ids)
+// -> gather scan of tile counts in depth order (decoupled look-back) ->
+// [one host sync: intersection total] -> grow capacity if needed -> emit ->
+// stable tile sort (onesweep over bits_for(tiles) bits) -> tile starts ->
+// rasterize. This is the reference's prepare_isects/finalize sequence
+// (src/render.rs:274-460) with its 3-launch-per-digit sort and hierarchical
+// scan replaced, and with capacity grown before emission instead of the
+// reference's silent truncation (src/raster.rs:38-46).
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+#include "sf_internal.h"
+
+using namespace sfk;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define SF_CK(expr)                                                                        \
+    do {                                                                                   \
+        cudaError_t e_ = (expr);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            if (e_ == cudaErrorMemoryAllocation)                                           \
+                return fail(SF_ERR_NOMEM, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+            return fail(SF_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));  \
+        }                                                                                  \
+    } while (0)
+
+#define SF_TRY(body)                                                  \
+    try {                                                             \
+        body                                                          \
+    } catch (const std::bad_alloc&) {                                 \
+        return fail(SF_ERR_NOMEM, "host allocation failed");          \
+    } catch (const std::exception& ex) {                              \
+        return fail(SF_ERR_ARG, ex.what());                           \
+    } catch (...) {                                                   \
+        return fail(SF_ERR_ARG, "unknown exception");                 \
+    }
+
+inline cudaStream_t S(sf_stream s) { return reinterpret_cast<cudaStream_t>(s); }
+
+cudaError_t use_device(int dev) {
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return e;
+    return cur == dev ? cudaSuccess : cudaSetDevice(dev);
+}
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+}
+
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree(reinterpret_cast<void*>(p));
+    p = nullptr;
+}
+
+uint32_t bits_for_u32(uint32_t max_exclusive) {
+    const uint32_t m = max_exclusive > 0 ? max_exclusive - 1 : 0;
+    return m == 0 ? 0u : 32u - (uint32_t)__builtin_clz(m);
+}
+
+uint64_t next_pow2(uint64_t v) {
+    uint64_t p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+uint32_t frac_bits(uint32_t w, uint32_t h) {
+    const uint64_t pixels = (uint64_t)w * h;
+    uint32_t tz = 0;
+    uint64_t p2 = 1;
+    while (p2 < pixels) { p2 <<= 1; ++tz; }
+    return tz >= 32 ? 0u : 32u - tz;
+}
+
+// Largest intersection capacity: the look-back status words carry 30-bit
+// counts.
+constexpr uint64_t kMaxIsects = (1ull << 30) - 1;
+// First-frame capacity cap (the reference's INITIAL_ISECTS_CAP, render.rs:18).
+constexpr uint64_t kInitialIsects = 1ull << 22;
+
+}  // namespace
+
+struct sf_ctx_t {
+    int device = 0;
+    int sm_count = 148;
+    float* lut = nullptr;
+};
+
+struct sf_splats_t {
+    sf_ctx ctx = nullptr;
+    uint32_t n = 0, K = 1;
+    float* attr = nullptr;
+    float* sh = nullptr;
+    float bounds[6] = {0, 0, 0, 0, 0, 0};
+};
+
+struct sf_scratch_t {
+    sf_ctx ctx = nullptr;
+    uint32_t total = 0, w = 0, h = 0, tiles_x = 0, tiles_y = 0, row_stride = 0;
+    uint32_t* depth_keys = nullptr;
+    uint32_t* tile_counts = nullptr;
+    uint2* bbox = nullptr;
+    float4* geo0 = nullptr;
+    float4* geo1 = nullptr;
+    float4* color = nullptr;
+    uint32_t *keys_a = nullptr, *keys_b = nullptr, *order_a = nullptr, *order_b = nullptr;
+    const uint32_t* order = nullptr;
+    uint32_t* offsets = nullptr;
+    void* sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+    void* scan_tmp = nullptr;
+    uint64_t cap = 0;
+    uint32_t *tid_e = nullptr, *gid_e = nullptr, *tid_a = nullptr, *gid_a = nullptr;
+    const uint32_t* tids = nullptr;
+    const uint32_t* gids = nullptr;
+    uint32_t* tile_start = nullptr;
+    uint32_t* bitmap = nullptr;
+    float4* rgba = nullptr;
+    float* final_t = nullptr;
+    uint32_t* n_contrib = nullptr;
+    // device words: [0] visible, [1] error bits, [2..3] spare, then u64 total at +16
+    uint32_t* words = nullptr;
+    uint32_t* host_words = nullptr;  // pinned mirror
+    unsigned long long* stats = nullptr;  // raster pair statistics of the last finalize
+    uint32_t num_visible = 0, num_isects = 0;
+    uint64_t last_isects_raw = 0;
+    bool prepared = false;
+};
+
+struct sf_accum_t {
+    sf_ctx ctx = nullptr;
+    uint32_t total = 0;
+    uint32_t *resp = nullptr, *fg = nullptr, *bg = nullptr;
+    float scale = 1.0f;
+};
+
+struct sf_mask_t {
+    uint32_t w = 0, h = 0, wpr = 0;
+    uint32_t* bits = nullptr;
+};
+
+struct sf_beta_t {
+    sf_ctx ctx = nullptr;
+    uint32_t n = 0;
+    float *a = nullptr, *b = nullptr;
+    double* partials = nullptr;
+    uint32_t blocks = 1;
+    double* out = nullptr;
+    double* host_out = nullptr;
+};
+
+struct sf_radix_t {
+    sf_ctx ctx = nullptr;
+    uint32_t max = 0;
+    uint32_t *ka = nullptr, *va = nullptr, *kb = nullptr, *vb = nullptr;
+    void* tmp = nullptr;
+    uint32_t* err = nullptr;
+};
+
+struct sf_scan_t {
+    sf_ctx ctx = nullptr;
+    uint32_t max = 0;
+    void* tmp = nullptr;
+    unsigned long long* total = nullptr;
+    uint32_t* err = nullptr;
+};
+
+// ---------------------------------------------------------------- helpers
+
+namespace {
+
+cudaError_t ensure_lut(sf_ctx ctx) {
+    if (ctx->lut) return cudaSuccess;
+    std::vector<float> t((size_t)kGridPts * kGridPts);
+    build_entropy_table(t.data());
+    cudaError_t e = dalloc(&ctx->lut, t.size());
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(ctx->lut, t.data(), t.size() * 4, cudaMemcpyHostToDevice);
+}
+
+void scratch_free_frame(sf_scratch s) {
+    dfree(s->depth_keys); dfree(s->tile_counts); dfree(s->bbox); dfree(s->geo0); dfree(s->geo1);
+    dfree(s->color); dfree(s->keys_a); dfree(s->keys_b); dfree(s->order_a); dfree(s->order_b);
+    dfree(s->offsets); dfree(s->scan_tmp); dfree(s->tile_start); dfree(s->bitmap);
+    dfree(s->rgba); dfree(s->final_t); dfree(s->n_contrib);
+    s->order = nullptr;
+    s->prepared = false;
+}
+
+void scratch_free_isects(sf_scratch s) {
+    dfree(s->tid_e); dfree(s->gid_e); dfree(s->tid_a); dfree(s->gid_a);
+    if (s->sort_tmp) cudaFree(s->sort_tmp);
+    s->sort_tmp = nullptr;
+    s->sort_tmp_bytes = 0;
+    s->cap = 0;
+    s->tids = s->gids = nullptr;
+}
+
+cudaError_t ensure_sort_tmp(sf_scratch s, size_t bytes) {
+    if (s->sort_tmp_bytes >= bytes) return cudaSuccess;
+    if (s->sort_tmp) cudaFree(s->sort_tmp);
+    s->sort_tmp = nullptr;
+    s->sort_tmp_bytes = 0;
+    cudaError_t e = cudaMalloc(&s->sort_tmp, bytes);
+    if (e == cudaSuccess) s->sort_tmp_bytes = bytes;
+    return e;
+}
+
+cudaError_t grow_isects(sf_scratch s, uint64_t want) {
+    if (want <= s->cap && s->tid_e) return cudaSuccess;
+    const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(next_pow2(want), 1024), kMaxIsects + 1);
+    dfree(s->tid_e); dfree(s->gid_e); dfree(s->tid_a); dfree(s->gid_a);
+    s->cap = 0;
+    cudaError_t e;
+    if ((e = dalloc(&s->tid_e, cap)) != cudaSuccess) return e;
+    if ((e = dalloc(&s->gid_e, cap)) != cudaSuccess) return e;
+    if ((e = dalloc(&s->tid_a, cap)) != cudaSuccess) return e;
+    if ((e = dalloc(&s->gid_a, cap)) != cudaSuccess) return e;
+    s->cap = cap;
+    return ensure_sort_tmp(s, std::max(radix_temp_bytes((uint32_t)std::min<uint64_t>(cap, kMaxIsects), 4),
+                                       radix_temp_bytes(s->total, 4)));
+}
+
+cudaError_t scratch_build(sf_scratch s, uint32_t total, uint32_t w, uint32_t h) {
+    scratch_free_frame(s);
+    s->total = total;
+    s->w = w;
+    s->h = h;
+    s->tiles_x = (w + 15) / 16;
+    s->tiles_y = (h + 15) / 16;
+    s->row_stride = ((4 * w + 255) / 256 * 256) / 4;
+    cudaError_t e;
+#define SF_AL(ptr, cnt) if ((e = dalloc(&(ptr), (cnt))) != cudaSuccess) return e
+    SF_AL(s->depth_keys, total);
+    SF_AL(s->tile_counts, total);
+    SF_AL(s->bbox, total);
+    SF_AL(s->geo0, total);
+    SF_AL(s->geo1, total);
+    SF_AL(s->color, total);
+    SF_AL(s->keys_a, total);
+    SF_AL(s->keys_b, total);
+    SF_AL(s->order_a, total);
+    SF_AL(s->order_b, total);
+    SF_AL(s->offsets, total);
+    SF_AL(s->tile_start, (size_t)s->tiles_x * s->tiles_y + 1);
+    SF_AL(s->bitmap, (size_t)h * s->row_stride);
+#undef SF_AL
+    if ((e = cudaMalloc(&s->scan_tmp, scan_temp_bytes(total))) != cudaSuccess) return e;
+    if (!s->words) {
+        if ((e = dalloc(&s->stats, 4)) != cudaSuccess) return e;
+        if ((e = dalloc(&s->words, 8)) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(reinterpret_cast<void**>(&s->host_words), 32)) != cudaSuccess) return e;
+    }
+    // Capacity: keep the larger of the growth hint and the reference's first
+    // frame rule min(tiles*total, 2^22) (render.rs:146-147, 177-183).
+    const uint64_t first = std::min<uint64_t>((uint64_t)s->tiles_x * s->tiles_y * total, kInitialIsects);
+    return grow_isects(s, std::max<uint64_t>(std::max<uint64_t>(first, s->last_isects_raw), s->cap));
+}
+
+// prepare_isects (src/render.rs:274-364).
+int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32_t h,
+            cudaStream_t st, sf_isects* out) {
+    if (!sp || !s || !cam) return fail(SF_ERR_ARG, "null argument");
+    if (w == 0 || h == 0 || w > 65535 * 16 || h > 65535 * 16) return fail(SF_ERR_SHAPE, "bad image size");
+    SF_CK(use_device(s->ctx->device));
+    if (s->total != sp->n || s->w != w || s->h != h) SF_CK(scratch_build(s, sp->n, w, h));
+    sf_view view;
+    view_for_camera(*cam, w, h, &view);
+    const uint32_t n = sp->n;
+    uint32_t* words = s->words;
+    unsigned long long* total_dev = reinterpret_cast<unsigned long long*>(words + 4);
+    SF_CK(cudaMemsetAsync(words, 0, 32, st));
+    ProjOut po{s->depth_keys, s->tile_counts, s->bbox, s->geo0, s->geo1, s->color, words};
+    SF_CK(launch_project(view, sp->attr, sp->sh, n, sp->K, po, st));
+    int in_b = 0;
+    SF_CK(ensure_sort_tmp(s, radix_temp_bytes(n, 4)));
+    SF_CK(radix_sort_pairs(s->depth_keys, nullptr, s->keys_a, s->order_a, s->keys_b, s->order_b, n,
+                           nullptr, n, 32, false, true, s->sort_tmp, words + 1, s->ctx->sm_count, st,
+                           &in_b));
+    s->order = in_b ? s->order_b : s->order_a;
+    SF_CK(exclusive_scan(s->order, s->tile_counts, s->offsets, n, nullptr, n, s->scan_tmp, total_dev,
+                         words + 1, st));
+    SF_CK(cudaMemcpyAsync(s->host_words, words, 32, cudaMemcpyDeviceToHost, st));
+    SF_CK(cudaStreamSynchronize(st));
+    if (s->host_words[1] & SF_DEV_ERR_TIMEOUT) return fail(SF_ERR_TIMEOUT, "device look-back wait timed out");
+    uint64_t total = 0;
+    std::memcpy(&total, s->host_words + 4, 8);
+    s->num_visible = s->host_words[0];
+    s->last_isects_raw = total;
+    if (total > kMaxIsects) return fail(SF_ERR_CAPACITY, "intersection count exceeds 2^30-1");
+    if (total > s->cap) {
+        std::fprintf(stderr, "splatfield_b200: intersection capacity %llu reached (%llu emitted); growing\n",
+                     (unsigned long long)s->cap, (unsigned long long)total);
+        SF_CK(grow_isects(s, total));
+    }
+    const uint32_t I = (uint32_t)total;
+    SF_CK(launch_emit(s->order, s->bbox, s->offsets, n, s->tiles_x, (uint32_t)s->cap, s->tid_e,
+                      s->gid_e, words + 1, st));
+    const uint32_t tiles = s->tiles_x * s->tiles_y;
+    const uint32_t tbits = bits_for_u32(tiles);
+    if (I <= 1 || tbits == 0) {
+        s->tids = s->tid_e;
+        s->gids = s->gid_e;
+    } else {
+        SF_CK(radix_sort_pairs(s->tid_e, s->gid_e, s->tid_a, s->gid_a, s->tid_e, s->gid_e, I, nullptr, I,
+                               tbits, true, false, s->sort_tmp, words + 1, s->ctx->sm_count, st, &in_b));
+        s->tids = in_b ? s->tid_e : s->tid_a;
+        s->gids = in_b ? s->gid_e : s->gid_a;
+    }
+    SF_CK(launch_tile_starts(s->tids, I, nullptr, I, tiles, s->tile_start, st));
+    s->num_isects = I;
+    s->prepared = true;
+    if (out) {
+        out->tile_ids = s->tids;
+        out->gaussian_ids = s->gids;
+        out->tile_start = s->tile_start;
+        out->num_isects = I;
+        out->num_visible = s->num_visible;
+        out->tile_bounds[0] = s->tiles_x;
+        out->tile_bounds[1] = s->tiles_y;
+        out->row_stride = s->row_stride;
+    }
+    return SF_OK;
+}
+
+RasterArgs raster_args(sf_scratch s, const sf_isects* is) {
+    RasterArgs a{};
+    a.w = s->w;
+    a.h = s->h;
+    a.tiles_x = s->tiles_x;
+    a.tiles_y = s->tiles_y;
+    a.row_stride = s->row_stride;
+    a.tile_start = is ? is->tile_start : s->tile_start;
+    a.gaussian_ids = is ? is->gaussian_ids : s->gids;
+    a.geo0 = s->geo0;
+    a.geo1 = s->geo1;
+    a.color = s->color;
+    a.stats = s->stats;
+    return a;
+}
+
+int finalize_rgb(sf_scratch s, const sf_isects* is, bool want_float, cudaStream_t st) {
+    RasterArgs a = raster_args(s, is);
+    a.bitmap = s->bitmap;
+    if (want_float) {
+        if (!s->rgba) SF_CK(dalloc(&s->rgba, (size_t)s->w * s->h));
+        a.rgba = s->rgba;
+    }
+    SF_CK(cudaMemsetAsync(s->stats, 0, 32, st));
+    SF_CK(launch_raster(0, a, st));
+    return SF_OK;
+}
+
+int accumulate(sf_scratch s, const sf_isects* is, uint32_t w, uint32_t h, sf_accum acc, sf_mask mask,
+               cudaStream_t st) {
+    if (acc->total != s->total) return fail(SF_ERR_SHAPE, "accumulator size does not match the scratch");
+    acc->scale = (float)((uint64_t)1 << frac_bits(w, h));
+    RasterArgs a = raster_args(s, is);
+    a.scale = acc->scale;
+    SF_CK(cudaMemsetAsync(s->stats, 0, 32, st));
+    if (!mask) {
+        SF_CK(cudaMemsetAsync(acc->resp, 0, (size_t)acc->total * 4, st));
+        a.resp = acc->resp;
+        SF_CK(launch_raster(1, a, st));
+    } else {
+        if (mask->w != w || mask->h != h) return fail(SF_ERR_SHAPE, "mask size does not match the frame");
+        SF_CK(cudaMemsetAsync(acc->fg, 0, (size_t)acc->total * 4, st));
+        SF_CK(cudaMemsetAsync(acc->bg, 0, (size_t)acc->total * 4, st));
+        a.mask = mask->bits;
+        a.mask_wpr = mask->wpr;
+        a.fg = acc->fg;
+        a.bg = acc->bg;
+        SF_CK(launch_raster(2, a, st));
+    }
+    return SF_OK;
+}
+
+}  // namespace
+
+// ================================================================ C ABI
+
+extern "C" {
+
+const char* sf_last_error(void) { return g_err.c_str(); }
+uint64_t sf_kernel_launches(void) { return sfk::launches(); }
+int sf_abi_version(void) { return SF_ABI_VERSION; }
+
+int sf_ctx_create(int device, sf_ctx* out) {
+    SF_TRY({
+        if (!out) return fail(SF_ERR_ARG, "null out");
+        *out = nullptr;
+        int count = 0;
+        SF_CK(cudaGetDeviceCount(&count));
+        if (device < 0 || device >= count) return fail(SF_ERR_ARG, "no such CUDA device");
+        SF_CK(cudaSetDevice(device));
+        auto* c = new sf_ctx_t();
+        c->device = device;
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->sm_count = prop.multiProcessorCount;
+        *out = c;
+        return SF_OK;
+    })
+}
+
+int sf_ctx_destroy(sf_ctx ctx) {
+    if (!ctx) return SF_OK;
+    use_device(ctx->device);
+    dfree(ctx->lut);
+    delete ctx;
+    return SF_OK;
+}
+
+int sf_buffer_alloc(sf_ctx ctx, size_t bytes, void** dptr) {
+    if (!ctx || !dptr) return fail(SF_ERR_ARG, "null argument");
+    SF_CK(use_device(ctx->device));
+    SF_CK(cudaMalloc(dptr, bytes ? bytes : 1));
+    return SF_OK;
+}
+
+int sf_buffer_free(sf_ctx ctx, void* dptr) {
+    if (!ctx) return fail(SF_ERR_ARG, "null ctx");
+    if (dptr) SF_CK(cudaFree(dptr));
+    return SF_OK;
+}
+
+int sf_memcpy_htod(void* dst, const void* src, size_t bytes, sf_stream stream) {
+    if (bytes == 0) return SF_OK;
+    SF_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, S(stream)));
+    return SF_OK;
+}
+
+int sf_memcpy_dtoh(void* dst, const void* src, size_t bytes, sf_stream stream) {
+    if (bytes == 0) return SF_OK;
+    SF_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, S(stream)));
+    SF_CK(cudaStreamSynchronize(S(stream)));
+    return SF_OK;
+}
+
+int sf_memset(void* dst, int value, size_t bytes, sf_stream stream) {
+    if (bytes == 0) return SF_OK;
+    SF_CK(cudaMemsetAsync(dst, value, bytes, S(stream)));
+    return SF_OK;
+}
+
+int sf_stream_sync(sf_stream stream) {
+    SF_CK(cudaStreamSynchronize(S(stream)));
+    return SF_OK;
+}
+
+int sf_host_alloc(size_t bytes, void** hptr) {
+    if (!hptr) return fail(SF_ERR_ARG, "null argument");
+    SF_CK(cudaMallocHost(hptr, bytes ? bytes : 1));
+    return SF_OK;
+}
+
+int sf_host_free(void* hptr) {
+    if (hptr) SF_CK(cudaFreeHost(hptr));
+    return SF_OK;
+}
+
+int sf_camera_look_at(const float position[3], const float target[3], sf_camera* out) {
+    if (!position || !target || !out) return fail(SF_ERR_ARG, "null argument");
+    camera_look_at(position, target, out);
+    return SF_OK;
+}
+
+int sf_camera_focal(const sf_camera* cam, uint32_t w, uint32_t h, float out[2]) {
+    if (!cam || !out) return fail(SF_ERR_ARG, "null argument");
+    sf_view v;
+    view_for_camera(*cam, w, h, &v);
+    out[0] = v.focal[0];
+    out[1] = v.focal[1];
+    return SF_OK;
+}
+
+int sf_view_for_camera(const sf_camera* cam, uint32_t w, uint32_t h, sf_view* out) {
+    if (!cam || !out) return fail(SF_ERR_ARG, "null argument");
+    view_for_camera(*cam, w, h, out);
+    return SF_OK;
+}
+
+int sf_splats_create(sf_ctx ctx, const float* attributes, const float* sh, uint32_t n,
+                     uint32_t sh_per_ch, sf_splats* out) {
+    SF_TRY({
+        if (!ctx || !attributes || !sh || !out) return fail(SF_ERR_ARG, "null argument");
+        *out = nullptr;
+        if (n == 0) return fail(SF_ERR_SHAPE, "Splats::new: zero splats");
+        if (sh_per_ch != 1 && sh_per_ch != 4 && sh_per_ch != 9 && sh_per_ch != 16)
+            return fail(SF_ERR_SHAPE, "sh_per_ch must be 1, 4, 9 or 16");
+        SF_CK(use_device(ctx->device));
+        auto* s = new sf_splats_t();
+        s->ctx = ctx;
+        s->n = n;
+        s->K = sh_per_ch;
+        cudaError_t e = dalloc(&s->attr, (size_t)11 * n);
+        if (e == cudaSuccess) e = dalloc(&s->sh, (size_t)3 * sh_per_ch * n);
+        if (e == cudaSuccess) e = cudaMemcpy(s->attr, attributes, (size_t)11 * n * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(s->sh, sh, (size_t)3 * sh_per_ch * n * 4, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            dfree(s->attr);
+            dfree(s->sh);
+            delete s;
+            return fail(e == cudaErrorMemoryAllocation ? SF_ERR_NOMEM : SF_ERR_CUDA, cudaGetErrorString(e));
+        }
+        for (int k = 0; k < 3; ++k) { s->bounds[k] = 3.4028235e38f; s->bounds[3 + k] = -3.4028235e38f; }
+        for (uint32_t i = 0; i < n; ++i)
+            for (int k = 0; k < 3; ++k) {
+                const float v = attributes[(size_t)k * n + i];
+                s->bounds[k] = std::min(s->bounds[k], v);
+                s->bounds[3 + k] = std::max(s->bounds[3 + k], v);
+            }
+        *out = s;
+        return SF_OK;
+    })
+}
+
+int sf_splats_destroy(sf_splats s) {
+    if (!s) return SF_OK;
+    use_device(s->ctx->device);
+    dfree(s->attr);
+    dfree(s->sh);
+    delete s;
+    return SF_OK;
+}
+
+int sf_splats_info(sf_splats s, uint32_t* n, uint32_t* sh_per_ch, float bounds[6],
+                   const float** attributes_dev, const float** sh_dev) {
+    if (!s) return fail(SF_ERR_ARG, "null splats");
+    if (n) *n = s->n;
+    if (sh_per_ch) *sh_per_ch = s->K;
+    if (bounds) std::memcpy(bounds, s->bounds, sizeof(s->bounds));
+    if (attributes_dev) *attributes_dev = s->attr;
+    if (sh_dev) *sh_dev = s->sh;
+    return SF_OK;
+}
+
+int sf_scratch_create(sf_ctx ctx, uint32_t total, uint32_t w, uint32_t h, sf_scratch* out) {
+    SF_TRY({
+        if (!ctx || !out) return fail(SF_ERR_ARG, "null argument");
+        *out = nullptr;
+        if (w == 0 || h == 0) return fail(SF_ERR_SHAPE, "zero image size");
+        SF_CK(use_device(ctx->device));
+        auto* s = new sf_scratch_t();
+        s->ctx = ctx;
+        cudaError_t e = scratch_build(s, total, w, h);
+        if (e != cudaSuccess) {
+            scratch_free_frame(s);
+            scratch_free_isects(s);
+            delete s;
+            return fail(e == cudaErrorMemoryAllocation ? SF_ERR_NOMEM : SF_ERR_CUDA, cudaGetErrorString(e));
+        }
+        *out = s;
+        return SF_OK;
+    })
+}
+
+int sf_scratch_destroy(sf_scratch s) {
+    if (!s) return SF_OK;
+    use_device(s->ctx->device);
+    scratch_free_frame(s);
+    scratch_free_isects(s);
+    dfree(s->words);
+    dfree(s->stats);
+    if (s->host_words) cudaFreeHost(s->host_words);
+    delete s;
+    return SF_OK;
+}
+
+int sf_scratch_capacity(sf_scratch s, uint64_t* capacity) {
+    if (!s || !capacity) return fail(SF_ERR_ARG, "null argument");
+    *capacity = s->cap;
+    return SF_OK;
+}
+
+int sf_prepare_isects(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                      sf_stream stream, sf_isects* out) {
+    SF_TRY({ return prepare(s, scratch, cam, w, h, S(stream), out); })
+}
+
+int sf_finalize_rgb(sf_splats s, sf_scratch scratch, const sf_isects* isects, uint32_t w, uint32_t h,
+                    int want_float, sf_stream stream) {
+    SF_TRY({
+        if (!s || !scratch || !isects) return fail(SF_ERR_ARG, "null argument");
+        if (!scratch->prepared || scratch->w != w || scratch->h != h)
+            return fail(SF_ERR_SHAPE, "finalize without a matching prepare");
+        return finalize_rgb(scratch, isects, want_float != 0, S(stream));
+    })
+}
+
+int sf_render_with(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                   sf_stream stream, const uint32_t** bitmap, uint32_t* row_stride) {
+    SF_TRY({
+        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr);
+        if (rc != SF_OK) return rc;
+        rc = finalize_rgb(scratch, nullptr, false, S(stream));
+        if (rc != SF_OK) return rc;
+        if (bitmap) *bitmap = scratch->bitmap;
+        if (row_stride) *row_stride = scratch->row_stride;
+        return SF_OK;
+    })
+}
+
+int sf_render_float(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                    sf_stream stream, const float** rgba) {
+    SF_TRY({
+        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr);
+        if (rc != SF_OK) return rc;
+        rc = finalize_rgb(scratch, nullptr, true, S(stream));
+        if (rc != SF_OK) return rc;
+        if (rgba) *rgba = reinterpret_cast<const float*>(scratch->rgba);
+        return SF_OK;
+    })
+}
+
+int sf_render_to_host(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                      sf_stream stream, uint32_t* out) {
+    SF_TRY({
+        if (!out) return fail(SF_ERR_ARG, "null out");
+        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr);
+        if (rc != SF_OK) return rc;
+        rc = finalize_rgb(scratch, nullptr, false, S(stream));
+        if (rc != SF_OK) return rc;
+        SF_CK(cudaMemcpy2DAsync(out, (size_t)w * 4, scratch->bitmap, (size_t)scratch->row_stride * 4,
+                                (size_t)w * 4, h, cudaMemcpyDeviceToHost, S(stream)));
+        SF_CK(cudaStreamSynchronize(S(stream)));
+        return SF_OK;
+    })
+}
+
+int sf_scratch_stats(sf_scratch s, uint64_t out[4], sf_stream stream) {
+    if (!s || !out) return fail(SF_ERR_ARG, "null argument");
+    SF_CK(use_device(s->ctx->device));
+    SF_CK(cudaMemcpyAsync(out, s->stats, 32, cudaMemcpyDeviceToHost, S(stream)));
+    SF_CK(cudaStreamSynchronize(S(stream)));
+    return SF_OK;
+}
+
+int sf_scratch_buffers(sf_scratch s, const uint32_t** bitmap, const float** rgba, uint32_t* row_stride) {
+    if (!s) return fail(SF_ERR_ARG, "null scratch");
+    if (bitmap) *bitmap = s->bitmap;
+    if (rgba) *rgba = reinterpret_cast<const float*>(s->rgba);
+    if (row_stride) *row_stride = s->row_stride;
+    return SF_OK;
+}
+
+int sf_scratch_read(sf_scratch s, int what, void* host, size_t bytes, sf_stream stream) {
+    SF_TRY({
+        if (!s || !host) return fail(SF_ERR_ARG, "null argument");
+        cudaStream_t st = S(stream);
+        SF_CK(use_device(s->ctx->device));
+        const void* src = nullptr;
+        size_t avail = 0;
+        float* rows = nullptr;
+        switch (what) {
+            case SF_READ_DEPTH_KEYS: src = s->depth_keys; avail = (size_t)s->total * 4; break;
+            case SF_READ_TILE_COUNTS: src = s->tile_counts; avail = (size_t)s->total * 4; break;
+            case SF_READ_BBOX: src = s->bbox; avail = (size_t)s->total * 8; break;
+            case SF_READ_PROJECTED:
+                SF_CK(dalloc(&rows, (size_t)s->total * 9));
+                SF_CK(launch_export_rows(s->geo0, s->geo1, s->color, s->depth_keys, s->total, rows, st));
+                src = rows;
+                avail = (size_t)s->total * 36;
+                break;
+            case SF_READ_ORDER: src = s->order; avail = (size_t)s->num_visible * 4; break;
+            case SF_READ_OFFSETS: src = s->offsets; avail = (size_t)s->num_visible * 4; break;
+            case SF_READ_TILE_IDS: src = s->tids; avail = (size_t)s->num_isects * 4; break;
+            case SF_READ_GAUSSIAN_IDS: src = s->gids; avail = (size_t)s->num_isects * 4; break;
+            case SF_READ_TILE_START: src = s->tile_start; avail = ((size_t)s->tiles_x * s->tiles_y + 1) * 4; break;
+            case SF_READ_BITMAP: src = s->bitmap; avail = (size_t)s->h * s->row_stride * 4; break;
+            case SF_READ_RGBA: src = s->rgba; avail = s->rgba ? (size_t)s->w * s->h * 16 : 0; break;
+            case SF_READ_FINAL_T: src = s->final_t; avail = s->final_t ? (size_t)s->w * s->h * 4 : 0; break;
+            case SF_READ_N_CONTRIB: src = s->n_contrib; avail = s->n_contrib ? (size_t)s->w * s->h * 4 : 0; break;
+            default: return fail(SF_ERR_ARG, "unknown scratch field");
+        }
+        if (bytes > avail || (bytes && !src)) {
+            dfree(rows);
+            return fail(SF_ERR_SHAPE, "read exceeds the field's size");
+        }
+        cudaError_t e = bytes ? cudaMemcpyAsync(host, src, bytes, cudaMemcpyDeviceToHost, st) : cudaSuccess;
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        dfree(rows);
+        SF_CK(e);
+        return SF_OK;
+    })
+}
+
+// ------------------------------------------------------------ accumulators
+
+uint32_t sf_fractional_bits(uint32_t w, uint32_t h) { return frac_bits(w, h); }
+
+int sf_accum_create(sf_ctx ctx, uint32_t total, sf_accum* out) {
+    SF_TRY({
+        if (!ctx || !out) return fail(SF_ERR_ARG, "null argument");
+        *out = nullptr;
+        SF_CK(use_device(ctx->device));
+        auto* a = new sf_accum_t();
+        a->ctx = ctx;
+        a->total = total;
+        cudaError_t e = dalloc(&a->resp, total);
+        if (e == cudaSuccess) e = dalloc(&a->fg, total);
+        if (e == cudaSuccess) e = dalloc(&a->bg, total);
+        if (e == cudaSuccess) e = cudaMemset(a->resp, 0, (size_t)std::max(total, 1u) * 4);
+        if (e == cudaSuccess) e = cudaMemset(a->fg, 0, (size_t)std::max(total, 1u) * 4);
+        if (e == cudaSuccess) e = cudaMemset(a->bg, 0, (size_t)std::max(total, 1u) * 4);
+        if (e != cudaSuccess) {
+            dfree(a->resp); dfree(a->fg); dfree(a->bg);
+            delete a;
+            return fail(SF_ERR_NOMEM, cudaGetErrorString(e));
+        }
+        *out = a;
+        return SF_OK;
+    })
+}
+
+int sf_accum_destroy(sf_accum a) {
+    if (!a) return SF_OK;
+    use_device(a->ctx->device);
+    dfree(a->resp); dfree(a->fg); dfree(a->bg);
+    delete a;
+    return SF_OK;
+}
+
+int sf_accum_info(sf_accum a, float* scale, const uint32_t** resp, const uint32_t** fg,
+                  const uint32_t** bg) {
+    if (!a) return fail(SF_ERR_ARG, "null accumulator");
+    if (scale) *scale = a->scale;
+    if (resp) *resp = a->resp;
+    if (fg) *fg = a->fg;
+    if (bg) *bg = a->bg;
+    return SF_OK;
+}
+
+int sf_accum_set_scale(sf_accum a, float scale) {
+    if (!a) return fail(SF_ERR_ARG, "null accumulator");
+    if (!(scale > 0.0f)) return fail(SF_ERR_ARG, "scale must be positive");
+    a->scale = scale;
+    return SF_OK;
+}
+
+int sf_mask_create_packed(sf_ctx ctx, uint32_t w, uint32_t h, const uint32_t* words, sf_mask* out) {
+    SF_TRY({
+        if (!ctx || !words || !out) return fail(SF_ERR_ARG, "null argument");
+        *out = nullptr;
+        SF_CK(use_device(ctx->device));
+        auto* m = new sf_mask_t();
+        m->w = w;
+        m->h = h;
+        m->wpr = (w + 31) / 32;
+        const size_t cnt = (size_t)m->wpr * h;
+        cudaError_t e = dalloc(&m->bits, cnt);
+        if (e == cudaSuccess && cnt) e = cudaMemcpy(m->bits, words, cnt * 4, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            dfree(m->bits);
+            delete m;
+            return fail(SF_ERR_CUDA, cudaGetErrorString(e));
+        }
+        *out = m;
+        return SF_OK;
+    })
+}
+
+int sf_mask_create(sf_ctx ctx, uint32_t w, uint32_t h, const uint8_t* bytes, sf_mask* out,
+                   uint32_t* fg_pixels) {
+    SF_TRY({
+        if (!bytes) return fail(SF_ERR_ARG, "null mask bytes");
+        const uint32_t wpr = (w + 31) / 32;
+        std::vector<uint32_t> bits((size_t)wpr * h, 0u);
+        uint32_t fg = 0;
+        for (uint32_t y = 0; y < h; ++y)
+            for (uint32_t x = 0; x < w; ++x)
+                if (bytes[(size_t)y * w + x]) {
+                    bits[(size_t)y * wpr + x / 32] |= 1u << (x % 32);
+                    ++fg;
+                }
+        if (fg_pixels) *fg_pixels = fg;
+        return sf_mask_create_packed(ctx, w, h, bits.data(), out);
+    })
+}
+
+int sf_mask_destroy(sf_mask m) {
+    if (!m) return SF_OK;
+    dfree(m->bits);
+    delete m;
+    return SF_OK;
+}
+
+int sf_render_responsibility(sf_splats s, sf_scratch scratch, sf_accum acc, const sf_camera* cam,
+                             uint32_t w, uint32_t h, sf_stream stream) {
+    SF_TRY({
+        if (!acc) return fail(SF_ERR_ARG, "null accumulator");
+        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr);
+        if (rc != SF_OK) return rc;
+        return accumulate(scratch, nullptr, w, h, acc, nullptr, S(stream));
+    })
+}
+
+int sf_accumulate_prepared(sf_splats s, sf_scratch scratch, const sf_isects* isects, uint32_t w,
+                           uint32_t h, sf_accum acc, sf_mask mask, sf_stream stream) {
+    SF_TRY({
+        if (!s || !scratch || !isects || !acc) return fail(SF_ERR_ARG, "null argument");
+        if (!scratch->prepared || scratch->w != w || scratch->h != h)
+            return fail(SF_ERR_SHAPE, "accumulate without a matching prepare");
+        SF_CK(use_device(scratch->ctx->device));
+        return accumulate(scratch, isects, w, h, acc, mask, S(stream));
+    })
+}
+
+// ------------------------------------------------------------------ Beta
+
+static int beta_alloc(sf_ctx ctx, uint32_t n, sf_beta* out) {
+    auto* b = new sf_beta_t();
+    b->ctx = ctx;
+    b->n = n;
+    b->blocks = eig_blocks(n, ctx->sm_count);
+    cudaError_t e = dalloc(&b->a, n);
+    if (e == cudaSuccess) e = dalloc(&b->b, n);
+    if (e == cudaSuccess) e = dalloc(&b->partials, b->blocks);
+    if (e == cudaSuccess) e = dalloc(&b->out, 1);
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&b->host_out), 8);
+    if (e == cudaSuccess) e = ensure_lut(ctx);
+    if (e != cudaSuccess) {
+        dfree(b->a); dfree(b->b); dfree(b->partials); dfree(b->out);
+        if (b->host_out) cudaFreeHost(b->host_out);
+        delete b;
+        return fail(SF_ERR_NOMEM, cudaGetErrorString(e));
+    }
+    *out = b;
+    return SF_OK;
+}
+
+int sf_beta_create_uniform(sf_ctx ctx, uint32_t total, sf_beta* out) {
+    SF_TRY({
+        if (!ctx || !out) return fail(SF_ERR_ARG, "null argument");
+        *out = nullptr;
+        SF_CK(use_device(ctx->device));
+        std::vector<float> ones(std::max(total, 1u), 1.0f);
+        sf_beta b = nullptr;
+        int rc = beta_alloc(ctx, total, &b);
+        if (rc != SF_OK) return rc;
+        SF_CK(cudaMemcpy(b->a, ones.data(), (size_t)total * 4, cudaMemcpyHostToDevice));
+        SF_CK(cudaMemcpy(b->b, ones.data(), (size_t)total * 4, cudaMemcpyHostToDevice));
+        *out = b;
+        return SF_OK;
+    })
+}
+
+int sf_beta_create(sf_ctx ctx, const float* a, const float* bb, uint32_t n, sf_beta* out) {
+    SF_TRY({
+        if (!ctx || !a || !bb || !out) return fail(SF_ERR_ARG, "null argument");
+        *out = nullptr;
+        SF_CK(use_device(ctx->device));
+        sf_beta b = nullptr;
+        int rc = beta_alloc(ctx, n, &b);
+        if (rc != SF_OK) return rc;
+        SF_CK(cudaMemcpy(b->a, a, (size_t)n * 4, cudaMemcpyHostToDevice));
+        SF_CK(cudaMemcpy(b->b, bb, (size_t)n * 4, cudaMemcpyHostToDevice));
+        *out = b;
+        return SF_OK;
+    })
+}
+
+int sf_beta_destroy(sf_beta b) {
+    if (!b) return SF_OK;
+    use_device(b->ctx->device);
+    dfree(b->a); dfree(b->b); dfree(b->partials); dfree(b->out);
+    if (b->host_out) cudaFreeHost(b->host_out);
+    delete b;
+    return SF_OK;
+}
+
+int sf_beta_read(sf_beta b, float* a, float* bb, sf_stream stream) {
+    if (!b) return fail(SF_ERR_ARG, "null beta");
+    if (a) SF_CK(cudaMemcpyAsync(a, b->a, (size_t)b->n * 4, cudaMemcpyDeviceToHost, S(stream)));
+    if (bb) SF_CK(cudaMemcpyAsync(bb, b->b, (size_t)b->n * 4, cudaMemcpyDeviceToHost, S(stream)));
+    SF_CK(cudaStreamSynchronize(S(stream)));
+    return SF_OK;
+}
+
+int sf_beta_info(sf_beta b, uint32_t* n, float** a_dev, float** b_dev) {
+    if (!b) return fail(SF_ERR_ARG, "null beta");
+    if (n) *n = b->n;
+    if (a_dev) *a_dev = b->a;
+    if (b_dev) *b_dev = b->b;
+    return SF_OK;
+}
+
+int sf_beta_eig_async(sf_beta b, sf_accum acc, int mode, double* eig_dev, sf_stream stream) {
+    SF_TRY({
+        if (!b || !acc || !eig_dev) return fail(SF_ERR_ARG, "null argument");
+        if (mode != SF_EIG_LUT_F32 && mode != SF_EIG_FP64) return fail(SF_ERR_ARG, "bad EIG mode");
+        if (acc->total != b->n) return fail(SF_ERR_SHAPE, "accumulator and posterior sizes differ");
+        SF_CK(use_device(b->ctx->device));
+        SF_CK(launch_eig(mode, b->a, b->b, acc->resp, b->n, acc->scale, b->ctx->lut, b->partials,
+                         b->blocks, eig_dev, S(stream)));
+        return SF_OK;
+    })
+}
+
+int sf_beta_eig(sf_beta b, sf_accum acc, int mode, sf_stream stream, double* eig) {
+    SF_TRY({
+        if (!eig) return fail(SF_ERR_ARG, "null out");
+        int rc = sf_beta_eig_async(b, acc, mode, b ? b->out : nullptr, stream);
+        if (rc != SF_OK) return rc;
+        SF_CK(cudaMemcpyAsync(b->host_out, b->out, 8, cudaMemcpyDeviceToHost, S(stream)));
+        SF_CK(cudaStreamSynchronize(S(stream)));
+        *eig = *b->host_out;
+        return SF_OK;
+    })
+}
+
+int sf_beta_update(sf_beta b, sf_accum acc, sf_stream stream) {
+    SF_TRY({
+        if (!b || !acc) return fail(SF_ERR_ARG, "null argument");
+        if (acc->total != b->n) return fail(SF_ERR_SHAPE, "accumulator and posterior sizes differ");
+        SF_CK(use_device(b->ctx->device));
+        SF_CK(launch_beta_update(acc->scale, acc->fg, acc->bg, b->a, b->b, b->n, S(stream)));
+        return SF_OK;
+    })
+}
+
+int sf_map_labels(const float* a, const float* b, uint32_t n, uint8_t* out) {
+    if ((!a || !b || !out) && n) return fail(SF_ERR_ARG, "null argument");
+    for (uint32_t i = 0; i < n; ++i) out[i] = a[i] > b[i] ? 1 : 0;
+    return SF_OK;
+}
+
+int sf_entropy_table(float* out) {
+    SF_TRY({
+        if (!out) return fail(SF_ERR_ARG, "null out");
+        build_entropy_table(out);
+        return SF_OK;
+    })
+}
+
+int sf_table_entropy(sf_ctx ctx, const float* a, const float* b, uint32_t n, float* out,
+                     sf_stream stream) {
+    SF_TRY({
+        if (!ctx || ((!a || !b || !out) && n)) return fail(SF_ERR_ARG, "null argument");
+        SF_CK(use_device(ctx->device));
+        SF_CK(ensure_lut(ctx));
+        SF_CK(launch_table_probe(a, b, n, ctx->lut, out, S(stream)));
+        return SF_OK;
+    })
+}
+
+// ------------------------------------------------------------ sort / scan
+
+uint32_t sf_bits_for(uint32_t max_exclusive) { return bits_for_u32(max_exclusive); }
+
+int sf_radix_create(sf_ctx ctx, uint32_t max_elems, sf_radix* out) {
+    SF_TRY({
+        if (!ctx || !out) return fail(SF_ERR_ARG, "null argument");
+        *out = nullptr;
+        if (max_elems > kMaxIsects) return fail(SF_ERR_SHAPE, "radix capacity exceeds 2^30-1");
+        SF_CK(use_device(ctx->device));
+        auto* r = new sf_radix_t();
+        r->ctx = ctx;
+        r->max = max_elems;
+        cudaError_t e = dalloc(&r->ka, max_elems);
+        if (e == cudaSuccess) e = dalloc(&r->va, max_elems);
+        if (e == cudaSuccess) e = dalloc(&r->kb, max_elems);
+        if (e == cudaSuccess) e = dalloc(&r->vb, max_elems);
+        if (e == cudaSuccess) e = cudaMalloc(&r->tmp, radix_temp_bytes(max_elems, 4));
+        if (e == cudaSuccess) e = dalloc(&r->err, 1);
+        if (e == cudaSuccess) e = cudaMemset(r->err, 0, 4);
+        if (e != cudaSuccess) {
+            dfree(r->ka); dfree(r->va); dfree(r->kb); dfree(r->vb); dfree(r->err);
+            if (r->tmp) cudaFree(r->tmp);
+            delete r;
+            return fail(SF_ERR_NOMEM, cudaGetErrorString(e));
+        }
+        *out = r;
+        return SF_OK;
+    })
+}
+
+int sf_radix_destroy(sf_radix r) {
+    if (!r) return SF_OK;
+    use_device(r->ctx->device);
+    dfree(r->ka); dfree(r->va); dfree(r->kb); dfree(r->vb); dfree(r->err);
+    if (r->tmp) cudaFree(r->tmp);
+    delete r;
+    return SF_OK;
+}
+
+int sf_radix_argsort(sf_radix r, const uint32_t* keys, const uint32_t* vals, uint32_t n, uint32_t bits,
+                     int write_keys, sf_stream stream, const uint32_t** keys_out,
+                     const uint32_t** vals_out) {
+    SF_TRY({
+        if (!r || !keys_out || !vals_out) return fail(SF_ERR_ARG, "null argument");
+        if (bits > 32) return fail(SF_ERR_ARG, "bits > 32");
+        if (n <= 1 || bits == 0) {
+            *keys_out = keys;
+            *vals_out = vals;
+            return SF_OK;
+        }
+        if (!keys) return fail(SF_ERR_ARG, "null keys");
+        if (n > r->max)
+            return fail(SF_ERR_SHAPE, "radix scratch undersized: sorted " + std::to_string(n) +
+                                          " elements, capacity " + std::to_string(r->max));
+        SF_CK(use_device(r->ctx->device));
+        int in_b = 0;
+        SF_CK(radix_sort_pairs(keys, vals, r->ka, r->va, r->kb, r->vb, n, nullptr, n, bits,
+                               write_keys != 0, vals == nullptr, r->tmp, r->err, r->ctx->sm_count,
+                               S(stream), &in_b));
+        *keys_out = in_b ? r->kb : r->ka;
+        *vals_out = in_b ? r->vb : r->va;
+        return SF_OK;
+    })
+}
+
+int sf_scan_create(sf_ctx ctx, uint32_t max_elems, sf_scan* out) {
+    SF_TRY({
+        if (!ctx || !out) return fail(SF_ERR_ARG, "null argument");
+        *out = nullptr;
+        SF_CK(use_device(ctx->device));
+        auto* s = new sf_scan_t();
+        s->ctx = ctx;
+        s->max = max_elems;
+        cudaError_t e = cudaMalloc(&s->tmp, scan_temp_bytes(max_elems));
+        if (e == cudaSuccess) e = dalloc(&s->total, 1);
+        if (e == cudaSuccess) e = dalloc(&s->err, 1);
+        if (e == cudaSuccess) e = cudaMemset(s->err, 0, 4);
+        if (e != cudaSuccess) {
+            if (s->tmp) cudaFree(s->tmp);
+            dfree(s->total); dfree(s->err);
+            delete s;
+            return fail(SF_ERR_NOMEM, cudaGetErrorString(e));
+        }
+        *out = s;
+        return SF_OK;
+    })
+}
+
+int sf_scan_destroy(sf_scan s) {
+    if (!s) return SF_OK;
+    use_device(s->ctx->device);
+    if (s->tmp) cudaFree(s->tmp);
+    dfree(s->total); dfree(s->err);
+    delete s;
+    return SF_OK;
+}
+
+int sf_exclusive_scan_gather(sf_scan s, const uint32_t* gids, const uint32_t* counts, uint32_t* offsets,
+                             uint32_t n, sf_stream stream) {
+    SF_TRY({
+        if (!s) return fail(SF_ERR_ARG, "null scan scratch");
+        if (n == 0) return SF_OK;
+        if (!counts || !offsets) return fail(SF_ERR_ARG, "null buffer");
+        if (n > s->max)
+            return fail(SF_ERR_SHAPE, "offsets undersized: scanned " + std::to_string(n) +
+                                          " elements, capacity " + std::to_string(s->max));
+        SF_CK(use_device(s->ctx->device));
+        SF_CK(exclusive_scan(gids, counts, offsets, n, nullptr, n, s->tmp, s->total, s->err, S(stream)));
+        return SF_OK;
+    })
+}
+
+int sf_exclusive_scan(sf_scan s, uint32_t* buf, uint32_t n, sf_stream stream) {
+    return sf_exclusive_scan_gather(s, nullptr, buf, buf, n, stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+// Internal declarations shared by the CUDA translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstddef>
+#include <cstdint>
+#include "../../include/splatfield_cuda.h"
+
+// Device error word bits (sticky, OR-ed by kernels, read by the host at sync
+// points).
+#define SF_DEV_ERR_TIMEOUT 1u
+#define SF_DEV_ERR_CAPACITY 2u
+
+namespace sfk {
+
+// Process-wide count of kernels launched by this library.
+void note_launches(uint32_t k);
+uint64_t launches();
+
+// Per-splat projected record, split so that the responsibility modes read 32
+// bytes and the RGB mode 48:
+//   geo0 = {mean.x, mean.y, 0.5*conic.x, conic.y}
+//   geo1 = {0.5*conic.z, opacity, power_max, 0}  (power_max: above it alpha < 1/255)
+//   color = {r+0.5, g+0.5, b+0.5, 0}
+struct ProjOut {
+    uint32_t* depth_keys;   // [n] f32 bits of camera z; 0xFFFFFFFF culled
+    uint32_t* tile_counts;  // [n]
+    uint2* bbox;            // [n] packed min / max
+    float4* geo0;           // [n]
+    float4* geo1;           // [n]
+    float4* color;          // [n] (may be null: colour not needed)
+    uint32_t* visible;      // atomic counter (may be null)
+};
+
+cudaError_t launch_project(const sf_view& view, const float* attr, const float* sh, uint32_t n,
+                           uint32_t sh_per_ch, const ProjOut& out, cudaStream_t stream);
+
+cudaError_t launch_emit(const uint32_t* order, const uint2* bbox, const uint32_t* offsets,
+                        uint32_t n, uint32_t tiles_per_row, uint32_t capacity, uint32_t* tile_ids,
+                        uint32_t* gaussian_ids, uint32_t* err, cudaStream_t stream);
+
+// tile_start[t] = lower_bound(t) over sorted ids, t in [0, num_tiles].
+cudaError_t launch_tile_starts(const uint32_t* sorted_tile_ids, uint32_t num_isects,
+                               const uint32_t* num_isects_dev, uint32_t max_isects,
+                               uint32_t num_tiles, uint32_t* tile_start, cudaStream_t stream);
+
+struct RasterArgs {
+    uint32_t w, h, tiles_x, tiles_y, row_stride;
+    const uint32_t* tile_start;
+    const uint32_t* gaussian_ids;
+    const float4* geo0;
+    const float4* geo1;
+    const float4* color;
+    float scale;
+    const uint32_t* mask;
+    uint32_t mask_wpr;
+    uint32_t* bitmap;
+    float4* rgba;
+    uint32_t* resp;
+    uint32_t* fg;
+    uint32_t* bg;
+    float* final_t;
+    uint32_t* n_contrib;
+    // Optional pair statistics, added to: [0] (pixel, splat) pairs visited
+    // (256 per tile-list entry walked before the tile's early exit), [1]
+    // exponentials evaluated, [2] contributing pairs (alpha >= 1/255).
+    unsigned long long* stats;
+};
+// mode 0 = RGB, 1 = total responsibility, 2 = evidence.
+cudaError_t launch_raster(int mode, const RasterArgs& a, cudaStream_t stream);
+
+// Reference-layout projected rows [n][9] from the split records.
+cudaError_t launch_export_rows(const float4* geo0, const float4* geo1, const float4* color,
+                               const uint32_t* depth_keys, uint32_t n, float* rows,
+                               cudaStream_t stream);
+
+// ---- sort / scan (sf_sort.cu)
+uint32_t radix_passes(uint32_t bits);
+size_t radix_temp_bytes(uint32_t max_elems, uint32_t max_passes);
+// Sorts keys_in/vals_in by the low `bits` bits into the (a, b) ping-pong
+// buffers; *out_in_b tells which holds the result. n_dev (optional) supplies
+// the element count on the device, with max_n sizing the grid.
+cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_a,
+                             uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, uint32_t n,
+                             const uint32_t* n_dev, uint32_t max_n, uint32_t bits, bool write_keys,
+                             bool vals_iota, void* temp, uint32_t* err, int sm_count,
+                             cudaStream_t stream, int* out_in_b);
+size_t scan_temp_bytes(uint32_t max_elems);
+cudaError_t exclusive_scan(const uint32_t* gids, const uint32_t* counts, uint32_t* out, uint32_t n,
+                           const uint32_t* n_dev, uint32_t max_n, void* temp,
+                           unsigned long long* total_out, uint32_t* err, cudaStream_t stream);
+
+// ---- segmentation (sf_seg.cu)
+constexpr int kGridPts = 445;
+constexpr float kLnStep = 0.015611423f;
+void build_entropy_table(float* table);  // host, f64 formulas
+double beta_entropy_host(double a, double b);
+// Per-block f64 partial sums of dH; then a single-block final sum into out.
+cudaError_t launch_eig(int mode, const float* a, const float* b, const uint32_t* resp, uint32_t n,
+                       float scale, const float* table, double* partials, uint32_t max_blocks,
+                       double* out, cudaStream_t stream);
+uint32_t eig_blocks(uint32_t n, int sm_count);
+cudaError_t launch_beta_update(float scale, const uint32_t* fg, const uint32_t* bg, float* a,
+                               float* b, uint32_t n, cudaStream_t stream);
+cudaError_t launch_table_probe(const float* a, const float* b, uint32_t n, const float* table,
+                               float* out, cudaStream_t stream);
+
+// ---- camera (sf_camera.cpp)
+void camera_look_at(const float position[3], const float target[3], sf_camera* out);
+void view_for_camera(const sf_camera& cam, uint32_t w, uint32_t h, sf_view* out);
+
+}  // namespace sfk

@@ -1,0 +1,415 @@
+// Render kernels for sm_100a: projection, intersection emission, tile ranges
+// and the tile rasterizer in its RGB / total-responsibility / evidence modes.
+//
+// Reference: src/project.rs:235-327 (project_splats), src/raster.rs:13-48
+// (map_isects), :53-65 (lower_bound), :88-230 (rasterize_kernel). The
+// arithmetic is the reference's in a fixed f32 operation order (sf_math.cuh)
+// so that counts, keys, bboxes, images and fixed-point words match the CPU
+// oracle bit for bit. Everything here is FP32/integer work: no step is a dense
+// contraction, so the tensor cores have no part in it.
+#include <cstdint>
+#include "sf_internal.h"
+#include "sf_math.cuh"
+
+namespace sfk {
+
+namespace {
+
+using namespace sfm;
+
+constexpr float kAlphaCutoff = 10.0f / 255.0f;
+constexpr float kSHC0 = 0.2820948f, kSHC1 = 0.48860252f;
+constexpr float kSHC2_0 = 0.9461747f, kSHC2_1 = 0.31539157f, kSHC2_2 = -1.0925485f,
+                kSHC2_3 = 0.54627424f;
+// power above which alpha = op*exp(-power) < 1/255 for sure: ln(255*op) plus
+// a 1% relative margin in alpha, far above the exp/log rounding (<1e-6).
+constexpr float kPowerMargin = 0.01f;
+
+struct V3 { float x, y, z; };
+__device__ __forceinline__ float dot3(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+
+template <int K>
+__device__ __forceinline__ void sh_to_rgb(V3 d, const float* __restrict__ shs, uint32_t s, uint32_t n,
+                                          float& r, float& g, float& b) {
+    auto sh = [&](int k) { return __ldg(shs + (size_t)k * n + s); };
+    r = kSHC0 * sh(0);
+    g = kSHC0 * sh(1);
+    b = kSHC0 * sh(2);
+    if (K >= 4) {
+        r += kSHC1 * ((-d.y * sh(3) + d.z * sh(6)) - d.x * sh(9));
+        g += kSHC1 * ((-d.y * sh(4) + d.z * sh(7)) - d.x * sh(10));
+        b += kSHC1 * ((-d.y * sh(5) + d.z * sh(8)) - d.x * sh(11));
+    }
+    if (K >= 9) {
+        const float b4 = (kSHC2_2 * d.z) * d.x;
+        const float b5 = (kSHC2_2 * d.z) * d.y;
+        const float b6 = (kSHC2_0 * d.z) * d.z - kSHC2_1;
+        const float b7 = ((kSHC2_3 * 2.0f) * d.x) * d.y;
+        const float b8 = kSHC2_3 * (d.x * d.x - d.y * d.y);
+        r += (((b6 * sh(18) + b7 * sh(12)) + b5 * sh(15)) + b4 * sh(21)) + b8 * sh(24);
+        g += (((b6 * sh(19) + b7 * sh(13)) + b5 * sh(16)) + b4 * sh(22)) + b8 * sh(25);
+        b += (((b6 * sh(20) + b7 * sh(14)) + b5 * sh(17)) + b4 * sh(23)) + b8 * sh(26);
+    }
+    if (K >= 16) {
+        const float c1x = d.x * d.x - d.y * d.y;
+        const float c1y = (2.0f * d.x) * d.y;
+        const float tmp0c = (-2.285229f * d.z) * d.z + 0.4570458f;
+        const float tmp1b = 1.4453057f * d.z;
+        const float b9 = (-0.5900436f * d.x) * c1y + d.y * c1x;
+        const float b10 = (-0.5900436f * d.x) * c1x - d.y * c1y;
+        const float b11 = tmp0c * d.y;
+        const float b12 = tmp0c * d.x;
+        const float b13 = d.z * ((1.8658817f * d.z) * d.z - 1.119529f);
+        const float b14 = tmp1b * c1y;
+        const float b15 = tmp1b * c1x;
+        r += (((((b9 * sh(27) + b10 * sh(30)) + b11 * sh(33)) + b12 * sh(36)) + b13 * sh(39)) +
+              b14 * sh(42)) + b15 * sh(45);
+        g += (((((b9 * sh(28) + b10 * sh(31)) + b11 * sh(34)) + b12 * sh(37)) + b13 * sh(40)) +
+              b14 * sh(43)) + b15 * sh(46);
+        b += (((((b9 * sh(29) + b10 * sh(32)) + b11 * sh(35)) + b12 * sh(38)) + b13 * sh(41)) +
+              b14 * sh(44)) + b15 * sh(47);
+    }
+}
+
+// project_splats (src/project.rs:235-327), one thread per splat. Field-major
+// planes make every plane load a coalesced 128-byte warp access.
+template <int K>
+__global__ __launch_bounds__(256) void project_kernel(sf_view v, const float* __restrict__ attr,
+                                                      const float* __restrict__ shs, uint32_t n,
+                                                      ProjOut o) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t N = n;
+    const float op_raw = __ldg(attr + 10 * N + i);
+    const float opacity = sigmoid_(op_raw);
+    const V3 mean{__ldg(attr + 0 * N + i), __ldg(attr + 1 * N + i), __ldg(attr + 2 * N + i)};
+    const V3 rot0{v.rot0[0], v.rot0[1], v.rot0[2]};
+    const V3 rot1{v.rot1[0], v.rot1[1], v.rot1[2]};
+    const V3 rot2{v.rot2[0], v.rot2[1], v.rot2[2]};
+    const float cam_z = dot3(rot2, mean) + v.trans[2];
+    if (!(opacity >= kAlphaCutoff) || !(cam_z > 0.1f)) {
+        o.depth_keys[i] = 0xffffffffu;
+        o.tile_counts[i] = 0u;
+        o.bbox[i] = make_uint2(0u, 0u);
+        return;
+    }
+    const float cam_x = dot3(rot0, mean) + v.trans[0];
+    const float cam_y = dot3(rot1, mean) + v.trans[1];
+    const float qw = __ldg(attr + 3 * N + i), qx = __ldg(attr + 4 * N + i),
+                qy = __ldg(attr + 5 * N + i), qz = __ldg(attr + 6 * N + i);
+    const V3 s{exp_(__ldg(attr + 7 * N + i)), exp_(__ldg(attr + 8 * N + i)),
+               exp_(__ldg(attr + 9 * N + i))};
+    const float inv_z = 1.0f / cam_z;
+
+    const float x2 = qx * qx, y2 = qy * qy, z2 = qz * qz;
+    const float xy = qx * qy, xz = qx * qz, yz = qy * qz;
+    const float wx = qw * qx, wy = qw * qy, wz = qw * qz;
+    const V3 r0{1.0f - 2.0f * (y2 + z2), 2.0f * (xy - wz), 2.0f * (xz + wy)};
+    const V3 r1{2.0f * (xy + wz), 1.0f - 2.0f * (x2 + z2), 2.0f * (yz - wx)};
+    const V3 r2{2.0f * (xz - wy), 2.0f * (yz + wx), 1.0f - 2.0f * (x2 + y2)};
+    const V3 m0{r0.x * s.x, r0.y * s.y, r0.z * s.z};
+    const V3 m1{r1.x * s.x, r1.y * s.y, r1.z * s.z};
+    const V3 m2{r2.x * s.x, r2.y * s.y, r2.z * s.z};
+    const float lim_x = (1.3f * v.img[0]) / (2.0f * v.focal[0]);
+    const float lim_y = (1.3f * v.img[1]) / (2.0f * v.focal[1]);
+    const float u = clamp_(cam_x * inv_z, -lim_x, lim_x);
+    const float vv = clamp_(cam_y * inv_z, -lim_y, lim_y);
+    const float fx_iz = v.focal[0] * inv_z;
+    const float fu_iz = fx_iz * u;
+    const V3 t0{fx_iz * rot0.x - fu_iz * rot2.x, fx_iz * rot0.y - fu_iz * rot2.y,
+                fx_iz * rot0.z - fu_iz * rot2.z};
+    const float fy_iz = v.focal[1] * inv_z;
+    const float fv_iz = fy_iz * vv;
+    const V3 t1{fy_iz * rot1.x - fv_iz * rot2.x, fy_iz * rot1.y - fv_iz * rot2.y,
+                fy_iz * rot1.z - fv_iz * rot2.z};
+    const V3 j0{(t0.x * m0.x + t0.y * m1.x) + t0.z * m2.x, (t0.x * m0.y + t0.y * m1.y) + t0.z * m2.y,
+                (t0.x * m0.z + t0.y * m1.z) + t0.z * m2.z};
+    const V3 j1{(t1.x * m0.x + t1.y * m1.x) + t1.z * m2.x, (t1.x * m0.y + t1.y * m1.y) + t1.z * m2.y,
+                (t1.x * m0.z + t1.y * m1.z) + t1.z * m2.z};
+    const float ca = dot3(j0, j0) + 0.3f;
+    const float cb = dot3(j0, j1);
+    const float cc = dot3(j1, j1) + 0.3f;
+    const float det = max_(ca * cc - cb * cb, 1e-6f);
+    const float inv_det = 1.0f / det;
+    const float cx = cc * inv_det, cy = -cb * inv_det, cz = ca * inv_det;
+
+    const float mx = (v.focal[0] * cam_x) * inv_z + v.img[0] * 0.5f;
+    const float my = (v.focal[1] * cam_y) * inv_z + v.img[1] * 0.5f;
+
+    if (o.color) {
+        V3 dir{mean.x - v.world_pos[0], mean.y - v.world_pos[1], mean.z - v.world_pos[2]};
+        const float inv = 1.0f / sqrtf(dot3(dir, dir));
+        dir = V3{dir.x * inv, dir.y * inv, dir.z * inv};
+        float r, g, b;
+        sh_to_rgb<K>(dir, shs, i, n, r, g, b);
+        o.color[i] = make_float4(r + 0.5f, g + 0.5f, b + 0.5f, 0.0f);
+    }
+    const float cutoff = log_(opacity / kAlphaCutoff);
+    const float ext_x = sqrtf((2.0f * cutoff) * ca);
+    const float ext_y = sqrtf((2.0f * cutoff) * cc);
+    const float inv_tile = 1.0f / 16.0f;
+    const uint32_t min_x = sat_u32(clamp_((mx - ext_x) * inv_tile, 0.0f, v.tile_bounds[0]));
+    const uint32_t min_y = sat_u32(clamp_((my - ext_y) * inv_tile, 0.0f, v.tile_bounds[1]));
+    const uint32_t max_x = sat_u32(clamp_((mx + ext_x) * inv_tile + 1.0f, 0.0f, v.tile_bounds[0]));
+    const uint32_t max_y = sat_u32(clamp_((my + ext_y) * inv_tile + 1.0f, 0.0f, v.tile_bounds[1]));
+    const float power_max = log_(255.0f * opacity) + kPowerMargin;
+
+    o.depth_keys[i] = f2u(cam_z);
+    o.tile_counts[i] = (max_x - min_x) * (max_y - min_y);
+    o.bbox[i] = make_uint2(min_x | (min_y << 16), max_x | (max_y << 16));
+    o.geo0[i] = make_float4(mx, my, 0.5f * cx, cy);
+    o.geo1[i] = make_float4(0.5f * cz, opacity, power_max, 0.0f);
+    if (o.visible) {
+        // Warp-aggregated visible count.
+        const uint32_t active = __activemask();
+        if ((threadIdx.x & 31u) == (uint32_t)(__ffs(active) - 1)) atomicAdd(o.visible, __popc(active));
+    }
+}
+
+// map_isects (src/raster.rs:13-48): rank r writes its bbox tiles row-major at
+// its scan offset. Past capacity the write is dropped and flagged.
+__global__ __launch_bounds__(256) void emit_kernel(const uint32_t* __restrict__ order,
+                                                   const uint2* __restrict__ bbox,
+                                                   const uint32_t* __restrict__ offsets, uint32_t n,
+                                                   uint32_t tiles_per_row, uint32_t capacity,
+                                                   uint32_t* __restrict__ tile_ids,
+                                                   uint32_t* __restrict__ gaussian_ids,
+                                                   uint32_t* err) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint32_t vis = order[r];
+    const uint2 bb = bbox[vis];
+    const uint32_t min_x = bb.x & 0xffffu, min_y = bb.x >> 16;
+    const uint32_t max_x = bb.y & 0xffffu, max_y = bb.y >> 16;
+    uint32_t slot = offsets[r];
+    bool over = false;
+    for (uint32_t ty = min_y; ty < max_y; ++ty)
+        for (uint32_t tx = min_x; tx < max_x; ++tx) {
+            if (slot < capacity) {
+                tile_ids[slot] = tx + ty * tiles_per_row;
+                gaussian_ids[slot] = vis;
+            } else {
+                over = true;
+            }
+            ++slot;
+        }
+    if (over) atomicOr(err, SF_DEV_ERR_CAPACITY);
+}
+
+__global__ void tile_start_kernel(const uint32_t* __restrict__ ids, uint32_t n_static,
+                                  const uint32_t* n_dev, uint32_t num_tiles,
+                                  uint32_t* __restrict__ start) {
+    const uint32_t n = n_dev ? *n_dev : n_static;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    const uint32_t lo = (i == 0) ? 0u : ids[i - 1] + 1u;
+    const uint32_t hi = (i == n) ? num_tiles : min(ids[i], num_tiles);
+    for (uint32_t t = lo; t <= hi; ++t) start[t] = i;
+}
+
+// rasterize_kernel (src/raster.rs:88-230). One 256-thread block per 16x16
+// tile; each warp owns an 8x4 pixel block. Chunks of 256 splat records are
+// staged in shared memory; pairs whose power exceeds the splat's power_max
+// (alpha < 1/255 there, the reference's skip) bypass the exponential. The
+// whole tile stops once every pixel's transmittance fell below 1/255.
+// Responsibility/evidence words are reduced per warp (redux.sync), then per
+// tile in shared memory, then added to global memory once per (tile, splat):
+// integer sums, so the words equal the reference's per-pixel atomics exactly.
+template <int MODE>
+__global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
+    __shared__ float4 s_g0[256];
+    __shared__ float4 s_g1[256];
+    __shared__ float4 s_col[MODE == 0 ? 256 : 1];
+    __shared__ uint32_t s_gid[MODE == 0 ? 1 : 256];
+    __shared__ uint32_t s_acc0[MODE == 0 ? 1 : 256];
+    __shared__ uint32_t s_acc1[MODE == 2 ? 256 : 1];
+
+    const uint32_t tile = blockIdx.x;
+    const uint32_t tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t px = tx * 16 + (warp & 1u) * 8 + (lane & 7u);
+    const uint32_t py = ty * 16 + (warp >> 1) * 4 + (lane >> 3);
+    const bool in_bounds = px < a.w && py < a.h;
+    const float fx = (float)px + 0.5f, fy = (float)py + 0.5f;
+    uint32_t inside = 0;
+    if (MODE == 2 && in_bounds) inside = (a.mask[px / 32 + py * a.mask_wpr] >> (px % 32)) & 1u;
+    const uint32_t start = a.tile_start[tile], end = a.tile_start[tile + 1];
+    const float inv255 = 1.0f / 255.0f;
+    float T = 1.0f, pr = 0.0f, pg = 0.0f, pb = 0.0f;
+    uint32_t last = 0;
+    bool done = !in_bounds;
+    uint32_t n_eval = 0, n_hit = 0, visited = 0;
+
+    for (uint32_t chunk = start; chunk < end; chunk += 256) {
+        __syncthreads();
+        const uint32_t idx = chunk + tid;
+        if (idx < end) {
+            const uint32_t g = a.gaussian_ids[idx];
+            s_g0[tid] = a.geo0[g];
+            s_g1[tid] = a.geo1[g];
+            if (MODE == 0) {
+                s_col[tid] = a.color[g];
+            } else {
+                s_gid[tid] = g;
+                s_acc0[tid] = 0u;
+                if (MODE == 2) s_acc1[tid] = 0u;
+            }
+        }
+        if (__syncthreads_count(done) == 256) break;
+        const uint32_t cnt = min(256u, end - chunk);
+        visited += cnt;
+        for (uint32_t j = 0; j < cnt; ++j) {
+            uint32_t q = 0;
+            if (!done) {
+                const float4 g0 = s_g0[j];
+                const float4 g1 = s_g1[j];
+                const float dx = g0.x - fx, dy = g0.y - fy;
+                const float power = fma_(g0.z * dx, dx, fma_(g1.x * dy, dy, (g0.w * dx) * dy));
+                if (!(power > g1.z)) {
+                    ++n_eval;
+                    const float alpha = fminf(g1.y * exp_neg_(-power), 0.999f);
+                    if (alpha >= inv255) {
+                        ++n_hit;
+                        const float vis = alpha * T;
+                        if (MODE == 0) {
+                            const float4 c = s_col[j];
+                            pr = fma_(c.x, vis, pr);
+                            pg = fma_(c.y, vis, pg);
+                            pb = fma_(c.z, vis, pb);
+                        } else {
+                            q = sat_u32(vis * a.scale);
+                        }
+                        T = T * (1.0f - alpha);
+                        last = chunk - start + j + 1;
+                        if (T < inv255) done = true;
+                    }
+                }
+            }
+            if (MODE == 1) {
+                const uint32_t s = __reduce_add_sync(0xffffffffu, q);
+                if (lane == 0 && s) atomicAdd(&s_acc0[j], s);
+            } else if (MODE == 2) {
+                const uint32_t qf = inside ? q : 0u;
+                const uint32_t sf = __reduce_add_sync(0xffffffffu, qf);
+                const uint32_t sb = __reduce_add_sync(0xffffffffu, q - qf);
+                if (lane == 0) {
+                    if (sf) atomicAdd(&s_acc0[j], sf);
+                    if (sb) atomicAdd(&s_acc1[j], sb);
+                }
+            }
+        }
+        if (MODE != 0) {
+            __syncthreads();
+            if (tid < cnt) {
+                const uint32_t g = s_gid[tid];
+                if (MODE == 1) {
+                    if (s_acc0[tid]) atomicAdd(a.resp + g, s_acc0[tid]);
+                } else {
+                    if (s_acc0[tid]) atomicAdd(a.fg + g, s_acc0[tid]);
+                    if (s_acc1[tid]) atomicAdd(a.bg + g, s_acc1[tid]);
+                }
+            }
+        }
+    }
+    if (a.stats) {
+        const uint32_t e = __reduce_add_sync(0xffffffffu, n_eval);
+        const uint32_t c = __reduce_add_sync(0xffffffffu, n_hit);
+        if (lane == 0) {
+            atomicAdd(a.stats + 1, (unsigned long long)e);
+            atomicAdd(a.stats + 2, (unsigned long long)c);
+        }
+        if (tid == 0) atomicAdd(a.stats, 256ull * visited);
+    }
+    if (!in_bounds) return;
+    const size_t pix = (size_t)py * a.w + px;
+    if (MODE == 0) {
+        if (a.bitmap) {
+            const uint32_t r = sat_u32(clamp_(pr * 255.0f, 0.0f, 255.0f));
+            const uint32_t g = sat_u32(clamp_(pg * 255.0f, 0.0f, 255.0f));
+            const uint32_t b = sat_u32(clamp_(pb * 255.0f, 0.0f, 255.0f));
+            const uint32_t al = sat_u32(clamp_((1.0f - T) * 255.0f, 0.0f, 255.0f));
+            a.bitmap[(size_t)py * a.row_stride + px] = r | (g << 8) | (b << 16) | (al << 24);
+        }
+        if (a.rgba) a.rgba[pix] = make_float4(pr, pg, pb, 1.0f - T);
+    }
+    if (a.final_t) a.final_t[pix] = T;
+    if (a.n_contrib) a.n_contrib[pix] = last;
+}
+
+__global__ void export_rows_kernel(const float4* __restrict__ geo0, const float4* __restrict__ geo1,
+                                   const float4* __restrict__ color,
+                                   const uint32_t* __restrict__ keys, uint32_t n,
+                                   float* __restrict__ rows) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float* r = rows + (size_t)i * 9;
+    if (keys[i] == 0xffffffffu) {
+        for (int k = 0; k < 9; ++k) r[k] = 0.0f;
+        return;
+    }
+    const float4 g0 = geo0[i], g1 = geo1[i];
+    const float4 c = color ? color[i] : make_float4(0, 0, 0, 0);
+    r[0] = g0.x; r[1] = g0.y; r[2] = 2.0f * g0.z; r[3] = g0.w; r[4] = 2.0f * g1.x;
+    r[5] = c.x; r[6] = c.y; r[7] = c.z; r[8] = g1.y;
+}
+
+}  // namespace
+
+cudaError_t launch_project(const sf_view& view, const float* attr, const float* sh, uint32_t n,
+                           uint32_t sh_per_ch, const ProjOut& out, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    const uint32_t grid = (n + 255) / 256;
+    switch (sh_per_ch) {
+        case 1: project_kernel<1><<<grid, 256, 0, stream>>>(view, attr, sh, n, out); break;
+        case 4: project_kernel<4><<<grid, 256, 0, stream>>>(view, attr, sh, n, out); break;
+        case 9: project_kernel<9><<<grid, 256, 0, stream>>>(view, attr, sh, n, out); break;
+        case 16: project_kernel<16><<<grid, 256, 0, stream>>>(view, attr, sh, n, out); break;
+        default: return cudaErrorInvalidValue;
+    }
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_emit(const uint32_t* order, const uint2* bbox, const uint32_t* offsets,
+                        uint32_t n, uint32_t tiles_per_row, uint32_t capacity, uint32_t* tile_ids,
+                        uint32_t* gaussian_ids, uint32_t* err, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    emit_kernel<<<(n + 255) / 256, 256, 0, stream>>>(order, bbox, offsets, n, tiles_per_row,
+                                                      capacity, tile_ids, gaussian_ids, err);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tile_starts(const uint32_t* sorted_tile_ids, uint32_t num_isects,
+                               const uint32_t* num_isects_dev, uint32_t max_isects,
+                               uint32_t num_tiles, uint32_t* tile_start, cudaStream_t stream) {
+    const uint32_t grid_n = (num_isects_dev ? max_isects : num_isects) + 1;
+    tile_start_kernel<<<(grid_n + 255) / 256, 256, 0, stream>>>(sorted_tile_ids, num_isects,
+                                                                num_isects_dev, num_tiles, tile_start);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_raster(int mode, const RasterArgs& a, cudaStream_t stream) {
+    const uint32_t tiles = a.tiles_x * a.tiles_y;
+    if (tiles == 0) return cudaSuccess;
+    switch (mode) {
+        case 0: raster_kernel<0><<<tiles, 256, 0, stream>>>(a); break;
+        case 1: raster_kernel<1><<<tiles, 256, 0, stream>>>(a); break;
+        case 2: raster_kernel<2><<<tiles, 256, 0, stream>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_export_rows(const float4* geo0, const float4* geo1, const float4* color,
+                               const uint32_t* depth_keys, uint32_t n, float* rows,
+                               cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    export_rows_kernel<<<(n + 255) / 256, 256, 0, stream>>>(geo0, geo1, color, depth_keys, n, rows);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace sfk

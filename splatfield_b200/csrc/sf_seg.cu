@@ -1,0 +1,202 @@
+// Segmentation-evidence kernels: analytic EIG over Beta posteriors (f32 LUT
+// and on-GPU FP64 entropy) and the conjugate Beta update.
+//
+// Reference: src/seg/beta.rs:55-212. The reference sums per-workgroup f32
+// partials on the host after a blocking read-back (beta.rs:265-267); here the
+// sum is an f64 two-level reduction on the device in a fixed order, so the
+// result is deterministic and a batched round needs no host sync per view.
+#include <cmath>
+#include <cstdint>
+#include "sf_internal.h"
+#include "sf_math.cuh"
+
+namespace sfk {
+
+// ---- host: the f64 entropy formulas and the LUT (beta.rs:55-112)
+namespace {
+double lgamma_h(double x) {
+    const double z = x - 1.0;
+    static const double c[8] = {676.5203681218851,    -1259.1392167224028, 771.3234287776531,
+                                -176.6150291621406,   12.507343278686905,  -0.13857109526572012,
+                                9.984369578019572e-6, 1.5056327351493116e-7};
+    double series = 0.9999999999998099;
+    for (int k = 0; k < 8; ++k) series += c[k] / (z + (double)k + 1.0);
+    const double t = z + 7.5;
+    return 0.5 * std::log(2.0 * 3.141592653589793) + (z + 0.5) * std::log(t) - t + std::log(series);
+}
+double digamma_h(double x) {
+    double r = 0.0;
+    while (x < 6.0) { r -= 1.0 / x; x += 1.0; }
+    const double inv = 1.0 / x, inv2 = inv * inv;
+    return r + std::log(x) - 0.5 * inv - inv2 / 12.0 + inv2 * inv2 / 120.0 -
+           inv2 * inv2 * inv2 / 252.0;
+}
+}  // namespace
+
+double beta_entropy_host(double a, double b) {
+    const double s = a + b;
+    return lgamma_h(a) + lgamma_h(b) - lgamma_h(s) - (a - 1.0) * digamma_h(a) -
+           (b - 1.0) * digamma_h(b) + (s - 2.0) * digamma_h(s);
+}
+
+void build_entropy_table(float* table) {
+    double axis[kGridPts];
+    for (int i = 0; i < kGridPts; ++i) axis[i] = std::exp((double)((float)i * kLnStep));
+    for (int i = 0; i < kGridPts; ++i)
+        for (int j = 0; j < kGridPts; ++j)
+            table[i * kGridPts + j] = (float)beta_entropy_host(axis[i], axis[j]);
+}
+
+namespace {
+
+using namespace sfm;
+
+// ---- device f64 entropy: the same formulas, CUDA double log.
+__device__ __forceinline__ double lgamma_d(double x) {
+    const double z = x - 1.0;
+    double series = 0.9999999999998099;
+    series += 676.5203681218851 / (z + 1.0);
+    series += -1259.1392167224028 / (z + 2.0);
+    series += 771.3234287776531 / (z + 3.0);
+    series += -176.6150291621406 / (z + 4.0);
+    series += 12.507343278686905 / (z + 5.0);
+    series += -0.13857109526572012 / (z + 6.0);
+    series += 9.984369578019572e-6 / (z + 7.0);
+    series += 1.5056327351493116e-7 / (z + 8.0);
+    const double t = z + 7.5;
+    return 0.5 * log(2.0 * 3.141592653589793) + (z + 0.5) * log(t) - t + log(series);
+}
+__device__ __forceinline__ double digamma_d(double x) {
+    double r = 0.0;
+    while (x < 6.0) { r -= 1.0 / x; x += 1.0; }
+    const double inv = 1.0 / x, inv2 = inv * inv;
+    return r + log(x) - 0.5 * inv - inv2 / 12.0 + inv2 * inv2 / 120.0 - inv2 * inv2 * inv2 / 252.0;
+}
+__device__ __forceinline__ double beta_entropy_d(double a, double b) {
+    const double s = a + b;
+    return lgamma_d(a) + lgamma_d(b) - lgamma_d(s) - (a - 1.0) * digamma_d(a) -
+           (b - 1.0) * digamma_d(b) + (s - 2.0) * digamma_d(s);
+}
+
+// table_entropy (beta.rs:128-144).
+__device__ __forceinline__ float table_entropy_d(float a, float b, const float* __restrict__ t) {
+    const float xa = log_(a) / kLnStep;
+    const float xb = log_(b) / kLnStep;
+    const float ia = min_(max_(floorf(xa), 0.0f), (float)(kGridPts - 2));
+    const float ib = min_(max_(floorf(xb), 0.0f), (float)(kGridPts - 2));
+    const float ta = clamp_(xa - ia, 0.0f, 1.0f);
+    const float tb = clamp_(xb - ib, 0.0f, 1.0f);
+    const uint32_t row = sat_u32(ia) * kGridPts + sat_u32(ib);
+    const float h00 = __ldg(t + row), h10 = __ldg(t + row + kGridPts);
+    const float h01 = __ldg(t + row + 1), h11 = __ldg(t + row + kGridPts + 1);
+    return (((h00 * (1.0f - ta)) * (1.0f - tb) + (h10 * ta) * (1.0f - tb)) + (h01 * (1.0f - ta)) * tb) +
+           (h11 * ta) * tb;
+}
+
+constexpr int kEigThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* s_warp) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) s_warp[warp] = v;
+    __syncthreads();
+    double total = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < kEigThreads / 32; ++w) total += s_warp[w];
+    return total;
+}
+
+// entropy_delta_kernel (beta.rs:152-201): per splat with eps > 0,
+// dH = max(0, H(a,b) - H(k a, k b)), k = 1 + eps/(a+b).
+template <int MODE>
+__global__ __launch_bounds__(kEigThreads) void eig_kernel(const float* __restrict__ a,
+                                                          const float* __restrict__ b,
+                                                          const uint32_t* __restrict__ resp,
+                                                          uint32_t n, float scale,
+                                                          const float* __restrict__ table,
+                                                          double* __restrict__ partials) {
+    __shared__ double s_warp[kEigThreads / 32];
+    double acc = 0.0;
+    const uint32_t stride = gridDim.x * kEigThreads;
+    for (uint32_t i = blockIdx.x * kEigThreads + threadIdx.x; i < n; i += stride) {
+        const uint32_t bits = resp[i];
+        if (bits == 0u) continue;
+        const float ai = a[i], bi = b[i];
+        if (MODE == SF_EIG_LUT_F32) {
+            const float eps = (float)bits / scale;
+            const float k = 1.0f + eps / (ai + bi);
+            const float d = max_(table_entropy_d(ai, bi, table) - table_entropy_d(ai * k, bi * k, table), 0.0f);
+            acc += (double)d;
+        } else {
+            const double eps = (double)bits / (double)scale;
+            const double ad = ai, bd = bi;
+            const double k = 1.0 + eps / (ad + bd);
+            const double d = beta_entropy_d(ad, bd) - beta_entropy_d(ad * k, bd * k);
+            acc += d > 0.0 ? d : 0.0;
+        }
+    }
+    const double total = block_sum(acc, s_warp);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total;
+}
+
+__global__ __launch_bounds__(kEigThreads) void eig_final_kernel(const double* __restrict__ partials,
+                                                                uint32_t nb, double* out) {
+    __shared__ double s_warp[kEigThreads / 32];
+    double acc = 0.0;
+    for (uint32_t i = threadIdx.x; i < nb; i += kEigThreads) acc += partials[i];
+    const double total = block_sum(acc, s_warp);
+    if (threadIdx.x == 0) *out = total;
+}
+
+__global__ void beta_update_kernel(float scale, const uint32_t* __restrict__ fg,
+                                   const uint32_t* __restrict__ bg, float* __restrict__ a,
+                                   float* __restrict__ b, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    a[i] = a[i] + (float)fg[i] / scale;
+    b[i] = b[i] + (float)bg[i] / scale;
+}
+
+__global__ void table_probe_kernel(const float* a, const float* b, uint32_t n, const float* table,
+                                   float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = table_entropy_d(a[i], b[i], table);
+}
+
+}  // namespace
+
+uint32_t eig_blocks(uint32_t n, int sm_count) {
+    const uint32_t want = (n + kEigThreads * 4 - 1) / (kEigThreads * 4);
+    return std::max(1u, std::min(want, (uint32_t)sm_count * 8));
+}
+
+cudaError_t launch_eig(int mode, const float* a, const float* b, const uint32_t* resp, uint32_t n,
+                       float scale, const float* table, double* partials, uint32_t blocks,
+                       double* out, cudaStream_t stream) {
+    if (mode == SF_EIG_LUT_F32)
+        eig_kernel<SF_EIG_LUT_F32><<<blocks, kEigThreads, 0, stream>>>(a, b, resp, n, scale, table, partials);
+    else
+        eig_kernel<SF_EIG_FP64><<<blocks, kEigThreads, 0, stream>>>(a, b, resp, n, scale, table, partials);
+    eig_final_kernel<<<1, kEigThreads, 0, stream>>>(partials, blocks, out);
+    note_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_beta_update(float scale, const uint32_t* fg, const uint32_t* bg, float* a,
+                               float* b, uint32_t n, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    beta_update_kernel<<<(n + 255) / 256, 256, 0, stream>>>(scale, fg, bg, a, b, n);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_table_probe(const float* a, const float* b, uint32_t n, const float* table,
+                               float* out, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    table_probe_kernel<<<(n + 255) / 256, 256, 0, stream>>>(a, b, n, table, out);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace sfk

@@ -1,0 +1,409 @@
+// Onesweep LSD radix sort and decoupled-look-back prefix scan (sm_100a).
+//
+// Replaces crates/sort/src/sort.rs (count_kernel + scan + scatter_plane_kernel
+// per 6-bit digit, 3 launches a digit) and crates/sort/src/scan.rs
+// (block_sums + scan_serial + apply_block_offsets). Design (Adinets & Merrill,
+// "Onesweep: A Faster Least Significant Digit Radix Sort for GPUs", 2022):
+//  * one upfront kernel reads the keys once and builds the 256-bin histogram
+//    of every 8-bit digit position;
+//  * one kernel per digit: a partition of 4096 keys is ranked in registers and
+//    shared memory (warp match-any ranking, stable), publishes its digit
+//    counts, resolves its global digit offsets by decoupled look-back over the
+//    preceding partitions, and scatters through shared memory so each digit's
+//    run is written contiguously.
+// Partition indices come from an atomic ticket in launch order, so a block
+// only ever waits on blocks that already hold a ticket (forward progress).
+// Every wait is bounded: after kSpinLimit polls the block records
+// SF_DEV_ERR_TIMEOUT in the error word and carries on, so a lost predecessor
+// can corrupt the result but never hang the GPU.
+#include <cstdint>
+#include "sf_internal.h"
+
+namespace sfk {
+
+namespace {
+
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kThreads = 256;
+constexpr int kItems = 16;
+constexpr int kTile = kThreads * kItems;  // 4096 keys per partition
+constexpr int kWarps = kThreads / 32;
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagPrefix = 2u << 30;
+constexpr uint32_t kCountMask = (1u << 30) - 1u;
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ uint32_t load_n(const uint32_t* n_dev, uint32_t n_static) {
+    return n_dev ? *n_dev : n_static;
+}
+
+// Upfront digit histograms: hist[pass * 256 + digit] over all n keys.
+__global__ __launch_bounds__(kThreads) void radix_histogram_kernel(
+    const uint32_t* __restrict__ keys, const uint32_t* n_dev, uint32_t n_static,
+    uint32_t num_passes, uint32_t bits, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t s_hist[4 * kRadix];
+    const uint32_t n = load_n(n_dev, n_static);
+    for (uint32_t i = threadIdx.x; i < num_passes * kRadix; i += kThreads) s_hist[i] = 0;
+    __syncthreads();
+    const uint32_t stride = gridDim.x * kThreads;
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        const uint32_t k = keys[i];
+        for (uint32_t p = 0; p < num_passes; ++p) {
+            const uint32_t shift = p * kRadixBits;
+            const uint32_t w = bits - shift < (uint32_t)kRadixBits ? bits - shift : kRadixBits;
+            const uint32_t d = (k >> shift) & ((1u << w) - 1u);
+            atomicAdd(&s_hist[p * kRadix + d], 1u);
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < num_passes * kRadix; i += kThreads)
+        if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
+}
+
+// One 8-bit digit pass. `vals_iota` substitutes vals_in[i] = i.
+__global__ __launch_bounds__(kThreads) void onesweep_pass_kernel(
+    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, const uint32_t* n_dev,
+    uint32_t n_static, uint32_t shift, uint32_t digit_mask, const uint32_t* __restrict__ pass_hist,
+    uint32_t* lookback, uint32_t* ticket, uint32_t* err, int vals_iota, int write_keys) {
+    __shared__ uint32_t s_part;
+    __shared__ uint32_t s_warp_hist[kWarps][kRadix];
+    __shared__ uint32_t s_local_start[kRadix];
+    __shared__ uint32_t s_global_base[kRadix];
+    __shared__ uint32_t s_scan[kWarps];
+    __shared__ uint32_t s_keys[kTile];
+    __shared__ uint32_t s_vals[kTile];
+
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t n = load_n(n_dev, n_static);
+    const uint32_t num_parts = (n + kTile - 1) / kTile;
+    if (tid == 0) s_part = atomicAdd(ticket, 1u);
+    for (uint32_t i = tid; i < kWarps * kRadix; i += kThreads) (&s_warp_hist[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t part = s_part;
+    if (part >= num_parts) return;
+    const uint32_t base = part * kTile;
+    const uint32_t wbase = base + warp * (kItems * 32);
+
+    uint32_t k[kItems], rank[kItems];
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+        const uint32_t idx = wbase + i * 32 + lane;
+        k[i] = idx < n ? keys_in[idx] : 0u;
+    }
+    // Stable warp ranking: items in index order, lanes in lane order.
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+        const uint32_t idx = wbase + i * 32 + lane;
+        const bool valid = idx < n;
+        const uint32_t d = valid ? ((k[i] >> shift) & digit_mask) : (uint32_t)kRadix;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t prev = 0;
+        if (valid && lane == leader) {
+            prev = s_warp_hist[warp][d];
+            s_warp_hist[warp][d] = prev + __popc(peers);
+        }
+        prev = __shfl_sync(0xffffffffu, prev, leader);
+        rank[i] = prev + __popc(peers & lt);
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // Per digit: exclusive prefix over warps, block total, publish.
+    uint32_t digit_total = 0;
+    if (tid < kRadix) {
+        uint32_t sum = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = s_warp_hist[w][tid];
+            s_warp_hist[w][tid] = sum;
+            sum += c;
+        }
+        digit_total = sum;
+        st_relaxed(&lookback[(size_t)part * kRadix + tid], (part == 0 ? kFlagPrefix : kFlagAgg) | sum);
+    }
+    // Block exclusive scan of digit totals (digit order) -> local starts.
+    {
+        uint32_t v = digit_total;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= (uint32_t)o) v += t;
+        }
+        if (lane == 31) s_scan[warp] = v;
+        __syncthreads();
+        if (tid < 32) {
+            uint32_t w = tid < (uint32_t)kWarps ? s_scan[tid] : 0u;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= (uint32_t)o) w += t;
+            }
+            if (tid < (uint32_t)kWarps) s_scan[tid] = w;
+        }
+        __syncthreads();
+        if (tid < kRadix) s_local_start[tid] = v - digit_total + (warp ? s_scan[warp - 1] : 0u);
+    }
+    // Global digit offsets of this pass (exclusive over digits of pass_hist).
+    uint32_t gstart = 0;
+    {
+        const uint32_t h = tid < kRadix ? pass_hist[tid] : 0u;
+        uint32_t v = h;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= (uint32_t)o) v += t;
+        }
+        __syncthreads();
+        if (lane == 31) s_scan[warp] = v;
+        __syncthreads();
+        if (tid < 32) {
+            uint32_t w = tid < (uint32_t)kWarps ? s_scan[tid] : 0u;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= (uint32_t)o) w += t;
+            }
+            if (tid < (uint32_t)kWarps) s_scan[tid] = w;
+        }
+        __syncthreads();
+        gstart = v - h + (warp ? s_scan[warp - 1] : 0u);
+    }
+    // Decoupled look-back, one digit per thread.
+    if (tid < kRadix) {
+        uint32_t excl = 0;
+        if (part > 0) {
+            int64_t p = (int64_t)part - 1;
+            uint32_t spins = 0;
+            while (p >= 0) {
+                const uint32_t s = ld_relaxed(&lookback[(size_t)p * kRadix + tid]);
+                const uint32_t flag = s & ~kCountMask;
+                if (flag == 0u) {
+                    if (++spins > kSpinLimit) {
+                        atomicOr(err, SF_DEV_ERR_TIMEOUT);
+                        break;
+                    }
+                    continue;
+                }
+                excl += s & kCountMask;
+                if (flag == kFlagPrefix) break;
+                --p;
+            }
+            st_relaxed(&lookback[(size_t)part * kRadix + tid], kFlagPrefix | ((excl + digit_total) & kCountMask));
+        }
+        s_global_base[tid] = gstart + excl - s_local_start[tid];
+    }
+    __syncthreads();
+
+    // Scatter into shared memory at the partition-local sorted position.
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+        const uint32_t idx = wbase + i * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = (k[i] >> shift) & digit_mask;
+            const uint32_t pos = s_local_start[d] + s_warp_hist[warp][d] + rank[i];
+            s_keys[pos] = k[i];
+            s_vals[pos] = vals_iota ? idx : vals_in[idx];
+        }
+    }
+    __syncthreads();
+    const uint32_t cnt = min((uint32_t)kTile, n - base);
+    for (uint32_t j = tid; j < cnt; j += kThreads) {
+        const uint32_t key = s_keys[j];
+        const uint32_t d = (key >> shift) & digit_mask;
+        const uint32_t out = s_global_base[d] + j;
+        if (out >= n) continue;  // only after a timed-out look-back
+        if (write_keys) keys_out[out] = key;
+        vals_out[out] = s_vals[j];
+    }
+}
+
+// Single-pass exclusive scan with optional gather:
+// out[i] = sum_{j<i} counts[gids ? gids[j] : j], 64-bit running sums, the
+// u32 low word stored; *total_out = the 64-bit total.
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kThreads * kScanItems;
+constexpr unsigned long long kScanFlagAgg = 1ull << 62;
+constexpr unsigned long long kScanFlagPrefix = 2ull << 62;
+constexpr unsigned long long kScanValMask = (1ull << 62) - 1ull;
+
+__global__ __launch_bounds__(kThreads) void scan_kernel(
+    const uint32_t* __restrict__ gids, const uint32_t* counts, uint32_t* out, const uint32_t* n_dev,
+    uint32_t n_static, unsigned long long* lookback, uint32_t* ticket,
+    unsigned long long* total_out, uint32_t* err) {
+    __shared__ uint32_t s_part;
+    __shared__ unsigned long long s_warp[kWarps];
+    __shared__ unsigned long long s_prefix;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t n = load_n(n_dev, n_static);
+    const uint32_t num_parts = (n + kScanTile - 1) / kScanTile;
+    if (tid == 0) s_part = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t part = s_part;
+    if (n == 0) {
+        if (part == 0 && tid == 0 && total_out) *total_out = 0ull;
+        return;
+    }
+    if (part >= num_parts) return;
+    const uint32_t base = part * kScanTile + tid * kScanItems;
+    uint32_t v[kScanItems];
+    unsigned long long local = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        const uint32_t idx = base + i;
+        uint32_t c = 0;
+        if (idx < n) c = counts[gids ? gids[idx] : idx];
+        v[i] = c;
+        local += c;
+    }
+    // Block exclusive scan of the per-thread sums.
+    unsigned long long incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    unsigned long long warp_prefix = 0, block_total = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+        if ((uint32_t)w < warp) warp_prefix += s_warp[w];
+        block_total += s_warp[w];
+    }
+    if (tid == 0) {
+        unsigned long long excl = 0;
+        if (part == 0) {
+            st_relaxed64(&lookback[0], kScanFlagPrefix | block_total);
+        } else {
+            st_relaxed64(&lookback[part], kScanFlagAgg | block_total);
+            int64_t p = (int64_t)part - 1;
+            uint32_t spins = 0;
+            while (p >= 0) {
+                const unsigned long long s = ld_relaxed64(&lookback[p]);
+                const unsigned long long flag = s & ~kScanValMask;
+                if (flag == 0ull) {
+                    if (++spins > kSpinLimit) {
+                        atomicOr(err, SF_DEV_ERR_TIMEOUT);
+                        break;
+                    }
+                    continue;
+                }
+                excl += s & kScanValMask;
+                if (flag == kScanFlagPrefix) break;
+                --p;
+            }
+            st_relaxed64(&lookback[part], kScanFlagPrefix | (excl + block_total));
+        }
+        s_prefix = excl;
+        if (part == num_parts - 1 && total_out) *total_out = excl + block_total;
+    }
+    __syncthreads();
+    unsigned long long running = s_prefix + warp_prefix + (incl - local);
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        const uint32_t idx = base + i;
+        if (idx < n) out[idx] = (uint32_t)running;
+        running += v[i];
+    }
+}
+
+}  // namespace
+
+uint32_t radix_passes(uint32_t bits) { return (bits + kRadixBits - 1) / kRadixBits; }
+
+size_t radix_temp_bytes(uint32_t max_elems, uint32_t max_passes) {
+    const size_t parts = (max_elems + kTile - 1) / kTile;
+    // hist [4][256] + tickets [4] + lookback [passes][parts][256]
+    return 4 * kRadix * 4 + 64 + (size_t)max_passes * parts * kRadix * 4;
+}
+
+cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_a,
+                             uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, uint32_t n,
+                             const uint32_t* n_dev, uint32_t max_n, uint32_t bits, bool write_keys,
+                             bool vals_iota, void* temp, uint32_t* err, int sm_count,
+                             cudaStream_t stream, int* out_in_b) {
+    const uint32_t passes = radix_passes(bits);
+    const uint32_t grid_n = n_dev ? max_n : n;
+    uint8_t* t = static_cast<uint8_t*>(temp);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(t);
+    uint32_t* tickets = reinterpret_cast<uint32_t*>(t + 4 * kRadix * 4);
+    uint32_t* lookback = reinterpret_cast<uint32_t*>(t + 4 * kRadix * 4 + 64);
+    const size_t parts = (grid_n + kTile - 1) / kTile;
+    cudaError_t e = cudaMemsetAsync(temp, 0, 4 * kRadix * 4 + 64 + passes * parts * kRadix * 4, stream);
+    if (e != cudaSuccess) return e;
+    if (parts == 0) { *out_in_b = 0; return cudaSuccess; }
+    const uint32_t hist_blocks = (uint32_t)std::min<size_t>((grid_n + kThreads * 8 - 1) / (kThreads * 8),
+                                                             (size_t)sm_count * 4);
+    radix_histogram_kernel<<<std::max(hist_blocks, 1u), kThreads, 0, stream>>>(
+        keys_in, n_dev, n, passes, bits, hist);
+    const uint32_t* kin = keys_in;
+    const uint32_t* vin = vals_in;
+    int in_b = 0;
+    for (uint32_t p = 0; p < passes; ++p) {
+        const uint32_t shift = p * kRadixBits;
+        const uint32_t w = std::min<uint32_t>(bits - shift, kRadixBits);
+        uint32_t* kout = (p % 2 == 0) ? keys_a : keys_b;
+        uint32_t* vout = (p % 2 == 0) ? vals_a : vals_b;
+        const bool wk = write_keys || (p + 1 < passes);
+        onesweep_pass_kernel<<<(uint32_t)parts, kThreads, 0, stream>>>(
+            kin, vin, kout, vout, n_dev, n, shift, (1u << w) - 1u, hist + p * kRadix,
+            lookback + (size_t)p * parts * kRadix, tickets + p, err, (vals_iota && p == 0) ? 1 : 0,
+            wk ? 1 : 0);
+        kin = kout;
+        vin = vout;
+        in_b = (p % 2 == 1);
+    }
+    *out_in_b = in_b;
+    note_launches(1 + passes);
+    return cudaGetLastError();
+}
+
+size_t scan_temp_bytes(uint32_t max_elems) {
+    const size_t parts = (max_elems + kScanTile - 1) / kScanTile;
+    return 64 + std::max<size_t>(parts, 1) * 8;
+}
+
+cudaError_t exclusive_scan(const uint32_t* gids, const uint32_t* counts, uint32_t* out, uint32_t n,
+                           const uint32_t* n_dev, uint32_t max_n, void* temp,
+                           unsigned long long* total_out, uint32_t* err, cudaStream_t stream) {
+    const uint32_t grid_n = n_dev ? max_n : n;
+    const size_t parts = std::max<size_t>((grid_n + kScanTile - 1) / kScanTile, 1);
+    uint8_t* t = static_cast<uint8_t*>(temp);
+    uint32_t* ticket = reinterpret_cast<uint32_t*>(t);
+    unsigned long long* lookback = reinterpret_cast<unsigned long long*>(t + 64);
+    cudaError_t e = cudaMemsetAsync(temp, 0, 64 + parts * 8, stream);
+    if (e != cudaSuccess) return e;
+    scan_kernel<<<(uint32_t)parts, kThreads, 0, stream>>>(gids, counts, out, n_dev, n, lookback,
+                                                           ticket, total_out, err);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace sfk

@@ -1,0 +1,85 @@
+"""Scenes and cameras of the reference's tests, shared by the test modules.
+
+Each helper names the reference fixture it restates.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+
+import numpy as np
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def known_answers():
+    with open(os.path.join(GOLDEN_DIR, "reference_known_answers.json")) as f:
+        return json.load(f)
+
+
+def opaque(positions) -> np.ndarray:
+    """sample_opaque_attributes (src/render.rs:478-494)."""
+    pos = np.asarray(positions, np.float32).reshape(-1, 3)
+    n = pos.shape[0]
+    a = np.zeros((11, n), np.float32)
+    a[0:3] = pos.T
+    a[3] = 1.0
+    a[7:10] = -2.0
+    a[10] = 8.0
+    return a.reshape(-1)
+
+
+def zero_sh(n: int, k: int = 1) -> np.ndarray:
+    return np.zeros(3 * k * n, np.float32)
+
+
+def stacked_positions(n=5):
+    return [(0.0, 0.0, 1.0 + i * 0.5) for i in range(n)]
+
+
+def row_positions(n: int, z: float, spacing: float):
+    """row_attributes (src/seg/tests.rs:11-15)."""
+    return [((i - (n - 1) * 0.5) * spacing, 0.0, z) for i in range(n)]
+
+
+def overdraw_positions():
+    """overdraw_scene (src/seg/tests.rs:78-89)."""
+    out = []
+    for i in range(40):
+        x = float(i % 4) - 1.5
+        y = float(i % 3) - 1.0
+        out.append((np.float32(x) * np.float32(0.04), np.float32(y) * np.float32(0.04),
+                    np.float32(1.0) + np.float32(i) * np.float32(0.5)))
+    return out
+
+
+def left_half_mask(w: int, h: int) -> np.ndarray:
+    """left_half_mask (src/seg/tests.rs:67-72)."""
+    p = np.arange(w * h)
+    return ((p % w) < (w // 2)).astype(np.uint8)
+
+
+def yawed_rotation():
+    """Quat::from_rotation_y(pi/2) in f32 (src/render.rs:679-683)."""
+    h = np.float32(math.pi / 2) * np.float32(0.5)
+    return (0.0, float(np.sin(h, dtype=np.float32)), 0.0, float(np.cos(h, dtype=np.float32)))
+
+
+def rgba(px):
+    px = int(px)
+    return [px & 255, (px >> 8) & 255, (px >> 16) & 255, (px >> 24) & 255]
+
+
+def sine_attributes(n: int, freq: float, amp: float) -> np.ndarray:
+    """The (i * f).sin() * amp attribute fill of test_render_reuses_scratch
+    (src/render.rs:715-717) and test_scratch_stops_allocating (:737-739)."""
+    i = np.arange(n * 11, dtype=np.float32)
+    return (np.sin(i * np.float32(freq)) * np.float32(amp)).astype(np.float32)
+
+
+def small_scene(n: int, k: int, seed: int):
+    """A seeded uniform scene (the small workload's distributions) of n splats."""
+    from splatfield_b200 import synth
+
+    return synth.scene_uniform(n, k, seed)

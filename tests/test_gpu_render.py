@@ -1,0 +1,245 @@
+"""CUDA render path vs the CPU oracle, through the C ABI (GPU).
+
+Bit-exact: per-splat depth keys, tile counts, bboxes and projected rows;
+depth order; gather-scan offsets; sorted tile ids and splat ids; tile starts;
+the RGBA8 bitmap and the float RGBA plane. Plus the reference's own render
+tests (known answers and determinism properties)."""
+import numpy as np
+import pytest
+
+import splatfield_b200 as sf
+from splatfield_b200 import _lib as L
+from helpers import (known_answers, opaque, rgba, sine_attributes, stacked_positions,
+                     yawed_rotation, zero_sh)
+
+pytestmark = pytest.mark.gpu
+
+KA = known_answers()
+
+
+def gpu_frame(splats, scratch, cam, w, h, n):
+    isects = splats.prepare_isects(scratch, cam, (w, h))
+    bitmap = splats.finalize_rgb(scratch, isects, (w, h), want_float=True).read()
+    rgba_f = sf.DeviceView(scratch.rgba_ptr(), np.float32, (h, w, 4)).read()
+    V, I = isects.num_visible, isects.num_isects
+    tiles = isects.tile_bounds[0] * isects.tile_bounds[1]
+    return dict(
+        depth_keys=scratch.read(L.READ_DEPTH_KEYS, n),
+        tile_counts=scratch.read(L.READ_TILE_COUNTS, n),
+        bbox=scratch.read(L.READ_BBOX, 2 * n),
+        projected=scratch.read(L.READ_PROJECTED, 9 * n, np.float32).reshape(n, 9),
+        order=scratch.read(L.READ_ORDER, V),
+        offsets=scratch.read(L.READ_OFFSETS, V),
+        tile_ids=isects.tile_ids().read(),
+        gaussian_ids=isects.gaussian_ids().read(),
+        tile_start=scratch.read(L.READ_TILE_START, tiles + 1),
+        bitmap=bitmap, rgba=rgba_f, num_visible=V, num_isects=I)
+
+
+def assert_frame_equal(got, want):
+    np.testing.assert_array_equal(got["depth_keys"], want["depth_keys"])
+    np.testing.assert_array_equal(got["tile_counts"], want["tile_counts"])
+    np.testing.assert_array_equal(got["bbox"], want["bbox"])
+    np.testing.assert_array_equal(got["projected"].view(np.uint32), want["projected"].view(np.uint32))
+    assert got["num_visible"] == want["num_visible"]
+    assert got["num_isects"] == want["num_isects"]
+    np.testing.assert_array_equal(got["order"], want["order"])
+    np.testing.assert_array_equal(got["offsets"], want["offsets"])
+    np.testing.assert_array_equal(got["tile_ids"], want["tile_ids"])
+    np.testing.assert_array_equal(got["gaussian_ids"], want["gaussian_ids"])
+    ranges = want["ranges"]
+    np.testing.assert_array_equal(got["tile_start"][:-1], ranges[:, 0])
+    np.testing.assert_array_equal(got["tile_start"][1:], ranges[:, 1])
+
+
+@pytest.mark.parametrize("n,k,w,h,seed", [
+    (2000, 1, 128, 128, 1),
+    (20000, 4, 256, 192, 2),
+    (50000, 16, 320, 240, 3),
+    (30000, 9, 70, 70, 4),
+])
+def test_frame_bit_exact_vs_oracle(ctx, oracle_mod, n, k, w, h, seed):
+    O = oracle_mod
+    from splatfield_b200 import synth
+
+    attr, sh = synth.scene_uniform(n, k, seed)
+    cam_o = O.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    cam_o.fov[0], cam_o.fov[1] = synth.fov_for(w, h)
+    cam = sf.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    cam.fov[0], cam.fov[1] = synth.fov_for(w, h)
+    want = O.prepare(cam_o, w, h, attr, sh, k)
+    wr = O.rasterize(want, 0)
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    got = gpu_frame(splats, scratch, cam, w, h, n)
+    assert_frame_equal(got, want)
+    np.testing.assert_array_equal(got["bitmap"], wr["bitmap"])
+    np.testing.assert_array_equal(got["rgba"].view(np.uint32), wr["rgba"].view(np.uint32))
+
+
+def test_project_counts_tiles_and_packs_bbox(ctx):
+    """src/project.rs:399-446 through the GPU path."""
+    ka = KA["project_one_splat"]
+    splats = sf.Splats(np.array(ka["attributes"], np.float32), np.array(ka["sh"], np.float32))
+    scratch = sf.RenderScratch(1, (64, 64))
+    isects = splats.prepare_isects(scratch, sf.camera_default(), (64, 64))
+    assert isects.num_visible == ka["visible"]
+    assert isects.num_isects == ka["isects"]
+    assert list(scratch.read(L.READ_TILE_COUNTS, 1)) == ka["tile_counts"]
+    assert list(scratch.read(L.READ_BBOX, 2)) == ka["bbox"]
+
+
+@pytest.mark.parametrize("case", ["stacked", "yawed"])
+def test_render_golden_center(ctx, case):
+    """src/render.rs:671-710."""
+    ka = KA["render_golden_center"]
+    if case == "stacked":
+        attr, cam = opaque(stacked_positions()), sf.camera_default()
+    else:
+        attr = opaque([(0.0, 0.0, 0.0)] * 5)
+        cam = sf.make_camera(position=(-2.0, 0.0, 0.0), rotation=yawed_rotation())
+    splats = sf.Splats(attr, zero_sh(5))
+    scratch = sf.RenderScratch(5, (32, 32))
+    bm = splats.render_with(scratch, cam, (32, 32)).read()
+    r, g, b, a = rgba(bm[16, 16])
+    assert a >= ka["min_center_alpha"]
+    assert rgba(bm[0, 0])[3] == 0
+    for got, want in zip((r, g, b), ka["center_rgb"]):
+        assert abs(got - want) <= 1
+
+
+def test_render_reuses_scratch(ctx):
+    """src/render.rs:712-732: re-render through the same scratch is bit-identical."""
+    attr = sine_attributes(50, 0.13, 0.5)
+    splats = sf.Splats(attr, np.full(150, 0.1, np.float32))
+    cam = sf.make_camera(position=(0.0, -1.0, 0.0))
+    scratch = sf.RenderScratch(50, (64, 64))
+    b = splats.render_with(scratch, cam, (64, 64)).read()
+    c = splats.render_with(scratch, cam, (64, 64)).read()
+    np.testing.assert_array_equal(b, c)
+
+
+def test_render_ties_deterministic(ctx):
+    """src/render.rs:790-812: 200 identical splats at one depth."""
+    n = 200
+    splats = sf.Splats(opaque([(0.0, 0.0, 1.0)] * n), zero_sh(n))
+    cam = sf.camera_default()
+    scratch = sf.RenderScratch(n, (64, 64))
+    a = splats.render_with(scratch, cam, (64, 64)).read()
+    b = splats.render_with(scratch, cam, (64, 64)).read()
+    fresh = sf.RenderScratch(n, (64, 64))
+    c = splats.render_with(fresh, cam, (64, 64)).read()
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(a, c)
+
+
+def test_delete_then_undo_restores_render_bitwise(ctx):
+    """src/render.rs:626-647 (gather = plane-wise selection on the host)."""
+    attr = opaque([(i - 1.0, 0.0, 5.0) for i in range(3)])
+
+    def gather(keep):
+        a = attr.reshape(11, 3)[:, keep]
+        return np.ascontiguousarray(a).reshape(-1)
+
+    def render(keep):
+        s = sf.Splats(gather(keep), zero_sh(len(keep)))
+        scratch = sf.RenderScratch(len(keep), (32, 32))
+        return s.render_with(scratch, sf.camera_default(), (32, 32)).read()
+
+    before = render([0, 1, 2])
+    assert not np.array_equal(render([1, 2]), before)
+    np.testing.assert_array_equal(render([0, 1, 2]), before)
+
+
+def test_scratch_stops_allocating_after_first_frame(ctx):
+    """src/render.rs:734-763: steady-state frames keep the same capacity."""
+    attr = sine_attributes(100, 0.07, 0.4)
+    splats = sf.Splats(attr, zero_sh(100))
+    cam = sf.make_camera(position=(0.0, -1.2, 0.0))
+    scratch = sf.RenderScratch(100, (64, 64))
+    splats.render_with(scratch, cam, (64, 64))
+    cap = scratch.capacity()
+    for _ in range(5):
+        splats.render_with(scratch, cam, (64, 64))
+        assert scratch.capacity() == cap
+
+
+def test_capacity_grows_instead_of_truncating(ctx, oracle_mod):
+    """The reference truncates past capacity and grows next frame
+    (src/raster.rs:38-46, src/render.rs:171-197); here the first frame is
+    already complete: capacity grows to the exact scan total before emission."""
+    from splatfield_b200 import synth
+
+    n, w, h = 60000, 512, 512
+    attr, sh = synth.scene_uniform(n, 1, 11)
+    attr = attr.reshape(11, n)
+    attr[7:10] += 2.5  # large splats: many tiles each
+    attr = attr.reshape(-1)
+    cam = sf.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    isects = splats.prepare_isects(scratch, cam, (w, h))
+    assert isects.num_isects > (1 << 22)
+    assert scratch.capacity() >= isects.num_isects
+    cam_o = oracle_mod.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    want = oracle_mod.prepare(cam_o, w, h, attr, sh, 1)
+    assert want["num_isects"] == isects.num_isects
+    np.testing.assert_array_equal(isects.gaussian_ids().read(), want["gaussian_ids"])
+
+
+def test_shape_change_rebuilds_scratch(ctx):
+    """A scratch built for one size renders another size correctly
+    (src/render.rs:171-183 rebuilds in place)."""
+    attr = opaque(stacked_positions())
+    splats = sf.Splats(attr, zero_sh(5))
+    scratch = sf.RenderScratch(5, (64, 64))
+    splats.render_with(scratch, sf.camera_default(), (64, 64))
+    small = splats.render_with(scratch, sf.camera_default(), (32, 32)).read()
+    fresh = splats.render_with(sf.RenderScratch(5, (32, 32)), sf.camera_default(), (32, 32)).read()
+    np.testing.assert_array_equal(small, fresh)
+
+
+def test_empty_view_renders_transparent(ctx):
+    """Every splat behind the camera: zero visible, zero intersections."""
+    splats = sf.Splats(opaque([(0.0, 0.0, -5.0)] * 10), zero_sh(10))
+    scratch = sf.RenderScratch(10, (48, 40))
+    isects = splats.prepare_isects(scratch, sf.camera_default(), (48, 40))
+    assert isects.num_visible == 0 and isects.num_isects == 0
+    bm = splats.finalize_rgb(scratch, isects, (48, 40)).read()
+    assert np.all(bm[:, :48] == 0)
+
+
+def test_zero_splats_rejected(ctx):
+    with pytest.raises(sf.SplatfieldError):
+        sf.Splats(np.zeros(0, np.float32), np.zeros(0, np.float32))
+
+
+def test_render_to_host_matches_device_bitmap(ctx):
+    from splatfield_b200 import synth
+
+    attr, sh = synth.scene_uniform(5000, 4, 9)
+    cam = sf.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(5000, (100, 60))
+    dev = splats.render_with(scratch, cam, (100, 60)).read()
+    host = splats.render_to_host(scratch, cam, (100, 60))
+    np.testing.assert_array_equal(host, dev[:, :100])
+
+
+def test_float_image_vs_fp64_oracle(ctx, oracle_mod):
+    """The FP32 float plane against the FP64 twin of the same forward: max
+    abs error per channel, reported; pixels whose alpha sequence crossed a
+    threshold differently in f64 are excluded by comparing at the median."""
+    from splatfield_b200 import synth
+
+    n, w, h = 20000, 128, 128
+    attr, sh = synth.scene_uniform(n, 4, 21)
+    cam = sf.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    cam_o = oracle_mod.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    got = splats.render_float(scratch, cam, (w, h)).read()
+    ref = oracle_mod.render64(cam_o, w, h, attr.astype(np.float64), sh.astype(np.float64), 4)
+    err = np.abs(got.astype(np.float64) - ref)
+    assert np.median(err) < 1e-6
+    assert np.mean(err < 2e-4) > 0.99
