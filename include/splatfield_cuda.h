@@ -140,6 +140,16 @@ int sf_scratch_destroy(sf_scratch s);
 /* Current intersection capacity (entries). */
 int sf_scratch_capacity(sf_scratch s, uint64_t* capacity);
 
+/* Kernel forms a scratch launches; all forms give identical results (the
+ * autotuner picks by measured time). */
+typedef struct {
+    uint32_t raster_cull; /* 0: every warp walks every staged entry;
+                             1: per-warp culling by each splat's power_max box */
+    uint32_t reserved[7];
+} sf_tuning;
+int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t);
+int sf_scratch_get_tuning(sf_scratch s, sf_tuning* t);
+
 /* ---------------------------------------------------------------- render */
 /* Splats::render_with (src/render.rs:371-380): one RGBA8 frame. Syncs once
  * (intersection total). *bitmap receives a device pointer [h][row_stride]
@@ -171,7 +181,8 @@ int sf_scratch_buffers(sf_scratch s, const uint32_t** bitmap, const float** rgba
 /* Pair statistics of the scratch's last rasterization (syncs): out[0] =
  * (pixel, splat) pairs visited (256 per tile-list entry walked before the
  * tile's early exit), out[1] = exponentials evaluated, out[2] = contributing
- * pairs (alpha >= 1/255), out[3] = 0. */
+ * pairs (alpha >= 1/255), out[3] = pairs processed after the per-warp
+ * culling (32 per warp-splat walked). */
 int sf_scratch_stats(sf_scratch s, uint64_t out[4], sf_stream stream);
 
 /* Intermediates of the last prepare, copied to host (syncs), for parity

@@ -48,6 +48,12 @@ class View(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    """sf_tuning: kernel forms of a scratch (results are identical across forms)."""
+
+    _fields_ = [("raster_cull", C.c_uint32), ("reserved", C.c_uint32 * 7)]
+
+
 class Isects(C.Structure):
     """TileIsects (src/render.rs:463-471)."""
 
@@ -88,6 +94,8 @@ SIGNATURES = {
         "sf_scratch_create": (i32, [P, u32, u32, u32, PP]),
         "sf_scratch_destroy": (i32, [P]),
         "sf_scratch_capacity": (i32, [P, P]),
+        "sf_scratch_set_tuning": (i32, [P, P]),
+        "sf_scratch_get_tuning": (i32, [P, P]),
         "sf_render_with": (i32, [P, P, P, u32, u32, P, PP, P]),
         "sf_render_float": (i32, [P, P, P, u32, u32, P, PP]),
         "sf_render_to_host": (i32, [P, P, P, u32, u32, P, P]),

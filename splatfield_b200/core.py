@@ -331,6 +331,16 @@ class RenderScratch:
         check(lib().sf_scratch_capacity(self.handle, C.byref(c)))
         return int(c.value)
 
+    def set_tuning(self, raster_cull: int = 0) -> None:
+        t = L.Tuning()
+        t.raster_cull = int(raster_cull)
+        check(lib().sf_scratch_set_tuning(self.handle, C.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = L.Tuning()
+        check(lib().sf_scratch_get_tuning(self.handle, C.byref(t)))
+        return {"raster_cull": int(t.raster_cull)}
+
     def read(self, what: int, count: int, dtype=np.uint32, stream=None) -> np.ndarray:
         out = np.empty(count, dtype)
         check(lib().sf_scratch_read(self.handle, what, _vp(out), out.nbytes, _stream(stream)))
@@ -340,7 +350,8 @@ class RenderScratch:
         """Pair statistics of the last rasterization on this scratch."""
         out = np.zeros(4, np.uint64)
         check(lib().sf_scratch_stats(self.handle, _vp(out), _stream(stream)))
-        return dict(pairs_visited=int(out[0]), exp_evaluated=int(out[1]), contributing=int(out[2]))
+        return dict(pairs_visited=int(out[0]), exp_evaluated=int(out[1]), contributing=int(out[2]),
+                    pairs_processed=int(out[3]))
 
     def bitmap_ptr(self) -> int:
         b = C.c_void_p()

@@ -121,6 +121,7 @@ struct sf_scratch_t {
     float4* geo0 = nullptr;
     float4* geo1 = nullptr;
     float4* color = nullptr;
+    float2* ext = nullptr;
     uint32_t *keys_a = nullptr, *keys_b = nullptr, *order_a = nullptr, *order_b = nullptr;
     const uint32_t* order = nullptr;
     uint32_t* offsets = nullptr;
@@ -143,6 +144,7 @@ struct sf_scratch_t {
     uint32_t num_visible = 0, num_isects = 0;
     uint64_t last_isects_raw = 0;
     bool prepared = false;
+    sf_tuning tuning{};
 };
 
 struct sf_accum_t {
@@ -198,7 +200,7 @@ cudaError_t ensure_lut(sf_ctx ctx) {
 
 void scratch_free_frame(sf_scratch s) {
     dfree(s->depth_keys); dfree(s->tile_counts); dfree(s->bbox); dfree(s->geo0); dfree(s->geo1);
-    dfree(s->color); dfree(s->keys_a); dfree(s->keys_b); dfree(s->order_a); dfree(s->order_b);
+    dfree(s->color); dfree(s->ext); dfree(s->keys_a); dfree(s->keys_b); dfree(s->order_a); dfree(s->order_b);
     dfree(s->offsets); dfree(s->scan_tmp); dfree(s->tile_start); dfree(s->bitmap);
     dfree(s->rgba); dfree(s->final_t); dfree(s->n_contrib);
     s->order = nullptr;
@@ -255,6 +257,7 @@ cudaError_t scratch_build(sf_scratch s, uint32_t total, uint32_t w, uint32_t h) 
     SF_AL(s->geo0, total);
     SF_AL(s->geo1, total);
     SF_AL(s->color, total);
+    SF_AL(s->ext, total);
     SF_AL(s->keys_a, total);
     SF_AL(s->keys_b, total);
     SF_AL(s->order_a, total);
@@ -263,6 +266,9 @@ cudaError_t scratch_build(sf_scratch s, uint32_t total, uint32_t w, uint32_t h) 
     SF_AL(s->tile_start, (size_t)s->tiles_x * s->tiles_y + 1);
     SF_AL(s->bitmap, (size_t)h * s->row_stride);
 #undef SF_AL
+    // Row padding (row_stride past w) is never rendered: clear it once so
+    // read-backs of whole rows are deterministic.
+    if ((e = cudaMemset(s->bitmap, 0, (size_t)h * s->row_stride * 4)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&s->scan_tmp, scan_temp_bytes(total))) != cudaSuccess) return e;
     if (!s->words) {
         if ((e = dalloc(&s->stats, 4)) != cudaSuccess) return e;
@@ -288,7 +294,7 @@ int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32
     uint32_t* words = s->words;
     unsigned long long* total_dev = reinterpret_cast<unsigned long long*>(words + 4);
     SF_CK(cudaMemsetAsync(words, 0, 32, st));
-    ProjOut po{s->depth_keys, s->tile_counts, s->bbox, s->geo0, s->geo1, s->color, words};
+    ProjOut po{s->depth_keys, s->tile_counts, s->bbox, s->geo0, s->geo1, s->color, words, s->ext};
     SF_CK(launch_project(view, sp->attr, sp->sh, n, sp->K, po, st));
     int in_b = 0;
     SF_CK(ensure_sort_tmp(s, radix_temp_bytes(n, 4)));
@@ -353,6 +359,8 @@ RasterArgs raster_args(sf_scratch s, const sf_isects* is) {
     a.geo0 = s->geo0;
     a.geo1 = s->geo1;
     a.color = s->color;
+    a.ext = s->ext;
+    a.cull = s->tuning.raster_cull;
     a.stats = s->stats;
     return a;
 }
@@ -581,6 +589,19 @@ int sf_scratch_destroy(sf_scratch s) {
     dfree(s->stats);
     if (s->host_words) cudaFreeHost(s->host_words);
     delete s;
+    return SF_OK;
+}
+
+int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t) {
+    if (!s || !t) return fail(SF_ERR_ARG, "null argument");
+    if (t->raster_cull > 1) return fail(SF_ERR_ARG, "raster_cull must be 0 or 1");
+    s->tuning = *t;
+    return SF_OK;
+}
+
+int sf_scratch_get_tuning(sf_scratch s, sf_tuning* t) {
+    if (!s || !t) return fail(SF_ERR_ARG, "null argument");
+    *t = s->tuning;
     return SF_OK;
 }
 

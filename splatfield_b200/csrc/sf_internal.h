@@ -30,6 +30,7 @@ struct ProjOut {
     float4* geo1;           // [n]
     float4* color;          // [n] (may be null: colour not needed)
     uint32_t* visible;      // atomic counter (may be null)
+    float2* ext;            // [n] half extents of the box holding power <= power_max
 };
 
 cudaError_t launch_project(const sf_view& view, const float* attr, const float* sh, uint32_t n,
@@ -51,6 +52,7 @@ struct RasterArgs {
     const float4* geo0;
     const float4* geo1;
     const float4* color;
+    const float2* ext;
     float scale;
     const uint32_t* mask;
     uint32_t mask_wpr;
@@ -61,6 +63,9 @@ struct RasterArgs {
     uint32_t* bg;
     float* final_t;
     uint32_t* n_contrib;
+    // Raster form: 0 walks every staged entry in every warp, 1 culls per warp
+    // block with the power_max boxes (needs ext).
+    uint32_t cull;
     // Optional pair statistics, added to: [0] (pixel, splat) pairs visited
     // (256 per tile-list entry walked before the tile's early exit), [1]
     // exponentials evaluated, [2] contributing pairs (alpha >= 1/255).

@@ -28,10 +28,11 @@ constexpr float kPowerMargin = 0.01f;
 struct V3 { float x, y, z; };
 __device__ __forceinline__ float dot3(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
 
+// sh_to_rgb (src/project.rs:344-388) over coefficients already in registers,
+// c[k*3 + channel].
 template <int K>
-__device__ __forceinline__ void sh_to_rgb(V3 d, const float* __restrict__ shs, uint32_t s, uint32_t n,
-                                          float& r, float& g, float& b) {
-    auto sh = [&](int k) { return __ldg(shs + (size_t)k * n + s); };
+__device__ __forceinline__ void sh_to_rgb(V3 d, const float (&c)[3 * K], float& r, float& g, float& b) {
+    auto sh = [&](int k) { return c[k]; };
     r = kSHC0 * sh(0);
     g = kSHC0 * sh(1);
     b = kSHC0 * sh(2);
@@ -80,9 +81,19 @@ __global__ __launch_bounds__(256) void project_kernel(sf_view v, const float* __
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const size_t N = n;
-    const float op_raw = __ldg(attr + 10 * N + i);
-    const float opacity = sigmoid_(op_raw);
-    const V3 mean{__ldg(attr + 0 * N + i), __ldg(attr + 1 * N + i), __ldg(attr + 2 * N + i)};
+    // Every load is issued before any use (all planes in flight at once);
+    // culled splats (a few percent) read their colour planes for nothing.
+    float a[11];
+#pragma unroll
+    for (int k = 0; k < 11; ++k) a[k] = __ldg(attr + k * N + i);
+    float c[3 * K];
+    const bool want_color = o.color != nullptr;
+    if (want_color) {
+#pragma unroll
+        for (int k = 0; k < 3 * K; ++k) c[k] = __ldg(shs + k * N + i);
+    }
+    const float opacity = sigmoid_(a[10]);
+    const V3 mean{a[0], a[1], a[2]};
     const V3 rot0{v.rot0[0], v.rot0[1], v.rot0[2]};
     const V3 rot1{v.rot1[0], v.rot1[1], v.rot1[2]};
     const V3 rot2{v.rot2[0], v.rot2[1], v.rot2[2]};
@@ -95,10 +106,8 @@ __global__ __launch_bounds__(256) void project_kernel(sf_view v, const float* __
     }
     const float cam_x = dot3(rot0, mean) + v.trans[0];
     const float cam_y = dot3(rot1, mean) + v.trans[1];
-    const float qw = __ldg(attr + 3 * N + i), qx = __ldg(attr + 4 * N + i),
-                qy = __ldg(attr + 5 * N + i), qz = __ldg(attr + 6 * N + i);
-    const V3 s{exp_(__ldg(attr + 7 * N + i)), exp_(__ldg(attr + 8 * N + i)),
-               exp_(__ldg(attr + 9 * N + i))};
+    const float qw = a[3], qx = a[4], qy = a[5], qz = a[6];
+    const V3 s{exp_(a[7]), exp_(a[8]), exp_(a[9])};
     const float inv_z = 1.0f / cam_z;
 
     const float x2 = qx * qx, y2 = qy * qy, z2 = qz * qz;
@@ -141,7 +150,7 @@ __global__ __launch_bounds__(256) void project_kernel(sf_view v, const float* __
         const float inv = 1.0f / sqrtf(dot3(dir, dir));
         dir = V3{dir.x * inv, dir.y * inv, dir.z * inv};
         float r, g, b;
-        sh_to_rgb<K>(dir, shs, i, n, r, g, b);
+        sh_to_rgb<K>(dir, c, r, g, b);
         o.color[i] = make_float4(r + 0.5f, g + 0.5f, b + 0.5f, 0.0f);
     }
     const float cutoff = log_(opacity / kAlphaCutoff);
@@ -159,6 +168,22 @@ __global__ __launch_bounds__(256) void project_kernel(sf_view v, const float* __
     o.bbox[i] = make_uint2(min_x | (min_y << 16), max_x | (max_y << 16));
     o.geo0[i] = make_float4(mx, my, 0.5f * cx, cy);
     o.geo1[i] = make_float4(0.5f * cz, opacity, power_max, 0.0f);
+    if (o.ext) {
+        // Half extents of the box around {power <= P}, P = power_max with a
+        // 1e-4 margin for rounding: for q = hx dx^2 + hz dy^2 + cy dx dy the
+        // level set's x extent is sqrt(P * hz / det), det = hx hz - cy^2/4.
+        // Outside the box the computed power exceeds power_max, so the
+        // rasterizer may skip the pair. A degenerate form gets no box.
+        const float hx = 0.5f * cx, hz = 0.5f * cz;
+        const float dq = hx * hz - 0.25f * (cy * cy);
+        const float P = power_max * 1.0001f + 1e-4f;
+        float ex = INFINITY, ey = INFINITY;
+        if (dq > 0.0f && P > 0.0f) {
+            ex = sqrtf(P * hz / dq) * 1.0001f + 1e-3f;
+            ey = sqrtf(P * hx / dq) * 1.0001f + 1e-3f;
+        }
+        o.ext[i] = make_float2(ex, ey);
+    }
     if (o.visible) {
         // Warp-aggregated visible count.
         const uint32_t active = __activemask();
@@ -167,7 +192,11 @@ __global__ __launch_bounds__(256) void project_kernel(sf_view v, const float* __
 }
 
 // map_isects (src/raster.rs:13-48): rank r writes its bbox tiles row-major at
-// its scan offset. Past capacity the write is dropped and flagged.
+// its scan offset. The 32 ranks of a warp own one contiguous output run
+// (their offsets are consecutive), so the warp writes that run cooperatively:
+// lane l emits outputs l, l+32, ... and finds the owning rank by a 5-step
+// shuffle search over the lanes' inclusive ends. Every store is coalesced.
+// Past capacity the write is dropped and flagged.
 __global__ __launch_bounds__(256) void emit_kernel(const uint32_t* __restrict__ order,
                                                    const uint2* __restrict__ bbox,
                                                    const uint32_t* __restrict__ offsets, uint32_t n,
@@ -175,47 +204,113 @@ __global__ __launch_bounds__(256) void emit_kernel(const uint32_t* __restrict__ 
                                                    uint32_t* __restrict__ tile_ids,
                                                    uint32_t* __restrict__ gaussian_ids,
                                                    uint32_t* err) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    const uint32_t vis = order[r];
-    const uint2 bb = bbox[vis];
-    const uint32_t min_x = bb.x & 0xffffu, min_y = bb.x >> 16;
-    const uint32_t max_x = bb.y & 0xffffu, max_y = bb.y >> 16;
-    uint32_t slot = offsets[r];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t r0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;
+    if (r0 >= n) return;
+    const uint32_t r = r0 + lane;
+    const bool valid = r < n;
+    uint32_t vis = 0, min_x = 0, min_y = 0, width = 1, cnt = 0, off = 0;
+    if (valid) {
+        vis = order[r];
+        const uint2 bb = bbox[vis];
+        min_x = bb.x & 0xffffu;
+        min_y = bb.x >> 16;
+        const uint32_t max_x = bb.y & 0xffffu, max_y = bb.y >> 16;
+        width = max(max_x - min_x, 1u);
+        cnt = (max_x - min_x) * (max_y - min_y);
+        off = offsets[r];
+    }
+    const uint32_t base = __shfl_sync(0xffffffffu, off, 0);
+    uint32_t incl = valid ? off - base + cnt : 0u;
+    const uint32_t total = __reduce_max_sync(0xffffffffu, incl);
+    if (!valid) incl = total;
     bool over = false;
-    for (uint32_t ty = min_y; ty < max_y; ++ty)
-        for (uint32_t tx = min_x; tx < max_x; ++tx) {
+    // `total` is warp-uniform: every lane runs every iteration (the owner lane
+    // of a shuffle must be active), only the stores are predicated.
+    for (uint32_t p0 = 0; p0 < total; p0 += 32) {
+        const uint32_t p = p0 + lane;
+        // Owner: the first lane whose inclusive end exceeds p.
+        uint32_t o = 0;
+#pragma unroll
+        for (uint32_t step = 16; step > 0; step >>= 1) {
+            const uint32_t v = __shfl_sync(0xffffffffu, incl, o + step - 1);
+            if (v <= p) o += step;
+        }
+        const uint32_t oend = __shfl_sync(0xffffffffu, incl, o);
+        const uint32_t ocnt = __shfl_sync(0xffffffffu, cnt, o);
+        const uint32_t ow = __shfl_sync(0xffffffffu, width, o);
+        const uint32_t ox = __shfl_sync(0xffffffffu, min_x, o);
+        const uint32_t oy = __shfl_sync(0xffffffffu, min_y, o);
+        const uint32_t ovis = __shfl_sync(0xffffffffu, vis, o);
+        if (p < total) {
+            const uint32_t k = p - (oend - ocnt);
+            const uint32_t slot = base + p;
             if (slot < capacity) {
-                tile_ids[slot] = tx + ty * tiles_per_row;
-                gaussian_ids[slot] = vis;
+                tile_ids[slot] = (ox + k % ow) + (oy + k / ow) * tiles_per_row;
+                gaussian_ids[slot] = ovis;
             } else {
                 over = true;
             }
-            ++slot;
         }
+    }
     if (over) atomicOr(err, SF_DEV_ERR_CAPACITY);
 }
 
-__global__ void tile_start_kernel(const uint32_t* __restrict__ ids, uint32_t n_static,
-                                  const uint32_t* n_dev, uint32_t num_tiles,
-                                  uint32_t* __restrict__ start) {
+// tile_start[t] = lower_bound(ids, t) for t in [0, num_tiles]: each thread
+// scans 8 consecutive sorted ids and writes the starts of the tiles whose
+// first entry (or an empty tile's insertion point) falls in its range.
+constexpr uint32_t kStartItems = 8;
+__global__ __launch_bounds__(256) void tile_start_kernel(const uint32_t* __restrict__ ids,
+                                                         uint32_t n_static, const uint32_t* n_dev,
+                                                         uint32_t num_tiles,
+                                                         uint32_t* __restrict__ start) {
     const uint32_t n = n_dev ? *n_dev : n_static;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > n) return;
-    const uint32_t lo = (i == 0) ? 0u : ids[i - 1] + 1u;
-    const uint32_t hi = (i == n) ? num_tiles : min(ids[i], num_tiles);
-    for (uint32_t t = lo; t <= hi; ++t) start[t] = i;
+    const uint32_t i0 = (blockIdx.x * blockDim.x + threadIdx.x) * kStartItems;
+    if (i0 > n) return;
+    uint32_t prev = (i0 == 0) ? 0u : ids[i0 - 1] + 1u;
+    for (uint32_t k = 0; k < kStartItems; ++k) {
+        const uint32_t i = i0 + k;
+        if (i > n) break;
+        const uint32_t hi = (i == n) ? num_tiles : min(ids[i], num_tiles);
+        for (uint32_t t = prev; t <= hi; ++t) start[t] = i;
+        if (i == n) break;
+        prev = max(prev, hi + 1u);
+    }
+}
+
+// Bit w set: the box around the splat's {power <= power_max} (half extents
+// `e`, computed with margin by the projection) overlaps the pixel centres of
+// warp w's 8x4 block of tile (tx, ty). A pair outside the box has computed
+// power above power_max, which the per-pixel path skips as well, so dropping
+// it changes nothing.
+__device__ __forceinline__ uint32_t warp_mask(float mx, float my, float2 e, uint32_t tx, uint32_t ty) {
+    const float bx = (float)(tx * 16) + 0.5f, by = (float)(ty * 16) + 0.5f;
+    const float lx = mx - e.x - bx, hxr = mx + e.x - bx;  // box relative to the tile's first centre
+    const float ly = my - e.y - by, hyr = my + e.y - by;
+    // columns [0,7] and [8,15]; rows [0,3], [4,7], [8,11], [12,15]
+    const uint32_t cx = (uint32_t)(lx <= 7.0f && hxr >= 0.0f) | ((uint32_t)(lx <= 15.0f && hxr >= 8.0f) << 1);
+    uint32_t m = 0;
+#pragma unroll
+    for (uint32_t r = 0; r < 4; ++r) {
+        const float y0 = (float)(r * 4);
+        if (ly <= y0 + 3.0f && hyr >= y0) m |= cx << (2 * r);
+    }
+    return m;
 }
 
 // rasterize_kernel (src/raster.rs:88-230). One 256-thread block per 16x16
 // tile; each warp owns an 8x4 pixel block. Chunks of 256 splat records are
-// staged in shared memory; pairs whose power exceeds the splat's power_max
+// staged in shared memory. Pairs whose power exceeds the splat's power_max
 // (alpha < 1/255 there, the reference's skip) bypass the exponential. The
-// whole tile stops once every pixel's transmittance fell below 1/255.
+// tile stops once every pixel is saturated (T < 1/255).
+// CULL: each staged splat also gets an 8-bit mask of the warp blocks its
+// power_max box reaches (warp_mask) and a warp walks only its splats (and
+// stops once its own pixels are saturated) — fewer steps, more registers;
+// which form is faster depends on the scene, so both are kept.
 // Responsibility/evidence words are reduced per warp (redux.sync), then per
 // tile in shared memory, then added to global memory once per (tile, splat):
 // integer sums, so the words equal the reference's per-pixel atomics exactly.
-template <int MODE>
+template <int MODE, bool CULL>
 __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
     __shared__ float4 s_g0[256];
     __shared__ float4 s_g1[256];
@@ -223,6 +318,7 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
     __shared__ uint32_t s_gid[MODE == 0 ? 1 : 256];
     __shared__ uint32_t s_acc0[MODE == 0 ? 1 : 256];
     __shared__ uint32_t s_acc1[MODE == 2 ? 256 : 1];
+    __shared__ uint8_t s_mask[256];
 
     const uint32_t tile = blockIdx.x;
     const uint32_t tx = tile % a.tiles_x, ty = tile / a.tiles_x;
@@ -238,15 +334,17 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
     float T = 1.0f, pr = 0.0f, pg = 0.0f, pb = 0.0f;
     uint32_t last = 0;
     bool done = !in_bounds;
-    uint32_t n_eval = 0, n_hit = 0, visited = 0;
+    uint32_t n_eval = 0, n_hit = 0, n_proc = 0, visited = 0;
 
     for (uint32_t chunk = start; chunk < end; chunk += 256) {
         __syncthreads();
         const uint32_t idx = chunk + tid;
         if (idx < end) {
             const uint32_t g = a.gaussian_ids[idx];
-            s_g0[tid] = a.geo0[g];
-            s_g1[tid] = a.geo1[g];
+            const float4 g0 = a.geo0[g], g1 = a.geo1[g];
+            s_g0[tid] = g0;
+            s_g1[tid] = g1;
+            if (CULL) s_mask[tid] = (uint8_t)warp_mask(g0.x, g0.y, a.ext[g], tx, ty);
             if (MODE == 0) {
                 s_col[tid] = a.color[g];
             } else {
@@ -258,7 +356,9 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
         if (__syncthreads_count(done) == 256) break;
         const uint32_t cnt = min(256u, end - chunk);
         visited += cnt;
-        for (uint32_t j = 0; j < cnt; ++j) {
+        // One (warp, entry) step: every lane of the warp runs it together.
+        auto step = [&](uint32_t j) {
+            ++n_proc;
             uint32_t q = 0;
             if (!done) {
                 const float4 g0 = s_g0[j];
@@ -297,6 +397,22 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
                     if (sb) atomicAdd(&s_acc1[j], sb);
                 }
             }
+        };
+        if (CULL) {
+            // This warp's entries of the chunk, 32 candidates per ballot;
+            // only entries with the warp's bit are walked, in list order.
+            for (uint32_t g32 = 0; g32 < cnt; g32 += 32) {
+                if (__all_sync(0xffffffffu, done)) break;
+                uint32_t word = __ballot_sync(0xffffffffu,
+                                              g32 + lane < cnt && ((s_mask[g32 + lane] >> warp) & 1u));
+                while (word) {
+                    const uint32_t j = g32 + (uint32_t)(__ffs(word) - 1);
+                    word &= word - 1u;
+                    step(j);
+                }
+            }
+        } else {
+            for (uint32_t j = 0; j < cnt; ++j) step(j);
         }
         if (MODE != 0) {
             __syncthreads();
@@ -314,9 +430,11 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
     if (a.stats) {
         const uint32_t e = __reduce_add_sync(0xffffffffu, n_eval);
         const uint32_t c = __reduce_add_sync(0xffffffffu, n_hit);
+        const uint32_t pr_ = __reduce_add_sync(0xffffffffu, n_proc);
         if (lane == 0) {
             atomicAdd(a.stats + 1, (unsigned long long)e);
             atomicAdd(a.stats + 2, (unsigned long long)c);
+            atomicAdd(a.stats + 3, (unsigned long long)pr_);
         }
         if (tid == 0) atomicAdd(a.stats, 256ull * visited);
     }
@@ -383,7 +501,7 @@ cudaError_t launch_emit(const uint32_t* order, const uint2* bbox, const uint32_t
 cudaError_t launch_tile_starts(const uint32_t* sorted_tile_ids, uint32_t num_isects,
                                const uint32_t* num_isects_dev, uint32_t max_isects,
                                uint32_t num_tiles, uint32_t* tile_start, cudaStream_t stream) {
-    const uint32_t grid_n = (num_isects_dev ? max_isects : num_isects) + 1;
+    const uint32_t grid_n = ((num_isects_dev ? max_isects : num_isects) + 1 + kStartItems - 1) / kStartItems;
     tile_start_kernel<<<(grid_n + 255) / 256, 256, 0, stream>>>(sorted_tile_ids, num_isects,
                                                                 num_isects_dev, num_tiles, tile_start);
     note_launches(1);
@@ -394,9 +512,18 @@ cudaError_t launch_raster(int mode, const RasterArgs& a, cudaStream_t stream) {
     const uint32_t tiles = a.tiles_x * a.tiles_y;
     if (tiles == 0) return cudaSuccess;
     switch (mode) {
-        case 0: raster_kernel<0><<<tiles, 256, 0, stream>>>(a); break;
-        case 1: raster_kernel<1><<<tiles, 256, 0, stream>>>(a); break;
-        case 2: raster_kernel<2><<<tiles, 256, 0, stream>>>(a); break;
+        case 0:
+            if (a.cull) raster_kernel<0, true><<<tiles, 256, 0, stream>>>(a);
+            else raster_kernel<0, false><<<tiles, 256, 0, stream>>>(a);
+            break;
+        case 1:
+            if (a.cull) raster_kernel<1, true><<<tiles, 256, 0, stream>>>(a);
+            else raster_kernel<1, false><<<tiles, 256, 0, stream>>>(a);
+            break;
+        case 2:
+            if (a.cull) raster_kernel<2, true><<<tiles, 256, 0, stream>>>(a);
+            else raster_kernel<2, false><<<tiles, 256, 0, stream>>>(a);
+            break;
         default: return cudaErrorInvalidValue;
     }
     note_launches(1);

@@ -51,10 +51,69 @@ __device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned lon
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+__device__ __forceinline__ uint32_t ld_status(const uint32_t* p) { return ld_relaxed(p); }
+__device__ __forceinline__ unsigned long long ld_status(const unsigned long long* p) {
+    return ld_relaxed64(p);
+}
+
+// Decoupled look-back from partition `part` over status words stat[p * stride]
+// (flag in the top two bits: 0 = not ready, aggregate, inclusive prefix).
+// kWindow predecessors are loaded at once, so a chain of aggregates costs one
+// L2 round trip per kWindow partitions instead of one per partition. Returns
+// the exclusive prefix. A wait that outlasts kSpinLimit polls records
+// SF_DEV_ERR_TIMEOUT and returns what it has.
+constexpr int kWindow = 8;
+template <typename W>
+__device__ __forceinline__ W lookback_window(const W* stat, size_t stride, uint32_t part, W flag_prefix,
+                                             W value_mask, uint32_t* err) {
+    W excl = 0;
+    int64_t p = (int64_t)part - 1;
+    uint32_t spins = 0;
+    while (p >= 0) {
+        W s[kWindow];
+#pragma unroll
+        for (int w = 0; w < kWindow; ++w)
+            s[w] = (p - w >= 0) ? ld_status(stat + (size_t)(p - w) * stride) : flag_prefix;
+        int used = 0;
+        bool found = false;
+        for (; used < kWindow; ++used) {
+            const W flag = s[used] & ~value_mask;
+            if (flag == 0) break;
+            excl += s[used] & value_mask;
+            if (flag == flag_prefix) {
+                found = true;
+                break;
+            }
+        }
+        if (found) break;
+        if (used == 0 && ++spins > kSpinLimit) {
+            atomicOr(err, SF_DEV_ERR_TIMEOUT);
+            break;
+        }
+        p -= used;
+    }
+    return excl;
+}
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
+}
+
+// Lanes holding the same 8-bit digit (and the same validity) as this lane:
+// one ballot per digit bit, inverted where this lane's bit is clear, ANDed.
+// Fixed cost of nine votes, far cheaper on this part than match.any.
+__device__ __forceinline__ uint32_t match_digit(uint32_t d, bool valid) {
+    uint32_t peers = __ballot_sync(0xffffffffu, valid);
+    if (!valid) peers = ~peers;
+#pragma unroll
+    for (int b = 0; b < kRadixBits; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const uint32_t v = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? v : ~v;
+    }
+    return peers;
 }
 
 __device__ __forceinline__ uint32_t load_n(const uint32_t* n_dev, uint32_t n_static) {
@@ -69,14 +128,29 @@ __global__ __launch_bounds__(kThreads) void radix_histogram_kernel(
     const uint32_t n = load_n(n_dev, n_static);
     for (uint32_t i = threadIdx.x; i < num_passes * kRadix; i += kThreads) s_hist[i] = 0;
     __syncthreads();
+    // Whole warps iterate together (the bound is rounded up) so that runs of
+    // equal digits in neighbouring lanes are merged before the shared atomic:
+    // emitted tile ids come in runs, and 32 lanes on one bin would otherwise
+    // serialise. A lane whose digit differs from its left neighbour's adds the
+    // length of its run.
     const uint32_t stride = gridDim.x * kThreads;
-    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
-        const uint32_t k = keys[i];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t n_round = (n + 31u) & ~31u;
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n_round; i += stride) {
+        const bool valid = i < n;
+        const uint32_t k = valid ? keys[i] : 0u;
         for (uint32_t p = 0; p < num_passes; ++p) {
             const uint32_t shift = p * kRadixBits;
             const uint32_t w = bits - shift < (uint32_t)kRadixBits ? bits - shift : kRadixBits;
-            const uint32_t d = (k >> shift) & ((1u << w) - 1u);
-            atomicAdd(&s_hist[p * kRadix + d], 1u);
+            const uint32_t d = valid ? ((k >> shift) & ((1u << w) - 1u)) : (uint32_t)kRadix;
+            const uint32_t left = __shfl_up_sync(0xffffffffu, d, 1);
+            const bool head = lane == 0 || left != d;
+            const uint32_t heads = __ballot_sync(0xffffffffu, head);
+            if (valid && head) {
+                const uint32_t above = heads & ~((2u << lane) - 1u);
+                const uint32_t next = above ? (uint32_t)(__ffs(above) - 1) : 32u;
+                atomicAdd(&s_hist[p * kRadix + d], next - lane);
+            }
         }
     }
     __syncthreads();
@@ -85,7 +159,7 @@ __global__ __launch_bounds__(kThreads) void radix_histogram_kernel(
 }
 
 // One 8-bit digit pass. `vals_iota` substitutes vals_in[i] = i.
-__global__ __launch_bounds__(kThreads) void onesweep_pass_kernel(
+__global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, const uint32_t* n_dev,
     uint32_t n_static, uint32_t shift, uint32_t digit_mask, const uint32_t* __restrict__ pass_hist,
@@ -122,7 +196,7 @@ __global__ __launch_bounds__(kThreads) void onesweep_pass_kernel(
         const uint32_t idx = wbase + i * 32 + lane;
         const bool valid = idx < n;
         const uint32_t d = valid ? ((k[i] >> shift) & digit_mask) : (uint32_t)kRadix;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t peers = match_digit(d, valid);
         const uint32_t leader = __ffs(peers) - 1;
         uint32_t prev = 0;
         if (valid && lane == leader) {
@@ -195,26 +269,11 @@ __global__ __launch_bounds__(kThreads) void onesweep_pass_kernel(
         __syncthreads();
         gstart = v - h + (warp ? s_scan[warp - 1] : 0u);
     }
-    // Decoupled look-back, one digit per thread.
+    // Decoupled look-back, one digit per thread, kWindow predecessors per step.
     if (tid < kRadix) {
         uint32_t excl = 0;
         if (part > 0) {
-            int64_t p = (int64_t)part - 1;
-            uint32_t spins = 0;
-            while (p >= 0) {
-                const uint32_t s = ld_relaxed(&lookback[(size_t)p * kRadix + tid]);
-                const uint32_t flag = s & ~kCountMask;
-                if (flag == 0u) {
-                    if (++spins > kSpinLimit) {
-                        atomicOr(err, SF_DEV_ERR_TIMEOUT);
-                        break;
-                    }
-                    continue;
-                }
-                excl += s & kCountMask;
-                if (flag == kFlagPrefix) break;
-                --p;
-            }
+            excl = lookback_window<uint32_t>(lookback + tid, kRadix, part, kFlagPrefix, kCountMask, err);
             st_relaxed(&lookback[(size_t)part * kRadix + tid], kFlagPrefix | ((excl + digit_total) & kCountMask));
         }
         s_global_base[tid] = gstart + excl - s_local_start[tid];
@@ -260,6 +319,7 @@ __global__ __launch_bounds__(kThreads) void scan_kernel(
     __shared__ uint32_t s_part;
     __shared__ unsigned long long s_warp[kWarps];
     __shared__ unsigned long long s_prefix;
+    __shared__ uint32_t s_tile[kThreads * (kScanItems + 1)];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t n = load_n(n_dev, n_static);
     const uint32_t num_parts = (n + kScanTile - 1) / kScanTile;
@@ -271,16 +331,26 @@ __global__ __launch_bounds__(kThreads) void scan_kernel(
         return;
     }
     if (part >= num_parts) return;
-    const uint32_t base = part * kScanTile + tid * kScanItems;
+    // Coalesced striped loads, transposed through shared memory so each
+    // thread scans kScanItems consecutive elements (row pitch 17 words keeps
+    // the transposed reads conflict-free).
+    const uint32_t tile0 = part * kScanTile;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        const uint32_t e = i * kThreads + tid;
+        const uint32_t idx = tile0 + e;
+        uint32_t c = 0;
+        if (idx < n) c = counts[gids ? gids[idx] : idx];
+        s_tile[(e / kScanItems) * (kScanItems + 1) + e % kScanItems] = c;
+    }
+    __syncthreads();
+    const uint32_t base = tile0 + tid * kScanItems;
     uint32_t v[kScanItems];
     unsigned long long local = 0;
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
-        const uint32_t idx = base + i;
-        uint32_t c = 0;
-        if (idx < n) c = counts[gids ? gids[idx] : idx];
-        v[i] = c;
-        local += c;
+        v[i] = s_tile[tid * (kScanItems + 1) + i];
+        local += v[i];
     }
     // Block exclusive scan of the per-thread sums.
     unsigned long long incl = local;
@@ -303,22 +373,7 @@ __global__ __launch_bounds__(kThreads) void scan_kernel(
             st_relaxed64(&lookback[0], kScanFlagPrefix | block_total);
         } else {
             st_relaxed64(&lookback[part], kScanFlagAgg | block_total);
-            int64_t p = (int64_t)part - 1;
-            uint32_t spins = 0;
-            while (p >= 0) {
-                const unsigned long long s = ld_relaxed64(&lookback[p]);
-                const unsigned long long flag = s & ~kScanValMask;
-                if (flag == 0ull) {
-                    if (++spins > kSpinLimit) {
-                        atomicOr(err, SF_DEV_ERR_TIMEOUT);
-                        break;
-                    }
-                    continue;
-                }
-                excl += s & kScanValMask;
-                if (flag == kScanFlagPrefix) break;
-                --p;
-            }
+            excl = lookback_window<unsigned long long>(lookback, 1, part, kScanFlagPrefix, kScanValMask, err);
             st_relaxed64(&lookback[part], kScanFlagPrefix | (excl + block_total));
         }
         s_prefix = excl;
@@ -328,9 +383,16 @@ __global__ __launch_bounds__(kThreads) void scan_kernel(
     unsigned long long running = s_prefix + warp_prefix + (incl - local);
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
-        const uint32_t idx = base + i;
-        if (idx < n) out[idx] = (uint32_t)running;
+        s_tile[tid * (kScanItems + 1) + i] = (uint32_t)running;
         running += v[i];
+    }
+    (void)base;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        const uint32_t e = i * kThreads + tid;
+        const uint32_t idx = tile0 + e;
+        if (idx < n) out[idx] = s_tile[(e / kScanItems) * (kScanItems + 1) + e % kScanItems];
     }
 }
 

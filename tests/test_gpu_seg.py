@@ -133,8 +133,9 @@ def test_beta_update_uses_evidence(ctx):
     assert abs(b[1] - (1 + bg[1])) < 1e-5
 
 
+@pytest.mark.parametrize("cull", [0, 1])
 @pytest.mark.parametrize("n,k,w,h,seed", [(30000, 4, 256, 256, 5), (8000, 1, 70, 50, 6)])
-def test_seeded_responsibility_and_evidence_bit_exact(ctx, oracle_mod, n, k, w, h, seed):
+def test_seeded_responsibility_and_evidence_bit_exact(ctx, oracle_mod, n, k, w, h, seed, cull):
     from splatfield_b200 import synth
 
     attr, sh = synth.scene_uniform(n, k, seed)
@@ -143,6 +144,7 @@ def test_seeded_responsibility_and_evidence_bit_exact(ctx, oracle_mod, n, k, w, 
     mask = synth.ellipse_mask(w, h, seed)
     splats = sf.Splats(attr, sh)
     scratch = sf.RenderScratch(n, (w, h))
+    scratch.set_tuning(raster_cull=cull)
     acc = sf.Accumulators(n)
     isects = splats.prepare_isects(scratch, cam, (w, h))
     splats.accumulate_prepared(scratch, isects, (w, h), acc, None)
