@@ -164,6 +164,23 @@ int sf_render_float(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint3
  * written to host memory `out`; syncs. */
 int sf_render_to_host(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w,
                       uint32_t h, sf_stream stream, uint32_t* out);
+/* Adjoint (no counterpart in the reference, which renders forward only).
+ * sf_render_forward: sf_render_float that also keeps, per pixel, the final
+ * transmittance and the position of the last contributor, for the backward.
+ * sf_render_backward: for L = sum_p <dl_drgba[p], rgba[p]> (dl_drgba: device
+ * [h][w][4]) of that forward (same camera and size, nothing rendered on the
+ * scratch in between), writes dL/d(attributes) [11*n] and dL/d(sh)
+ * [3*sh_per_ch*n] to device memory, field-major like the inputs. d_proj
+ * (device [n][9], may be NULL) receives the per-splat 2D adjoint
+ * (mean2d xy, conic xyz, colour rgb, opacity); its colour entries with
+ * dl_drgba = (m, 1-m, 1, 0) are the real-valued mask/background/total
+ * responsibilities sum_p m_p alpha T. */
+int sf_render_forward(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                      sf_stream stream, const float** rgba);
+int sf_render_backward(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                       const float* dl_drgba, float* d_attr, float* d_sh, float* d_proj,
+                       sf_stream stream);
+
 /* Splats::prepare_isects (src/render.rs:274-364): project, depth sort, gather
  * scan, emit, stable tile sort, tile ranges. Syncs once. */
 int sf_prepare_isects(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,

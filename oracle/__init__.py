@@ -341,10 +341,15 @@ def render64(cam: Camera, w: int, h: int, attributes, sh, sh_per_ch: int):
     return out.reshape(h, w, 4)
 
 
-def render64_backward(cam: Camera, w: int, h: int, attributes, sh, sh_per_ch: int, dl_drgb):
+def render64_backward(cam: Camera, w: int, h: int, attributes, sh, sh_per_ch: int, dl_drgba):
+    """dL/d(attributes), dL/d(sh) of L = sum(dl_drgba * rgba) (dl_drgba [h, w, 4];
+    a [h, w, 3] array is taken as zero gradient on alpha)."""
     attributes = _c(attributes, np.float64)
     sh = _c(sh, np.float64)
-    dl = _c(dl_drgb, np.float64)
+    dl = np.asarray(dl_drgba, np.float64)
+    if dl.shape[-1] == 3:
+        dl = np.concatenate([dl, np.zeros(dl.shape[:-1] + (1,))], axis=-1)
+    dl = _c(dl, np.float64)
     n = attributes.size // 11
     d_attr = np.empty(11 * n, np.float64)
     d_sh = np.empty(3 * sh_per_ch * n, np.float64)

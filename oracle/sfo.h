@@ -134,11 +134,11 @@ void sfo_beta_update(float scale, const uint32_t* fg, const uint32_t* bg, float*
 /* Same pipeline in double with libm exp/log: float RGBA [h*w*4]. */
 int sfo64_render(const sfo_camera* cam, uint32_t w, uint32_t h, const double* attributes,
                  const double* sh, uint32_t n, uint32_t sh_per_ch, double* rgba);
-/* L = sum(dl_drgb * rgb) over pixels (RGB channels of the FP64 render);
+/* L = sum(dl_drgba * rgba) over pixels of the FP64 render (alpha = 1 - T);
  * writes dL/d(attributes) [11n] and dL/d(sh) [3*K*n]. */
 int sfo64_render_backward(const sfo_camera* cam, uint32_t w, uint32_t h,
                           const double* attributes, const double* sh, uint32_t n,
-                          uint32_t sh_per_ch, const double* dl_drgb, double* d_attr,
+                          uint32_t sh_per_ch, const double* dl_drgba, double* d_attr,
                           double* d_sh);
 
 /* threads the OpenMP regions use */

@@ -3,7 +3,7 @@
 //
 // Forward: the same steps as sfo_render.cpp (src/project.rs:235-327,
 // src/raster.rs:88-230) in double with libm exp/log. Backward: reverse-mode
-// derivative of that forward for L = sum_p <dl_drgb[p], rgba[p]>, with
+// derivative of that forward for L = sum_p <dl_drgba[p], rgba[p]>, with
 //   alpha = min(op*exp(-power), 0.999)  (zero gradient where the clamp binds),
 //   pairs with alpha < 1/255 skipped, a pixel stopping after the contributor
 //   that takes T below 1/255 (src/raster.rs:212-218),
@@ -242,7 +242,7 @@ extern "C" int sfo64_render(const sfo_camera* cam, uint32_t w, uint32_t h, const
 
 extern "C" int sfo64_render_backward(const sfo_camera* cam, uint32_t w, uint32_t h,
                                      const double* attributes, const double* sh, uint32_t n,
-                                     uint32_t K, const double* dl_drgb, double* d_attr,
+                                     uint32_t K, const double* dl_drgba, double* d_attr,
                                      double* d_sh) {
     const View64 v = make_view(cam, w, h);
     Binned bn;
@@ -261,14 +261,15 @@ extern "C" int sfo64_render_backward(const sfo_camera* cam, uint32_t w, uint32_t
             cs.clear();
             double rgb[3];
             const double pxc = px + 0.5, pyc = py + 0.5;
-            walk_pixel(bn, list, pxc, pyc, &cs, rgb);
-            const double* g = dl_drgb + 3 * pix;
+            const double t_final = walk_pixel(bn, list, pxc, pyc, &cs, rgb);
+            const double* g = dl_drgba + 4 * pix;
             double S[3] = {0, 0, 0};  // colour behind, normalised by T_{k+1}
             for (int64_t k = (int64_t)cs.size() - 1; k >= 0; --k) {
                 const Contrib& c = cs[k];
                 const Proj& p = bn.proj[c.id];
                 double* a = my + (size_t)c.id * 9;
-                double dalpha = 0;
+                // alpha channel a = 1 - T_final: d a / d alpha_k = T_final / (1 - alpha_k)
+                double dalpha = g[3] * t_final / (1.0 - c.alpha);
                 for (int ch = 0; ch < 3; ++ch) {
                     a[5 + ch] += g[ch] * c.alpha * c.T;
                     dalpha += g[ch] * c.T * (p.color[ch] - S[ch]);

@@ -99,6 +99,8 @@ SIGNATURES = {
         "sf_render_with": (i32, [P, P, P, u32, u32, P, PP, P]),
         "sf_render_float": (i32, [P, P, P, u32, u32, P, PP]),
         "sf_render_to_host": (i32, [P, P, P, u32, u32, P, P]),
+        "sf_render_forward": (i32, [P, P, P, u32, u32, P, PP]),
+        "sf_render_backward": (i32, [P, P, P, u32, u32, P, P, P, P, P]),
         "sf_prepare_isects": (i32, [P, P, P, u32, u32, P, P]),
         "sf_finalize_rgb": (i32, [P, P, P, u32, u32, i32, P]),
         "sf_scratch_buffers": (i32, [P, PP, PP, P]),

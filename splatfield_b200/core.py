@@ -255,6 +255,32 @@ class Splats:
                                     C.byref(ptr)))
         return DeviceView(ptr.value, np.float32, (h, w, 4), scratch)
 
+    def render_forward(self, scratch: "RenderScratch", camera: Camera, img_size, stream=None) -> DeviceView:
+        """Float RGBA frame that keeps the per-pixel state render_backward replays."""
+        w, h = img_size
+        ptr = C.c_void_p()
+        check(lib().sf_render_forward(self.handle, scratch.handle, C.byref(camera), w, h, _stream(stream),
+                                      C.byref(ptr)))
+        return DeviceView(ptr.value, np.float32, (h, w, 4), scratch)
+
+    def render_backward(self, scratch: "RenderScratch", camera: Camera, img_size, dl_drgba,
+                        want_proj: bool = False, stream=None):
+        """dL/d(attributes) [11, n] and dL/d(sh) [K, 3, n] (field-major) for
+        L = sum(dl_drgba * rgba) of the last render_forward; with want_proj also
+        the per-splat 2D adjoint [n, 9] (mean2d xy, conic xyz, rgb, opacity)."""
+        w, h = img_size
+        dl = dl_drgba if isinstance(dl_drgba, DeviceView) else DeviceBuffer.from_array(
+            np.ascontiguousarray(dl_drgba, np.float32).reshape(h, w, 4), self.ctx)
+        d_attr = DeviceBuffer.empty(11 * self.n, np.float32, self.ctx)
+        d_sh = DeviceBuffer.empty(3 * self.sh_per_ch * self.n, np.float32, self.ctx)
+        d_proj = DeviceBuffer.empty(9 * self.n, np.float32, self.ctx) if want_proj else None
+        check(lib().sf_render_backward(self.handle, scratch.handle, C.byref(camera), w, h, _vp(dl),
+                                       _vp(d_attr), _vp(d_sh), _vp(d_proj), _stream(stream)))
+        out = (d_attr.read().reshape(11, self.n), d_sh.read().reshape(self.sh_per_ch, 3, self.n))
+        if want_proj:
+            out = out + (d_proj.read().reshape(self.n, 9),)
+        return out
+
     def render_to_host(self, scratch: "RenderScratch", camera: Camera, img_size, out=None, stream=None):
         w, h = img_size
         if out is None:

@@ -145,6 +145,11 @@ struct sf_scratch_t {
     uint64_t last_isects_raw = 0;
     bool prepared = false;
     sf_tuning tuning{};
+    // Adjoint state: the camera of the last forward that kept per-pixel
+    // final T / last contributor, and the per-splat 2D adjoint buffer.
+    bool has_forward = false;
+    sf_camera fwd_cam{};
+    float* d2d = nullptr;
 };
 
 struct sf_accum_t {
@@ -202,9 +207,10 @@ void scratch_free_frame(sf_scratch s) {
     dfree(s->depth_keys); dfree(s->tile_counts); dfree(s->bbox); dfree(s->geo0); dfree(s->geo1);
     dfree(s->color); dfree(s->ext); dfree(s->keys_a); dfree(s->keys_b); dfree(s->order_a); dfree(s->order_b);
     dfree(s->offsets); dfree(s->scan_tmp); dfree(s->tile_start); dfree(s->bitmap);
-    dfree(s->rgba); dfree(s->final_t); dfree(s->n_contrib);
+    dfree(s->rgba); dfree(s->final_t); dfree(s->n_contrib); dfree(s->d2d);
     s->order = nullptr;
     s->prepared = false;
+    s->has_forward = false;
 }
 
 void scratch_free_isects(sf_scratch s) {
@@ -288,6 +294,7 @@ int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32
     if (w == 0 || h == 0 || w > 65535 * 16 || h > 65535 * 16) return fail(SF_ERR_SHAPE, "bad image size");
     SF_CK(use_device(s->ctx->device));
     if (s->total != sp->n || s->w != w || s->h != h) SF_CK(scratch_build(s, sp->n, w, h));
+    s->has_forward = false;
     sf_view view;
     view_for_camera(*cam, w, h, &view);
     const uint32_t n = sp->n;
@@ -365,12 +372,20 @@ RasterArgs raster_args(sf_scratch s, const sf_isects* is) {
     return a;
 }
 
-int finalize_rgb(sf_scratch s, const sf_isects* is, bool want_float, cudaStream_t st) {
+int finalize_rgb(sf_scratch s, const sf_isects* is, bool want_float, cudaStream_t st,
+                 bool keep_state = false) {
     RasterArgs a = raster_args(s, is);
     a.bitmap = s->bitmap;
     if (want_float) {
         if (!s->rgba) SF_CK(dalloc(&s->rgba, (size_t)s->w * s->h));
         a.rgba = s->rgba;
+    }
+    s->has_forward = false;
+    if (keep_state) {
+        if (!s->final_t) SF_CK(dalloc(&s->final_t, (size_t)s->w * s->h));
+        if (!s->n_contrib) SF_CK(dalloc(&s->n_contrib, (size_t)s->w * s->h));
+        a.final_t = s->final_t;
+        a.n_contrib = s->n_contrib;
     }
     SF_CK(cudaMemsetAsync(s->stats, 0, 32, st));
     SF_CK(launch_raster(0, a, st));
@@ -647,6 +662,59 @@ int sf_render_float(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint3
         rc = finalize_rgb(scratch, nullptr, true, S(stream));
         if (rc != SF_OK) return rc;
         if (rgba) *rgba = reinterpret_cast<const float*>(scratch->rgba);
+        return SF_OK;
+    })
+}
+
+int sf_render_forward(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                      sf_stream stream, const float** rgba) {
+    SF_TRY({
+        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr);
+        if (rc != SF_OK) return rc;
+        rc = finalize_rgb(scratch, nullptr, true, S(stream), true);
+        if (rc != SF_OK) return rc;
+        scratch->has_forward = true;
+        scratch->fwd_cam = *cam;
+        if (rgba) *rgba = reinterpret_cast<const float*>(scratch->rgba);
+        return SF_OK;
+    })
+}
+
+int sf_render_backward(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                       const float* dl_drgba, float* d_attr, float* d_sh, float* d_proj,
+                       sf_stream stream) {
+    SF_TRY({
+        if (!s || !scratch || !cam || !dl_drgba || !d_attr || !d_sh)
+            return fail(SF_ERR_ARG, "null argument");
+        if (!scratch->has_forward || scratch->w != w || scratch->h != h || scratch->total != s->n ||
+            std::memcmp(&scratch->fwd_cam, cam, sizeof(sf_camera)) != 0)
+            return fail(SF_ERR_SHAPE, "backward needs the scratch's last sf_render_forward of this camera and size");
+        cudaStream_t st = S(stream);
+        SF_CK(use_device(scratch->ctx->device));
+        float* d2d = d_proj;
+        if (!d2d) {
+            if (!scratch->d2d) SF_CK(dalloc(&scratch->d2d, (size_t)scratch->total * 9));
+            d2d = scratch->d2d;
+        }
+        SF_CK(cudaMemsetAsync(d2d, 0, (size_t)scratch->total * 9 * sizeof(float), st));
+        BwdArgs a{};
+        a.w = w;
+        a.h = h;
+        a.tiles_x = scratch->tiles_x;
+        a.tiles_y = scratch->tiles_y;
+        a.tile_start = scratch->tile_start;
+        a.gaussian_ids = scratch->gids;
+        a.geo0 = scratch->geo0;
+        a.geo1 = scratch->geo1;
+        a.color = scratch->color;
+        a.final_t = scratch->final_t;
+        a.n_contrib = scratch->n_contrib;
+        a.dl = reinterpret_cast<const float4*>(dl_drgba);
+        a.d2d = d2d;
+        SF_CK(launch_raster_bwd(a, st));
+        sf_view view;
+        view_for_camera(*cam, w, h, &view);
+        SF_CK(launch_project_bwd(view, s->attr, s->sh, s->n, s->K, d2d, d_attr, d_sh, st));
         return SF_OK;
     })
 }

@@ -74,6 +74,24 @@ struct RasterArgs {
 // mode 0 = RGB, 1 = total responsibility, 2 = evidence.
 cudaError_t launch_raster(int mode, const RasterArgs& a, cudaStream_t stream);
 
+// Adjoint (sf_backward.cu).
+struct BwdArgs {
+    uint32_t w, h, tiles_x, tiles_y;
+    const uint32_t* tile_start;
+    const uint32_t* gaussian_ids;
+    const float4* geo0;
+    const float4* geo1;
+    const float4* color;
+    const float* final_t;      // forward's final transmittance per pixel
+    const uint32_t* n_contrib; // forward's 1-based last contributor per pixel
+    const float4* dl;          // dL/d(r, g, b, a) per pixel
+    float* d2d;                // [n][9] accumulated: mean2d xy, conic xyz, rgb, opacity
+};
+cudaError_t launch_raster_bwd(const BwdArgs& a, cudaStream_t stream);
+cudaError_t launch_project_bwd(const sf_view& view, const float* attr, const float* sh, uint32_t n,
+                               uint32_t sh_per_ch, const float* d2d, float* d_attr, float* d_sh,
+                               cudaStream_t stream);
+
 // Reference-layout projected rows [n][9] from the split records.
 cudaError_t launch_export_rows(const float4* geo0, const float4* geo1, const float4* color,
                                const uint32_t* depth_keys, uint32_t n, float* rows,

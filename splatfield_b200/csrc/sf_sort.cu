@@ -133,23 +133,33 @@ __global__ __launch_bounds__(kThreads) void radix_histogram_kernel(
     // emitted tile ids come in runs, and 32 lanes on one bin would otherwise
     // serialise. A lane whose digit differs from its left neighbour's adds the
     // length of its run.
-    const uint32_t stride = gridDim.x * kThreads;
+    // Each warp takes 128 consecutive keys per step (4 loads in flight per
+    // lane, each covering 32 consecutive keys across the lanes).
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t n_round = (n + 31u) & ~31u;
-    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n_round; i += stride) {
-        const bool valid = i < n;
-        const uint32_t k = valid ? keys[i] : 0u;
-        for (uint32_t p = 0; p < num_passes; ++p) {
-            const uint32_t shift = p * kRadixBits;
-            const uint32_t w = bits - shift < (uint32_t)kRadixBits ? bits - shift : kRadixBits;
-            const uint32_t d = valid ? ((k >> shift) & ((1u << w) - 1u)) : (uint32_t)kRadix;
-            const uint32_t left = __shfl_up_sync(0xffffffffu, d, 1);
-            const bool head = lane == 0 || left != d;
-            const uint32_t heads = __ballot_sync(0xffffffffu, head);
-            if (valid && head) {
-                const uint32_t above = heads & ~((2u << lane) - 1u);
-                const uint32_t next = above ? (uint32_t)(__ffs(above) - 1) : 32u;
-                atomicAdd(&s_hist[p * kRadix + d], next - lane);
+    const uint32_t warp_global = (blockIdx.x * kThreads + threadIdx.x) >> 5;
+    const uint32_t warps_total = (gridDim.x * kThreads) >> 5;
+    for (uint32_t base = warp_global * 128u; base < n; base += warps_total * 128u) {
+        uint32_t kk[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t i = base + u * 32u + lane;
+            kk[u] = i < n ? keys[i] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const bool valid = base + u * 32u + lane < n;
+            for (uint32_t p = 0; p < num_passes; ++p) {
+                const uint32_t shift = p * kRadixBits;
+                const uint32_t w = bits - shift < (uint32_t)kRadixBits ? bits - shift : kRadixBits;
+                const uint32_t d = valid ? ((kk[u] >> shift) & ((1u << w) - 1u)) : (uint32_t)kRadix;
+                const uint32_t left = __shfl_up_sync(0xffffffffu, d, 1);
+                const bool head = lane == 0 || left != d;
+                const uint32_t heads = __ballot_sync(0xffffffffu, head);
+                if (valid && head) {
+                    const uint32_t above = heads & ~((2u << lane) - 1u);
+                    const uint32_t next = above ? (uint32_t)(__ffs(above) - 1) : 32u;
+                    atomicAdd(&s_hist[p * kRadix + d], next - lane);
+                }
             }
         }
     }

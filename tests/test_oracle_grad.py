@@ -43,11 +43,11 @@ def test_fp64_adjoint_matches_central_differences(oracle_mod, k):
     attr, sh = scene(n, k, 100 + k)
     cam = O.look_at((0.2, -0.1, -2.5), (0.0, 0.0, 0.0))
     rng = np.random.default_rng(7)
-    dl = rng.normal(size=(h, w, 3))
+    dl = rng.normal(size=(h, w, 4))
 
     def loss(at, s):
         img = O.render64(cam, w, h, at, s, k)
-        return float(np.sum(img[..., :3] * dl))
+        return float(np.sum(img * dl))
 
     d_attr, d_sh = O.render64_backward(cam, w, h, attr, sh, k, dl)
     checks, kinks, bad = 0, 0, []
