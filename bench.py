@@ -146,6 +146,44 @@ def cpu_frame_time(attr, sh, max_frames=3, budget_s=30.0):
     return float(np.median(times)), len(times), O.num_threads()
 
 
+def time_backward(sf, splats, scratch, attr, sh, cam, stream, args):
+    """Adjoint workload: the frame scene, one camera, L2 loss against the render
+    of a copy with means + N(0, 0.01) and opacity logits + N(0, 0.2). Times
+    sf_render_forward (the float frame that keeps per-pixel state) and
+    sf_render_backward (raster replay + projection adjoint) with CUDA events."""
+    import torch
+
+    from splatfield_b200 import synth
+
+    size = (WIDTH, HEIGHT)
+    target_splats = sf.Splats(synth.perturbed(attr, N_SPLATS, seed=0), sh, splats.ctx)
+    target_scratch = sf.RenderScratch(N_SPLATS, size, splats.ctx)
+    target = target_splats.render_forward(target_scratch, cam, size, stream=stream).read()
+    img = splats.render_forward(scratch, cam, size, stream=stream).read()
+    dl = sf.DeviceBuffer.from_array((2.0 * (img - target)).astype(np.float32), splats.ctx)
+    del target_splats, target_scratch
+    d_attr = sf.DeviceBuffer.empty(11 * N_SPLATS, np.float32, splats.ctx)
+    d_sh = sf.DeviceBuffer.empty(3 * SH_PER_CH * N_SPLATS, np.float32, splats.ctx)
+    reps = max(3, min(args.steps // 30, 50))
+    fwd_ms, bwd_ms = [], []
+    for i in range(reps + 2):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        splats.render_forward(scratch, cam, size, stream=stream)
+        e1.record(stream)
+        splats.render_backward_into(scratch, cam, size, dl, d_attr, d_sh, stream=stream)
+        e2.record(stream)
+        torch.cuda.synchronize()
+        if i >= 2:
+            fwd_ms.append(e0.elapsed_time(e1))
+            bwd_ms.append(e1.elapsed_time(e2))
+    f, b = float(np.median(fwd_ms)), float(np.median(bwd_ms))
+    return {"workload": "adjoint: frame scene, 1 camera, L2 vs perturbed-copy render",
+            "forward_ms": f, "backward_ms": b, "ratio": b / f, "target_ratio": 3.0, "reps": reps,
+            "note": "device-timed; forward = sf_render_forward (keeps per-pixel T and last "
+                    "contributor), backward = sf_render_backward into device gradient buffers"}
+
+
 def run_reference(args, rank, world):
     """The reference arm: the CPU implementation of the path on this host."""
     if rank != 0:
@@ -285,6 +323,8 @@ def run_ours(args, rank, world):
         _lib.lib().sf_host_free(pin)
     e2e_fps = world * args.steps / e2e_s
 
+    bwd = time_backward(sf, splats, scratch, attr, sh, my_cams[0], stream, args)
+
     if rank != 0:
         return
     cpu_s, cpu_frames, cores = cpu_frame_time(attr, sh)
@@ -314,6 +354,7 @@ def run_ours(args, rank, world):
         "raster_stats": {k: v / n_split for k, v in stats.items()},
         "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "frames/s", "cores": cores, "kind": "port",
                          "sample": f"{cpu_frames} full frame(s) of the workload, median"},
+        "backward": bwd,
         "clocks": clk,
         "gpu_launches": int(launches),
         "peaks": {"source": which, "hbm_gbs": peaks.get("hbm_gbs")},

@@ -277,6 +277,42 @@ int sf_entropy_table(float* out);
 int sf_table_entropy(sf_ctx ctx, const float* a, const float* b, uint32_t n, float* out,
                      sf_stream stream);
 
+/* ------------------------------------------------------ batched round */
+/* A round of candidate views scored together (the batched form of
+ * Segmenter::select_view, src/seg/active.rs:113-129, which renders and
+ * scores one view at a time with two blocking read-backs each). Every view's
+ * project -> depth sort -> scan -> emit -> tile sort -> responsibility
+ * raster -> EIG is captured once into a CUDA graph with device-side counts
+ * and replayed each round; views may have different sizes. */
+typedef struct sf_round_t* sf_round;
+typedef struct {
+    uint32_t lanes;       /* capture streams the views are spread over (1..64) */
+    uint32_t raster_cull; /* as sf_tuning.raster_cull */
+    uint32_t reserved[6];
+} sf_round_tuning;
+int sf_round_create(sf_ctx ctx, uint32_t total, uint32_t n_views, const uint32_t* widths,
+                    const uint32_t* heights, sf_round* out);
+int sf_round_destroy(sf_round r);
+int sf_round_set_tuning(sf_round r, const sf_round_tuning* t);
+int sf_round_get_tuning(sf_round r, sf_round_tuning* t);
+/* One round for cameras cams[n_views]: every view's total responsibility
+ * and, when beta is non-NULL, its EIG (mode SF_EIG_LUT_F32 / SF_EIG_FP64)
+ * into host eig[n_views]. Syncs once. A view whose intersections outgrow the
+ * round's capacity is re-run after the capacity grows. The words equal the
+ * per-view sf_render_responsibility words bit for bit. */
+int sf_round_eig(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, int mode,
+                 sf_stream stream, double* eig);
+/* View `view` of the last round: device responsibility words [total], the
+ * fixed-point scale, the intersection count and the visible count. */
+int sf_round_responsibility(sf_round r, uint32_t view, const uint32_t** resp, float* scale,
+                            uint64_t* num_isects, uint32_t* num_visible);
+/* Autotuner: times the round over lanes {1,2,4,8} x raster_cull {0,1}, keeps
+ * the fastest on the round and in a process-wide cache keyed by (device,
+ * splats, view sizes); a cached shape is not re-timed unless best_ms is
+ * requested. */
+int sf_round_autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, int mode,
+                      sf_stream stream, sf_round_tuning* best, double* best_ms);
+
 /* ------------------------------------------------------- sort / scan */
 /* bits_for (crates/sort/src/sort.rs:259-261). */
 uint32_t sf_bits_for(uint32_t max_exclusive);

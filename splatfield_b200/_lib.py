@@ -54,6 +54,12 @@ class Tuning(C.Structure):
     _fields_ = [("raster_cull", C.c_uint32), ("reserved", C.c_uint32 * 7)]
 
 
+class RoundTuning(C.Structure):
+    """sf_round_tuning."""
+
+    _fields_ = [("lanes", C.c_uint32), ("raster_cull", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+
+
 class Isects(C.Structure):
     """TileIsects (src/render.rs:463-471)."""
 
@@ -127,6 +133,13 @@ SIGNATURES = {
         "sf_map_labels": (i32, [P, P, u32, P]),
         "sf_entropy_table": (i32, [P]),
         "sf_table_entropy": (i32, [P, P, P, u32, P, P]),
+        "sf_round_create": (i32, [P, u32, u32, P, P, PP]),
+        "sf_round_destroy": (i32, [P]),
+        "sf_round_set_tuning": (i32, [P, P]),
+        "sf_round_get_tuning": (i32, [P, P]),
+        "sf_round_eig": (i32, [P, P, P, P, i32, P, P]),
+        "sf_round_responsibility": (i32, [P, u32, PP, P, P, P]),
+        "sf_round_autotune": (i32, [P, P, P, P, i32, P, P, P]),
         "sf_bits_for": (u32, [u32]),
         "sf_radix_create": (i32, [P, u32, PP]),
         "sf_radix_destroy": (i32, [P]),

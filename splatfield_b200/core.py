@@ -25,7 +25,7 @@ __all__ = [
     "DeviceView", "camera_default", "look_at", "focal", "view_for_camera", "CpuSplats", "Splats",
     "RenderScratch", "TileIsects", "Accumulators", "Mask", "BetaState", "map_labels", "bits_for",
     "RadixScratch", "ScanScratch", "exclusive_scan_gather", "exclusive_scan_buf", "entropy_table",
-    "table_entropy", "fractional_bits", "row_stride_for", "EIG_LUT_F32", "EIG_FP64",
+    "table_entropy", "fractional_bits", "row_stride_for", "EIG_LUT_F32", "EIG_FP64", "Round",
 ]
 
 EIG_LUT_F32, EIG_FP64 = L.EIG_LUT_F32, L.EIG_FP64
@@ -280,6 +280,13 @@ class Splats:
         if want_proj:
             out = out + (d_proj.read().reshape(self.n, 9),)
         return out
+
+    def render_backward_into(self, scratch: "RenderScratch", camera: Camera, img_size, dl_drgba,
+                             d_attr, d_sh, d_proj=None, stream=None) -> None:
+        """render_backward into caller-owned device buffers; enqueues only."""
+        w, h = img_size
+        check(lib().sf_render_backward(self.handle, scratch.handle, C.byref(camera), w, h, _vp(dl_drgba),
+                                       _vp(d_attr), _vp(d_sh), _vp(d_proj), _stream(stream)))
 
     def render_to_host(self, scratch: "RenderScratch", camera: Camera, img_size, out=None, stream=None):
         w, h = img_size
@@ -591,6 +598,84 @@ def table_entropy(a, b, ctx: Context | None = None) -> np.ndarray:
     out = DeviceBuffer.empty(da.shape[0], np.float32, ctx)
     check(lib().sf_table_entropy(ctx.handle, _vp(da), _vp(db), da.shape[0], _vp(out), None))
     return out.read()
+
+
+# ------------------------------------------------------------ batched round
+
+class Round:
+    """Every candidate view of a segmentation round scored in one CUDA graph
+    (the batched Segmenter::select_view, src/seg/active.rs:113-129)."""
+
+    def __init__(self, total: int, sizes, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        sizes = [(int(w), int(h)) for w, h in sizes]
+        ws = np.array([s[0] for s in sizes], np.uint32)
+        hs = np.array([s[1] for s in sizes], np.uint32)
+        hd = C.c_void_p()
+        check(lib().sf_round_create(self.ctx.handle, total, len(sizes), _vp(ws), _vp(hs), C.byref(hd)))
+        self.handle = hd
+        self.total = total
+        self.sizes = sizes
+
+    @property
+    def views(self) -> int:
+        return len(self.sizes)
+
+    def set_tuning(self, lanes: int = 4, raster_cull: int = 0) -> None:
+        t = L.RoundTuning()
+        t.lanes, t.raster_cull = int(lanes), int(raster_cull)
+        check(lib().sf_round_set_tuning(self.handle, C.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = L.RoundTuning()
+        check(lib().sf_round_get_tuning(self.handle, C.byref(t)))
+        return {"lanes": int(t.lanes), "raster_cull": int(t.raster_cull)}
+
+    @staticmethod
+    def _cams(cameras):
+        arr = (Camera * len(cameras))()
+        for i, c in enumerate(cameras):
+            arr[i] = c
+        return arr
+
+    def eig(self, splats: Splats, beta: "BetaState | None", cameras, mode: int = EIG_LUT_F32,
+            stream=None) -> np.ndarray:
+        """Responsibility of every view and (with a posterior) its EIG."""
+        if len(cameras) != self.views:
+            raise SplatfieldError(L.SF_ERR_SHAPE, "one camera per view")
+        out = np.zeros(self.views, np.float64)
+        check(lib().sf_round_eig(self.handle, splats.handle, beta.handle if beta else None,
+                                 self._cams(cameras), mode, _stream(stream), _vp(out)))
+        return out
+
+    def responsibility(self, view: int) -> tuple:
+        """(device words, scale, intersections, visible) of a view of the last round."""
+        p = C.c_void_p()
+        scale = C.c_float()
+        nis = C.c_uint64()
+        vis = C.c_uint32()
+        check(lib().sf_round_responsibility(self.handle, view, C.byref(p), C.byref(scale), C.byref(nis),
+                                            C.byref(vis)))
+        return DeviceView(p.value, np.uint32, (self.total,), self), float(scale.value), int(nis.value), int(vis.value)
+
+    def autotune(self, splats: Splats, beta: "BetaState | None", cameras, mode: int = EIG_LUT_F32,
+                 stream=None) -> tuple:
+        t = L.RoundTuning()
+        ms = C.c_double()
+        check(lib().sf_round_autotune(self.handle, splats.handle, beta.handle if beta else None,
+                                      self._cams(cameras), mode, _stream(stream), C.byref(t), C.byref(ms)))
+        return {"lanes": int(t.lanes), "raster_cull": int(t.raster_cull)}, float(ms.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sf_round_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ------------------------------------------------------------- sort / scan

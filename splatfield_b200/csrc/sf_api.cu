@@ -15,18 +15,24 @@
 #include <new>
 #include <string>
 #include <vector>
-#include "sf_internal.h"
+#include "sf_handles.h"
 
 using namespace sfk;
 
 namespace {
-
 thread_local std::string g_err;
+}  // namespace
 
-int fail(int code, const std::string& msg) {
+namespace sfk {
+int set_error(int code, const std::string& msg) {
     g_err = msg;
     return code;
 }
+}  // namespace sfk
+
+namespace {
+
+int fail(int code, const std::string& msg) { return set_error(code, msg); }
 
 #define SF_CK(expr)                                                                        \
     do {                                                                                   \
@@ -98,20 +104,6 @@ constexpr uint64_t kInitialIsects = 1ull << 22;
 
 }  // namespace
 
-struct sf_ctx_t {
-    int device = 0;
-    int sm_count = 148;
-    float* lut = nullptr;
-};
-
-struct sf_splats_t {
-    sf_ctx ctx = nullptr;
-    uint32_t n = 0, K = 1;
-    float* attr = nullptr;
-    float* sh = nullptr;
-    float bounds[6] = {0, 0, 0, 0, 0, 0};
-};
-
 struct sf_scratch_t {
     sf_ctx ctx = nullptr;
     uint32_t total = 0, w = 0, h = 0, tiles_x = 0, tiles_y = 0, row_stride = 0;
@@ -150,28 +142,6 @@ struct sf_scratch_t {
     bool has_forward = false;
     sf_camera fwd_cam{};
     float* d2d = nullptr;
-};
-
-struct sf_accum_t {
-    sf_ctx ctx = nullptr;
-    uint32_t total = 0;
-    uint32_t *resp = nullptr, *fg = nullptr, *bg = nullptr;
-    float scale = 1.0f;
-};
-
-struct sf_mask_t {
-    uint32_t w = 0, h = 0, wpr = 0;
-    uint32_t* bits = nullptr;
-};
-
-struct sf_beta_t {
-    sf_ctx ctx = nullptr;
-    uint32_t n = 0;
-    float *a = nullptr, *b = nullptr;
-    double* partials = nullptr;
-    uint32_t blocks = 1;
-    double* out = nullptr;
-    double* host_out = nullptr;
 };
 
 struct sf_radix_t {

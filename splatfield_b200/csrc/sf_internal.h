@@ -33,8 +33,10 @@ struct ProjOut {
     float2* ext;            // [n] half extents of the box holding power <= power_max
 };
 
+// view_dev (optional) supplies the view from device memory instead.
 cudaError_t launch_project(const sf_view& view, const float* attr, const float* sh, uint32_t n,
-                           uint32_t sh_per_ch, const ProjOut& out, cudaStream_t stream);
+                           uint32_t sh_per_ch, const ProjOut& out, cudaStream_t stream,
+                           const sf_view* view_dev = nullptr);
 
 cudaError_t launch_emit(const uint32_t* order, const uint2* bbox, const uint32_t* offsets,
                         uint32_t n, uint32_t tiles_per_row, uint32_t capacity, uint32_t* tile_ids,

@@ -75,11 +75,15 @@ __device__ __forceinline__ void sh_to_rgb(V3 d, const float (&c)[3 * K], float& 
 // project_splats (src/project.rs:235-327), one thread per splat. Field-major
 // planes make every plane load a coalesced 128-byte warp access.
 template <int K>
-__global__ __launch_bounds__(256) void project_kernel(sf_view v, const float* __restrict__ attr,
+__global__ __launch_bounds__(256) void project_kernel(sf_view v_arg, const sf_view* __restrict__ v_dev,
+                                                      const float* __restrict__ attr,
                                                       const float* __restrict__ shs, uint32_t n,
                                                       ProjOut o) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    // The view comes by value, or (for captured graphs re-run with new
+    // cameras) from device memory.
+    const sf_view v = v_dev ? *v_dev : v_arg;
     const size_t N = n;
     // Every load is issued before any use (all planes in flight at once);
     // culled splats (a few percent) read their colour planes for nothing.
@@ -474,14 +478,15 @@ __global__ void export_rows_kernel(const float4* __restrict__ geo0, const float4
 }  // namespace
 
 cudaError_t launch_project(const sf_view& view, const float* attr, const float* sh, uint32_t n,
-                           uint32_t sh_per_ch, const ProjOut& out, cudaStream_t stream) {
+                           uint32_t sh_per_ch, const ProjOut& out, cudaStream_t stream,
+                           const sf_view* view_dev) {
     if (n == 0) return cudaSuccess;
     const uint32_t grid = (n + 255) / 256;
     switch (sh_per_ch) {
-        case 1: project_kernel<1><<<grid, 256, 0, stream>>>(view, attr, sh, n, out); break;
-        case 4: project_kernel<4><<<grid, 256, 0, stream>>>(view, attr, sh, n, out); break;
-        case 9: project_kernel<9><<<grid, 256, 0, stream>>>(view, attr, sh, n, out); break;
-        case 16: project_kernel<16><<<grid, 256, 0, stream>>>(view, attr, sh, n, out); break;
+        case 1: project_kernel<1><<<grid, 256, 0, stream>>>(view, view_dev, attr, sh, n, out); break;
+        case 4: project_kernel<4><<<grid, 256, 0, stream>>>(view, view_dev, attr, sh, n, out); break;
+        case 9: project_kernel<9><<<grid, 256, 0, stream>>>(view, view_dev, attr, sh, n, out); break;
+        case 16: project_kernel<16><<<grid, 256, 0, stream>>>(view, view_dev, attr, sh, n, out); break;
         default: return cudaErrorInvalidValue;
     }
     note_launches(1);

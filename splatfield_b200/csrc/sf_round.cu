@@ -1,0 +1,518 @@
+// Batched segmentation-evidence round: the responsibility render and EIG of
+// every candidate view of a round, all in one CUDA graph.
+//
+// The reference scores candidates one at a time (Segmenter::select_view,
+// src/seg/active.rs:113-129): per view a render_responsibility with a blocking
+// counters read-back (src/render.rs:308) and an EIG with a blocking partials
+// read-back (src/seg/beta.rs:265-267) — 40 host round trips for 20 views.
+// Here each view's project -> depth sort -> gather scan -> emit -> tile sort
+// -> tile starts -> responsibility raster -> EIG runs with its counts kept on
+// the device (grids sized by capacity, kernels read the live count), views
+// are spread over `lanes` capture streams so independent views overlap on the
+// GPU, and the whole round is captured once into a graph and replayed; the
+// cameras reach the graph through a pinned host buffer copied in by the
+// graph's first node. The host syncs once per round, reads every view's EIG
+// and checks the per-view intersection totals: a view that outgrew its
+// capacity is re-run after the capacity grows (the graph is rebuilt then).
+// The per-view words are bit-identical to the plain per-view path: same
+// kernels, same inputs, integer sums.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+#include "sf_handles.h"
+
+namespace sfk {
+namespace {
+
+__global__ void clamp_count_kernel(const unsigned long long* total, uint32_t cap, uint32_t* n32,
+                                   uint32_t* err) {
+    const unsigned long long t = *total;
+    if (t > cap) atomicOr(err, SF_DEV_ERR_CAPACITY);
+    *n32 = (uint32_t)(t < cap ? t : cap);
+}
+
+uint32_t bits_for(uint32_t max_exclusive) {
+    const uint32_t m = max_exclusive > 0 ? max_exclusive - 1 : 0;
+    return m == 0 ? 0u : 32u - (uint32_t)__builtin_clz(m);
+}
+
+uint64_t next_pow2(uint64_t v) {
+    uint64_t p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+uint32_t frac_bits(uint32_t w, uint32_t h) {
+    const uint64_t pixels = (uint64_t)w * h;
+    uint32_t tz = 0;
+    uint64_t p2 = 1;
+    while (p2 < pixels) { p2 <<= 1; ++tz; }
+    return tz >= 32 ? 0u : 32u - tz;
+}
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+    *p = nullptr;
+    return cudaMalloc(reinterpret_cast<void**>(p), (count ? count : 1) * sizeof(T));
+}
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree(reinterpret_cast<void*>(p));
+    p = nullptr;
+}
+
+}  // namespace
+
+// Buffers of one capture stream: the views it runs reuse them in turn.
+struct RoundLane {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t join = nullptr;
+    uint32_t *keys = nullptr, *counts = nullptr;
+    uint2* bbox = nullptr;
+    float4 *geo0 = nullptr, *geo1 = nullptr;
+    float2* ext = nullptr;
+    uint32_t *keys_a = nullptr, *keys_b = nullptr, *order_a = nullptr, *order_b = nullptr;
+    uint32_t* offsets = nullptr;
+    void* scan_tmp = nullptr;
+    void* sort_tmp = nullptr;
+    uint64_t cap = 0;
+    uint32_t *tid_e = nullptr, *gid_e = nullptr, *tid_a = nullptr, *gid_a = nullptr;
+    uint32_t* tile_start = nullptr;
+    double* partials = nullptr;
+};
+
+}  // namespace sfk
+
+using namespace sfk;
+
+struct sf_round_t {
+    sf_ctx_t* ctx = nullptr;
+    int device = 0;
+    int sm_count = 148;
+    uint32_t n = 0, views = 0;
+    std::vector<uint32_t> w, h;
+    uint32_t max_tiles = 0;
+    sf_round_tuning tuning{};
+    std::vector<RoundLane> lanes;
+    sf_view* views_dev = nullptr;
+    sf_view* views_host = nullptr;  // pinned
+    uint32_t* words = nullptr;      // [views][8]: 0 visible, 1 err, 2 n32, 4..5 total u64
+    uint32_t* words_host = nullptr; // pinned
+    double* eig_dev = nullptr;
+    double* eig_host = nullptr;     // pinned
+    uint32_t* resp = nullptr;       // [views][n]
+    uint32_t eig_blocks = 1;
+    uint64_t want_cap = 0;
+    // graph cache
+    cudaStream_t main = nullptr;
+    cudaEvent_t fork = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const void* g_splats = nullptr;
+    const void* g_beta = nullptr;
+    int g_mode = -1;
+    uint32_t g_lanes = 0, g_cull = 0;
+};
+
+namespace {
+
+void lane_free(RoundLane& L) {
+    dfree(L.keys); dfree(L.counts); dfree(L.bbox); dfree(L.geo0); dfree(L.geo1); dfree(L.ext);
+    dfree(L.keys_a); dfree(L.keys_b); dfree(L.order_a); dfree(L.order_b); dfree(L.offsets);
+    if (L.scan_tmp) cudaFree(L.scan_tmp);
+    if (L.sort_tmp) cudaFree(L.sort_tmp);
+    L.scan_tmp = L.sort_tmp = nullptr;
+    dfree(L.tid_e); dfree(L.gid_e); dfree(L.tid_a); dfree(L.gid_a);
+    dfree(L.tile_start); dfree(L.partials);
+    if (L.stream) cudaStreamDestroy(L.stream);
+    if (L.join) cudaEventDestroy(L.join);
+    L.stream = nullptr;
+    L.join = nullptr;
+    L.cap = 0;
+}
+
+cudaError_t lane_alloc(sf_round_t* r, RoundLane& L, uint64_t cap) {
+    const uint32_t n = r->n;
+    cudaError_t e;
+#define RA(ptr, cnt) if ((e = dalloc(&(ptr), (cnt))) != cudaSuccess) return e
+    RA(L.keys, n); RA(L.counts, n); RA(L.bbox, n); RA(L.geo0, n); RA(L.geo1, n); RA(L.ext, n);
+    RA(L.keys_a, n); RA(L.keys_b, n); RA(L.order_a, n); RA(L.order_b, n); RA(L.offsets, n);
+    RA(L.tid_e, cap); RA(L.gid_e, cap); RA(L.tid_a, cap); RA(L.gid_a, cap);
+    RA(L.tile_start, (size_t)r->max_tiles + 1);
+    RA(L.partials, r->eig_blocks);
+#undef RA
+    if ((e = cudaMalloc(&L.scan_tmp, scan_temp_bytes(n))) != cudaSuccess) return e;
+    const size_t st = std::max(radix_temp_bytes(n, 4), radix_temp_bytes((uint32_t)cap, 4));
+    if ((e = cudaMalloc(&L.sort_tmp, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&L.join, cudaEventDisableTiming)) != cudaSuccess) return e;
+    L.cap = cap;
+    return cudaSuccess;
+}
+
+void graph_drop(sf_round_t* r) {
+    if (r->exec) cudaGraphExecDestroy(r->exec);
+    r->exec = nullptr;
+}
+
+cudaError_t lanes_build(sf_round_t* r, uint32_t lanes, uint64_t cap) {
+    graph_drop(r);
+    for (auto& L : r->lanes) lane_free(L);
+    r->lanes.assign(lanes, RoundLane());
+    for (auto& L : r->lanes) {
+        cudaError_t e = lane_alloc(r, L, cap);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// One view's pipeline on lane L's stream.
+cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splats_t& sp,
+                         const float* beta_a, const float* beta_b, const float* lut, int mode) {
+    cudaStream_t st = L.stream;
+    const uint32_t n = r->n;
+    uint32_t* words = r->words + 8 * v;
+    unsigned long long* total = reinterpret_cast<unsigned long long*>(words + 4);
+    const uint32_t w = r->w[v], h = r->h[v];
+    const uint32_t tx = (w + 15) / 16, ty = (h + 15) / 16;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(words, 0, 32, st)) != cudaSuccess) return e;
+    ProjOut po{L.keys, L.counts, L.bbox, L.geo0, L.geo1, nullptr, words, r->tuning.raster_cull ? L.ext : nullptr};
+    sf_view dummy{};
+    if ((e = launch_project(dummy, sp.attr, sp.sh, n, sp.K, po, st, r->views_dev + v)) != cudaSuccess) return e;
+    int in_b = 0;
+    if ((e = radix_sort_pairs(L.keys, nullptr, L.keys_a, L.order_a, L.keys_b, L.order_b, n, nullptr, n, 32,
+                              false, true, L.sort_tmp, words + 1, r->sm_count, st, &in_b)) != cudaSuccess)
+        return e;
+    const uint32_t* order = in_b ? L.order_b : L.order_a;
+    if ((e = exclusive_scan(order, L.counts, L.offsets, n, nullptr, n, L.scan_tmp, total, words + 1, st)) !=
+        cudaSuccess)
+        return e;
+    if ((e = launch_emit(order, L.bbox, L.offsets, n, tx, (uint32_t)L.cap, L.tid_e, L.gid_e, words + 1, st)) !=
+        cudaSuccess)
+        return e;
+    clamp_count_kernel<<<1, 1, 0, st>>>(total, (uint32_t)L.cap, words + 2, words + 1);
+    note_launches(1);
+    const uint32_t tiles = tx * ty;
+    const uint32_t tbits = bits_for(tiles);
+    const uint32_t *tids = L.tid_e, *gids = L.gid_e;
+    if (tbits > 0) {
+        if ((e = radix_sort_pairs(L.tid_e, L.gid_e, L.tid_a, L.gid_a, L.tid_e, L.gid_e, 0, words + 2,
+                                  (uint32_t)L.cap, tbits, true, false, L.sort_tmp, words + 1, r->sm_count, st,
+                                  &in_b)) != cudaSuccess)
+            return e;
+        tids = in_b ? L.tid_e : L.tid_a;
+        gids = in_b ? L.gid_e : L.gid_a;
+    }
+    if ((e = launch_tile_starts(tids, 0, words + 2, (uint32_t)L.cap, tiles, L.tile_start, st)) != cudaSuccess)
+        return e;
+    uint32_t* resp = r->resp + (size_t)v * n;
+    if ((e = cudaMemsetAsync(resp, 0, (size_t)n * 4, st)) != cudaSuccess) return e;
+    RasterArgs a{};
+    a.w = w;
+    a.h = h;
+    a.tiles_x = tx;
+    a.tiles_y = ty;
+    a.tile_start = L.tile_start;
+    a.gaussian_ids = gids;
+    a.geo0 = L.geo0;
+    a.geo1 = L.geo1;
+    a.ext = L.ext;
+    a.cull = r->tuning.raster_cull;
+    a.scale = (float)((uint64_t)1 << frac_bits(w, h));
+    a.resp = resp;
+    if ((e = launch_raster(1, a, st)) != cudaSuccess) return e;
+    if (beta_a) {
+        if ((e = launch_eig(mode, beta_a, beta_b, resp, n, a.scale, lut, L.partials, r->eig_blocks,
+                            r->eig_dev + v, st)) != cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+namespace {
+
+int rfail(int code, const std::string& msg) { return sfk::set_error(code, msg); }
+
+#define RF_CK(expr)                                                                              \
+    do {                                                                                         \
+        cudaError_t e_ = (expr);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return rfail(e_ == cudaErrorMemoryAllocation ? SF_ERR_NOMEM : SF_ERR_CUDA,           \
+                         std::string(#expr) + ": " + cudaGetErrorString(e_));                    \
+    } while (0)
+
+cudaError_t use_dev(int dev) {
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return e;
+    return cur == dev ? cudaSuccess : cudaSetDevice(dev);
+}
+
+// Capture the whole round into r->exec.
+int build_graph(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, int mode) {
+    graph_drop(r);
+    RF_CK(cudaStreamBeginCapture(r->main, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaMemcpyAsync(r->views_dev, r->views_host, sizeof(sf_view) * r->views,
+                                    cudaMemcpyHostToDevice, r->main);
+    if (e == cudaSuccess) e = cudaEventRecord(r->fork, r->main);
+    for (auto& L : r->lanes)
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(L.stream, r->fork, 0);
+    for (uint32_t v = 0; v < r->views && e == cudaSuccess; ++v) {
+        RoundLane& L = r->lanes[v % r->lanes.size()];
+        e = enqueue_view(r, L, v, *sp, beta ? beta->a : nullptr, beta ? beta->b : nullptr,
+                         beta ? beta->ctx->lut : nullptr, mode);
+    }
+    for (auto& L : r->lanes) {
+        if (e == cudaSuccess) e = cudaEventRecord(L.join, L.stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(r->main, L.join, 0);
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(r->words_host, r->words, 32 * r->views, cudaMemcpyDeviceToHost, r->main);
+    if (e == cudaSuccess && beta)
+        e = cudaMemcpyAsync(r->eig_host, r->eig_dev, 8 * r->views, cudaMemcpyDeviceToHost, r->main);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(r->main, &graph);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return rfail(SF_ERR_CUDA, std::string("round graph capture: ") +
+                                      cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    e = cudaGraphInstantiate(&r->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        r->exec = nullptr;
+        return rfail(SF_ERR_CUDA, std::string("round graph instantiate: ") + cudaGetErrorString(e));
+    }
+    r->g_splats = sp;
+    r->g_beta = beta;
+    r->g_mode = mode;
+    r->g_lanes = (uint32_t)r->lanes.size();
+    r->g_cull = r->tuning.raster_cull;
+    return SF_OK;
+}
+
+// Launch the round (rebuilding buffers/graph when needed), wait, check.
+int run_round(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, const sf_camera* cams, int mode,
+              cudaStream_t user) {
+    for (uint32_t v = 0; v < r->views; ++v) view_for_camera(cams[v], r->w[v], r->h[v], &r->views_host[v]);
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        const uint32_t lanes = std::max(1u, std::min(r->tuning.lanes ? r->tuning.lanes : 4u, r->views));
+        if (r->lanes.size() != lanes || r->lanes[0].cap < r->want_cap) {
+            RF_CK(lanes_build(r, lanes, std::max<uint64_t>(r->want_cap, r->lanes.empty() ? 1024 : r->lanes[0].cap)));
+        }
+        if (!r->exec || r->g_splats != sp || r->g_beta != beta || r->g_mode != mode ||
+            r->g_cull != r->tuning.raster_cull) {
+            const int rc = build_graph(r, sp, beta, mode);
+            if (rc != SF_OK) return rc;
+        }
+        // Order after the caller's prior work on its stream.
+        cudaEvent_t ev;
+        RF_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        RF_CK(cudaEventRecord(ev, user));
+        RF_CK(cudaStreamWaitEvent(r->main, ev, 0));
+        cudaEventDestroy(ev);
+        RF_CK(cudaGraphLaunch(r->exec, r->main));
+        RF_CK(cudaStreamSynchronize(r->main));
+        uint64_t worst = 0;
+        bool over = false;
+        for (uint32_t v = 0; v < r->views; ++v) {
+            const uint32_t* w = r->words_host + 8 * v;
+            if (w[1] & SF_DEV_ERR_TIMEOUT) return rfail(SF_ERR_TIMEOUT, "device look-back wait timed out");
+            uint64_t total;
+            std::memcpy(&total, w + 4, 8);
+            worst = std::max(worst, total);
+            if (w[1] & SF_DEV_ERR_CAPACITY) over = true;
+        }
+        if (!over) return SF_OK;
+        if (worst > (1ull << 30) - 1) return rfail(SF_ERR_CAPACITY, "intersection count exceeds 2^30-1");
+        r->want_cap = next_pow2(worst);
+        std::fprintf(stderr, "splatfield_b200: round capacity grown to %llu intersections per view\n",
+                     (unsigned long long)r->want_cap);
+    }
+    return rfail(SF_ERR_CAPACITY, "round capacity did not settle");
+}
+
+// Process-wide autotuning cache: (device, splats, views, sizes) -> tuning.
+std::mutex g_tune_mu;
+std::map<std::string, sf_round_tuning> g_tune_cache;
+
+std::string tune_key(const sf_round_t* r) {
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, r->device);
+    std::string k = std::string(prop.name) + "|" + std::to_string(r->n) + "|" + std::to_string(r->views);
+    for (uint32_t v = 0; v < r->views; ++v) k += "|" + std::to_string(r->w[v]) + "x" + std::to_string(r->h[v]);
+    return k;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sf_round_create(sf_ctx ctx, uint32_t total, uint32_t n_views, const uint32_t* widths,
+                    const uint32_t* heights, sf_round* out) {
+    if (!ctx || !widths || !heights || !out) return rfail(SF_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (total == 0 || n_views == 0) return rfail(SF_ERR_SHAPE, "round needs splats and views");
+    for (uint32_t v = 0; v < n_views; ++v)
+        if (widths[v] == 0 || heights[v] == 0 || widths[v] > 65535 * 16 || heights[v] > 65535 * 16)
+            return rfail(SF_ERR_SHAPE, "bad view size");
+    RF_CK(use_dev(ctx->device));
+    auto* r = new sf_round_t();
+    r->ctx = ctx;
+    r->device = ctx->device;
+    r->sm_count = ctx->sm_count;
+    r->n = total;
+    r->views = n_views;
+    r->w.assign(widths, widths + n_views);
+    r->h.assign(heights, heights + n_views);
+    for (uint32_t v = 0; v < n_views; ++v)
+        r->max_tiles = std::max(r->max_tiles, ((widths[v] + 15) / 16) * ((heights[v] + 15) / 16));
+    r->eig_blocks = eig_blocks(total, ctx->sm_count);
+    r->tuning.lanes = 4;
+    r->want_cap = std::min<uint64_t>((uint64_t)r->max_tiles * total, 1ull << 22);
+    cudaError_t e = cudaStreamCreateWithFlags(&r->main, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = dalloc(&r->views_dev, n_views);
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&r->views_host), sizeof(sf_view) * n_views);
+    if (e == cudaSuccess) e = dalloc(&r->words, 8 * (size_t)n_views);
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&r->words_host), 32 * (size_t)n_views);
+    if (e == cudaSuccess) e = dalloc(&r->eig_dev, n_views);
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&r->eig_host), 8 * (size_t)n_views);
+    if (e == cudaSuccess) e = dalloc(&r->resp, (size_t)n_views * total);
+    if (e != cudaSuccess) {
+        sf_round_destroy(r);
+        return rfail(e == cudaErrorMemoryAllocation ? SF_ERR_NOMEM : SF_ERR_CUDA, cudaGetErrorString(e));
+    }
+    *out = r;
+    return SF_OK;
+}
+
+int sf_round_destroy(sf_round r) {
+    if (!r) return SF_OK;
+    use_dev(r->device);
+    graph_drop(r);
+    for (auto& L : r->lanes) lane_free(L);
+    dfree(r->views_dev); dfree(r->words); dfree(r->eig_dev); dfree(r->resp);
+    if (r->views_host) cudaFreeHost(r->views_host);
+    if (r->words_host) cudaFreeHost(r->words_host);
+    if (r->eig_host) cudaFreeHost(r->eig_host);
+    if (r->fork) cudaEventDestroy(r->fork);
+    if (r->main) cudaStreamDestroy(r->main);
+    delete r;
+    return SF_OK;
+}
+
+int sf_round_set_tuning(sf_round r, const sf_round_tuning* t) {
+    if (!r || !t) return rfail(SF_ERR_ARG, "null argument");
+    if (t->raster_cull > 1 || t->lanes > 64) return rfail(SF_ERR_ARG, "bad tuning");
+    r->tuning = *t;
+    return SF_OK;
+}
+
+int sf_round_get_tuning(sf_round r, sf_round_tuning* t) {
+    if (!r || !t) return rfail(SF_ERR_ARG, "null argument");
+    *t = r->tuning;
+    return SF_OK;
+}
+
+int sf_round_eig(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, int mode, sf_stream stream,
+                 double* eig) {
+    try {
+        if (!r || !s || !cams) return rfail(SF_ERR_ARG, "null argument");
+        if (s->n != r->n) return rfail(SF_ERR_SHAPE, "splat count differs from the round's");
+        if (beta && beta->n != r->n) return rfail(SF_ERR_SHAPE, "posterior size differs from the round's");
+        if (beta && mode != SF_EIG_LUT_F32 && mode != SF_EIG_FP64) return rfail(SF_ERR_ARG, "bad EIG mode");
+        if (beta && !eig) return rfail(SF_ERR_ARG, "null eig output");
+        RF_CK(use_dev(r->device));
+        const int rc = run_round(r, s, beta, cams, mode, reinterpret_cast<cudaStream_t>(stream));
+        if (rc != SF_OK) return rc;
+        if (beta) std::memcpy(eig, r->eig_host, 8 * r->views);
+        return SF_OK;
+    } catch (const std::bad_alloc&) {
+        return rfail(SF_ERR_NOMEM, "host allocation failed");
+    }
+}
+
+int sf_round_responsibility(sf_round r, uint32_t view, const uint32_t** resp, float* scale,
+                            uint64_t* num_isects, uint32_t* num_visible) {
+    if (!r) return rfail(SF_ERR_ARG, "null round");
+    if (view >= r->views) return rfail(SF_ERR_SHAPE, "no such view");
+    if (resp) *resp = r->resp + (size_t)view * r->n;
+    if (scale) *scale = (float)((uint64_t)1 << frac_bits(r->w[view], r->h[view]));
+    const uint32_t* w = r->words_host + 8 * view;
+    if (num_isects) std::memcpy(num_isects, w + 4, 8);
+    if (num_visible) *num_visible = w[0];
+    return SF_OK;
+}
+
+int sf_round_autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, int mode,
+                      sf_stream stream, sf_round_tuning* best, double* best_ms) {
+    try {
+        if (!r || !s || !cams) return rfail(SF_ERR_ARG, "null argument");
+        RF_CK(use_dev(r->device));
+        const std::string key = tune_key(r);
+        {
+            std::lock_guard<std::mutex> g(g_tune_mu);
+            auto it = g_tune_cache.find(key);
+            if (it != g_tune_cache.end() && best_ms == nullptr) {
+                r->tuning = it->second;
+                if (best) *best = it->second;
+                return SF_OK;
+            }
+        }
+        cudaEvent_t e0, e1;
+        RF_CK(cudaEventCreate(&e0));
+        RF_CK(cudaEventCreate(&e1));
+        sf_round_tuning winner = r->tuning;
+        float winner_ms = 1e30f;
+        std::vector<double> eig(r->views);
+        const uint32_t lane_options[] = {1, 2, 4, 8};
+        for (uint32_t cull = 0; cull <= 1; ++cull)
+            for (uint32_t lanes : lane_options) {
+                if (lanes > r->views) continue;
+                sf_round_tuning t{};
+                t.lanes = lanes;
+                t.raster_cull = cull;
+                r->tuning = t;
+                int rc = sf_round_eig(r, s, beta, cams, mode, stream, eig.data());  // warm-up / build
+                if (rc != SF_OK) return rc;
+                float ms_best = 1e30f;
+                for (int rep = 0; rep < 3; ++rep) {
+                    RF_CK(cudaEventRecord(e0, r->main));
+                    rc = sf_round_eig(r, s, beta, cams, mode, stream, eig.data());
+                    if (rc != SF_OK) return rc;
+                    RF_CK(cudaEventRecord(e1, r->main));
+                    RF_CK(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    ms_best = std::min(ms_best, ms);
+                }
+                if (ms_best < winner_ms) {
+                    winner_ms = ms_best;
+                    winner = t;
+                }
+            }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        r->tuning = winner;
+        {
+            std::lock_guard<std::mutex> g(g_tune_mu);
+            g_tune_cache[key] = winner;
+        }
+        if (best) *best = winner;
+        if (best_ms) *best_ms = winner_ms;
+        return SF_OK;
+    } catch (const std::bad_alloc&) {
+        return rfail(SF_ERR_NOMEM, "host allocation failed");
+    }
+}
+
+}  // extern "C"

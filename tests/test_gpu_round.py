@@ -1,0 +1,111 @@
+"""The batched round (one CUDA graph over all candidate views) vs the plain
+per-view path (sf_render_responsibility + sf_beta_eig per view, the
+reference's Segmenter::select_view loop, src/seg/active.rs:113-129): the
+responsibility words must be bit-identical per view and the EIG identical
+(same kernels, same fixed-order reductions) (GPU)."""
+import numpy as np
+import pytest
+
+import splatfield_b200 as sf
+from splatfield_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def plain(splats, beta, cams, sizes, mode):
+    out = []
+    for cam, (w, h) in zip(cams, sizes):
+        scratch = sf.RenderScratch(splats.n, (w, h))
+        acc = sf.Accumulators(splats.n)
+        splats.render_responsibility(scratch, acc, cam, (w, h))
+        out.append((acc.bits.read(), acc.scale, beta.eig(acc, mode) if beta else None))
+    return out
+
+
+def cams_on_sphere(k, radius, seed):
+    return synth.sphere_cameras(k, radius, seed, sf.look_at)
+
+
+@pytest.mark.parametrize("lanes,cull", [(1, 0), (3, 0), (4, 1)])
+def test_round_matches_plain_per_view(ctx, lanes, cull):
+    n = 30000
+    attr, sh = synth.scene_clustered(n, 4, seed=3, clusters=4, sigma=0.25, extent=1.0)
+    a, b = synth.beta_posterior(n, seed=3)
+    splats = sf.Splats(attr, sh)
+    beta = sf.BetaState.from_host(a, b)
+    sizes = [(64, 48), (128, 128), (96, 160), (70, 70), (33, 17)]
+    cams = cams_on_sphere(len(sizes), 3.0, 5)
+    rnd = sf.Round(n, sizes)
+    rnd.set_tuning(lanes=lanes, raster_cull=cull)
+    for mode in (sf.EIG_LUT_F32, sf.EIG_FP64):
+        eig = rnd.eig(splats, beta, cams, mode)
+        want = plain(splats, beta, cams, sizes, mode)
+        for v, (words, scale, e) in enumerate(want):
+            got, gscale, _, _ = rnd.responsibility(v)
+            np.testing.assert_array_equal(got.read(), words)
+            assert gscale == scale
+            assert eig[v] == e, (v, eig[v], e)
+
+
+def test_round_graph_replays_with_new_cameras(ctx):
+    n = 20000
+    attr, sh = synth.scene_uniform(n, 1, 8)
+    a, b = synth.beta_posterior(n, seed=8)
+    splats = sf.Splats(attr, sh)
+    beta = sf.BetaState.from_host(a, b)
+    sizes = [(96, 96)] * 4
+    rnd = sf.Round(n, sizes)
+    for seed in (1, 2, 3):
+        cams = cams_on_sphere(4, 3.0, seed)
+        eig = rnd.eig(splats, beta, cams, sf.EIG_LUT_F32)
+        want = plain(splats, beta, cams, sizes, sf.EIG_LUT_F32)
+        for v in range(4):
+            np.testing.assert_array_equal(rnd.responsibility(v)[0].read(), want[v][0])
+            assert eig[v] == want[v][2]
+
+
+def test_round_capacity_grows_and_reruns(ctx):
+    """Large splats push the intersections past the first-round capacity
+    (min(tiles * n, 2^22)); the round grows and re-runs, results unchanged."""
+    n = 60000
+    attr, sh = synth.scene_uniform(n, 1, 11)
+    attr = attr.reshape(11, n)
+    attr[7:10] += 2.5
+    attr = attr.reshape(-1)
+    splats = sf.Splats(attr, sh)
+    sizes = [(512, 512), (256, 256)]
+    cams = [sf.look_at((0.0, 0.0, -3.0), (0, 0, 0)), sf.look_at((0.5, 0.3, -3.0), (0, 0, 0))]
+    rnd = sf.Round(n, sizes)
+    rnd.eig(splats, None, cams)
+    _, _, nis, _ = rnd.responsibility(0)
+    assert nis > (1 << 22)
+    want = plain(splats, None, cams, sizes, 0)
+    for v in range(2):
+        np.testing.assert_array_equal(rnd.responsibility(v)[0].read(), want[v][0])
+
+
+def test_round_autotune_keeps_results(ctx):
+    n = 20000
+    attr, sh = synth.scene_uniform(n, 1, 12)
+    a, b = synth.beta_posterior(n, seed=12)
+    splats = sf.Splats(attr, sh)
+    beta = sf.BetaState.from_host(a, b)
+    sizes = [(128, 128)] * 6
+    cams = cams_on_sphere(6, 3.0, 4)
+    rnd = sf.Round(n, sizes)
+    before = rnd.eig(splats, beta, cams, sf.EIG_FP64)
+    tuning, ms = rnd.autotune(splats, beta, cams, sf.EIG_FP64)
+    assert tuning["lanes"] in (1, 2, 4, 8) and tuning["raster_cull"] in (0, 1) and ms > 0
+    assert rnd.get_tuning() == tuning
+    after = rnd.eig(splats, beta, cams, sf.EIG_FP64)
+    np.testing.assert_array_equal(before, after)
+
+
+def test_round_rejects_mismatched_inputs(ctx):
+    attr, sh = synth.scene_uniform(100, 1, 1)
+    splats = sf.Splats(attr, sh)
+    rnd = sf.Round(200, [(32, 32)])
+    with pytest.raises(sf.SplatfieldError):
+        rnd.eig(splats, None, [sf.camera_default()])
+    with pytest.raises(sf.SplatfieldError):
+        sf.Round(100, [])
