@@ -306,6 +306,17 @@ int sf_round_eig(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, i
  * fixed-point scale, the intersection count and the visible count. */
 int sf_round_responsibility(sf_round r, uint32_t view, const uint32_t** resp, float* scale,
                             uint64_t* num_isects, uint32_t* num_visible);
+/* Evidence round: the observe half of Segmenter::step (src/seg/active.rs:
+ * 133-176, the masked finalize of src/render.rs:387-470) batched over several
+ * views. masks[n_views] (each the size
+ * of its view) split every view's weights into fg / bg words, as
+ * sf_accumulate_prepared with a mask does; when beta is non-NULL each view's
+ * EIG over eps = fg + bg goes to eig[n_views]. Syncs once. After it,
+ * sf_round_responsibility returns the fg words. */
+int sf_round_evidence(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams,
+                      const sf_mask* masks, int mode, sf_stream stream, double* eig);
+/* View `view` of the last evidence round: device fg and bg words [total]. */
+int sf_round_evidence_words(sf_round r, uint32_t view, const uint32_t** fg, const uint32_t** bg);
 /* Autotuner: times the round over lanes {1,2,4,8} x raster_cull {0,1}, keeps
  * the fastest on the round and in a process-wide cache keyed by (device,
  * splats, view sizes); a cached shape is not re-timed unless best_ms is

@@ -139,6 +139,8 @@ SIGNATURES = {
         "sf_round_get_tuning": (i32, [P, P]),
         "sf_round_eig": (i32, [P, P, P, P, i32, P, P]),
         "sf_round_responsibility": (i32, [P, u32, PP, P, P, P]),
+        "sf_round_evidence": (i32, [P, P, P, P, P, i32, P, P]),
+        "sf_round_evidence_words": (i32, [P, u32, PP, PP]),
         "sf_round_autotune": (i32, [P, P, P, P, i32, P, P, P]),
         "sf_bits_for": (u32, [u32]),
         "sf_radix_create": (i32, [P, u32, PP]),

@@ -648,6 +648,26 @@ class Round:
                                  self._cams(cameras), mode, _stream(stream), _vp(out)))
         return out
 
+    def evidence(self, splats: Splats, beta: "BetaState | None", cameras, masks, mode: int = EIG_LUT_F32,
+                 stream=None) -> np.ndarray:
+        """Masked evidence of every view (fg / bg words, read with
+        ``evidence_words``) and, with a posterior, each view's EIG."""
+        if len(cameras) != self.views or len(masks) != self.views:
+            raise SplatfieldError(L.SF_ERR_SHAPE, "one camera and one mask per view")
+        hs = (C.c_void_p * self.views)(*[m.handle for m in masks])
+        self._masks = list(masks)  # the graph holds their device words
+        out = np.zeros(self.views, np.float64)
+        check(lib().sf_round_evidence(self.handle, splats.handle, beta.handle if beta else None,
+                                      self._cams(cameras), hs, mode, _stream(stream), _vp(out)))
+        return out
+
+    def evidence_words(self, view: int) -> tuple:
+        """(fg, bg) device words of a view of the last evidence round."""
+        fg, bg = C.c_void_p(), C.c_void_p()
+        check(lib().sf_round_evidence_words(self.handle, view, C.byref(fg), C.byref(bg)))
+        return (DeviceView(fg.value, np.uint32, (self.total,), self),
+                DeviceView(bg.value, np.uint32, (self.total,), self))
+
     def responsibility(self, view: int) -> tuple:
         """(device words, scale, intersections, visible) of a view of the last round."""
         p = C.c_void_p()

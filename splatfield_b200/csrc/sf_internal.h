@@ -121,9 +121,10 @@ constexpr float kLnStep = 0.015611423f;
 void build_entropy_table(float* table);  // host, f64 formulas
 double beta_entropy_host(double a, double b);
 // Per-block f64 partial sums of dH; then a single-block final sum into out.
+// resp2 (optional) is added word for word: eps = fg + bg of an evidence split.
 cudaError_t launch_eig(int mode, const float* a, const float* b, const uint32_t* resp, uint32_t n,
                        float scale, const float* table, double* partials, uint32_t max_blocks,
-                       double* out, cudaStream_t stream);
+                       double* out, cudaStream_t stream, const uint32_t* resp2 = nullptr);
 uint32_t eig_blocks(uint32_t n, int sm_count);
 cudaError_t launch_beta_update(float scale, const uint32_t* fg, const uint32_t* bg, float* a,
                                float* b, uint32_t n, cudaStream_t stream);

@@ -105,7 +105,9 @@ struct sf_round_t {
     uint32_t* words_host = nullptr; // pinned
     double* eig_dev = nullptr;
     double* eig_host = nullptr;     // pinned
-    uint32_t* resp = nullptr;       // [views][n]
+    uint32_t* resp = nullptr;       // [views][n]: total responsibility, or fg under masks
+    uint32_t* bg = nullptr;         // [views][n]: bg under masks (allocated on first use)
+    std::vector<const sf_mask_t*> masks;  // this round's per-view masks (empty: responsibility)
     uint32_t eig_blocks = 1;
     uint64_t want_cap = 0;
     // graph cache
@@ -116,6 +118,7 @@ struct sf_round_t {
     const void* g_beta = nullptr;
     int g_mode = -1;
     uint32_t g_lanes = 0, g_cull = 0;
+    std::vector<const sf_mask_t*> g_masks;
 };
 
 namespace {
@@ -211,7 +214,9 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
     if ((e = launch_tile_starts(tids, 0, words + 2, (uint32_t)L.cap, tiles, L.tile_start, st)) != cudaSuccess)
         return e;
     uint32_t* resp = r->resp + (size_t)v * n;
+    uint32_t* bg = r->masks.empty() ? nullptr : r->bg + (size_t)v * n;
     if ((e = cudaMemsetAsync(resp, 0, (size_t)n * 4, st)) != cudaSuccess) return e;
+    if (bg && (e = cudaMemsetAsync(bg, 0, (size_t)n * 4, st)) != cudaSuccess) return e;
     RasterArgs a{};
     a.w = w;
     a.h = h;
@@ -224,11 +229,21 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
     a.ext = L.ext;
     a.cull = r->tuning.raster_cull;
     a.scale = (float)((uint64_t)1 << frac_bits(w, h));
-    a.resp = resp;
-    if ((e = launch_raster(1, a, st)) != cudaSuccess) return e;
+    if (bg) {
+        // Evidence: the mask splits each pixel's weights into fg / bg.
+        a.mask = r->masks[v]->bits;
+        a.mask_wpr = r->masks[v]->wpr;
+        a.fg = resp;
+        a.bg = bg;
+        if ((e = launch_raster(2, a, st)) != cudaSuccess) return e;
+    } else {
+        a.resp = resp;
+        if ((e = launch_raster(1, a, st)) != cudaSuccess) return e;
+    }
     if (beta_a) {
+        // Under masks the EIG sees eps = fg + bg, the same words mode 1 sums.
         if ((e = launch_eig(mode, beta_a, beta_b, resp, n, a.scale, lut, L.partials, r->eig_blocks,
-                            r->eig_dev + v, st)) != cudaSuccess)
+                            r->eig_dev + v, st, bg)) != cudaSuccess)
             return e;
     }
     return cudaSuccess;
@@ -296,6 +311,7 @@ int build_graph(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, int
     r->g_mode = mode;
     r->g_lanes = (uint32_t)r->lanes.size();
     r->g_cull = r->tuning.raster_cull;
+    r->g_masks = r->masks;
     return SF_OK;
 }
 
@@ -309,7 +325,7 @@ int run_round(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, const
             RF_CK(lanes_build(r, lanes, std::max<uint64_t>(r->want_cap, r->lanes.empty() ? 1024 : r->lanes[0].cap)));
         }
         if (!r->exec || r->g_splats != sp || r->g_beta != beta || r->g_mode != mode ||
-            r->g_cull != r->tuning.raster_cull) {
+            r->g_cull != r->tuning.raster_cull || r->g_masks != r->masks) {
             const int rc = build_graph(r, sp, beta, mode);
             if (rc != SF_OK) return rc;
         }
@@ -400,7 +416,7 @@ int sf_round_destroy(sf_round r) {
     use_dev(r->device);
     graph_drop(r);
     for (auto& L : r->lanes) lane_free(L);
-    dfree(r->views_dev); dfree(r->words); dfree(r->eig_dev); dfree(r->resp);
+    dfree(r->views_dev); dfree(r->words); dfree(r->eig_dev); dfree(r->resp); dfree(r->bg);
     if (r->views_host) cudaFreeHost(r->views_host);
     if (r->words_host) cudaFreeHost(r->words_host);
     if (r->eig_host) cudaFreeHost(r->eig_host);
@@ -432,6 +448,7 @@ int sf_round_eig(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, i
         if (beta && mode != SF_EIG_LUT_F32 && mode != SF_EIG_FP64) return rfail(SF_ERR_ARG, "bad EIG mode");
         if (beta && !eig) return rfail(SF_ERR_ARG, "null eig output");
         RF_CK(use_dev(r->device));
+        r->masks.clear();
         const int rc = run_round(r, s, beta, cams, mode, reinterpret_cast<cudaStream_t>(stream));
         if (rc != SF_OK) return rc;
         if (beta) std::memcpy(eig, r->eig_host, 8 * r->views);
@@ -439,6 +456,40 @@ int sf_round_eig(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, i
     } catch (const std::bad_alloc&) {
         return rfail(SF_ERR_NOMEM, "host allocation failed");
     }
+}
+
+int sf_round_evidence(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, const sf_mask* masks,
+                      int mode, sf_stream stream, double* eig) {
+    try {
+        if (!r || !s || !cams || !masks) return rfail(SF_ERR_ARG, "null argument");
+        if (s->n != r->n) return rfail(SF_ERR_SHAPE, "splat count differs from the round's");
+        if (beta && beta->n != r->n) return rfail(SF_ERR_SHAPE, "posterior size differs from the round's");
+        if (beta && mode != SF_EIG_LUT_F32 && mode != SF_EIG_FP64) return rfail(SF_ERR_ARG, "bad EIG mode");
+        if (beta && !eig) return rfail(SF_ERR_ARG, "null eig output");
+        for (uint32_t v = 0; v < r->views; ++v) {
+            if (!masks[v]) return rfail(SF_ERR_ARG, "null mask");
+            if (masks[v]->w != r->w[v] || masks[v]->h != r->h[v])
+                return rfail(SF_ERR_SHAPE, "mask size does not match its view");
+        }
+        RF_CK(use_dev(r->device));
+        if (!r->bg) RF_CK(dalloc(&r->bg, (size_t)r->views * r->n));
+        r->masks.assign(masks, masks + r->views);
+        const int rc = run_round(r, s, beta, cams, mode, reinterpret_cast<cudaStream_t>(stream));
+        if (rc != SF_OK) return rc;
+        if (beta) std::memcpy(eig, r->eig_host, 8 * r->views);
+        return SF_OK;
+    } catch (const std::bad_alloc&) {
+        return rfail(SF_ERR_NOMEM, "host allocation failed");
+    }
+}
+
+int sf_round_evidence_words(sf_round r, uint32_t view, const uint32_t** fg, const uint32_t** bg) {
+    if (!r) return rfail(SF_ERR_ARG, "null round");
+    if (view >= r->views) return rfail(SF_ERR_SHAPE, "no such view");
+    if (r->masks.empty()) return rfail(SF_ERR_ARG, "the last round had no masks");
+    if (fg) *fg = r->resp + (size_t)view * r->n;
+    if (bg) *bg = r->bg + (size_t)view * r->n;
+    return SF_OK;
 }
 
 int sf_round_responsibility(sf_round r, uint32_t view, const uint32_t** resp, float* scale,

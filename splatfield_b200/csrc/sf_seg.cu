@@ -113,6 +113,7 @@ template <int MODE>
 __global__ __launch_bounds__(kEigThreads) void eig_kernel(const float* __restrict__ a,
                                                           const float* __restrict__ b,
                                                           const uint32_t* __restrict__ resp,
+                                                          const uint32_t* __restrict__ resp2,
                                                           uint32_t n, float scale,
                                                           const float* __restrict__ table,
                                                           double* __restrict__ partials) {
@@ -120,7 +121,8 @@ __global__ __launch_bounds__(kEigThreads) void eig_kernel(const float* __restric
     double acc = 0.0;
     const uint32_t stride = gridDim.x * kEigThreads;
     for (uint32_t i = blockIdx.x * kEigThreads + threadIdx.x; i < n; i += stride) {
-        const uint32_t bits = resp[i];
+        // eps words; with an evidence split, eps = fg + bg exactly.
+        const uint32_t bits = resp[i] + (resp2 ? resp2[i] : 0u);
         if (bits == 0u) continue;
         const float ai = a[i], bi = b[i];
         if (MODE == SF_EIG_LUT_F32) {
@@ -173,11 +175,11 @@ uint32_t eig_blocks(uint32_t n, int sm_count) {
 
 cudaError_t launch_eig(int mode, const float* a, const float* b, const uint32_t* resp, uint32_t n,
                        float scale, const float* table, double* partials, uint32_t blocks,
-                       double* out, cudaStream_t stream) {
+                       double* out, cudaStream_t stream, const uint32_t* resp2) {
     if (mode == SF_EIG_LUT_F32)
-        eig_kernel<SF_EIG_LUT_F32><<<blocks, kEigThreads, 0, stream>>>(a, b, resp, n, scale, table, partials);
+        eig_kernel<SF_EIG_LUT_F32><<<blocks, kEigThreads, 0, stream>>>(a, b, resp, resp2, n, scale, table, partials);
     else
-        eig_kernel<SF_EIG_FP64><<<blocks, kEigThreads, 0, stream>>>(a, b, resp, n, scale, table, partials);
+        eig_kernel<SF_EIG_FP64><<<blocks, kEigThreads, 0, stream>>>(a, b, resp, resp2, n, scale, table, partials);
     eig_final_kernel<<<1, kEigThreads, 0, stream>>>(partials, blocks, out);
     note_launches(2);
     return cudaGetLastError();

@@ -109,3 +109,42 @@ def test_round_rejects_mismatched_inputs(ctx):
         rnd.eig(splats, None, [sf.camera_default()])
     with pytest.raises(sf.SplatfieldError):
         sf.Round(100, [])
+
+
+@pytest.mark.parametrize("lanes", [1, 3])
+def test_round_evidence_matches_plain_masked_accumulate(ctx, lanes):
+    """Evidence round vs per-view prepare + masked accumulate: fg / bg words
+    bit-identical, EIG over fg + bg equal to the plain EIG of the same view's
+    total responsibility."""
+    n = 30000
+    attr, sh = synth.scene_clustered(n, 4, seed=21, clusters=4, sigma=0.25, extent=1.0)
+    a, b = synth.beta_posterior(n, seed=21)
+    splats = sf.Splats(attr, sh)
+    beta = sf.BetaState.from_host(a, b)
+    sizes = [(64, 48), (128, 128), (96, 160), (33, 17)]
+    cams = cams_on_sphere(len(sizes), 3.0, 9)
+    masks = [sf.Mask.from_bytes((w, h), synth.ellipse_mask(w, h, seed=40 + i)) for i, (w, h) in enumerate(sizes)]
+    rnd = sf.Round(n, sizes)
+    rnd.set_tuning(lanes=lanes)
+    for mode in (sf.EIG_LUT_F32, sf.EIG_FP64):
+        eig = rnd.evidence(splats, beta, cams, masks, mode)
+        want = plain(splats, beta, cams, sizes, mode)
+        for v, ((w, h), cam, m) in enumerate(zip(sizes, cams, masks)):
+            scratch = sf.RenderScratch(n, (w, h))
+            acc = sf.Accumulators(n)
+            isects = splats.prepare_isects(scratch, cam, (w, h))
+            splats.accumulate_prepared(scratch, isects, (w, h), acc, m)
+            fg, bg = rnd.evidence_words(v)
+            np.testing.assert_array_equal(fg.read(), acc.fg.read())
+            np.testing.assert_array_equal(bg.read(), acc.bg.read())
+            np.testing.assert_array_equal(fg.read() + bg.read(), want[v][0])
+            assert eig[v] == want[v][2], (v, eig[v], want[v][2])
+    # A responsibility round after an evidence round rebuilds its graph.
+    eig = rnd.eig(splats, beta, cams, sf.EIG_LUT_F32)
+    want = plain(splats, beta, cams, sizes, sf.EIG_LUT_F32)
+    for v in range(len(sizes)):
+        np.testing.assert_array_equal(rnd.responsibility(v)[0].read(), want[v][0])
+    with pytest.raises(sf.SplatfieldError):
+        rnd.evidence_words(0)
+    with pytest.raises(sf.SplatfieldError):
+        rnd.evidence(splats, beta, cams, masks[::-1], sf.EIG_LUT_F32)
