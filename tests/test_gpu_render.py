@@ -79,6 +79,27 @@ def test_frame_bit_exact_vs_oracle(ctx, oracle_mod, n, k, w, h, seed, cull):
     np.testing.assert_array_equal(got["rgba"].view(np.uint32), wr["rgba"].view(np.uint32))
 
 
+def test_full_size_frame_bit_exact_vs_oracle(ctx, oracle_mod):
+    """The bench workload itself: 1M SH3 splats in 8 clusters, 1920x1080, one
+    orbit camera. Every intermediate array and the image, bit for bit."""
+    O = oracle_mod
+    from splatfield_b200 import synth
+
+    n, k, w, h = 1_000_000, 16, 1920, 1080
+    attr, sh = synth.scene_clustered(n, k, seed=0)
+    cam_o = synth.orbit_cameras(30, 4.0, w, h, O.look_at)[7]
+    cam = synth.orbit_cameras(30, 4.0, w, h, sf.look_at)[7]
+    want = O.prepare(cam_o, w, h, attr, sh, k)
+    wr = O.rasterize(want, 0)
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    got = gpu_frame(splats, scratch, cam, w, h, n)
+    assert got["num_isects"] > (1 << 22)
+    assert_frame_equal(got, want)
+    np.testing.assert_array_equal(got["bitmap"], wr["bitmap"])
+    np.testing.assert_array_equal(got["rgba"].view(np.uint32), wr["rgba"].view(np.uint32))
+
+
 def test_project_counts_tiles_and_packs_bbox(ctx):
     """src/project.rs:399-446 through the GPU path."""
     ka = KA["project_one_splat"]
