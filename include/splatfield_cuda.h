@@ -349,6 +349,18 @@ int sf_exclusive_scan_gather(sf_scan s, const uint32_t* gids, const uint32_t* co
                              uint32_t* offsets, uint32_t n, sf_stream stream);
 /* exclusive_scan_buf (crates/sort/src/scan.rs:185-213): in place. */
 int sf_exclusive_scan(sf_scan s, uint32_t* buf, uint32_t n, sf_stream stream);
+/* No counterpart in the reference. sf_exclusive_scan_gather for callers that
+ * cannot call cudaMalloc (a host whose device memory belongs to another
+ * allocator's pool, or a per-frame loop that may not take cudaMalloc's
+ * device-wide synchronisation): same result, but the look-back scratch is a
+ * fixed static device array, so the call allocates nothing. Runs on the
+ * calling thread's current device; n > SF_SCAN_NOALLOC_MAX_ELEMS (2^24) is
+ * rejected with SF_ERR_SHAPE before any CUDA call. Every call on a device
+ * shares the one array: calls that overlap on the GPU race, so order them
+ * (one stream). */
+#define SF_SCAN_NOALLOC_MAX_ELEMS (1u << 24)
+int sf_exclusive_scan_gather_noalloc(const uint32_t* gids, const uint32_t* counts,
+                                     uint32_t* offsets, uint32_t n, sf_stream stream);
 
 #ifdef __cplusplus
 }

@@ -150,6 +150,7 @@ SIGNATURES = {
         "sf_scan_destroy": (i32, [P]),
         "sf_exclusive_scan_gather": (i32, [P, P, P, P, u32, P]),
         "sf_exclusive_scan": (i32, [P, P, u32, P]),
+        "sf_exclusive_scan_gather_noalloc": (i32, [P, P, P, u32, P]),
 }
 del P, u32, i32, sz, PP
 
