@@ -145,8 +145,18 @@ int sf_scratch_capacity(sf_scratch s, uint64_t* capacity);
 typedef struct {
     uint32_t raster_cull; /* 0: every warp walks every staged entry;
                              1: per-warp culling by each splat's power_max box */
-    uint32_t reserved[7];
+    /* Intersection build, same lists either way:
+     *   SF_ISECTS_BINNED (default, frames up to 49152 tiles): per-tile
+     *     counts in shared memory, place, then a sort of each tile's list by
+     *     (depth, id) (in shared memory up to 12288 entries);
+     *   SF_ISECTS_DEPTH_SORTED: the reference's order of steps
+     *     (src/render.rs:318-352): depth argsort, gather scan, emit, stable
+     *     tile sort; keeps the depth order and offsets for sf_scratch_read. */
+    uint32_t isect_build;
+    uint32_t reserved[6];
 } sf_tuning;
+#define SF_ISECTS_BINNED 0u
+#define SF_ISECTS_DEPTH_SORTED 1u
 int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t);
 int sf_scratch_get_tuning(sf_scratch s, sf_tuning* t);
 

@@ -26,6 +26,7 @@ READ_DEPTH_KEYS, READ_TILE_COUNTS, READ_BBOX, READ_PROJECTED, READ_ORDER, READ_O
 READ_TILE_IDS, READ_GAUSSIAN_IDS, READ_TILE_START, READ_BITMAP, READ_RGBA, READ_FINAL_T, READ_N_CONTRIB = range(6, 13)
 
 EIG_LUT_F32, EIG_FP64 = 0, 1
+ISECTS_BINNED, ISECTS_DEPTH_SORTED = 0, 1
 
 
 class SplatfieldError(RuntimeError):
@@ -51,7 +52,7 @@ class View(C.Structure):
 class Tuning(C.Structure):
     """sf_tuning: kernel forms of a scratch (results are identical across forms)."""
 
-    _fields_ = [("raster_cull", C.c_uint32), ("reserved", C.c_uint32 * 7)]
+    _fields_ = [("raster_cull", C.c_uint32), ("isect_build", C.c_uint32), ("reserved", C.c_uint32 * 6)]
 
 
 class RoundTuning(C.Structure):

@@ -26,9 +26,11 @@ __all__ = [
     "RenderScratch", "TileIsects", "Accumulators", "Mask", "BetaState", "map_labels", "bits_for",
     "RadixScratch", "ScanScratch", "exclusive_scan_gather", "exclusive_scan_buf", "entropy_table",
     "table_entropy", "fractional_bits", "row_stride_for", "EIG_LUT_F32", "EIG_FP64", "Round",
+    "ISECTS_BINNED", "ISECTS_DEPTH_SORTED",
 ]
 
 EIG_LUT_F32, EIG_FP64 = L.EIG_LUT_F32, L.EIG_FP64
+ISECTS_BINNED, ISECTS_DEPTH_SORTED = L.ISECTS_BINNED, L.ISECTS_DEPTH_SORTED
 BASE_FOV = 0.8  # Camera::BASE_FOV (src/camera.rs:86)
 
 
@@ -364,15 +366,18 @@ class RenderScratch:
         check(lib().sf_scratch_capacity(self.handle, C.byref(c)))
         return int(c.value)
 
-    def set_tuning(self, raster_cull: int = 0) -> None:
+    def set_tuning(self, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED) -> None:
+        """Kernel forms (results are identical across forms): raster_cull 0/1,
+        isect_build ISECTS_BINNED (default) or ISECTS_DEPTH_SORTED."""
         t = L.Tuning()
         t.raster_cull = int(raster_cull)
+        t.isect_build = int(isect_build)
         check(lib().sf_scratch_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:
         t = L.Tuning()
         check(lib().sf_scratch_get_tuning(self.handle, C.byref(t)))
-        return {"raster_cull": int(t.raster_cull)}
+        return {"raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build)}
 
     def read(self, what: int, count: int, dtype=np.uint32, stream=None) -> np.ndarray:
         out = np.empty(count, dtype)

@@ -125,11 +125,19 @@ struct sf_scratch_t {
     const uint32_t* tids = nullptr;
     const uint32_t* gids = nullptr;
     uint32_t* tile_start = nullptr;
+    // Binned build: [chunks][tiles] histogram / prefixes, per-tile totals,
+    // per-class tile lists.
+    uint32_t bin_chunks = 0;
+    uint32_t* bin_hist = nullptr;
+    uint32_t* bin_cnt = nullptr;
+    uint32_t* bin_lists = nullptr;
+    bool binned = false;
     uint32_t* bitmap = nullptr;
     float4* rgba = nullptr;
     float* final_t = nullptr;
     uint32_t* n_contrib = nullptr;
-    // device words: [0] visible, [1] error bits, [2..3] spare, then u64 total at +16
+    // device words: [0] visible, [1] error bits, [2..3] spare, [4..5] u64
+    // total, [6..10] binned-build tile statistics (sf_internal.h)
     uint32_t* words = nullptr;
     uint32_t* host_words = nullptr;  // pinned mirror
     unsigned long long* stats = nullptr;  // raster pair statistics of the last finalize
@@ -177,6 +185,7 @@ void scratch_free_frame(sf_scratch s) {
     dfree(s->depth_keys); dfree(s->tile_counts); dfree(s->bbox); dfree(s->geo0); dfree(s->geo1);
     dfree(s->color); dfree(s->ext); dfree(s->keys_a); dfree(s->keys_b); dfree(s->order_a); dfree(s->order_b);
     dfree(s->offsets); dfree(s->scan_tmp); dfree(s->tile_start); dfree(s->bitmap);
+    dfree(s->bin_hist); dfree(s->bin_cnt); dfree(s->bin_lists);
     dfree(s->rgba); dfree(s->final_t); dfree(s->n_contrib); dfree(s->d2d);
     s->order = nullptr;
     s->prepared = false;
@@ -184,7 +193,8 @@ void scratch_free_frame(sf_scratch s) {
 }
 
 void scratch_free_isects(sf_scratch s) {
-    dfree(s->tid_e); dfree(s->gid_e); dfree(s->tid_a); dfree(s->gid_a);
+    dfree(s->tid_e); dfree(s->gid_e); dfree(s->tid_a);
+    s->gid_a = nullptr;  // second half of the tid_a allocation
     if (s->sort_tmp) cudaFree(s->sort_tmp);
     s->sort_tmp = nullptr;
     s->sort_tmp_bytes = 0;
@@ -205,13 +215,16 @@ cudaError_t ensure_sort_tmp(sf_scratch s, size_t bytes) {
 cudaError_t grow_isects(sf_scratch s, uint64_t want) {
     if (want <= s->cap && s->tid_e) return cudaSuccess;
     const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(next_pow2(want), 1024), kMaxIsects + 1);
-    dfree(s->tid_e); dfree(s->gid_e); dfree(s->tid_a); dfree(s->gid_a);
+    dfree(s->tid_e); dfree(s->gid_e); dfree(s->tid_a);
+    s->gid_a = nullptr;
     s->cap = 0;
     cudaError_t e;
     if ((e = dalloc(&s->tid_e, cap)) != cudaSuccess) return e;
     if ((e = dalloc(&s->gid_e, cap)) != cudaSuccess) return e;
-    if ((e = dalloc(&s->tid_a, cap)) != cudaSuccess) return e;
-    if ((e = dalloc(&s->gid_a, cap)) != cudaSuccess) return e;
+    // tid_a and gid_a are one allocation: the binned build places packed
+    // (depth key, splat id) pairs across both.
+    if ((e = dalloc(&s->tid_a, 2 * cap)) != cudaSuccess) return e;
+    s->gid_a = s->tid_a + cap;
     s->cap = cap;
     return ensure_sort_tmp(s, std::max(radix_temp_bytes((uint32_t)std::min<uint64_t>(cap, kMaxIsects), 4),
                                        radix_temp_bytes(s->total, 4)));
@@ -239,22 +252,68 @@ cudaError_t scratch_build(sf_scratch s, uint32_t total, uint32_t w, uint32_t h) 
     SF_AL(s->order_a, total);
     SF_AL(s->order_b, total);
     SF_AL(s->offsets, total);
-    SF_AL(s->tile_start, (size_t)s->tiles_x * s->tiles_y + 1);
+    const size_t tiles = (size_t)s->tiles_x * s->tiles_y;
+    SF_AL(s->tile_start, tiles + 1);
+    if (tiles <= kBinMaxTiles) {
+        s->bin_chunks = bin_chunks(total, s->ctx->sm_count);
+        SF_AL(s->bin_hist, (size_t)s->bin_chunks * tiles);
+        SF_AL(s->bin_cnt, tiles + 1);
+        SF_AL(s->bin_lists, 4 * tiles);
+    }
     SF_AL(s->bitmap, (size_t)h * s->row_stride);
 #undef SF_AL
     // Row padding (row_stride past w) is never rendered: clear it once so
     // read-backs of whole rows are deterministic.
     if ((e = cudaMemset(s->bitmap, 0, (size_t)h * s->row_stride * 4)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&s->scan_tmp, scan_temp_bytes(total))) != cudaSuccess) return e;
+    const uint32_t scan_n = (uint32_t)std::max<size_t>(total, tiles + 1);
+    if ((e = cudaMalloc(&s->scan_tmp, scan_temp_bytes(scan_n))) != cudaSuccess) return e;
     if (!s->words) {
         if ((e = dalloc(&s->stats, 4)) != cudaSuccess) return e;
-        if ((e = dalloc(&s->words, 8)) != cudaSuccess) return e;
-        if ((e = cudaMallocHost(reinterpret_cast<void**>(&s->host_words), 32)) != cudaSuccess) return e;
+        if ((e = dalloc(&s->words, 16)) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(reinterpret_cast<void**>(&s->host_words), 64)) != cudaSuccess) return e;
     }
     // Capacity: keep the larger of the growth hint and the reference's first
     // frame rule min(tiles*total, 2^22) (render.rs:146-147, 177-183).
     const uint64_t first = std::min<uint64_t>((uint64_t)s->tiles_x * s->tiles_y * total, kInitialIsects);
     return grow_isects(s, std::max<uint64_t>(std::max<uint64_t>(first, s->last_isects_raw), s->cap));
+}
+
+int finish_prepare(sf_scratch s, sf_isects* out);
+
+// Binned intersection build (sf_bin.cu) after the projection: count, column
+// scan, tile scan, one sync for the total, place, per-tile sorts.
+int prepare_binned(sf_scratch s, uint32_t n, uint32_t tiles, cudaStream_t st, bool want_tile_ids) {
+    uint32_t* words = s->words;
+    unsigned long long* total_dev = reinterpret_cast<unsigned long long*>(words + 4);
+    SF_CK(launch_bin_count(s->bbox, n, s->tiles_x, tiles, s->bin_chunks, s->bin_hist, st));
+    SF_CK(launch_bin_colscan(s->bin_hist, s->bin_chunks, tiles, s->bin_cnt, s->bin_lists, words, st));
+    SF_CK(exclusive_scan(nullptr, s->bin_cnt, s->tile_start, tiles + 1, nullptr, tiles + 1, s->scan_tmp,
+                         total_dev, words + 1, st));
+    SF_CK(cudaMemcpyAsync(s->host_words, words, 64, cudaMemcpyDeviceToHost, st));
+    SF_CK(cudaStreamSynchronize(st));
+    const uint32_t* hw = s->host_words;
+    if (hw[1] & SF_DEV_ERR_TIMEOUT) return fail(SF_ERR_TIMEOUT, "device look-back wait timed out");
+    uint64_t total = 0;
+    std::memcpy(&total, hw + 4, 8);
+    s->num_visible = hw[0];
+    s->last_isects_raw = total;
+    if (total > kMaxIsects) return fail(SF_ERR_CAPACITY, "intersection count exceeds 2^30-1");
+    if (total > s->cap) {
+        std::fprintf(stderr, "splatfield_b200: intersection capacity %llu reached (%llu needed); growing\n",
+                     (unsigned long long)s->cap, (unsigned long long)total);
+        SF_CK(grow_isects(s, total));
+    }
+    uint2* pairs = reinterpret_cast<uint2*>(s->tid_a);
+    SF_CK(launch_bin_place(s->bbox, s->depth_keys, n, s->tiles_x, tiles, s->bin_chunks, s->bin_hist,
+                           s->tile_start, (uint32_t)s->cap, pairs, words + 1, st));
+    const uint32_t grids[4] = {hw[8], hw[9], hw[10], hw[7]};
+    SF_CK(launch_tile_sorts(grids, s->bin_lists, words, tiles, s->tile_start, (uint32_t)s->cap, pairs, s->gid_e,
+                            want_tile_ids ? s->tid_e : nullptr, s->tid_e, st));
+    s->tids = want_tile_ids ? s->tid_e : nullptr;
+    s->gids = s->gid_e;
+    s->num_isects = (uint32_t)total;
+    s->binned = true;
+    return SF_OK;
 }
 
 // prepare_isects (src/render.rs:274-364).
@@ -270,9 +329,18 @@ int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32
     const uint32_t n = sp->n;
     uint32_t* words = s->words;
     unsigned long long* total_dev = reinterpret_cast<unsigned long long*>(words + 4);
-    SF_CK(cudaMemsetAsync(words, 0, 32, st));
+    SF_CK(cudaMemsetAsync(words, 0, 64, st));
     ProjOut po{s->depth_keys, s->tile_counts, s->bbox, s->geo0, s->geo1, s->color, words, s->ext};
     SF_CK(launch_project(view, sp->attr, sp->sh, n, sp->K, po, st));
+    const uint32_t tiles = s->tiles_x * s->tiles_y;
+    s->order = nullptr;
+    s->tids = s->gids = nullptr;
+    if (s->tuning.isect_build == SF_ISECTS_BINNED && s->bin_hist) {
+        const int rc = prepare_binned(s, n, tiles, st, out != nullptr);
+        if (rc != SF_OK) return rc;
+        return finish_prepare(s, out);
+    }
+    s->binned = false;
     int in_b = 0;
     SF_CK(ensure_sort_tmp(s, radix_temp_bytes(n, 4)));
     SF_CK(radix_sort_pairs(s->depth_keys, nullptr, s->keys_a, s->order_a, s->keys_b, s->order_b, n,
@@ -281,7 +349,7 @@ int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32
     s->order = in_b ? s->order_b : s->order_a;
     SF_CK(exclusive_scan(s->order, s->tile_counts, s->offsets, n, nullptr, n, s->scan_tmp, total_dev,
                          words + 1, st));
-    SF_CK(cudaMemcpyAsync(s->host_words, words, 32, cudaMemcpyDeviceToHost, st));
+    SF_CK(cudaMemcpyAsync(s->host_words, words, 64, cudaMemcpyDeviceToHost, st));
     SF_CK(cudaStreamSynchronize(st));
     if (s->host_words[1] & SF_DEV_ERR_TIMEOUT) return fail(SF_ERR_TIMEOUT, "device look-back wait timed out");
     uint64_t total = 0;
@@ -297,7 +365,6 @@ int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32
     const uint32_t I = (uint32_t)total;
     SF_CK(launch_emit(s->order, s->bbox, s->offsets, n, s->tiles_x, (uint32_t)s->cap, s->tid_e,
                       s->gid_e, words + 1, st));
-    const uint32_t tiles = s->tiles_x * s->tiles_y;
     const uint32_t tbits = bits_for_u32(tiles);
     if (I <= 1 || tbits == 0) {
         s->tids = s->tid_e;
@@ -310,12 +377,16 @@ int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32
     }
     SF_CK(launch_tile_starts(s->tids, I, nullptr, I, tiles, s->tile_start, st));
     s->num_isects = I;
+    return finish_prepare(s, out);
+}
+
+int finish_prepare(sf_scratch s, sf_isects* out) {
     s->prepared = true;
     if (out) {
         out->tile_ids = s->tids;
         out->gaussian_ids = s->gids;
         out->tile_start = s->tile_start;
-        out->num_isects = I;
+        out->num_isects = s->num_isects;
         out->num_visible = s->num_visible;
         out->tile_bounds[0] = s->tiles_x;
         out->tile_bounds[1] = s->tiles_y;
@@ -580,6 +651,7 @@ int sf_scratch_destroy(sf_scratch s) {
 int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t) {
     if (!s || !t) return fail(SF_ERR_ARG, "null argument");
     if (t->raster_cull > 1) return fail(SF_ERR_ARG, "raster_cull must be 0 or 1");
+    if (t->isect_build > SF_ISECTS_DEPTH_SORTED) return fail(SF_ERR_ARG, "unknown isect_build");
     s->tuning = *t;
     return SF_OK;
 }
@@ -749,7 +821,12 @@ int sf_scratch_read(sf_scratch s, int what, void* host, size_t bytes, sf_stream 
             case SF_READ_N_CONTRIB: src = s->n_contrib; avail = s->n_contrib ? (size_t)s->w * s->h * 4 : 0; break;
             default: return fail(SF_ERR_ARG, "unknown scratch field");
         }
-        if (bytes > avail || (bytes && !src)) {
+        if (bytes && !src) {
+            dfree(rows);
+            return fail(SF_ERR_ARG, "field not produced by the last prepare (the binned build keeps no depth "
+                                    "order or offsets; tile ids only through sf_prepare_isects)");
+        }
+        if (bytes > avail) {
             dfree(rows);
             return fail(SF_ERR_SHAPE, "read exceeds the field's size");
         }

@@ -1,0 +1,661 @@
+// Binned intersection build: the tile-major, depth-minor (tile id, splat id)
+// list without a global sort.
+//
+// The reference orders intersections with two global sorts
+// (src/render.rs:318-352): splats by depth, then a stable sort of the
+// emitted (tile, splat) pairs by tile id. Within a tile this yields the
+// splats in ascending (depth key, splat id) order, since the depth argsort
+// breaks key ties by splat id. This file builds the same list in four
+// steps, and no step moves the whole list through a global sort:
+//
+//   1. bin_count: chunk c of the splats (in id order) is counted per tile in a
+//      shared-memory histogram, written as hist[c][tile].
+//   2. bin_colscan: per tile, the exclusive prefix of hist over the chunks (in
+//      place) and the tile's total; tiles are filed into size classes.
+//      An exclusive scan of the totals (sfk::exclusive_scan) gives tile_start.
+//   3. bin_place: chunk c re-walks its pairs and drops each (depth key, splat
+//      id) at tile_start[t] + hist[c][t] + a shared-memory cursor. The order
+//      inside a tile is not yet fixed.
+//   4. tile_sort: one CTA per tile sorts its segment in shared memory by
+//      (depth key, splat id) with a stable LSD radix sort over only the bits
+//      where the segment's keys differ, and writes the splat ids (and, when
+//      asked, the tile ids) back in place.
+//
+// The result is bit-identical to the reference's order: the pair set is the
+// same, and a total order on (key, id) has one sorted arrangement.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "sf_internal.h"
+
+namespace sfk {
+namespace {
+
+constexpr uint32_t kBinThreads = 512;
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Calls f(splat, tile) for every tile of every splat in [begin, end): warps
+// take 32 consecutive splats at a time and spread the pairs over their lanes
+// (owner found by a shuffle search over the lanes' inclusive ends), so a
+// splat covering many tiles does not stall its warp.
+template <typename F>
+__device__ __forceinline__ void for_each_pair(uint32_t begin, uint32_t end, const uint2* __restrict__ bbox,
+                                              uint32_t tiles_x, F&& f) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t nwarps = blockDim.x >> 5;
+    for (uint32_t g0 = begin + warp * 32u; g0 < end; g0 += nwarps * 32u) {
+        const uint32_t r = g0 + lane;
+        uint32_t min_x = 0, min_y = 0, width = 1, cnt = 0;
+        if (r < end) {
+            const uint2 bb = bbox[r];
+            min_x = bb.x & 0xffffu;
+            min_y = bb.x >> 16;
+            const uint32_t max_x = bb.y & 0xffffu, max_y = bb.y >> 16;
+            if (max_x > min_x && max_y > min_y) {
+                width = max_x - min_x;
+                cnt = width * (max_y - min_y);
+            }
+        }
+        uint32_t incl = cnt;
+#pragma unroll
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        for (uint32_t p0 = 0; p0 < total; p0 += 32) {
+            const uint32_t p = p0 + lane;
+            uint32_t o = 0;
+#pragma unroll
+            for (uint32_t step = 16; step > 0; step >>= 1) {
+                const uint32_t v = __shfl_sync(0xffffffffu, incl, o + step - 1);
+                if (v <= p) o += step;
+            }
+            const uint32_t oend = __shfl_sync(0xffffffffu, incl, o);
+            const uint32_t ocnt = __shfl_sync(0xffffffffu, cnt, o);
+            const uint32_t ow = __shfl_sync(0xffffffffu, width, o);
+            const uint32_t ox = __shfl_sync(0xffffffffu, min_x, o);
+            const uint32_t oy = __shfl_sync(0xffffffffu, min_y, o);
+            if (p < total) {
+                const uint32_t k = p - (oend - ocnt);
+                f(g0 + o, (ox + k % ow) + (oy + k / ow) * tiles_x);
+            }
+        }
+    }
+}
+
+__global__ __launch_bounds__(kBinThreads) void bin_count_kernel(const uint2* __restrict__ bbox, uint32_t n,
+                                                                uint32_t chunk, uint32_t tiles_x,
+                                                                uint32_t tiles, uint32_t* __restrict__ hist) {
+    extern __shared__ uint32_t s_hist[];
+    for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) s_hist[t] = 0;
+    __syncthreads();
+    const uint32_t begin = min(n, blockIdx.x * chunk);
+    const uint32_t end = min(n, begin + chunk);
+    for_each_pair(begin, end, bbox, tiles_x, [&](uint32_t, uint32_t t) { atomicAdd(&s_hist[t], 1u); });
+    __syncthreads();
+    uint32_t* row = hist + (size_t)blockIdx.x * tiles;
+    for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) row[t] = s_hist[t];
+}
+
+// Block (32, 32): x = tile within the block's 32, y = a group of chunks.
+// words: [6] max tile count (atomicMax), [7] tiles longer than the shared
+// classes (lists[3 * tiles + i]), [8 + k] tiles in shared class k
+// (lists[k * tiles + i]).
+__global__ __launch_bounds__(1024) void bin_colscan_kernel(uint32_t* __restrict__ hist, uint32_t chunks,
+                                                           uint32_t tiles, uint32_t* __restrict__ cnt,
+                                                           uint32_t* __restrict__ lists, uint32_t* words,
+                                                           uint32_t class0, uint32_t class1, uint32_t class2) {
+    __shared__ uint32_t s_part[32][33];
+    const uint32_t tx = threadIdx.x, ty = threadIdx.y;
+    const uint32_t t = blockIdx.x * 32u + tx;
+    const bool valid = t < tiles;
+    const uint32_t per = (chunks + 31u) / 32u;
+    const uint32_t c0 = min(chunks, ty * per), c1 = min(chunks, c0 + per);
+    uint32_t sum = 0;
+    if (valid)
+        for (uint32_t c = c0; c < c1; ++c) sum += hist[(size_t)c * tiles + t];
+    s_part[ty][tx] = sum;
+    __syncthreads();
+    if (ty == 0) {
+        uint32_t run = 0;
+        for (uint32_t y = 0; y < 32; ++y) {
+            const uint32_t v = s_part[y][tx];
+            s_part[y][tx] = run;
+            run += v;
+        }
+        if (valid) cnt[t] = run;
+        if (blockIdx.x == 0 && tx == 0) cnt[tiles] = 0;
+        // Size classes (warp-aggregated appends; the list order is free).
+        const uint32_t total = valid ? run : 0u;
+        const uint32_t cls = total == 0 ? 4u : total <= class0 ? 0u : total <= class1 ? 1u
+                           : total <= class2 ? 2u : 3u;
+        const uint32_t mx = __reduce_max_sync(0xffffffffu, total);
+        if (tx == 0 && mx) atomicMax(words + 6, mx);
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) {
+            const uint32_t m = __ballot_sync(0xffffffffu, cls == k);
+            if (!m) continue;
+            const uint32_t leader = __ffs(m) - 1;
+            uint32_t base = 0;
+            if (tx == leader) base = atomicAdd(words + (k == 3 ? 7u : 8u + k), __popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (cls == k) lists[k * tiles + base + __popc(m & lanemask_lt())] = t;
+        }
+    }
+    __syncthreads();
+    if (valid) {
+        uint32_t run = s_part[ty][tx];
+        for (uint32_t c = c0; c < c1; ++c) {
+            const size_t i = (size_t)c * tiles + t;
+            const uint32_t v = hist[i];
+            hist[i] = run;
+            run += v;
+        }
+    }
+}
+
+__global__ __launch_bounds__(kBinThreads) void bin_place_kernel(
+    const uint2* __restrict__ bbox, const uint32_t* __restrict__ depth_keys, uint32_t n, uint32_t chunk,
+    uint32_t tiles_x, uint32_t tiles, const uint32_t* __restrict__ hist, const uint32_t* __restrict__ tile_start,
+    uint32_t capacity, uint2* __restrict__ pairs, uint32_t* err) {
+    extern __shared__ uint32_t s_cur[];
+    const uint32_t* row = hist + (size_t)blockIdx.x * tiles;
+    for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) s_cur[t] = tile_start[t] + row[t];
+    __syncthreads();
+    const uint32_t begin = min(n, blockIdx.x * chunk);
+    const uint32_t end = min(n, begin + chunk);
+    bool over = false;
+    for_each_pair(begin, end, bbox, tiles_x, [&](uint32_t s, uint32_t t) {
+        const uint32_t slot = atomicAdd(&s_cur[t], 1u);
+        if (slot < capacity) {
+            pairs[slot] = make_uint2(depth_keys[s], s);
+        } else {
+            over = true;
+        }
+    });
+    if (over) atomicOr(err, SF_DEV_ERR_CAPACITY);
+}
+
+// ---- per-tile sort
+//
+// Each tile's placed (depth key, splat id) pairs are sorted by (key, id).
+// Main method, a bucket sort: (key - min) >> shift picks one of about 2n
+// buckets (monotone in the key); a counting pass and an atomic scatter fill
+// them; each entry's final place is its bucket's start plus its rank on
+// (key, id) among the bucket's entries, counted by its own thread. A bucket
+// past kMaxBucket entries (keys bunched within the tile, or equal keys) sends
+// the tile to a stable LSD radix sort on (key, id) in global memory (the
+// tile's own ranges of the pair and output buffers, L2-resident).
+
+constexpr uint32_t kMaxBucket = 256;
+
+// One stable LSD pass on digit (x >> shift) & 255, x = key or value, from
+// (sk, sv) into (dk, dv). s_base[256], s_wc[WARPS * 256] (zero on entry,
+// zero on exit), s_tmp[WARPS].
+template <uint32_t THREADS>
+__device__ void sort_pass(const uint32_t* sk, const uint32_t* sv, uint32_t* dk, uint32_t* dv, uint32_t n,
+                          uint32_t shift, bool by_val, uint32_t* s_base, uint32_t* s_wc, uint32_t* s_tmp) {
+    constexpr uint32_t WARPS = THREADS / 32;
+    static_assert(THREADS >= 256, "one thread per digit");
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    if (tid < 256) s_base[tid] = 0;
+    __syncthreads();
+    // Digit counts, one shared atomic per distinct digit of each warp (the
+    // digits of one tile's keys are far from uniform).
+    for (uint32_t c0 = 0; c0 < n; c0 += THREADS) {
+        const uint32_t i = c0 + tid;
+        const bool valid = i < n;
+        const uint32_t d = valid ? ((by_val ? sv[i] : sk[i]) >> shift) & 255u : 0u;
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (uint32_t b = 0; b < 8; ++b) {
+            const bool bit = (d >> b) & 1u;
+            const uint32_t bb = __ballot_sync(0xffffffffu, bit);
+            peers &= bit ? bb : ~bb;
+        }
+        if (valid && (peers & lanemask_lt()) == 0) atomicAdd(&s_base[d], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    // Exclusive scan of the 256 digit counts (threads 0..255, warps 0..7).
+    uint32_t c = 0, incl = 0;
+    if (tid < 256) {
+        c = s_base[tid];
+        incl = c;
+#pragma unroll
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+        }
+        if (lane == 31) s_tmp[warp] = incl;
+    }
+    __syncthreads();
+    if (tid < 256) {
+        uint32_t wbase = 0;
+        for (uint32_t w = 0; w < warp; ++w) wbase += s_tmp[w];
+        s_base[tid] = wbase + incl - c;
+    }
+    __syncthreads();
+    for (uint32_t c0 = 0; c0 < n; c0 += THREADS) {
+        const uint32_t i = c0 + tid;
+        const bool valid = i < n;
+        uint32_t k = 0, v = 0, d = 0;
+        if (valid) {
+            k = sk[i];
+            v = sv[i];
+            d = ((by_val ? v : k) >> shift) & 255u;
+        }
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (uint32_t b = 0; b < 8; ++b) {
+            const bool bit = (d >> b) & 1u;
+            const uint32_t bb = __ballot_sync(0xffffffffu, bit);
+            peers &= bit ? bb : ~bb;
+        }
+        const uint32_t rank = __popc(peers & lanemask_lt());
+        if (valid && rank == 0) s_wc[warp * 256u + d] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            uint32_t off = s_base[d] + rank;
+            for (uint32_t w = 0; w < warp; ++w) off += s_wc[w * 256u + d];
+            dk[off] = k;
+            dv[off] = v;
+        }
+        __syncthreads();
+        if (tid < 256) {
+            uint32_t add = 0;
+#pragma unroll
+            for (uint32_t w = 0; w < WARPS; ++w) {
+                add += s_wc[w * 256u + tid];
+                s_wc[w * 256u + tid] = 0;
+            }
+            s_base[tid] += add;
+        }
+        __syncthreads();
+    }
+}
+
+// Block min and max of per-thread partials (uniform result).
+template <uint32_t THREADS>
+__device__ void block_min_max(uint32_t lo, uint32_t hi, uint32_t* s_tmp, uint32_t& mn, uint32_t& mx) {
+    constexpr uint32_t WARPS = THREADS / 32;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    __syncthreads();
+    if (lane == 0) {
+        s_tmp[warp] = lo;
+        s_tmp[WARPS + warp] = hi;
+    }
+    __syncthreads();
+    mn = s_tmp[0];
+    mx = s_tmp[WARPS];
+    for (uint32_t w = 1; w < WARPS; ++w) {
+        mn = min(mn, s_tmp[w]);
+        mx = max(mx, s_tmp[WARPS + w]);
+    }
+    __syncthreads();
+}
+
+template <uint32_t THREADS>
+__device__ void array_min_max(const uint32_t* a, uint32_t n, uint32_t* s_tmp, uint32_t& mn, uint32_t& mx) {
+    uint32_t lo = 0xffffffffu, hi = 0;
+    for (uint32_t i = threadIdx.x; i < n; i += THREADS) {
+        lo = min(lo, a[i]);
+        hi = max(hi, a[i]);
+    }
+    block_min_max<THREADS>(lo, hi, s_tmp, mn, mx);
+}
+
+// Stable sort of (k, v) by the bits where [mn, mx] differ; the arrays
+// ping-pong through (k2, v2) and the result is copied back when the pass
+// count is odd.
+template <uint32_t THREADS>
+__device__ void sort_bits(uint32_t* k, uint32_t* v, uint32_t* k2, uint32_t* v2, uint32_t n, uint32_t mn,
+                          uint32_t mx, bool by_val, uint32_t* s_base, uint32_t* s_wc, uint32_t* s_tmp) {
+    const uint32_t bits = mn == mx ? 0u : 32u - __clz(mn ^ mx);
+    bool in_2 = false;
+    for (uint32_t shift = 0; shift < bits; shift += 8) {
+        if (!in_2) sort_pass<THREADS>(k, v, k2, v2, n, shift, by_val, s_base, s_wc, s_tmp);
+        else sort_pass<THREADS>(k2, v2, k, v, n, shift, by_val, s_base, s_wc, s_tmp);
+        in_2 = !in_2;
+    }
+    if (in_2) {
+        for (uint32_t i = threadIdx.x; i < n; i += THREADS) {
+            k[i] = k2[i];
+            v[i] = v2[i];
+        }
+        __syncthreads();
+    }
+}
+
+// The radix fallback on global memory: (ka, va) hold the tile's entries and
+// receive the result, (kb, vb) are scratch. scratch: 256 + WARPS * 256 words.
+template <uint32_t THREADS>
+__device__ void radix_tile(uint32_t* ka, uint32_t* va, uint32_t* kb, uint32_t* vb, uint32_t n, uint32_t mn,
+                           uint32_t mx, uint32_t* scratch, uint32_t* s_tmp) {
+    constexpr uint32_t WARPS = THREADS / 32;
+    uint32_t* s_base = scratch;
+    uint32_t* s_wc = scratch + 256;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < WARPS * 256; i += THREADS) s_wc[i] = 0;
+    __syncthreads();
+    sort_bits<THREADS>(ka, va, kb, vb, n, mn, mx, false, s_base, s_wc, s_tmp);
+    int tie = 0;
+    for (uint32_t i = threadIdx.x; i + 1 < n; i += THREADS) tie |= ka[i] == ka[i + 1];
+    if (__syncthreads_or(tie)) {
+        uint32_t imn, imx;
+        array_min_max<THREADS>(va, n, s_tmp, imn, imx);
+        sort_bits<THREADS>(ka, va, kb, vb, n, imn, imx, true, s_base, s_wc, s_tmp);
+        sort_bits<THREADS>(ka, va, kb, vb, n, mn, mx, false, s_base, s_wc, s_tmp);
+    }
+}
+
+struct BucketPlan {
+    uint32_t shift, nbins;
+};
+
+__device__ __forceinline__ BucketPlan bucket_plan(uint32_t n, uint32_t mn, uint32_t mx, uint32_t max_bins) {
+    const uint32_t range = mx - mn;
+    const uint32_t rbits = range == 0 ? 0u : 32u - __clz(range);
+    uint32_t lbits = 8;
+    while (lbits < 31 && (1u << lbits) < 2u * n) ++lbits;
+    while ((1u << lbits) > max_bins) --lbits;
+    const uint32_t shift = rbits > lbits ? rbits - lbits : 0u;
+    return {shift, (range >> shift) + 1u};  // nbins <= 2^lbits <= max_bins
+}
+
+// Turns bucket counts into bucket starts (exclusive scan, each thread a
+// consecutive run); returns the largest bucket (uniform).
+template <uint32_t THREADS>
+__device__ uint32_t bucket_starts(uint32_t* bins, uint32_t nbins, uint32_t* s_tmp) {
+    constexpr uint32_t WARPS = THREADS / 32;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t per = (nbins + THREADS - 1) / THREADS;
+    const uint32_t b0 = min(nbins, tid * per), b1 = min(nbins, b0 + per);
+    uint32_t run = 0, big = 0;
+    for (uint32_t b = b0; b < b1; ++b) {
+        run += bins[b];
+        big = max(big, bins[b]);
+    }
+    uint32_t incl = run;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += v;
+    }
+    big = __reduce_max_sync(0xffffffffu, big);
+    if (lane == 31) s_tmp[2 * WARPS + warp] = incl;
+    if (lane == 0) s_tmp[3 * WARPS + warp] = big;
+    __syncthreads();
+    uint32_t base = incl - run;
+    for (uint32_t w = 0; w < warp; ++w) base += s_tmp[2 * WARPS + w];
+    for (uint32_t w = 0; w < WARPS; ++w) big = max(big, s_tmp[3 * WARPS + w]);
+    if (big <= kMaxBucket) {
+        for (uint32_t b = b0; b < b1; ++b) {
+            const uint32_t c = bins[b];
+            bins[b] = base;
+            base += c;
+        }
+    }
+    __syncthreads();
+    return big;
+}
+
+// Ranks of the bucketed entries (kb, vb), written as splat ids to
+// out[rank] and the tile id to tids_out.
+template <uint32_t THREADS>
+__device__ void bucket_rank_store(const uint32_t* kb, const uint32_t* vb, const uint32_t* bins, uint32_t n,
+                                  uint32_t mn, uint32_t shift, uint32_t* out, uint32_t* tids_out, uint32_t t) {
+    for (uint32_t i = threadIdx.x; i < n; i += THREADS) {
+        const uint32_t k = kb[i], v = vb[i];
+        const uint32_t b = (k - mn) >> shift;
+        const uint32_t lo = b ? bins[b - 1] : 0u, hi = bins[b];
+        uint32_t rank = lo;
+        for (uint32_t j = lo; j < hi; ++j) {
+            const uint32_t kj = kb[j];
+            rank += (kj < k) || (kj == k && vb[j] < v);
+        }
+        out[rank] = v;
+        if (tids_out) tids_out[i] = t;
+    }
+}
+
+// Shared form: lists of up to MAXN entries, held in registers (ITEMS per
+// thread, all loads in flight together); shared memory holds the bucketed
+// copy (kb, vb) and the buckets.
+template <uint32_t MAXN, uint32_t BINS, uint32_t THREADS>
+__global__ __launch_bounds__(THREADS) void tile_sort_kernel(const uint32_t* __restrict__ list,
+                                                            const uint32_t* list_n,
+                                                            const uint32_t* __restrict__ tile_start,
+                                                            uint32_t capacity, uint2* pairs, uint32_t* ids,
+                                                            uint32_t* tids_out, uint32_t* keys_tmp) {
+    constexpr uint32_t ITEMS = MAXN / THREADS;
+    constexpr uint32_t WARPS = THREADS / 32;
+    static_assert(MAXN % THREADS == 0 && BINS >= 256 + WARPS * 256, "sort shape");
+    if (blockIdx.x >= *list_n) return;
+    extern __shared__ uint32_t sm[];
+    uint32_t* kb = sm;
+    uint32_t* vb = kb + MAXN;
+    uint32_t* bins = vb + MAXN;
+    uint32_t* s_tmp = bins + BINS;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t t = list[blockIdx.x];
+    const uint32_t start = tile_start[t], end = tile_start[t + 1];
+    const uint32_t n = end - start;
+    // The size class and the capacity check before this launch keep both
+    // conditions false; they guard the shared and global bounds regardless.
+    if (n > MAXN || end > capacity || end < start) return;
+    uint32_t k[ITEMS], v[ITEMS];
+    uint32_t lo = 0xffffffffu, hi = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < ITEMS; ++j) {
+        const uint32_t i = tid + j * THREADS;
+        k[j] = 0;
+        v[j] = 0;
+        if (i < n) {
+            const uint2 p = pairs[start + i];
+            k[j] = p.x;
+            v[j] = p.y;
+        }
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < ITEMS; ++j)
+        if (tid + j * THREADS < n) {
+            lo = min(lo, k[j]);
+            hi = max(hi, k[j]);
+        }
+    uint32_t mn, mx;
+    block_min_max<THREADS>(lo, hi, s_tmp, mn, mx);
+    const BucketPlan bp = bucket_plan(n, mn, mx, BINS);
+    for (uint32_t b = tid; b < bp.nbins; b += THREADS) bins[b] = 0;
+    __syncthreads();
+#pragma unroll
+    for (uint32_t j = 0; j < ITEMS; ++j)
+        if (tid + j * THREADS < n) atomicAdd(&bins[(k[j] - mn) >> bp.shift], 1u);
+    __syncthreads();
+    const uint32_t big = bucket_starts<THREADS>(bins, bp.nbins, s_tmp);
+    if (big > kMaxBucket) {
+        // Bunched keys: radix sort in the tile's global ranges.
+        uint32_t* ka = keys_tmp + start;
+        uint32_t* va = ids + start;
+#pragma unroll
+        for (uint32_t j = 0; j < ITEMS; ++j) {
+            const uint32_t i = tid + j * THREADS;
+            if (i < n) {
+                ka[i] = k[j];
+                va[i] = v[j];
+            }
+        }
+        uint32_t* gkb = reinterpret_cast<uint32_t*>(pairs + start);
+        radix_tile<THREADS>(ka, va, gkb, gkb + n, n, mn, mx, bins, s_tmp);
+        if (tids_out)
+            for (uint32_t i = tid; i < n; i += THREADS) tids_out[start + i] = t;
+        return;
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < ITEMS; ++j)
+        if (tid + j * THREADS < n) {
+            const uint32_t pos = atomicAdd(&bins[(k[j] - mn) >> bp.shift], 1u);
+            kb[pos] = k[j];
+            vb[pos] = v[j];
+        }
+    __syncthreads();
+    // bins[b] is now the end of bucket b.
+    bucket_rank_store<THREADS>(kb, vb, bins, n, mn, bp.shift, ids + start, tids_out ? tids_out + start : nullptr,
+                               t);
+}
+
+// Global form, lists longer than the largest shared class: the entries stay
+// in the tile's global ranges ((keys_tmp, ids) and the pair buffer as
+// scratch), only the buckets are in shared memory.
+template <uint32_t BINS, uint32_t THREADS>
+__global__ __launch_bounds__(THREADS) void tile_sort_global_kernel(const uint32_t* __restrict__ list,
+                                                                   const uint32_t* list_n,
+                                                                   const uint32_t* __restrict__ tile_start,
+                                                                   uint32_t capacity, uint2* pairs, uint32_t* ids,
+                                                                   uint32_t* tids_out, uint32_t* keys_tmp) {
+    if (blockIdx.x >= *list_n) return;
+    extern __shared__ uint32_t sm[];
+    uint32_t* bins = sm;
+    uint32_t* s_tmp = bins + BINS;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t t = list[blockIdx.x];
+    const uint32_t start = tile_start[t], end = tile_start[t + 1];
+    const uint32_t n = end - start;
+    if (end > capacity || end < start) return;
+    uint32_t* ka = keys_tmp + start;
+    uint32_t* va = ids + start;
+    uint32_t* kb = reinterpret_cast<uint32_t*>(pairs + start);
+    uint32_t* vb = kb + n;
+    uint32_t lo = 0xffffffffu, hi = 0;
+    for (uint32_t i = tid; i < n; i += THREADS) {
+        const uint2 p = pairs[start + i];
+        ka[i] = p.x;
+        va[i] = p.y;
+        lo = min(lo, p.x);
+        hi = max(hi, p.x);
+    }
+    uint32_t mn, mx;
+    block_min_max<THREADS>(lo, hi, s_tmp, mn, mx);  // its barriers also order the copies above
+    const BucketPlan bp = bucket_plan(n, mn, mx, BINS);
+    for (uint32_t b = tid; b < bp.nbins; b += THREADS) bins[b] = 0;
+    __syncthreads();
+    for (uint32_t i = tid; i < n; i += THREADS) atomicAdd(&bins[(ka[i] - mn) >> bp.shift], 1u);
+    __syncthreads();
+    const uint32_t big = bucket_starts<THREADS>(bins, bp.nbins, s_tmp);
+    if (big > kMaxBucket) {
+        radix_tile<THREADS>(ka, va, kb, vb, n, mn, mx, bins, s_tmp);
+        if (tids_out)
+            for (uint32_t i = tid; i < n; i += THREADS) tids_out[start + i] = t;
+        return;
+    }
+    for (uint32_t i = tid; i < n; i += THREADS) {
+        const uint32_t pos = atomicAdd(&bins[(ka[i] - mn) >> bp.shift], 1u);
+        kb[pos] = ka[i];
+        vb[pos] = va[i];
+    }
+    __syncthreads();
+    bucket_rank_store<THREADS>(kb, vb, bins, n, mn, bp.shift, va, tids_out ? tids_out + start : nullptr, t);
+}
+
+template <uint32_t MAXN, uint32_t BINS, uint32_t THREADS>
+constexpr size_t sort_smem() {
+    return (2ull * MAXN + BINS + 4 * (THREADS / 32)) * 4;
+}
+
+// Size classes of the shared-form sort (entries, buckets, threads); longer
+// lists take the global form.
+constexpr uint32_t kClass0 = 2048, kClass1 = 6144, kClass2 = 12288;
+constexpr uint32_t kBins0 = 4096, kBins1 = 8192, kBins2 = 16384, kBinsGiant = 32768;
+constexpr uint32_t kThreads0 = 256, kThreads1 = 512, kThreads2 = 1024;
+static_assert(sort_smem<kClass2, kBins2, kThreads2>() <= 227 * 1024, "per-tile sort exceeds shared memory");
+
+template <typename K>
+cudaError_t launch_sort_kernel(K kernel, uint32_t threads, size_t smem, uint32_t grid, const uint32_t* list,
+                               const uint32_t* list_n, const uint32_t* tile_start, uint32_t capacity, uint2* pairs,
+                               uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, cudaStream_t st) {
+    if (grid == 0) return cudaSuccess;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    kernel<<<grid, threads, smem, st>>>(list, list_n, tile_start, capacity, pairs, ids, tids_out, keys_tmp);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t smem_opt_in(const void* fn, size_t smem) {
+    if (smem <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+}  // namespace
+
+uint32_t bin_chunks(uint32_t n, int sm_count) {
+    const uint32_t c = (uint32_t)std::max(1, 2 * sm_count);
+    return std::max(1u, std::min(c, (n + 31) / 32));
+}
+
+uint32_t bin_chunk_size(uint32_t n, uint32_t chunks) { return ((n + chunks - 1) / chunks + 31) / 32 * 32; }
+
+uint32_t bin_class_limit(int k) { return k == 0 ? kClass0 : k == 1 ? kClass1 : kClass2; }
+
+cudaError_t launch_bin_count(const uint2* bbox, uint32_t n, uint32_t tiles_x, uint32_t tiles, uint32_t chunks,
+                             uint32_t* hist, cudaStream_t st) {
+    const size_t smem = (size_t)tiles * 4;
+    cudaError_t e = smem_opt_in((const void*)bin_count_kernel, smem);
+    if (e != cudaSuccess) return e;
+    bin_count_kernel<<<chunks, kBinThreads, smem, st>>>(bbox, n, bin_chunk_size(n, chunks), tiles_x, tiles, hist);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bin_colscan(uint32_t* hist, uint32_t chunks, uint32_t tiles, uint32_t* cnt, uint32_t* lists,
+                               uint32_t* words, cudaStream_t st) {
+    bin_colscan_kernel<<<(tiles + 31) / 32, dim3(32, 32), 0, st>>>(hist, chunks, tiles, cnt, lists, words,
+                                                                   kClass0, kClass1, kClass2);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bin_place(const uint2* bbox, const uint32_t* depth_keys, uint32_t n, uint32_t tiles_x,
+                             uint32_t tiles, uint32_t chunks, const uint32_t* hist, const uint32_t* tile_start,
+                             uint32_t capacity, uint2* pairs, uint32_t* err, cudaStream_t st) {
+    const size_t smem = (size_t)tiles * 4;
+    cudaError_t e = smem_opt_in((const void*)bin_place_kernel, smem);
+    if (e != cudaSuccess) return e;
+    bin_place_kernel<<<chunks, kBinThreads, smem, st>>>(bbox, depth_keys, n, bin_chunk_size(n, chunks), tiles_x,
+                                                        tiles, hist, tile_start, capacity, pairs, err);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tile_sorts(const uint32_t grids[4], const uint32_t* lists, const uint32_t* words,
+                              uint32_t tiles, const uint32_t* tile_start, uint32_t capacity, uint2* pairs,
+                              uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, cudaStream_t st) {
+    cudaError_t e;
+    // Each form reads and overwrites only its own tiles' ranges.
+    e = launch_sort_kernel(tile_sort_global_kernel<kBinsGiant, 512>, 512, (kBinsGiant + 64) * 4, grids[3],
+                           lists + 3 * (size_t)tiles, words + 7, tile_start, capacity, pairs, ids, tids_out,
+                           keys_tmp, st);
+    if (e != cudaSuccess) return e;
+    e = launch_sort_kernel(tile_sort_kernel<kClass0, kBins0, kThreads0>, kThreads0,
+                           sort_smem<kClass0, kBins0, kThreads0>(), grids[0], lists, words + 8, tile_start,
+                           capacity, pairs, ids, tids_out, keys_tmp, st);
+    if (e != cudaSuccess) return e;
+    e = launch_sort_kernel(tile_sort_kernel<kClass1, kBins1, kThreads1>, kThreads1,
+                           sort_smem<kClass1, kBins1, kThreads1>(), grids[1], lists + tiles, words + 9, tile_start,
+                           capacity, pairs, ids, tids_out, keys_tmp, st);
+    if (e != cudaSuccess) return e;
+    return launch_sort_kernel(tile_sort_kernel<kClass2, kBins2, kThreads2>, kThreads2,
+                              sort_smem<kClass2, kBins2, kThreads2>(), grids[2], lists + 2 * (size_t)tiles,
+                              words + 10, tile_start, capacity, pairs, ids, tids_out, keys_tmp, st);
+}
+
+}  // namespace sfk

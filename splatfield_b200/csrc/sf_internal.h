@@ -115,6 +115,34 @@ cudaError_t exclusive_scan(const uint32_t* gids, const uint32_t* counts, uint32_
                            const uint32_t* n_dev, uint32_t max_n, void* temp,
                            unsigned long long* total_out, uint32_t* err, cudaStream_t stream);
 
+// ---- binned intersection build (sf_bin.cu)
+// Tiles per frame the binned build handles (one u32 shared-memory counter
+// per tile in the count and place kernels).
+constexpr uint32_t kBinMaxTiles = 49152;
+uint32_t bin_chunks(uint32_t n, int sm_count);
+uint32_t bin_class_limit(int k);  // largest tile list sorted by size class k (0..2)
+// hist: [chunks][tiles] counts, then (after colscan) per-chunk exclusive
+// prefixes. cnt: [tiles + 1] per-tile totals (cnt[tiles] = 0). lists:
+// [4][tiles] tiles of each size class. words: [6] max tile total, [7] tiles
+// longer than the shared-memory classes, [8..10] tiles per shared class (all
+// zero on entry).
+cudaError_t launch_bin_count(const uint2* bbox, uint32_t n, uint32_t tiles_x, uint32_t tiles, uint32_t chunks,
+                             uint32_t* hist, cudaStream_t st);
+cudaError_t launch_bin_colscan(uint32_t* hist, uint32_t chunks, uint32_t tiles, uint32_t* cnt, uint32_t* lists,
+                               uint32_t* words, cudaStream_t st);
+cudaError_t launch_bin_place(const uint2* bbox, const uint32_t* depth_keys, uint32_t n, uint32_t tiles_x,
+                             uint32_t tiles, uint32_t chunks, const uint32_t* hist, const uint32_t* tile_start,
+                             uint32_t capacity, uint2* pairs, uint32_t* err, cudaStream_t st);
+// grids[k]: CTAs launched for class k (the class count when the host knows
+// it, else `tiles`; CTAs past the device count exit).
+// pairs: the placed (depth key, splat id) per slot (overwritten for the
+// longest lists); ids / tids_out receive the sorted splat ids / tile ids
+// (tids_out may be null); keys_tmp: capacity u32 of scratch (may alias
+// tids_out). grids[0..2]: shared classes, grids[3]: longer lists.
+cudaError_t launch_tile_sorts(const uint32_t grids[4], const uint32_t* lists, const uint32_t* words,
+                              uint32_t tiles, const uint32_t* tile_start, uint32_t capacity, uint2* pairs,
+                              uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, cudaStream_t st);
+
 // ---- segmentation (sf_seg.cu)
 constexpr int kGridPts = 445;
 constexpr float kLnStep = 0.015611423f;

@@ -1,0 +1,87 @@
+"""The binned intersection build (per-tile counts, place, per-tile shared-memory
+sort) against the oracle's reference-order build (depth argsort, scan, emit,
+stable tile sort; src/render.rs:318-352): sorted splat ids, tile ids and tile
+starts bit-identical, across every per-tile sort size class, with exact depth
+ties, and for tile lists too long for the shared-memory sort (GPU)."""
+import numpy as np
+import pytest
+
+import splatfield_b200 as sf
+from splatfield_b200 import _lib as L
+from splatfield_b200 import synth
+
+from helpers import opaque, zero_sh
+
+pytestmark = pytest.mark.gpu
+
+
+def build_both(oracle_mod, attr, sh, k, w, h, cam_pos=(0.0, 0.0, -3.0)):
+    O = oracle_mod
+    cam_o = O.look_at(cam_pos, (0.0, 0.0, 0.0))
+    cam_o.fov[0], cam_o.fov[1] = synth.fov_for(w, h)
+    cam = sf.look_at(cam_pos, (0.0, 0.0, 0.0))
+    cam.fov[0], cam.fov[1] = synth.fov_for(w, h)
+    want = O.prepare(cam_o, w, h, attr, sh, k)
+    n = attr.size // 11
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    scratch.set_tuning(isect_build=sf.ISECTS_BINNED)
+    isects = splats.prepare_isects(scratch, cam, (w, h))
+    tiles = isects.tile_bounds[0] * isects.tile_bounds[1]
+    got = dict(gaussian_ids=isects.gaussian_ids().read(), tile_ids=isects.tile_ids().read(),
+               tile_start=scratch.read(L.READ_TILE_START, tiles + 1), num_isects=isects.num_isects)
+    img = splats.finalize_rgb(scratch, isects, (w, h)).read()
+    want_img = O.rasterize(want, 0)["bitmap"]
+    return got, want, img, want_img
+
+
+def check(got, want, img, want_img):
+    assert got["num_isects"] == want["num_isects"]
+    np.testing.assert_array_equal(got["gaussian_ids"], want["gaussian_ids"])
+    np.testing.assert_array_equal(got["tile_ids"], want["tile_ids"])
+    np.testing.assert_array_equal(got["tile_start"][:-1], want["ranges"][:, 0])
+    np.testing.assert_array_equal(got["tile_start"][1:], want["ranges"][:, 1])
+    np.testing.assert_array_equal(img, want_img)
+
+
+def test_binned_covers_every_sort_class(ctx, oracle_mod):
+    """A dense cluster: tile lists from a handful to ~9k entries, so the
+    2048-, 6144- and 12288-entry sorts all run."""
+    n, w, h = 40000, 256, 256
+    attr, sh = synth.scene_clustered(n, 4, seed=31, clusters=1, sigma=0.25, extent=1.0)
+    got, want, img, want_img = build_both(oracle_mod, attr, sh, 4, w, h)
+    lens = np.diff(got["tile_start"])
+    assert lens.max() > 6144 and lens.max() <= 12288, lens.max()
+    assert ((lens > 2048) & (lens <= 6144)).any() and ((lens > 0) & (lens <= 2048)).any()
+    check(got, want, img, want_img)
+
+
+def test_binned_orders_exact_depth_ties_by_id(ctx, oracle_mod):
+    """Depths quantised to a few values: most tiles hold runs of equal depth
+    keys (buckets past the bucket sort's limit, so the per-tile radix sort
+    with its id passes runs), ordered by splat id as the reference's stable
+    depth sort does."""
+    n, w, h = 20000, 192, 160
+    attr, sh = synth.scene_uniform(n, 1, 32)
+    a = attr.reshape(11, n)
+    a[2] = np.round(a[2] * 4.0) / 4.0
+    got, want, img, want_img = build_both(oracle_mod, a.reshape(-1), sh, 1, w, h)
+    check(got, want, img, want_img)
+
+
+@pytest.mark.parametrize("quantised", [False, True])
+def test_binned_sorts_lists_beyond_shared_memory(ctx, oracle_mod, quantised):
+    """20,000 splats over one spot: the centre tiles' lists exceed the
+    largest shared-memory sort and are sorted in global memory. With depths
+    quantised to 5 values the buckets overflow and the global-memory radix
+    sort with its id passes runs."""
+    n = 20000
+    rng = np.random.default_rng(33)
+    z = rng.uniform(0, 1, n)
+    if quantised:
+        z = np.round(z * 4.0) / 4.0
+    pos = np.stack([rng.normal(0, 0.002, n), rng.normal(0, 0.002, n), 1.0 + z], 1)
+    attr = opaque(pos)
+    got, want, img, want_img = build_both(oracle_mod, attr, zero_sh(n), 1, 64, 64)
+    assert np.diff(got["tile_start"]).max() > 12288
+    check(got, want, img, want_img)

@@ -23,13 +23,16 @@ def gpu_frame(splats, scratch, cam, w, h, n):
     rgba_f = sf.DeviceView(scratch.rgba_ptr(), np.float32, (h, w, 4)).read()
     V, I = isects.num_visible, isects.num_isects
     tiles = isects.tile_bounds[0] * isects.tile_bounds[1]
+    depth_sorted = scratch.get_tuning()["isect_build"] == sf.ISECTS_DEPTH_SORTED
     return dict(
         depth_keys=scratch.read(L.READ_DEPTH_KEYS, n),
         tile_counts=scratch.read(L.READ_TILE_COUNTS, n),
         bbox=scratch.read(L.READ_BBOX, 2 * n),
         projected=scratch.read(L.READ_PROJECTED, 9 * n, np.float32).reshape(n, 9),
-        order=scratch.read(L.READ_ORDER, V),
-        offsets=scratch.read(L.READ_OFFSETS, V),
+        # The binned build keeps no depth order or offsets (they are not on
+        # its path); the depth-sorted build is checked on them.
+        order=scratch.read(L.READ_ORDER, V) if depth_sorted else None,
+        offsets=scratch.read(L.READ_OFFSETS, V) if depth_sorted else None,
         tile_ids=isects.tile_ids().read(),
         gaussian_ids=isects.gaussian_ids().read(),
         tile_start=scratch.read(L.READ_TILE_START, tiles + 1),
@@ -43,8 +46,9 @@ def assert_frame_equal(got, want):
     np.testing.assert_array_equal(got["projected"].view(np.uint32), want["projected"].view(np.uint32))
     assert got["num_visible"] == want["num_visible"]
     assert got["num_isects"] == want["num_isects"]
-    np.testing.assert_array_equal(got["order"], want["order"])
-    np.testing.assert_array_equal(got["offsets"], want["offsets"])
+    if got["order"] is not None:
+        np.testing.assert_array_equal(got["order"], want["order"])
+        np.testing.assert_array_equal(got["offsets"], want["offsets"])
     np.testing.assert_array_equal(got["tile_ids"], want["tile_ids"])
     np.testing.assert_array_equal(got["gaussian_ids"], want["gaussian_ids"])
     ranges = want["ranges"]
@@ -52,6 +56,10 @@ def assert_frame_equal(got, want):
     np.testing.assert_array_equal(got["tile_start"][1:], ranges[:, 1])
 
 
+BUILDS = [sf.ISECTS_BINNED, sf.ISECTS_DEPTH_SORTED]
+
+
+@pytest.mark.parametrize("build", BUILDS)
 @pytest.mark.parametrize("cull", [0, 1])
 @pytest.mark.parametrize("n,k,w,h,seed", [
     (2000, 1, 128, 128, 1),
@@ -59,7 +67,7 @@ def assert_frame_equal(got, want):
     (50000, 16, 320, 240, 3),
     (30000, 9, 70, 70, 4),
 ])
-def test_frame_bit_exact_vs_oracle(ctx, oracle_mod, n, k, w, h, seed, cull):
+def test_frame_bit_exact_vs_oracle(ctx, oracle_mod, n, k, w, h, seed, cull, build):
     O = oracle_mod
     from splatfield_b200 import synth
 
@@ -72,14 +80,15 @@ def test_frame_bit_exact_vs_oracle(ctx, oracle_mod, n, k, w, h, seed, cull):
     wr = O.rasterize(want, 0)
     splats = sf.Splats(attr, sh)
     scratch = sf.RenderScratch(n, (w, h))
-    scratch.set_tuning(raster_cull=cull)
+    scratch.set_tuning(raster_cull=cull, isect_build=build)
     got = gpu_frame(splats, scratch, cam, w, h, n)
     assert_frame_equal(got, want)
     np.testing.assert_array_equal(got["bitmap"], wr["bitmap"])
     np.testing.assert_array_equal(got["rgba"].view(np.uint32), wr["rgba"].view(np.uint32))
 
 
-def test_full_size_frame_bit_exact_vs_oracle(ctx, oracle_mod):
+@pytest.mark.parametrize("build", BUILDS)
+def test_full_size_frame_bit_exact_vs_oracle(ctx, oracle_mod, build):
     """The bench workload itself: 1M SH3 splats in 8 clusters, 1920x1080, one
     orbit camera. Every intermediate array and the image, bit for bit."""
     O = oracle_mod
@@ -93,6 +102,7 @@ def test_full_size_frame_bit_exact_vs_oracle(ctx, oracle_mod):
     wr = O.rasterize(want, 0)
     splats = sf.Splats(attr, sh)
     scratch = sf.RenderScratch(n, (w, h))
+    scratch.set_tuning(isect_build=build)
     got = gpu_frame(splats, scratch, cam, w, h, n)
     assert got["num_isects"] > (1 << 22)
     assert_frame_equal(got, want)
