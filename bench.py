@@ -3,8 +3,9 @@
 Headline workload ("frame"): 1M splats, SH degree 3 (16 coefficients per
 channel), means from 8 Gaussian clusters, 1920x1080, cameras on a 30-view
 radius-4 orbit. A step renders one frame through the reference-facing API
-(Splats::render_with: project, onesweep depth sort, look-back scan, emit,
-tile sort, rasterize, with its one host sync for the intersection total).
+(Splats::render_with: project, binned intersection build (per-tile counts,
+placement, per-tile sort by depth), rasterize, with its one host sync for the
+intersection total).
 
   value   frames/s, all ranks, device-timed with CUDA events on the launch
           stream, inputs resident in HBM (236 MB of splat planes > 126 MB L2,
@@ -12,9 +13,13 @@ tile sort, rasterize, with its one host sync for the intersection total).
   e2e     the same frames through sf_render_to_host: the camera goes in from
           host memory and each frame's RGBA8 image comes back into pinned
           host memory inside the timed region (wall clock);
-  roofline the rasterizer (the dominant kernel) against the FP32 pipe: 24
+  roofline the rasterizer (the largest kernel) against the FP32 pipe: 24
           FP32 operations per visited (pixel, splat) pair, pairs counted by
           the kernel itself;
+  backward the adjoint (forward that keeps per-pixel state, then the
+          backward) on one frame of the same scene;
+  eig_round a 20-view 512x512 segmentation round, batched into one CUDA
+          graph vs the plain per-view calls;
   cpu_baseline the CPU oracle (a C++/OpenMP restatement of the reference's
           kernels) on one frame of the same workload on this host's cores.
 
@@ -184,6 +189,84 @@ def time_backward(sf, splats, scratch, attr, sh, cam, stream, args):
                     "contributor), backward = sf_render_backward into device gradient buffers"}
 
 
+ROUND_VIEWS, ROUND_SIDE, ROUND_RADIUS = 20, 512, 3.5
+
+
+def time_eig_round(sf, splats, ctx, stream, args):
+    """Segmentation round on the frame scene: 20 candidate views at 512x512 on
+    a radius-3.5 sphere, posterior a, b log-uniform in [1, 1024]. Per view the
+    responsibility render and its EIG.
+
+    plain   the reference's Segmenter::select_view loop: per view
+            sf_render_responsibility (one host sync for the intersection
+            total) then sf_beta_eig (one sync for the sum);
+    batched sf_round_eig: all views in one CUDA graph, one sync per round
+            (lanes and raster form chosen by sf_round_autotune, untimed).
+    The evidence form renders each view's fg / bg words under a 1-3 ellipse
+    mask (prepare + masked sf_accumulate_prepared per view vs
+    sf_round_evidence), each arm reading a sample of every view's fg words.
+    Rounds are timed on the host clock around a synchronised round (the plain
+    path's host syncs are part of its cost); results must agree exactly."""
+    import torch
+
+    from splatfield_b200 import synth
+
+    size = (ROUND_SIDE, ROUND_SIDE)
+    a, b = synth.beta_posterior(N_SPLATS, seed=1)
+    beta = sf.BetaState.from_host(a, b, ctx)
+    cams = synth.sphere_cameras(ROUND_VIEWS, ROUND_RADIUS, 2, sf.look_at)
+    masks = [sf.Mask.from_bytes(size, synth.ellipse_mask(ROUND_SIDE, ROUND_SIDE, seed=100 + v), ctx)
+             for v in range(ROUND_VIEWS)]
+    scratch = sf.RenderScratch(N_SPLATS, size, ctx)
+    acc = sf.Accumulators(N_SPLATS, ctx)
+    rnd = sf.Round(N_SPLATS, [size] * ROUND_VIEWS, ctx)
+    reps = max(3, min(args.steps // 100, 15))
+
+    def plain_round(mode, evidence):
+        out = []
+        for v in range(ROUND_VIEWS):
+            if evidence:
+                isects = splats.prepare_isects(scratch, cams[v], size, stream=stream)
+                splats.accumulate_prepared(scratch, isects, size, acc, masks[v], stream=stream)
+                out.append(acc.fg.read(stream)[::997])
+            else:
+                splats.render_responsibility(scratch, acc, cams[v], size, stream=stream)
+                out.append(beta.eig(acc, mode, stream=stream))
+        return np.array(out)
+
+    def batched_round(mode, evidence):
+        if evidence:
+            rnd.evidence(splats, None, cams, masks, mode, stream=stream)
+            return np.array([rnd.evidence_words(v)[0].read(stream)[::997] for v in range(ROUND_VIEWS)])
+        return rnd.eig(splats, beta, cams, mode, stream=stream)
+
+    def timed(fn, *a):
+        fn(*a)
+        times = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn(*a)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        return float(np.median(times)), out
+
+    tuning, tune_ms = rnd.autotune(splats, beta, cams, sf.EIG_FP64, stream=stream)
+    result = {"workload": f"round: frame scene, {ROUND_VIEWS} views {ROUND_SIDE}x{ROUND_SIDE} on a "
+                          f"radius-{ROUND_RADIUS} sphere, a,b log-uniform [1,1024]",
+              "tuning": tuning, "reps": reps}
+    for name, mode, evidence in (("responsibility_lut_f32", sf.EIG_LUT_F32, False),
+                                 ("responsibility_fp64", sf.EIG_FP64, False),
+                                 ("evidence", sf.EIG_LUT_F32, True)):
+        tp, ep = timed(plain_round, mode, evidence)
+        tb, eb = timed(batched_round, mode, evidence)
+        result[name] = {
+            "plain_views_per_s": ROUND_VIEWS / tp, "batched_views_per_s": ROUND_VIEWS / tb,
+            "plain_ms_per_round": 1e3 * tp, "batched_ms_per_round": 1e3 * tb, "speedup": tp / tb,
+            ("words_identical" if evidence else "eig_identical"): bool(np.array_equal(ep, eb))}
+    return result
+
+
 def run_reference(args, rank, world):
     """The reference arm: the CPU implementation of the path on this host."""
     if rank != 0:
@@ -324,6 +407,7 @@ def run_ours(args, rank, world):
     e2e_fps = world * args.steps / e2e_s
 
     bwd = time_backward(sf, splats, scratch, attr, sh, my_cams[0], stream, args)
+    eig_round = time_eig_round(sf, splats, ctx, stream, args)
 
     if rank != 0:
         return
@@ -355,6 +439,7 @@ def run_ours(args, rank, world):
         "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "frames/s", "cores": cores, "kind": "port",
                          "sample": f"{cpu_frames} full frame(s) of the workload, median"},
         "backward": bwd,
+        "eig_round": eig_round,
         "clocks": clk,
         "gpu_launches": int(launches),
         "peaks": {"source": which, "hbm_gbs": peaks.get("hbm_gbs")},

@@ -298,7 +298,8 @@ typedef struct sf_round_t* sf_round;
 typedef struct {
     uint32_t lanes;       /* capture streams the views are spread over (1..64) */
     uint32_t raster_cull; /* as sf_tuning.raster_cull */
-    uint32_t reserved[6];
+    uint32_t isect_build; /* as sf_tuning.isect_build */
+    uint32_t reserved[5];
 } sf_round_tuning;
 int sf_round_create(sf_ctx ctx, uint32_t total, uint32_t n_views, const uint32_t* widths,
                     const uint32_t* heights, sf_round* out);

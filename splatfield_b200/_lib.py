@@ -58,7 +58,8 @@ class Tuning(C.Structure):
 class RoundTuning(C.Structure):
     """sf_round_tuning."""
 
-    _fields_ = [("lanes", C.c_uint32), ("raster_cull", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+    _fields_ = [("lanes", C.c_uint32), ("raster_cull", C.c_uint32), ("isect_build", C.c_uint32),
+                ("reserved", C.c_uint32 * 5)]
 
 
 class Isects(C.Structure):

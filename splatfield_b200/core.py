@@ -626,15 +626,15 @@ class Round:
     def views(self) -> int:
         return len(self.sizes)
 
-    def set_tuning(self, lanes: int = 4, raster_cull: int = 0) -> None:
+    def set_tuning(self, lanes: int = 4, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED) -> None:
         t = L.RoundTuning()
-        t.lanes, t.raster_cull = int(lanes), int(raster_cull)
+        t.lanes, t.raster_cull, t.isect_build = int(lanes), int(raster_cull), int(isect_build)
         check(lib().sf_round_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:
         t = L.RoundTuning()
         check(lib().sf_round_get_tuning(self.handle, C.byref(t)))
-        return {"lanes": int(t.lanes), "raster_cull": int(t.raster_cull)}
+        return {"lanes": int(t.lanes), "raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build)}
 
     @staticmethod
     def _cams(cameras):
@@ -689,7 +689,8 @@ class Round:
         ms = C.c_double()
         check(lib().sf_round_autotune(self.handle, splats.handle, beta.handle if beta else None,
                                       self._cams(cameras), mode, _stream(stream), C.byref(t), C.byref(ms)))
-        return {"lanes": int(t.lanes), "raster_cull": int(t.raster_cull)}, float(ms.value)
+        return ({"lanes": int(t.lanes), "raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build)},
+                float(ms.value))
 
     def close(self):
         if getattr(self, "handle", None):

@@ -308,7 +308,7 @@ int prepare_binned(sf_scratch s, uint32_t n, uint32_t tiles, cudaStream_t st, bo
                            s->tile_start, (uint32_t)s->cap, pairs, words + 1, st));
     const uint32_t grids[4] = {hw[8], hw[9], hw[10], hw[7]};
     SF_CK(launch_tile_sorts(grids, s->bin_lists, words, tiles, s->tile_start, (uint32_t)s->cap, pairs, s->gid_e,
-                            want_tile_ids ? s->tid_e : nullptr, s->tid_e, st));
+                            want_tile_ids ? s->tid_e : nullptr, s->tid_e, s->ctx->sm_count, st));
     s->tids = want_tile_ids ? s->tid_e : nullptr;
     s->gids = s->gid_e;
     s->num_isects = (uint32_t)total;

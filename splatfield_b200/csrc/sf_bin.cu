@@ -430,22 +430,17 @@ __device__ void bucket_rank_store(const uint32_t* kb, const uint32_t* vb, const 
 // thread, all loads in flight together); shared memory holds the bucketed
 // copy (kb, vb) and the buckets.
 template <uint32_t MAXN, uint32_t BINS, uint32_t THREADS>
-__global__ __launch_bounds__(THREADS) void tile_sort_kernel(const uint32_t* __restrict__ list,
-                                                            const uint32_t* list_n,
-                                                            const uint32_t* __restrict__ tile_start,
-                                                            uint32_t capacity, uint2* pairs, uint32_t* ids,
-                                                            uint32_t* tids_out, uint32_t* keys_tmp) {
+__device__ void sort_tile_shared(uint32_t t, const uint32_t* __restrict__ tile_start, uint32_t capacity,
+                                 uint2* pairs, uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp,
+                                 uint32_t* sm) {
     constexpr uint32_t ITEMS = MAXN / THREADS;
     constexpr uint32_t WARPS = THREADS / 32;
     static_assert(MAXN % THREADS == 0 && BINS >= 256 + WARPS * 256, "sort shape");
-    if (blockIdx.x >= *list_n) return;
-    extern __shared__ uint32_t sm[];
     uint32_t* kb = sm;
     uint32_t* vb = kb + MAXN;
     uint32_t* bins = vb + MAXN;
     uint32_t* s_tmp = bins + BINS;
     const uint32_t tid = threadIdx.x;
-    const uint32_t t = list[blockIdx.x];
     const uint32_t start = tile_start[t], end = tile_start[t + 1];
     const uint32_t n = end - start;
     // The size class and the capacity check before this launch keep both
@@ -511,21 +506,31 @@ __global__ __launch_bounds__(THREADS) void tile_sort_kernel(const uint32_t* __re
                                t);
 }
 
+// Persistent: each CTA takes the class's tiles in turn.
+template <uint32_t MAXN, uint32_t BINS, uint32_t THREADS>
+__global__ __launch_bounds__(THREADS) void tile_sort_kernel(const uint32_t* __restrict__ list,
+                                                            const uint32_t* list_n,
+                                                            const uint32_t* __restrict__ tile_start,
+                                                            uint32_t capacity, uint2* pairs, uint32_t* ids,
+                                                            uint32_t* tids_out, uint32_t* keys_tmp) {
+    extern __shared__ uint32_t sm[];
+    const uint32_t count = *list_n;
+    for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+        sort_tile_shared<MAXN, BINS, THREADS>(list[idx], tile_start, capacity, pairs, ids, tids_out, keys_tmp, sm);
+        __syncthreads();
+    }
+}
+
 // Global form, lists longer than the largest shared class: the entries stay
 // in the tile's global ranges ((keys_tmp, ids) and the pair buffer as
 // scratch), only the buckets are in shared memory.
 template <uint32_t BINS, uint32_t THREADS>
-__global__ __launch_bounds__(THREADS) void tile_sort_global_kernel(const uint32_t* __restrict__ list,
-                                                                   const uint32_t* list_n,
-                                                                   const uint32_t* __restrict__ tile_start,
-                                                                   uint32_t capacity, uint2* pairs, uint32_t* ids,
-                                                                   uint32_t* tids_out, uint32_t* keys_tmp) {
-    if (blockIdx.x >= *list_n) return;
-    extern __shared__ uint32_t sm[];
+__device__ void sort_tile_global(uint32_t t, const uint32_t* __restrict__ tile_start, uint32_t capacity,
+                                 uint2* pairs, uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp,
+                                 uint32_t* sm) {
     uint32_t* bins = sm;
     uint32_t* s_tmp = bins + BINS;
     const uint32_t tid = threadIdx.x;
-    const uint32_t t = list[blockIdx.x];
     const uint32_t start = tile_start[t], end = tile_start[t + 1];
     const uint32_t n = end - start;
     if (end > capacity || end < start) return;
@@ -564,6 +569,20 @@ __global__ __launch_bounds__(THREADS) void tile_sort_global_kernel(const uint32_
     bucket_rank_store<THREADS>(kb, vb, bins, n, mn, bp.shift, va, tids_out ? tids_out + start : nullptr, t);
 }
 
+template <uint32_t BINS, uint32_t THREADS>
+__global__ __launch_bounds__(THREADS, 1) void tile_sort_global_kernel(const uint32_t* __restrict__ list,
+                                                                   const uint32_t* list_n,
+                                                                   const uint32_t* __restrict__ tile_start,
+                                                                   uint32_t capacity, uint2* pairs, uint32_t* ids,
+                                                                   uint32_t* tids_out, uint32_t* keys_tmp) {
+    extern __shared__ uint32_t sm[];
+    const uint32_t count = *list_n;
+    for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+        sort_tile_global<BINS, THREADS>(list[idx], tile_start, capacity, pairs, ids, tids_out, keys_tmp, sm);
+        __syncthreads();
+    }
+}
+
 template <uint32_t MAXN, uint32_t BINS, uint32_t THREADS>
 constexpr size_t sort_smem() {
     return (2ull * MAXN + BINS + 4 * (THREADS / 32)) * 4;
@@ -576,11 +595,17 @@ constexpr uint32_t kBins0 = 4096, kBins1 = 8192, kBins2 = 16384, kBinsGiant = 32
 constexpr uint32_t kThreads0 = 256, kThreads1 = 512, kThreads2 = 1024;
 static_assert(sort_smem<kClass2, kBins2, kThreads2>() <= 227 * 1024, "per-tile sort exceeds shared memory");
 
+// grid: the class's tile count when the host knows it, else an upper bound;
+// capped at the CTAs resident at once (the kernels loop over their tiles).
 template <typename K>
-cudaError_t launch_sort_kernel(K kernel, uint32_t threads, size_t smem, uint32_t grid, const uint32_t* list,
-                               const uint32_t* list_n, const uint32_t* tile_start, uint32_t capacity, uint2* pairs,
-                               uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, cudaStream_t st) {
+cudaError_t launch_sort_kernel(K kernel, uint32_t threads, size_t smem, uint32_t grid, int sm_count,
+                               const uint32_t* list, const uint32_t* list_n, const uint32_t* tile_start,
+                               uint32_t capacity, uint2* pairs, uint32_t* ids, uint32_t* tids_out,
+                               uint32_t* keys_tmp, cudaStream_t st) {
     if (grid == 0) return cudaSuccess;
+    const uint32_t per_sm = std::max<uint32_t>(
+        1u, std::min<uint32_t>(2048u / threads, (uint32_t)(233472 / (smem + 1024))));
+    grid = std::min(grid, per_sm * (uint32_t)std::max(sm_count, 1));
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -638,24 +663,26 @@ cudaError_t launch_bin_place(const uint2* bbox, const uint32_t* depth_keys, uint
 
 cudaError_t launch_tile_sorts(const uint32_t grids[4], const uint32_t* lists, const uint32_t* words,
                               uint32_t tiles, const uint32_t* tile_start, uint32_t capacity, uint2* pairs,
-                              uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, cudaStream_t st) {
+                              uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, int sm_count,
+                              cudaStream_t st) {
     cudaError_t e;
     // Each form reads and overwrites only its own tiles' ranges.
     e = launch_sort_kernel(tile_sort_global_kernel<kBinsGiant, 512>, 512, (kBinsGiant + 64) * 4, grids[3],
-                           lists + 3 * (size_t)tiles, words + 7, tile_start, capacity, pairs, ids, tids_out,
-                           keys_tmp, st);
+                           sm_count, lists + 3 * (size_t)tiles, words + 7, tile_start, capacity, pairs, ids,
+                           tids_out, keys_tmp, st);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClass0, kBins0, kThreads0>, kThreads0,
-                           sort_smem<kClass0, kBins0, kThreads0>(), grids[0], lists, words + 8, tile_start,
-                           capacity, pairs, ids, tids_out, keys_tmp, st);
+                           sort_smem<kClass0, kBins0, kThreads0>(), grids[0], sm_count, lists, words + 8,
+                           tile_start, capacity, pairs, ids, tids_out, keys_tmp, st);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClass1, kBins1, kThreads1>, kThreads1,
-                           sort_smem<kClass1, kBins1, kThreads1>(), grids[1], lists + tiles, words + 9, tile_start,
-                           capacity, pairs, ids, tids_out, keys_tmp, st);
+                           sort_smem<kClass1, kBins1, kThreads1>(), grids[1], sm_count, lists + tiles, words + 9,
+                           tile_start, capacity, pairs, ids, tids_out, keys_tmp, st);
     if (e != cudaSuccess) return e;
     return launch_sort_kernel(tile_sort_kernel<kClass2, kBins2, kThreads2>, kThreads2,
-                              sort_smem<kClass2, kBins2, kThreads2>(), grids[2], lists + 2 * (size_t)tiles,
-                              words + 10, tile_start, capacity, pairs, ids, tids_out, keys_tmp, st);
+                              sort_smem<kClass2, kBins2, kThreads2>(), grids[2], sm_count,
+                              lists + 2 * (size_t)tiles, words + 10, tile_start, capacity, pairs, ids, tids_out,
+                              keys_tmp, st);
 }
 
 }  // namespace sfk

@@ -138,10 +138,12 @@ cudaError_t launch_bin_place(const uint2* bbox, const uint32_t* depth_keys, uint
 // pairs: the placed (depth key, splat id) per slot (overwritten for the
 // longest lists); ids / tids_out receive the sorted splat ids / tile ids
 // (tids_out may be null); keys_tmp: capacity u32 of scratch (may alias
-// tids_out). grids[0..2]: shared classes, grids[3]: longer lists.
+// tids_out). grids[0..2]: shared classes, grids[3]: longer lists (each the
+// class's tile count, or an upper bound when the counts are on the device).
 cudaError_t launch_tile_sorts(const uint32_t grids[4], const uint32_t* lists, const uint32_t* words,
                               uint32_t tiles, const uint32_t* tile_start, uint32_t capacity, uint2* pairs,
-                              uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, cudaStream_t st);
+                              uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, int sm_count,
+                              cudaStream_t st);
 
 // ---- segmentation (sf_seg.cu)
 constexpr int kGridPts = 445;

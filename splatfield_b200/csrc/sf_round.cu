@@ -36,6 +36,15 @@ __global__ void clamp_count_kernel(const unsigned long long* total, uint32_t cap
     *n32 = (uint32_t)(t < cap ? t : cap);
 }
 
+// Tile starts past the capacity (a view whose intersections outgrew it) are
+// cut back to it, so that the sorts and the raster only read slots below the
+// capacity, all of which the placement filled. The round then grows and
+// re-runs the view.
+__global__ void clamp_starts_kernel(uint32_t* tile_start, uint32_t count, uint32_t cap) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count && tile_start[i] > cap) tile_start[i] = cap;
+}
+
 uint32_t bits_for(uint32_t max_exclusive) {
     const uint32_t m = max_exclusive > 0 ? max_exclusive - 1 : 0;
     return m == 0 ? 0u : 32u - (uint32_t)__builtin_clz(m);
@@ -81,9 +90,13 @@ struct RoundLane {
     void* scan_tmp = nullptr;
     void* sort_tmp = nullptr;
     uint64_t cap = 0;
-    uint32_t *tid_e = nullptr, *gid_e = nullptr, *tid_a = nullptr, *gid_a = nullptr;
+    uint32_t *tid_e = nullptr, *gid_e = nullptr, *tid_a = nullptr, *gid_a = nullptr;  // gid_a: tid_a + cap
     uint32_t* tile_start = nullptr;
     double* partials = nullptr;
+    // Binned build: [chunks][max_tiles] histogram, per-tile totals, class lists.
+    uint32_t* hist = nullptr;
+    uint32_t* cnt = nullptr;
+    uint32_t* lists = nullptr;
 };
 
 }  // namespace sfk
@@ -101,7 +114,7 @@ struct sf_round_t {
     std::vector<RoundLane> lanes;
     sf_view* views_dev = nullptr;
     sf_view* views_host = nullptr;  // pinned
-    uint32_t* words = nullptr;      // [views][8]: 0 visible, 1 err, 2 n32, 4..5 total u64
+    uint32_t* words = nullptr;      // [views][16]: 0 visible, 1 err, 2 n32, 4..5 total u64, 6..10 binned stats
     uint32_t* words_host = nullptr; // pinned
     double* eig_dev = nullptr;
     double* eig_host = nullptr;     // pinned
@@ -117,7 +130,8 @@ struct sf_round_t {
     const void* g_splats = nullptr;
     const void* g_beta = nullptr;
     int g_mode = -1;
-    uint32_t g_lanes = 0, g_cull = 0;
+    uint32_t g_lanes = 0, g_cull = 0, g_build = 0;
+    uint32_t chunks = 1;
     std::vector<const sf_mask_t*> g_masks;
 };
 
@@ -129,8 +143,10 @@ void lane_free(RoundLane& L) {
     if (L.scan_tmp) cudaFree(L.scan_tmp);
     if (L.sort_tmp) cudaFree(L.sort_tmp);
     L.scan_tmp = L.sort_tmp = nullptr;
-    dfree(L.tid_e); dfree(L.gid_e); dfree(L.tid_a); dfree(L.gid_a);
+    dfree(L.tid_e); dfree(L.gid_e); dfree(L.tid_a);
+    L.gid_a = nullptr;
     dfree(L.tile_start); dfree(L.partials);
+    dfree(L.hist); dfree(L.cnt); dfree(L.lists);
     if (L.stream) cudaStreamDestroy(L.stream);
     if (L.join) cudaEventDestroy(L.join);
     L.stream = nullptr;
@@ -144,11 +160,17 @@ cudaError_t lane_alloc(sf_round_t* r, RoundLane& L, uint64_t cap) {
 #define RA(ptr, cnt) if ((e = dalloc(&(ptr), (cnt))) != cudaSuccess) return e
     RA(L.keys, n); RA(L.counts, n); RA(L.bbox, n); RA(L.geo0, n); RA(L.geo1, n); RA(L.ext, n);
     RA(L.keys_a, n); RA(L.keys_b, n); RA(L.order_a, n); RA(L.order_b, n); RA(L.offsets, n);
-    RA(L.tid_e, cap); RA(L.gid_e, cap); RA(L.tid_a, cap); RA(L.gid_a, cap);
+    RA(L.tid_e, cap); RA(L.gid_e, cap); RA(L.tid_a, 2 * cap);
+    L.gid_a = L.tid_a + cap;
     RA(L.tile_start, (size_t)r->max_tiles + 1);
     RA(L.partials, r->eig_blocks);
+    if (r->max_tiles <= kBinMaxTiles) {
+        RA(L.hist, (size_t)r->chunks * r->max_tiles);
+        RA(L.cnt, (size_t)r->max_tiles + 1);
+        RA(L.lists, 4 * (size_t)r->max_tiles);
+    }
 #undef RA
-    if ((e = cudaMalloc(&L.scan_tmp, scan_temp_bytes(n))) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&L.scan_tmp, scan_temp_bytes(std::max(n, r->max_tiles + 1)))) != cudaSuccess) return e;
     const size_t st = std::max(radix_temp_bytes(n, 4), radix_temp_bytes((uint32_t)cap, 4));
     if ((e = cudaMalloc(&L.sort_tmp, st)) != cudaSuccess) return e;
     if ((e = cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking)) != cudaSuccess) return e;
@@ -173,20 +195,12 @@ cudaError_t lanes_build(sf_round_t* r, uint32_t lanes, uint64_t cap) {
     return cudaSuccess;
 }
 
-// One view's pipeline on lane L's stream.
-cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splats_t& sp,
-                         const float* beta_a, const float* beta_b, const float* lut, int mode) {
-    cudaStream_t st = L.stream;
-    const uint32_t n = r->n;
-    uint32_t* words = r->words + 8 * v;
-    unsigned long long* total = reinterpret_cast<unsigned long long*>(words + 4);
-    const uint32_t w = r->w[v], h = r->h[v];
-    const uint32_t tx = (w + 15) / 16, ty = (h + 15) / 16;
+// The reference's order of steps with device-side counts: depth argsort,
+// gather scan, emit, stable tile sort, tile starts.
+cudaError_t depth_sorted_isects(sf_round_t* r, RoundLane& L, uint32_t n, uint32_t tx, uint32_t tiles,
+                                uint32_t* words, unsigned long long* total, cudaStream_t st,
+                                const uint32_t** tids_out, const uint32_t** gids_out) {
     cudaError_t e;
-    if ((e = cudaMemsetAsync(words, 0, 32, st)) != cudaSuccess) return e;
-    ProjOut po{L.keys, L.counts, L.bbox, L.geo0, L.geo1, nullptr, words, r->tuning.raster_cull ? L.ext : nullptr};
-    sf_view dummy{};
-    if ((e = launch_project(dummy, sp.attr, sp.sh, n, sp.K, po, st, r->views_dev + v)) != cudaSuccess) return e;
     int in_b = 0;
     if ((e = radix_sort_pairs(L.keys, nullptr, L.keys_a, L.order_a, L.keys_b, L.order_b, n, nullptr, n, 32,
                               false, true, L.sort_tmp, words + 1, r->sm_count, st, &in_b)) != cudaSuccess)
@@ -200,7 +214,6 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
         return e;
     clamp_count_kernel<<<1, 1, 0, st>>>(total, (uint32_t)L.cap, words + 2, words + 1);
     note_launches(1);
-    const uint32_t tiles = tx * ty;
     const uint32_t tbits = bits_for(tiles);
     const uint32_t *tids = L.tid_e, *gids = L.gid_e;
     if (tbits > 0) {
@@ -213,6 +226,17 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
     }
     if ((e = launch_tile_starts(tids, 0, words + 2, (uint32_t)L.cap, tiles, L.tile_start, st)) != cudaSuccess)
         return e;
+    *tids_out = tids;
+    *gids_out = gids;
+    return cudaSuccess;
+}
+
+// Responsibility (or evidence) raster of view v and its EIG.
+cudaError_t raster_and_eig(sf_round_t* r, RoundLane& L, uint32_t v, uint32_t tx, uint32_t ty, const uint32_t* gids,
+                           const float* beta_a, const float* beta_b, const float* lut, int mode, cudaStream_t st) {
+    cudaError_t e;
+    const uint32_t n = r->n;
+    const uint32_t w = r->w[v], h = r->h[v];
     uint32_t* resp = r->resp + (size_t)v * n;
     uint32_t* bg = r->masks.empty() ? nullptr : r->bg + (size_t)v * n;
     if ((e = cudaMemsetAsync(resp, 0, (size_t)n * 4, st)) != cudaSuccess) return e;
@@ -247,6 +271,50 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
             return e;
     }
     return cudaSuccess;
+}
+
+// One view's pipeline on lane L's stream.
+cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splats_t& sp,
+                         const float* beta_a, const float* beta_b, const float* lut, int mode) {
+    cudaStream_t st = L.stream;
+    const uint32_t n = r->n;
+    uint32_t* words = r->words + 16 * v;
+    unsigned long long* total = reinterpret_cast<unsigned long long*>(words + 4);
+    const uint32_t w = r->w[v], h = r->h[v];
+    const uint32_t tx = (w + 15) / 16, ty = (h + 15) / 16;
+    const uint32_t tiles = tx * ty;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(words, 0, 64, st)) != cudaSuccess) return e;
+    ProjOut po{L.keys, L.counts, L.bbox, L.geo0, L.geo1, nullptr, words, r->tuning.raster_cull ? L.ext : nullptr};
+    sf_view dummy{};
+    if ((e = launch_project(dummy, sp.attr, sp.sh, n, sp.K, po, st, r->views_dev + v)) != cudaSuccess) return e;
+    const uint32_t *tids = nullptr, *gids = nullptr;
+    if (r->tuning.isect_build == SF_ISECTS_BINNED && L.hist) {
+        // Binned build with device-side counts: the sorts take every tile as
+        // the bound of each class and read the class sizes on the device.
+        if ((e = launch_bin_count(L.bbox, n, tx, tiles, r->chunks, L.hist, st)) != cudaSuccess) return e;
+        if ((e = launch_bin_colscan(L.hist, r->chunks, tiles, L.cnt, L.lists, words, st)) != cudaSuccess) return e;
+        if ((e = exclusive_scan(nullptr, L.cnt, L.tile_start, tiles + 1, nullptr, tiles + 1, L.scan_tmp, total,
+                                words + 1, st)) != cudaSuccess)
+            return e;
+        clamp_count_kernel<<<1, 1, 0, st>>>(total, (uint32_t)L.cap, words + 2, words + 1);
+        note_launches(1);
+        uint2* pairs = reinterpret_cast<uint2*>(L.tid_a);
+        if ((e = launch_bin_place(L.bbox, L.keys, n, tx, tiles, r->chunks, L.hist, L.tile_start, (uint32_t)L.cap,
+                                  pairs, words + 1, st)) != cudaSuccess)
+            return e;
+        clamp_starts_kernel<<<(tiles + 1 + 255) / 256, 256, 0, st>>>(L.tile_start, tiles + 1, (uint32_t)L.cap);
+        note_launches(1);
+        const uint32_t grids[4] = {tiles, tiles, tiles, tiles};
+        if ((e = launch_tile_sorts(grids, L.lists, words, tiles, L.tile_start, (uint32_t)L.cap, pairs, L.gid_e,
+                                   nullptr, L.tid_e, r->sm_count, st)) != cudaSuccess)
+            return e;
+        gids = L.gid_e;
+    } else {
+        if ((e = depth_sorted_isects(r, L, n, tx, tiles, words, total, st, &tids, &gids)) != cudaSuccess)
+            return e;
+    }
+    return raster_and_eig(r, L, v, tx, ty, gids, beta_a, beta_b, lut, mode, st);
 }
 
 }  // namespace
@@ -289,7 +357,7 @@ int build_graph(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, int
         if (e == cudaSuccess) e = cudaStreamWaitEvent(r->main, L.join, 0);
     }
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(r->words_host, r->words, 32 * r->views, cudaMemcpyDeviceToHost, r->main);
+        e = cudaMemcpyAsync(r->words_host, r->words, 64 * r->views, cudaMemcpyDeviceToHost, r->main);
     if (e == cudaSuccess && beta)
         e = cudaMemcpyAsync(r->eig_host, r->eig_dev, 8 * r->views, cudaMemcpyDeviceToHost, r->main);
     cudaGraph_t graph = nullptr;
@@ -311,6 +379,7 @@ int build_graph(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, int
     r->g_mode = mode;
     r->g_lanes = (uint32_t)r->lanes.size();
     r->g_cull = r->tuning.raster_cull;
+    r->g_build = r->tuning.isect_build;
     r->g_masks = r->masks;
     return SF_OK;
 }
@@ -325,7 +394,7 @@ int run_round(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, const
             RF_CK(lanes_build(r, lanes, std::max<uint64_t>(r->want_cap, r->lanes.empty() ? 1024 : r->lanes[0].cap)));
         }
         if (!r->exec || r->g_splats != sp || r->g_beta != beta || r->g_mode != mode ||
-            r->g_cull != r->tuning.raster_cull || r->g_masks != r->masks) {
+            r->g_cull != r->tuning.raster_cull || r->g_build != r->tuning.isect_build || r->g_masks != r->masks) {
             const int rc = build_graph(r, sp, beta, mode);
             if (rc != SF_OK) return rc;
         }
@@ -340,7 +409,7 @@ int run_round(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, const
         uint64_t worst = 0;
         bool over = false;
         for (uint32_t v = 0; v < r->views; ++v) {
-            const uint32_t* w = r->words_host + 8 * v;
+            const uint32_t* w = r->words_host + 16 * v;
             if (w[1] & SF_DEV_ERR_TIMEOUT) return rfail(SF_ERR_TIMEOUT, "device look-back wait timed out");
             uint64_t total;
             std::memcpy(&total, w + 4, 8);
@@ -392,14 +461,15 @@ int sf_round_create(sf_ctx ctx, uint32_t total, uint32_t n_views, const uint32_t
     for (uint32_t v = 0; v < n_views; ++v)
         r->max_tiles = std::max(r->max_tiles, ((widths[v] + 15) / 16) * ((heights[v] + 15) / 16));
     r->eig_blocks = eig_blocks(total, ctx->sm_count);
+    r->chunks = bin_chunks(total, ctx->sm_count);
     r->tuning.lanes = 4;
     r->want_cap = std::min<uint64_t>((uint64_t)r->max_tiles * total, 1ull << 22);
     cudaError_t e = cudaStreamCreateWithFlags(&r->main, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = dalloc(&r->views_dev, n_views);
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&r->views_host), sizeof(sf_view) * n_views);
-    if (e == cudaSuccess) e = dalloc(&r->words, 8 * (size_t)n_views);
-    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&r->words_host), 32 * (size_t)n_views);
+    if (e == cudaSuccess) e = dalloc(&r->words, 16 * (size_t)n_views);
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&r->words_host), 64 * (size_t)n_views);
     if (e == cudaSuccess) e = dalloc(&r->eig_dev, n_views);
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&r->eig_host), 8 * (size_t)n_views);
     if (e == cudaSuccess) e = dalloc(&r->resp, (size_t)n_views * total);
@@ -428,7 +498,8 @@ int sf_round_destroy(sf_round r) {
 
 int sf_round_set_tuning(sf_round r, const sf_round_tuning* t) {
     if (!r || !t) return rfail(SF_ERR_ARG, "null argument");
-    if (t->raster_cull > 1 || t->lanes > 64) return rfail(SF_ERR_ARG, "bad tuning");
+    if (t->raster_cull > 1 || t->lanes > 64 || t->isect_build > SF_ISECTS_DEPTH_SORTED)
+        return rfail(SF_ERR_ARG, "bad tuning");
     r->tuning = *t;
     return SF_OK;
 }
@@ -498,7 +569,7 @@ int sf_round_responsibility(sf_round r, uint32_t view, const uint32_t** resp, fl
     if (view >= r->views) return rfail(SF_ERR_SHAPE, "no such view");
     if (resp) *resp = r->resp + (size_t)view * r->n;
     if (scale) *scale = (float)((uint64_t)1 << frac_bits(r->w[view], r->h[view]));
-    const uint32_t* w = r->words_host + 8 * view;
+    const uint32_t* w = r->words_host + 16 * view;
     if (num_isects) std::memcpy(num_isects, w + 4, 8);
     if (num_visible) *num_visible = w[0];
     return SF_OK;
@@ -529,7 +600,7 @@ int sf_round_autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* ca
         for (uint32_t cull = 0; cull <= 1; ++cull)
             for (uint32_t lanes : lane_options) {
                 if (lanes > r->views) continue;
-                sf_round_tuning t{};
+                sf_round_tuning t = r->tuning;
                 t.lanes = lanes;
                 t.raster_cull = cull;
                 r->tuning = t;
