@@ -153,7 +153,10 @@ typedef struct {
      *     (src/render.rs:318-352): depth argsort, gather scan, emit, stable
      *     tile sort; keeps the depth order and offsets for sf_scratch_read. */
     uint32_t isect_build;
-    uint32_t reserved[6];
+    /* 1: the rasterizer also counts out[1..3] of sf_scratch_stats (a slower
+     * diagnostic form); 0 (default): only out[0]. */
+    uint32_t raster_detail;
+    uint32_t reserved[5];
 } sf_tuning;
 #define SF_ISECTS_BINNED 0u
 #define SF_ISECTS_DEPTH_SORTED 1u
@@ -207,9 +210,10 @@ int sf_scratch_buffers(sf_scratch s, const uint32_t** bitmap, const float** rgba
 
 /* Pair statistics of the scratch's last rasterization (syncs): out[0] =
  * (pixel, splat) pairs visited (256 per tile-list entry walked before the
- * tile's early exit), out[1] = exponentials evaluated, out[2] = contributing
- * pairs (alpha >= 1/255), out[3] = pairs processed after the per-warp
- * culling (32 per warp-splat walked). */
+ * tile's early exit); with sf_tuning.raster_detail = 1 also out[1] =
+ * exponentials evaluated, out[2] = contributing pairs (alpha >= 1/255),
+ * out[3] = pairs processed (32 per warp-entry step the warps ran); else
+ * zero. */
 int sf_scratch_stats(sf_scratch s, uint64_t out[4], sf_stream stream);
 
 /* Intermediates of the last prepare, copied to host (syncs), for parity
@@ -279,6 +283,13 @@ int sf_beta_eig(sf_beta beta, sf_accum acc, int mode, sf_stream stream, double* 
 int sf_beta_eig_async(sf_beta beta, sf_accum acc, int mode, double* eig_dev, sf_stream stream);
 /* BetaState::update (src/seg/beta.rs:273-286): a += fg/scale, b += bg/scale. */
 int sf_beta_update(sf_beta beta, sf_accum acc, sf_stream stream);
+/* localize (src/seg/views.rs:24-66): weighted centre and mean distance of
+ * the foreground set {a > b}, weights m = a / (a + b), positions from the
+ * splats' mean planes. *found = 0 (and zeros) while no splat is foreground.
+ * Reduced on the device in f64 over a fixed partition (deterministic); the
+ * reference sums in f32 on the host after an a / b read-back. Syncs. */
+int sf_localize(sf_splats s, sf_beta beta, sf_stream stream, int* found, float center[3],
+                float* radius);
 /* map_labels (src/seg/beta.rs:294-297): out[i] = a[i] > b[i]. Host arrays. */
 int sf_map_labels(const float* a, const float* b, uint32_t n, uint8_t* out);
 /* The f32 entropy LUT the EIG kernel reads (445*445 floats, host copy). */

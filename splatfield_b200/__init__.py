@@ -9,5 +9,6 @@ ABI (ctypes); it has no CPU fallback.
 """
 from .core import *  # noqa: F401,F403
 from .core import make_camera, quat_from_rotation_y  # noqa: F401
+from . import segment  # noqa: F401
 
 __version__ = "0.1.0"

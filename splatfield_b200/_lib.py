@@ -52,7 +52,8 @@ class View(C.Structure):
 class Tuning(C.Structure):
     """sf_tuning: kernel forms of a scratch (results are identical across forms)."""
 
-    _fields_ = [("raster_cull", C.c_uint32), ("isect_build", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+    _fields_ = [("raster_cull", C.c_uint32), ("isect_build", C.c_uint32), ("raster_detail", C.c_uint32),
+                ("reserved", C.c_uint32 * 5)]
 
 
 class RoundTuning(C.Structure):
@@ -132,6 +133,7 @@ SIGNATURES = {
         "sf_beta_eig": (i32, [P, P, i32, P, P]),
         "sf_beta_eig_async": (i32, [P, P, i32, P, P]),
         "sf_beta_update": (i32, [P, P, P]),
+        "sf_localize": (i32, [P, P, P, P, P, P]),
         "sf_map_labels": (i32, [P, P, u32, P]),
         "sf_entropy_table": (i32, [P]),
         "sf_table_entropy": (i32, [P, P, P, u32, P, P]),

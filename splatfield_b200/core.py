@@ -366,18 +366,21 @@ class RenderScratch:
         check(lib().sf_scratch_capacity(self.handle, C.byref(c)))
         return int(c.value)
 
-    def set_tuning(self, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED) -> None:
+    def set_tuning(self, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED, raster_detail: int = 0) -> None:
         """Kernel forms (results are identical across forms): raster_cull 0/1,
-        isect_build ISECTS_BINNED (default) or ISECTS_DEPTH_SORTED."""
+        isect_build ISECTS_BINNED (default) or ISECTS_DEPTH_SORTED,
+        raster_detail 1 to count the per-pair diagnostics of ``stats``."""
         t = L.Tuning()
         t.raster_cull = int(raster_cull)
         t.isect_build = int(isect_build)
+        t.raster_detail = int(raster_detail)
         check(lib().sf_scratch_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:
         t = L.Tuning()
         check(lib().sf_scratch_get_tuning(self.handle, C.byref(t)))
-        return {"raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build)}
+        return {"raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build),
+                "raster_detail": int(t.raster_detail)}
 
     def read(self, what: int, count: int, dtype=np.uint32, stream=None) -> np.ndarray:
         out = np.empty(count, dtype)

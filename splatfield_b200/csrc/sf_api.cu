@@ -409,6 +409,7 @@ RasterArgs raster_args(sf_scratch s, const sf_isects* is) {
     a.color = s->color;
     a.ext = s->ext;
     a.cull = s->tuning.raster_cull;
+    a.detail = s->tuning.raster_detail;
     a.stats = s->stats;
     return a;
 }
@@ -650,7 +651,7 @@ int sf_scratch_destroy(sf_scratch s) {
 
 int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t) {
     if (!s || !t) return fail(SF_ERR_ARG, "null argument");
-    if (t->raster_cull > 1) return fail(SF_ERR_ARG, "raster_cull must be 0 or 1");
+    if (t->raster_cull > 1 || t->raster_detail > 1) return fail(SF_ERR_ARG, "raster flags must be 0 or 1");
     if (t->isect_build > SF_ISECTS_DEPTH_SORTED) return fail(SF_ERR_ARG, "unknown isect_build");
     s->tuning = *t;
     return SF_OK;
@@ -1017,7 +1018,9 @@ int sf_beta_destroy(sf_beta b) {
     if (!b) return SF_OK;
     use_device(b->ctx->device);
     dfree(b->a); dfree(b->b); dfree(b->partials); dfree(b->out);
+    dfree(b->loc_partials); dfree(b->loc_out);
     if (b->host_out) cudaFreeHost(b->host_out);
+    if (b->loc_host) cudaFreeHost(b->loc_host);
     delete b;
     return SF_OK;
 }
@@ -1068,6 +1071,28 @@ int sf_beta_update(sf_beta b, sf_accum acc, sf_stream stream) {
         if (acc->total != b->n) return fail(SF_ERR_SHAPE, "accumulator and posterior sizes differ");
         SF_CK(use_device(b->ctx->device));
         SF_CK(launch_beta_update(acc->scale, acc->fg, acc->bg, b->a, b->b, b->n, S(stream)));
+        return SF_OK;
+    })
+}
+
+int sf_localize(sf_splats s, sf_beta b, sf_stream stream, int* found, float center[3], float* radius) {
+    SF_TRY({
+        if (!s || !b || !found || !center || !radius) return fail(SF_ERR_ARG, "null argument");
+        if (s->n != b->n) return fail(SF_ERR_SHAPE, "splat count and posterior size differ");
+        SF_CK(use_device(b->ctx->device));
+        if (!b->loc_out) {
+            SF_CK(dalloc(&b->loc_partials, 4 * (size_t)b->blocks));
+            SF_CK(dalloc(&b->loc_out, 8));
+            SF_CK(cudaMallocHost(reinterpret_cast<void**>(&b->loc_host), 8 * sizeof(double)));
+        }
+        cudaStream_t st = S(stream);
+        SF_CK(launch_localize(s->attr, b->a, b->b, b->n, b->loc_partials, b->blocks, b->loc_out, st));
+        SF_CK(cudaMemcpyAsync(b->loc_host, b->loc_out, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        SF_CK(cudaStreamSynchronize(st));
+        const double* o = b->loc_host;
+        *found = o[0] > 0.0 ? 1 : 0;
+        for (int k = 0; k < 3; ++k) center[k] = *found ? (float)o[4 + k] : 0.0f;
+        *radius = *found ? (float)o[7] : 0.0f;
         return SF_OK;
     })
 }

@@ -30,7 +30,7 @@
 namespace sfk {
 namespace {
 
-constexpr uint32_t kBinThreads = 512;
+constexpr uint32_t kBinThreads = 1024;
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
@@ -38,21 +38,24 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
-// Calls f(splat, tile) for every tile of every splat in [begin, end): warps
-// take 32 consecutive splats at a time and spread the pairs over their lanes
-// (owner found by a shuffle search over the lanes' inclusive ends), so a
-// splat covering many tiles does not stall its warp.
+// Calls f(splat, tile, payload) for every tile of every splat in [begin,
+// end): warps take 32 consecutive splats at a time and spread the pairs over
+// their lanes (owner found by a shuffle search over the lanes' inclusive
+// ends), so a splat covering many tiles does not stall its warp. payload
+// (optional) is a per-splat word loaded once by the splat's lane with its box
+// and shuffled to the lanes that emit its pairs.
 template <typename F>
 __device__ __forceinline__ void for_each_pair(uint32_t begin, uint32_t end, const uint2* __restrict__ bbox,
-                                              uint32_t tiles_x, F&& f) {
+                                              const uint32_t* __restrict__ payload, uint32_t tiles_x, F&& f) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t nwarps = blockDim.x >> 5;
     for (uint32_t g0 = begin + warp * 32u; g0 < end; g0 += nwarps * 32u) {
         const uint32_t r = g0 + lane;
-        uint32_t min_x = 0, min_y = 0, width = 1, cnt = 0;
+        uint32_t min_x = 0, min_y = 0, width = 1, cnt = 0, pay = 0;
         if (r < end) {
             const uint2 bb = bbox[r];
+            if (payload) pay = payload[r];
             min_x = bb.x & 0xffffu;
             min_y = bb.x >> 16;
             const uint32_t max_x = bb.y & 0xffffu, max_y = bb.y >> 16;
@@ -81,9 +84,10 @@ __device__ __forceinline__ void for_each_pair(uint32_t begin, uint32_t end, cons
             const uint32_t ow = __shfl_sync(0xffffffffu, width, o);
             const uint32_t ox = __shfl_sync(0xffffffffu, min_x, o);
             const uint32_t oy = __shfl_sync(0xffffffffu, min_y, o);
+            const uint32_t opay = __shfl_sync(0xffffffffu, pay, o);
             if (p < total) {
                 const uint32_t k = p - (oend - ocnt);
-                f(g0 + o, (ox + k % ow) + (oy + k / ow) * tiles_x);
+                f(g0 + o, (ox + k % ow) + (oy + k / ow) * tiles_x, opay);
             }
         }
     }
@@ -97,7 +101,8 @@ __global__ __launch_bounds__(kBinThreads) void bin_count_kernel(const uint2* __r
     __syncthreads();
     const uint32_t begin = min(n, blockIdx.x * chunk);
     const uint32_t end = min(n, begin + chunk);
-    for_each_pair(begin, end, bbox, tiles_x, [&](uint32_t, uint32_t t) { atomicAdd(&s_hist[t], 1u); });
+    for_each_pair(begin, end, bbox, nullptr, tiles_x,
+                  [&](uint32_t, uint32_t t, uint32_t) { atomicAdd(&s_hist[t], 1u); });
     __syncthreads();
     uint32_t* row = hist + (size_t)blockIdx.x * tiles;
     for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) row[t] = s_hist[t];
@@ -171,10 +176,10 @@ __global__ __launch_bounds__(kBinThreads) void bin_place_kernel(
     const uint32_t begin = min(n, blockIdx.x * chunk);
     const uint32_t end = min(n, begin + chunk);
     bool over = false;
-    for_each_pair(begin, end, bbox, tiles_x, [&](uint32_t s, uint32_t t) {
+    for_each_pair(begin, end, bbox, depth_keys, tiles_x, [&](uint32_t s, uint32_t t, uint32_t key) {
         const uint32_t slot = atomicAdd(&s_cur[t], 1u);
         if (slot < capacity) {
-            pairs[slot] = make_uint2(depth_keys[s], s);
+            pairs[slot] = make_uint2(key, s);
         } else {
             over = true;
         }

@@ -38,6 +38,11 @@ struct sf_beta_t {
     uint32_t blocks = 1;
     double* out = nullptr;
     double* host_out = nullptr;
+    // Localization scratch (allocated on first use): [blocks][4] partials,
+    // [8] results, pinned mirror of the results.
+    double* loc_partials = nullptr;
+    double* loc_out = nullptr;
+    double* loc_host = nullptr;
 };
 
 namespace sfk {

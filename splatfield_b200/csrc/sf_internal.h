@@ -68,6 +68,8 @@ struct RasterArgs {
     // Raster form: 0 walks every staged entry in every warp, 1 culls per warp
     // block with the power_max boxes (needs ext).
     uint32_t cull;
+    // 1: also count the per-pair diagnostics stats[1..3] (slower form).
+    uint32_t detail;
     // Optional pair statistics, added to: [0] (pixel, splat) pairs visited
     // (256 per tile-list entry walked before the tile's early exit), [1]
     // exponentials evaluated, [2] contributing pairs (alpha >= 1/255).
@@ -156,6 +158,10 @@ cudaError_t launch_eig(int mode, const float* a, const float* b, const uint32_t*
                        float scale, const float* table, double* partials, uint32_t max_blocks,
                        double* out, cudaStream_t stream, const uint32_t* resp2 = nullptr);
 uint32_t eig_blocks(uint32_t n, int sm_count);
+// Object localization: partials [blocks][4] doubles, out [8] doubles
+// ([0] sum of weights, [4..6] centre, [7] radius).
+cudaError_t launch_localize(const float* attr, const float* a, const float* b, uint32_t n, double* partials,
+                            uint32_t blocks, double* out, cudaStream_t stream);
 cudaError_t launch_beta_update(float scale, const uint32_t* fg, const uint32_t* bg, float* a,
                                float* b, uint32_t n, cudaStream_t stream);
 cudaError_t launch_table_probe(const float* a, const float* b, uint32_t n, const float* table,

@@ -311,10 +311,12 @@ __device__ __forceinline__ uint32_t warp_mask(float mx, float my, float2 e, uint
 // power_max box reaches (warp_mask) and a warp walks only its splats (and
 // stops once its own pixels are saturated) — fewer steps, more registers;
 // which form is faster depends on the scene, so both are kept.
+// DETAIL: per-pair diagnostic counters (evaluated / contributing / walked
+// pairs); off in the timed kernels.
 // Responsibility/evidence words are reduced per warp (redux.sync), then per
 // tile in shared memory, then added to global memory once per (tile, splat):
 // integer sums, so the words equal the reference's per-pixel atomics exactly.
-template <int MODE, bool CULL>
+template <int MODE, bool CULL, bool DETAIL>
 __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
     __shared__ float4 s_g0[256];
     __shared__ float4 s_g1[256];
@@ -362,7 +364,7 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
         visited += cnt;
         // One (warp, entry) step: every lane of the warp runs it together.
         auto step = [&](uint32_t j) {
-            ++n_proc;
+            if (DETAIL) ++n_proc;
             uint32_t q = 0;
             if (!done) {
                 const float4 g0 = s_g0[j];
@@ -370,10 +372,10 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
                 const float dx = g0.x - fx, dy = g0.y - fy;
                 const float power = fma_(g0.z * dx, dx, fma_(g1.x * dy, dy, (g0.w * dx) * dy));
                 if (!(power > g1.z)) {
-                    ++n_eval;
+                    if (DETAIL) ++n_eval;
                     const float alpha = fminf(g1.y * exp_neg_(-power), 0.999f);
                     if (alpha >= inv255) {
-                        ++n_hit;
+                        if (DETAIL) ++n_hit;
                         const float vis = alpha * T;
                         if (MODE == 0) {
                             const float4 c = s_col[j];
@@ -432,13 +434,15 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
         }
     }
     if (a.stats) {
-        const uint32_t e = __reduce_add_sync(0xffffffffu, n_eval);
-        const uint32_t c = __reduce_add_sync(0xffffffffu, n_hit);
-        const uint32_t pr_ = __reduce_add_sync(0xffffffffu, n_proc);
-        if (lane == 0) {
-            atomicAdd(a.stats + 1, (unsigned long long)e);
-            atomicAdd(a.stats + 2, (unsigned long long)c);
-            atomicAdd(a.stats + 3, (unsigned long long)pr_);
+        if (DETAIL) {
+            const uint32_t e = __reduce_add_sync(0xffffffffu, n_eval);
+            const uint32_t c = __reduce_add_sync(0xffffffffu, n_hit);
+            const uint32_t pr_ = __reduce_add_sync(0xffffffffu, n_proc);
+            if (lane == 0) {
+                atomicAdd(a.stats + 1, (unsigned long long)e);
+                atomicAdd(a.stats + 2, (unsigned long long)c);
+                atomicAdd(a.stats + 3, (unsigned long long)pr_);
+            }
         }
         if (tid == 0) atomicAdd(a.stats, 256ull * visited);
     }
@@ -516,22 +520,24 @@ cudaError_t launch_tile_starts(const uint32_t* sorted_tile_ids, uint32_t num_ise
     return cudaGetLastError();
 }
 
+template <int MODE>
+void raster_dispatch(const RasterArgs& a, uint32_t tiles, cudaStream_t stream) {
+    if (a.cull) {
+        if (a.detail) raster_kernel<MODE, true, true><<<tiles, 256, 0, stream>>>(a);
+        else raster_kernel<MODE, true, false><<<tiles, 256, 0, stream>>>(a);
+    } else {
+        if (a.detail) raster_kernel<MODE, false, true><<<tiles, 256, 0, stream>>>(a);
+        else raster_kernel<MODE, false, false><<<tiles, 256, 0, stream>>>(a);
+    }
+}
+
 cudaError_t launch_raster(int mode, const RasterArgs& a, cudaStream_t stream) {
     const uint32_t tiles = a.tiles_x * a.tiles_y;
     if (tiles == 0) return cudaSuccess;
     switch (mode) {
-        case 0:
-            if (a.cull) raster_kernel<0, true><<<tiles, 256, 0, stream>>>(a);
-            else raster_kernel<0, false><<<tiles, 256, 0, stream>>>(a);
-            break;
-        case 1:
-            if (a.cull) raster_kernel<1, true><<<tiles, 256, 0, stream>>>(a);
-            else raster_kernel<1, false><<<tiles, 256, 0, stream>>>(a);
-            break;
-        case 2:
-            if (a.cull) raster_kernel<2, true><<<tiles, 256, 0, stream>>>(a);
-            else raster_kernel<2, false><<<tiles, 256, 0, stream>>>(a);
-            break;
+        case 0: raster_dispatch<0>(a, tiles, stream); break;
+        case 1: raster_dispatch<1>(a, tiles, stream); break;
+        case 2: raster_dispatch<2>(a, tiles, stream); break;
         default: return cudaErrorInvalidValue;
     }
     note_launches(1);

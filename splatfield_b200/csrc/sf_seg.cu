@@ -151,6 +151,69 @@ __global__ __launch_bounds__(kEigThreads) void eig_final_kernel(const double* __
     if (threadIdx.x == 0) *out = total;
 }
 
+// localize (src/seg/views.rs:24-66) over the foreground set {a > b} with
+// weights m = a / (a + b): pass 0 sums (m, m x, m y, m z), pass 1 sums
+// m |p - c| for the centre c of pass 0. Per-splat products in f32 as the
+// reference computes them; sums in f64 over a fixed partition (deterministic).
+__global__ __launch_bounds__(kEigThreads) void localize_kernel(const float* __restrict__ attr,
+                                                               const float* __restrict__ a,
+                                                               const float* __restrict__ b, uint32_t n,
+                                                               int pass, const double* __restrict__ out,
+                                                               double* __restrict__ partials) {
+    __shared__ double s_warp[kEigThreads / 32];
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+    if (pass == 1) {
+        cx = (float)out[4];
+        cy = (float)out[5];
+        cz = (float)out[6];
+    }
+    const uint32_t stride = gridDim.x * kEigThreads;
+    for (uint32_t i = blockIdx.x * kEigThreads + threadIdx.x; i < n; i += stride) {
+        const float ai = a[i], bi = b[i];
+        if (!(ai > bi)) continue;
+        const float m = ai / (ai + bi);
+        const float px = attr[i], py = attr[(size_t)n + i], pz = attr[2 * (size_t)n + i];
+        if (pass == 0) {
+            acc[0] += (double)m;
+            acc[1] += (double)(m * px);
+            acc[2] += (double)(m * py);
+            acc[3] += (double)(m * pz);
+        } else {
+            const float dx = px - cx, dy = py - cy, dz = pz - cz;
+            const float d = sqrtf((dx * dx + dy * dy) + dz * dz);
+            acc[0] += (double)(m * d);
+        }
+    }
+    const int sums = pass == 0 ? 4 : 1;
+    for (int j = 0; j < sums; ++j) {
+        const double total = block_sum(acc[j], s_warp);
+        if (threadIdx.x == 0) partials[blockIdx.x * 4 + j] = total;
+        __syncthreads();
+    }
+}
+
+// out: [0..3] pass-0 sums, [4..6] centre (f32 values), [7] radius.
+__global__ __launch_bounds__(kEigThreads) void localize_final_kernel(const double* __restrict__ partials,
+                                                                     uint32_t nb, int pass, double* out) {
+    __shared__ double s_warp[kEigThreads / 32];
+    const int sums = pass == 0 ? 4 : 1;
+    for (int j = 0; j < sums; ++j) {
+        double acc = 0.0;
+        for (uint32_t i = threadIdx.x; i < nb; i += kEigThreads) acc += partials[i * 4 + j];
+        const double total = block_sum(acc, s_warp);
+        if (threadIdx.x == 0) {
+            if (pass == 0) out[j] = total;
+            else out[7] = (double)(float)(total / out[0]);
+        }
+        __syncthreads();
+    }
+    if (pass == 0 && threadIdx.x == 0) {
+        const double sw = out[0];
+        for (int k = 0; k < 3; ++k) out[4 + k] = sw > 0.0 ? (double)(float)(out[1 + k] / sw) : 0.0;
+    }
+}
+
 __global__ void beta_update_kernel(float scale, const uint32_t* __restrict__ fg,
                                    const uint32_t* __restrict__ bg, float* __restrict__ a,
                                    float* __restrict__ b, uint32_t n) {
@@ -167,6 +230,16 @@ __global__ void table_probe_kernel(const float* a, const float* b, uint32_t n, c
 }
 
 }  // namespace
+
+cudaError_t launch_localize(const float* attr, const float* a, const float* b, uint32_t n, double* partials,
+                            uint32_t blocks, double* out, cudaStream_t stream) {
+    for (int pass = 0; pass < 2; ++pass) {
+        localize_kernel<<<blocks, kEigThreads, 0, stream>>>(attr, a, b, n, pass, out, partials);
+        localize_final_kernel<<<1, kEigThreads, 0, stream>>>(partials, blocks, pass, out);
+    }
+    note_launches(4);
+    return cudaGetLastError();
+}
 
 uint32_t eig_blocks(uint32_t n, int sm_count) {
     const uint32_t want = (n + kEigThreads * 4 - 1) / (kEigThreads * 4);

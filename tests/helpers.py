@@ -83,3 +83,23 @@ def small_scene(n: int, k: int, seed: int):
     from splatfield_b200 import synth
 
     return synth.scene_uniform(n, k, seed)
+
+
+def jitter(i: int):
+    """views.rs:99-107: deterministic offset of splat i in [-0.5, 0.5]^3."""
+    return np.array([((i * 73) % 17) / 17.0 - 0.5, ((i * 151) % 13) / 13.0 - 0.5,
+                     ((i * 201) % 11) / 11.0 - 0.5], np.float32)
+
+
+PER_CLUSTER = 40
+CLUSTER_CENTERS = [((1.2, 0.0, 0.0), 0.30), ((-1.6, 0.6, 0.4), 0.45), ((0.1, -0.4, 1.9), 0.40)]
+
+
+def cluster_scene():
+    """views.rs:113-129: three separated spherical clusters of 40 opaque
+    splats; cluster 0 is the segmentation target."""
+    pos = []
+    for i in range(len(CLUSTER_CENTERS) * PER_CLUSTER):
+        c, r = CLUSTER_CENTERS[i // PER_CLUSTER]
+        pos.append(np.asarray(c, np.float32) + np.float32(1.4 * r) * jitter(i))
+    return opaque(pos), CLUSTER_CENTERS

@@ -276,3 +276,25 @@ def test_float_image_vs_fp64_oracle(ctx, oracle_mod):
     err = np.abs(got.astype(np.float64) - ref)
     assert np.median(err) < 1e-6
     assert np.mean(err < 2e-4) > 0.99
+
+
+@pytest.mark.parametrize("cull", [0, 1])
+def test_raster_detail_counters_change_nothing(ctx, cull):
+    """The counting form gives the same image; only it fills the per-pair
+    diagnostics, and both forms count the same visited pairs."""
+    from splatfield_b200 import synth
+
+    attr, sh = synth.scene_uniform(20000, 4, 13)
+    cam = sf.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(20000, (200, 150))
+    scratch.set_tuning(raster_cull=cull)
+    a = splats.render_with(scratch, cam, (200, 150)).read()
+    plain = scratch.stats()
+    scratch.set_tuning(raster_cull=cull, raster_detail=1)
+    b = splats.render_with(scratch, cam, (200, 150)).read()
+    detail = scratch.stats()
+    np.testing.assert_array_equal(a, b)
+    assert plain["pairs_visited"] == detail["pairs_visited"] > 0
+    assert plain["exp_evaluated"] == 0 and detail["exp_evaluated"] >= detail["contributing"] > 0
+    assert detail["pairs_processed"] <= detail["pairs_visited"]
