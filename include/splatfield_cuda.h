@@ -121,7 +121,9 @@ int sf_view_for_camera(const sf_camera* cam, uint32_t w, uint32_t h, sf_view* ou
 /* ---------------------------------------------------------------- splats */
 /* Splats::new / CpuSplats::upload (src/render.rs:31-33, 242-269): uploads
  * field-major attributes [11*n] and SH [3*sh_per_ch*n] from host memory;
- * n must be > 0 (the reference asserts it) and sh_per_ch one of 1, 4, 9, 16. */
+ * n must be > 0 (the reference asserts it) and sh_per_ch >= 1; colour reads
+ * the largest whole SH degree the coefficients hold (1, 4, 9 or 16 per
+ * channel, src/project.rs:343-388), like the reference. */
 int sf_splats_create(sf_ctx ctx, const float* attributes, const float* sh, uint32_t n,
                      uint32_t sh_per_ch, sf_splats* out);
 int sf_splats_destroy(sf_splats s);
@@ -345,6 +347,22 @@ int sf_round_evidence_words(sf_round r, uint32_t view, const uint32_t** fg, cons
  * requested. */
 int sf_round_autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, int mode,
                       sf_stream stream, sf_round_tuning* best, double* best_ms);
+
+/* -------------------------------------------------------- PLY scenes */
+/* parse_ply's header rules (src/ply.rs:9-77) on a whole file image: the
+ * vertex count and SH coefficients per channel (1 + f_rest count / 3). Host only
+ * (no CUDA call). Errors: SF_ERR_ARG with the reference's messages
+ * ("Unsupported PLY format: ...", "Missing property: ...", ...). */
+int sf_ply_inspect(const void* bytes, size_t len, uint32_t* n, uint32_t* sh_per_ch);
+/* parse_ply (src/ply.rs:9-112) + CpuSplats::upload: the vertex block goes
+ * to the device as stored and one kernel writes the field-major planes
+ * (rotations normalised as glam does, bounds reduced on the device). */
+int sf_ply_load(sf_ctx ctx, const void* bytes, size_t len, sf_splats* out);
+int sf_ply_load_file(sf_ctx ctx, const char* path, sf_splats* out);
+/* CpuSplats::write_ply (src/ply.rs:115-180) from host planes: out = NULL
+ * reports the byte length in *len; else writes it (cap >= *len). */
+int sf_ply_write(const float* attr, const float* sh, uint32_t n, uint32_t sh_per_ch, void* out,
+                 size_t cap, size_t* len);
 
 /* ------------------------------------------------------- sort / scan */
 /* bits_for (crates/sort/src/sort.rs:259-261). */

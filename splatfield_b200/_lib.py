@@ -146,6 +146,10 @@ SIGNATURES = {
         "sf_round_evidence": (i32, [P, P, P, P, P, i32, P, P]),
         "sf_round_evidence_words": (i32, [P, u32, PP, PP]),
         "sf_round_autotune": (i32, [P, P, P, P, i32, P, P, P]),
+        "sf_ply_inspect": (i32, [P, sz, P, P]),
+        "sf_ply_load": (i32, [P, P, sz, PP]),
+        "sf_ply_load_file": (i32, [P, C.c_char_p, PP]),
+        "sf_ply_write": (i32, [P, P, u32, u32, P, sz, P]),
         "sf_bits_for": (u32, [u32]),
         "sf_radix_create": (i32, [P, u32, PP]),
         "sf_radix_destroy": (i32, [P]),

@@ -26,7 +26,7 @@ __all__ = [
     "RenderScratch", "TileIsects", "Accumulators", "Mask", "BetaState", "map_labels", "bits_for",
     "RadixScratch", "ScanScratch", "exclusive_scan_gather", "exclusive_scan_buf", "entropy_table",
     "table_entropy", "fractional_bits", "row_stride_for", "EIG_LUT_F32", "EIG_FP64", "Round",
-    "ISECTS_BINNED", "ISECTS_DEPTH_SORTED",
+    "ISECTS_BINNED", "ISECTS_DEPTH_SORTED", "ply_inspect", "load_ply",
 ]
 
 EIG_LUT_F32, EIG_FP64 = L.EIG_LUT_F32, L.EIG_FP64
@@ -197,6 +197,28 @@ def row_stride_for(w: int) -> int:
 
 # ------------------------------------------------------------------ splats
 
+def ply_inspect(data: bytes):
+    """parse_ply's header checks (src/ply.rs:9-77): (vertex count, SH
+    coefficients per channel); raises SplatfieldError with the reference's
+    messages."""
+    buf = np.frombuffer(data, np.uint8)
+    n, k = C.c_uint32(), C.c_uint32()
+    check(lib().sf_ply_inspect(_vp(buf) if buf.size else None, buf.size, C.byref(n), C.byref(k)))
+    return int(n.value), int(k.value)
+
+
+def load_ply(source, ctx: Context | None = None) -> "Splats":
+    """parse_ply + upload (src/ply.rs:9-112): a path or the file's bytes."""
+    ctx = ctx or default_context()
+    h = C.c_void_p()
+    if isinstance(source, (bytes, bytearray, memoryview)):
+        buf = np.frombuffer(bytes(source), np.uint8)
+        check(lib().sf_ply_load(ctx.handle, _vp(buf) if buf.size else None, buf.size, C.byref(h)))
+    else:
+        check(lib().sf_ply_load_file(ctx.handle, str(source).encode(), C.byref(h)))
+    return Splats._adopt(h, ctx)
+
+
 class CpuSplats:
     """Host splat payload, field-major (src/render.rs:20-28)."""
 
@@ -209,6 +231,17 @@ class CpuSplats:
 
     def upload(self, ctx: Context | None = None) -> "Splats":
         return Splats(self.attributes, self.sh_coeffs, ctx)
+
+    def write_ply(self) -> bytes:
+        """CpuSplats::write_ply (src/ply.rs:115-180): binary little-endian 3DGS PLY."""
+        n = self.count()
+        k = self.sh_coeffs.size // max(3 * n, 1) if n else 0
+        ln = C.c_size_t()
+        check(lib().sf_ply_write(_vp(self.attributes), _vp(self.sh_coeffs), n, k, None, 0, C.byref(ln)))
+        out = np.empty(ln.value, np.uint8)
+        check(lib().sf_ply_write(_vp(self.attributes), _vp(self.sh_coeffs), n, k, _vp(out), out.size,
+                                 C.byref(ln)))
+        return out.tobytes()
 
 
 class Splats:
@@ -229,6 +262,28 @@ class Splats:
         check(lib().sf_splats_info(h, None, None, _vp(b), None, None))
         self.bounds = (b[:3].copy(), b[3:].copy())
         self.positions = attributes[: 3 * n].copy()
+
+    @classmethod
+    def _adopt(cls, handle, ctx: Context) -> "Splats":
+        """Wraps a handle the library created (e.g. by the PLY loader)."""
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self.handle = handle
+        n, k = C.c_uint32(), C.c_uint32()
+        b = np.empty(6, np.float32)
+        check(lib().sf_splats_info(handle, C.byref(n), C.byref(k), _vp(b), None, None))
+        self.n, self.sh_per_ch = int(n.value), int(k.value)
+        self.bounds = (b[:3].copy(), b[3:].copy())
+        self.positions = self.read_planes()[0][: 3 * self.n].copy()
+        return self
+
+    def read_planes(self):
+        """Host copies of the device planes: (attributes [11 n], sh [3 k n])."""
+        pa, ps = C.c_void_p(), C.c_void_p()
+        check(lib().sf_splats_info(self.handle, None, None, None, C.byref(pa), C.byref(ps)))
+        attr = DeviceView(pa.value, np.float32, (11 * self.n,), self).read()
+        sh = DeviceView(ps.value, np.float32, (3 * self.sh_per_ch * self.n,), self).read()
+        return attr, sh
 
     def close(self):
         if getattr(self, "handle", None):

@@ -568,8 +568,7 @@ int sf_splats_create(sf_ctx ctx, const float* attributes, const float* sh, uint3
         if (!ctx || !attributes || !sh || !out) return fail(SF_ERR_ARG, "null argument");
         *out = nullptr;
         if (n == 0) return fail(SF_ERR_SHAPE, "Splats::new: zero splats");
-        if (sh_per_ch != 1 && sh_per_ch != 4 && sh_per_ch != 9 && sh_per_ch != 16)
-            return fail(SF_ERR_SHAPE, "sh_per_ch must be 1, 4, 9 or 16");
+        if (sh_per_ch == 0) return fail(SF_ERR_SHAPE, "sh_per_ch must be at least 1");
         SF_CK(use_device(ctx->device));
         auto* s = new sf_splats_t();
         s->ctx = ctx;

@@ -365,7 +365,15 @@ cudaError_t launch_project_bwd(const sf_view& view, const float* attr, const flo
                                cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
     const uint32_t grid = (n + 255) / 256;
-    switch (sh_per_ch) {
+    // Coefficients past the largest whole SH degree are never read by the
+    // forward (the reference's `chs >= 4/9/16` tests): zero gradient.
+    const uint32_t used = sh_degree_coeffs(sh_per_ch);
+    if (used < sh_per_ch) {
+        cudaError_t e = cudaMemsetAsync(d_sh + (size_t)3 * used * n, 0, (size_t)3 * (sh_per_ch - used) * n * 4,
+                                        stream);
+        if (e != cudaSuccess) return e;
+    }
+    switch (used) {
         case 1: project_bwd_kernel<1><<<grid, 256, 0, stream>>>(view, attr, sh, n, d2d, d_attr, d_sh); break;
         case 4: project_bwd_kernel<4><<<grid, 256, 0, stream>>>(view, attr, sh, n, d2d, d_attr, d_sh); break;
         case 9: project_bwd_kernel<9><<<grid, 256, 0, stream>>>(view, attr, sh, n, d2d, d_attr, d_sh); break;

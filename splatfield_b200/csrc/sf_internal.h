@@ -33,6 +33,13 @@ struct ProjOut {
     float2* ext;            // [n] half extents of the box holding power <= power_max
 };
 
+// Coefficients per channel the SH evaluation reads for sh_per_ch stored
+// ones: the largest whole degree, 1 / 4 / 9 / 16 (src/project.rs:343-388 tests
+// chs >= 4, >= 9, >= 16).
+inline uint32_t sh_degree_coeffs(uint32_t sh_per_ch) {
+    return sh_per_ch >= 16 ? 16u : sh_per_ch >= 9 ? 9u : sh_per_ch >= 4 ? 4u : 1u;
+}
+
 // view_dev (optional) supplies the view from device memory instead.
 cudaError_t launch_project(const sf_view& view, const float* attr, const float* sh, uint32_t n,
                            uint32_t sh_per_ch, const ProjOut& out, cudaStream_t stream,

@@ -488,7 +488,7 @@ cudaError_t launch_project(const sf_view& view, const float* attr, const float* 
     const uint32_t grid = (n + 255) / 256;
     // Without colour no SH plane is read: the 1-coefficient form has the
     // fewest registers (more warps in flight for the attribute loads).
-    if (!out.color) sh_per_ch = 1;
+    sh_per_ch = out.color ? sh_degree_coeffs(sh_per_ch) : 1u;
     switch (sh_per_ch) {
         case 1: project_kernel<1><<<grid, 256, 0, stream>>>(view, view_dev, attr, sh, n, out); break;
         case 4: project_kernel<4><<<grid, 256, 0, stream>>>(view, view_dev, attr, sh, n, out); break;
