@@ -171,6 +171,19 @@ int sf_scratch_get_tuning(sf_scratch s, sf_tuning* t);
  * aliasing the scratch, valid until the next render on it. */
 int sf_render_with(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
                    sf_stream stream, const uint32_t** bitmap, uint32_t* row_stride);
+/* Splats::render_posterior (src/seg/paint.rs:22-47): the frame with every
+ * splat painted grey by its posterior mean a / (a + b) (no +0.5 offset). A
+ * posterior of another size renders the plain colours, as the reference. */
+int sf_render_posterior(sf_splats s, sf_scratch scratch, sf_beta beta, const sf_camera* cam,
+                        uint32_t w, uint32_t h, sf_stream stream, const uint32_t** bitmap,
+                        uint32_t* row_stride);
+/* Splats::tint (src/seg/paint.rs:49-66): DC colour (r, g, b) for every
+ * foreground splat (a > b), in place. */
+int sf_splats_tint(sf_splats s, sf_beta beta, float r, float g, float b, sf_stream stream);
+/* Splats::save_colors / restore_colors (src/seg/paint.rs:68-95): the three
+ * DC planes (3 n floats) to / from a device buffer, on the copy engine. */
+int sf_splats_save_colors(sf_splats s, float* dst, sf_stream stream);
+int sf_splats_restore_colors(sf_splats s, const float* src, sf_stream stream);
 /* The same frame with a float RGBA plane [h][w][4] (r, g, b, 1-T before
  * quantisation) in addition to the RGBA8 bitmap. */
 int sf_render_float(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,

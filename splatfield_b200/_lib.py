@@ -106,6 +106,10 @@ SIGNATURES = {
         "sf_scratch_set_tuning": (i32, [P, P]),
         "sf_scratch_get_tuning": (i32, [P, P]),
         "sf_render_with": (i32, [P, P, P, u32, u32, P, PP, P]),
+        "sf_render_posterior": (i32, [P, P, P, P, u32, u32, P, PP, P]),
+        "sf_splats_tint": (i32, [P, P, C.c_float, C.c_float, C.c_float, P]),
+        "sf_splats_save_colors": (i32, [P, P, P]),
+        "sf_splats_restore_colors": (i32, [P, P, P]),
         "sf_render_float": (i32, [P, P, P, u32, u32, P, PP]),
         "sf_render_to_host": (i32, [P, P, P, u32, u32, P, P]),
         "sf_render_forward": (i32, [P, P, P, u32, u32, P, PP]),

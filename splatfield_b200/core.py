@@ -305,6 +305,30 @@ class Splats:
                                    C.byref(ptr), C.byref(rs)))
         return DeviceView(ptr.value, np.uint32, (h, rs.value), scratch)
 
+    def render_posterior(self, scratch: "RenderScratch", beta: "BetaState", camera: Camera, img_size,
+                         stream=None) -> DeviceView:
+        """Posterior-mean heatmap frame (src/seg/paint.rs:22-47)."""
+        w, h = img_size
+        ptr = C.c_void_p()
+        rs = C.c_uint32()
+        check(lib().sf_render_posterior(self.handle, scratch.handle, beta.handle if beta else None,
+                                        C.byref(camera), w, h, _stream(stream), C.byref(ptr), C.byref(rs)))
+        return DeviceView(ptr.value, np.uint32, (h, rs.value), scratch)
+
+    def tint(self, beta: "BetaState", color, stream=None) -> None:
+        """DC colour of the foreground splats (src/seg/paint.rs:49-66)."""
+        r, g, b = (float(c) for c in color)
+        check(lib().sf_splats_tint(self.handle, beta.handle, r, g, b, _stream(stream)))
+
+    def save_colors(self, stream=None) -> "DeviceBuffer":
+        """Device snapshot of the DC planes [3, n] (src/seg/paint.rs:68-75)."""
+        buf = DeviceBuffer.empty(3 * self.n, np.float32, self.ctx)
+        check(lib().sf_splats_save_colors(self.handle, C.c_void_p(buf.ptr), _stream(stream)))
+        return buf
+
+    def restore_colors(self, saved: "DeviceView", stream=None) -> None:
+        check(lib().sf_splats_restore_colors(self.handle, C.c_void_p(saved.ptr), _stream(stream)))
+
     def render_float(self, scratch: "RenderScratch", camera: Camera, img_size, stream=None) -> DeviceView:
         w, h = img_size
         ptr = C.c_void_p()

@@ -696,6 +696,52 @@ int sf_render_with(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32
     })
 }
 
+int sf_render_posterior(sf_splats s, sf_scratch scratch, sf_beta beta, const sf_camera* cam, uint32_t w,
+                        uint32_t h, sf_stream stream, const uint32_t** bitmap, uint32_t* row_stride) {
+    SF_TRY({
+        if (!s || !scratch) return fail(SF_ERR_ARG, "null argument");
+        // A posterior of another size (model swapped mid-run): the plain
+        // colour render, as the reference degrades (src/seg/paint.rs:30-32).
+        if (!beta || beta->n != s->n) return sf_render_with(s, scratch, cam, w, h, stream, bitmap, row_stride);
+        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr);
+        if (rc != SF_OK) return rc;
+        SF_CK(launch_paint_posterior(beta->a, beta->b, s->n, scratch->color, S(stream)));
+        rc = finalize_rgb(scratch, nullptr, false, S(stream));
+        if (rc != SF_OK) return rc;
+        if (bitmap) *bitmap = scratch->bitmap;
+        if (row_stride) *row_stride = scratch->row_stride;
+        return SF_OK;
+    })
+}
+
+int sf_splats_tint(sf_splats s, sf_beta beta, float r, float g, float b, sf_stream stream) {
+    SF_TRY({
+        if (!s || !beta) return fail(SF_ERR_ARG, "null argument");
+        if (beta->n != s->n) return fail(SF_ERR_SHAPE, "posterior size differs from the splat count");
+        SF_CK(use_device(s->ctx->device));
+        SF_CK(launch_tint(s->sh, beta->a, beta->b, s->n, r, g, b, S(stream)));
+        return SF_OK;
+    })
+}
+
+int sf_splats_save_colors(sf_splats s, float* dst, sf_stream stream) {
+    SF_TRY({
+        if (!s || !dst) return fail(SF_ERR_ARG, "null argument");
+        SF_CK(use_device(s->ctx->device));
+        SF_CK(cudaMemcpyAsync(dst, s->sh, (size_t)3 * s->n * 4, cudaMemcpyDeviceToDevice, S(stream)));
+        return SF_OK;
+    })
+}
+
+int sf_splats_restore_colors(sf_splats s, const float* src, sf_stream stream) {
+    SF_TRY({
+        if (!s || !src) return fail(SF_ERR_ARG, "null argument");
+        SF_CK(use_device(s->ctx->device));
+        SF_CK(cudaMemcpyAsync(s->sh, src, (size_t)3 * s->n * 4, cudaMemcpyDeviceToDevice, S(stream)));
+        return SF_OK;
+    })
+}
+
 int sf_render_float(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
                     sf_stream stream, const float** rgba) {
     SF_TRY({

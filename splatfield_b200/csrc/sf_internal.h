@@ -165,6 +165,11 @@ cudaError_t launch_eig(int mode, const float* a, const float* b, const uint32_t*
                        float scale, const float* table, double* partials, uint32_t max_blocks,
                        double* out, cudaStream_t stream, const uint32_t* resp2 = nullptr);
 uint32_t eig_blocks(uint32_t n, int sm_count);
+// Posterior heatmap colours and foreground tint (src/seg/paint.rs).
+cudaError_t launch_paint_posterior(const float* a, const float* b, uint32_t n, float4* color,
+                                   cudaStream_t stream);
+cudaError_t launch_tint(float* sh, const float* a, const float* b, uint32_t n, float r, float g, float bl,
+                        cudaStream_t stream);
 // Object localization: partials [blocks][4] doubles, out [8] doubles
 // ([0] sum of weights, [4..6] centre, [7] radius).
 cudaError_t launch_localize(const float* attr, const float* a, const float* b, uint32_t n, double* partials,

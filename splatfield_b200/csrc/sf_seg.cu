@@ -214,6 +214,27 @@ __global__ __launch_bounds__(kEigThreads) void localize_final_kernel(const doubl
     }
 }
 
+// paint_posterior (src/seg/paint.rs:104-114): each splat's projected colour
+// becomes its posterior mean m = a / (a + b) as grey, with no +0.5 offset.
+__global__ void paint_posterior_kernel(const float* __restrict__ a, const float* __restrict__ b, uint32_t n,
+                                       float4* __restrict__ color) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float m = a[i] / (a[i] + b[i]);
+    color[i] = make_float4(m, m, m, 0.0f);
+}
+
+// tint_colors (src/seg/paint.rs:116-126): DC planes of foreground splats
+// (a > b) set to (r, g, b).
+__global__ void tint_kernel(float* __restrict__ sh, const float* __restrict__ a, const float* __restrict__ b,
+                            uint32_t n, float r, float g, float bl) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !(a[i] > b[i])) return;
+    sh[i] = r;
+    sh[(size_t)n + i] = g;
+    sh[2 * (size_t)n + i] = bl;
+}
+
 __global__ void beta_update_kernel(float scale, const uint32_t* __restrict__ fg,
                                    const uint32_t* __restrict__ bg, float* __restrict__ a,
                                    float* __restrict__ b, uint32_t n) {
@@ -230,6 +251,22 @@ __global__ void table_probe_kernel(const float* a, const float* b, uint32_t n, c
 }
 
 }  // namespace
+
+cudaError_t launch_paint_posterior(const float* a, const float* b, uint32_t n, float4* color,
+                                   cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    paint_posterior_kernel<<<(n + 255) / 256, 256, 0, stream>>>(a, b, n, color);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tint(float* sh, const float* a, const float* b, uint32_t n, float r, float g, float bl,
+                        cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    tint_kernel<<<(n + 255) / 256, 256, 0, stream>>>(sh, a, b, n, r, g, bl);
+    note_launches(1);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_localize(const float* attr, const float* a, const float* b, uint32_t n, double* partials,
                             uint32_t blocks, double* out, cudaStream_t stream) {
