@@ -158,10 +158,21 @@ typedef struct {
     /* 1: the rasterizer also counts out[1..3] of sf_scratch_stats (a slower
      * diagnostic form); 0 (default): only out[0]. */
     uint32_t raster_detail;
-    uint32_t reserved[5];
+    /* Tile-list order for the render calls that hand no lists back
+     * (sf_render_with / _float / _to_host / _posterior /
+     * sf_render_responsibility, the round), binned build only:
+     *   SF_ORDER_SORTED (default): every tile list is sorted first;
+     *   SF_ORDER_IN_RASTER: the rasterizer orders each tile's placed pairs
+     *     slab by slab, only as far as the tile saturates.
+     * Same results either way. sf_prepare_isects and sf_render_forward always
+     * sort (their lists are handed out or replayed). */
+    uint32_t raster_order;
+    uint32_t reserved[4];
 } sf_tuning;
 #define SF_ISECTS_BINNED 0u
 #define SF_ISECTS_DEPTH_SORTED 1u
+#define SF_ORDER_SORTED 0u
+#define SF_ORDER_IN_RASTER 1u
 int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t);
 int sf_scratch_get_tuning(sf_scratch s, sf_tuning* t);
 
@@ -325,7 +336,8 @@ typedef struct {
     uint32_t lanes;       /* capture streams the views are spread over (1..64) */
     uint32_t raster_cull; /* as sf_tuning.raster_cull */
     uint32_t isect_build; /* as sf_tuning.isect_build */
-    uint32_t reserved[5];
+    uint32_t raster_order; /* as sf_tuning.raster_order */
+    uint32_t reserved[4];
 } sf_round_tuning;
 int sf_round_create(sf_ctx ctx, uint32_t total, uint32_t n_views, const uint32_t* widths,
                     const uint32_t* heights, sf_round* out);

@@ -27,6 +27,7 @@ READ_TILE_IDS, READ_GAUSSIAN_IDS, READ_TILE_START, READ_BITMAP, READ_RGBA, READ_
 
 EIG_LUT_F32, EIG_FP64 = 0, 1
 ISECTS_BINNED, ISECTS_DEPTH_SORTED = 0, 1
+ORDER_SORTED, ORDER_IN_RASTER = 0, 1
 
 
 class SplatfieldError(RuntimeError):
@@ -53,14 +54,14 @@ class Tuning(C.Structure):
     """sf_tuning: kernel forms of a scratch (results are identical across forms)."""
 
     _fields_ = [("raster_cull", C.c_uint32), ("isect_build", C.c_uint32), ("raster_detail", C.c_uint32),
-                ("reserved", C.c_uint32 * 5)]
+                ("raster_order", C.c_uint32), ("reserved", C.c_uint32 * 4)]
 
 
 class RoundTuning(C.Structure):
     """sf_round_tuning."""
 
     _fields_ = [("lanes", C.c_uint32), ("raster_cull", C.c_uint32), ("isect_build", C.c_uint32),
-                ("reserved", C.c_uint32 * 5)]
+                ("raster_order", C.c_uint32), ("reserved", C.c_uint32 * 4)]
 
 
 class Isects(C.Structure):

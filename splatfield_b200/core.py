@@ -26,11 +26,12 @@ __all__ = [
     "RenderScratch", "TileIsects", "Accumulators", "Mask", "BetaState", "map_labels", "bits_for",
     "RadixScratch", "ScanScratch", "exclusive_scan_gather", "exclusive_scan_buf", "entropy_table",
     "table_entropy", "fractional_bits", "row_stride_for", "EIG_LUT_F32", "EIG_FP64", "Round",
-    "ISECTS_BINNED", "ISECTS_DEPTH_SORTED", "ply_inspect", "load_ply",
+    "ISECTS_BINNED", "ISECTS_DEPTH_SORTED", "ORDER_IN_RASTER", "ORDER_SORTED", "ply_inspect", "load_ply",
 ]
 
 EIG_LUT_F32, EIG_FP64 = L.EIG_LUT_F32, L.EIG_FP64
 ISECTS_BINNED, ISECTS_DEPTH_SORTED = L.ISECTS_BINNED, L.ISECTS_DEPTH_SORTED
+ORDER_IN_RASTER, ORDER_SORTED = L.ORDER_IN_RASTER, L.ORDER_SORTED
 BASE_FOV = 0.8  # Camera::BASE_FOV (src/camera.rs:86)
 
 
@@ -445,21 +446,24 @@ class RenderScratch:
         check(lib().sf_scratch_capacity(self.handle, C.byref(c)))
         return int(c.value)
 
-    def set_tuning(self, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED, raster_detail: int = 0) -> None:
+    def set_tuning(self, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED, raster_detail: int = 0,
+                   raster_order: int = L.ORDER_SORTED) -> None:
         """Kernel forms (results are identical across forms): raster_cull 0/1,
         isect_build ISECTS_BINNED (default) or ISECTS_DEPTH_SORTED,
-        raster_detail 1 to count the per-pair diagnostics of ``stats``."""
+        raster_detail 1 to count the per-pair diagnostics of ``stats``,
+        raster_order ORDER_SORTED (default) or ORDER_IN_RASTER."""
         t = L.Tuning()
         t.raster_cull = int(raster_cull)
         t.isect_build = int(isect_build)
         t.raster_detail = int(raster_detail)
+        t.raster_order = int(raster_order)
         check(lib().sf_scratch_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:
         t = L.Tuning()
         check(lib().sf_scratch_get_tuning(self.handle, C.byref(t)))
         return {"raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build),
-                "raster_detail": int(t.raster_detail)}
+                "raster_detail": int(t.raster_detail), "raster_order": int(t.raster_order)}
 
     def read(self, what: int, count: int, dtype=np.uint32, stream=None) -> np.ndarray:
         out = np.empty(count, dtype)
@@ -708,15 +712,22 @@ class Round:
     def views(self) -> int:
         return len(self.sizes)
 
-    def set_tuning(self, lanes: int = 4, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED) -> None:
+    def set_tuning(self, lanes: int = 4, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED,
+                   raster_order: int = L.ORDER_SORTED) -> None:
         t = L.RoundTuning()
         t.lanes, t.raster_cull, t.isect_build = int(lanes), int(raster_cull), int(isect_build)
+        t.raster_order = int(raster_order)
         check(lib().sf_round_set_tuning(self.handle, C.byref(t)))
+
+    @staticmethod
+    def _tuning_dict(t) -> dict:
+        return {"lanes": int(t.lanes), "raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build),
+                "raster_order": int(t.raster_order)}
 
     def get_tuning(self) -> dict:
         t = L.RoundTuning()
         check(lib().sf_round_get_tuning(self.handle, C.byref(t)))
-        return {"lanes": int(t.lanes), "raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build)}
+        return self._tuning_dict(t)
 
     @staticmethod
     def _cams(cameras):
@@ -771,8 +782,7 @@ class Round:
         ms = C.c_double()
         check(lib().sf_round_autotune(self.handle, splats.handle, beta.handle if beta else None,
                                       self._cams(cameras), mode, _stream(stream), C.byref(t), C.byref(ms)))
-        return ({"lanes": int(t.lanes), "raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build)},
-                float(ms.value))
+        return self._tuning_dict(t), float(ms.value)
 
     def close(self):
         if getattr(self, "handle", None):

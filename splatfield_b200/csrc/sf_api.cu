@@ -132,6 +132,9 @@ struct sf_scratch_t {
     uint32_t* bin_cnt = nullptr;
     uint32_t* bin_lists = nullptr;
     bool binned = false;
+    // The last prepare left the binned build's placed pairs unsorted: the
+    // rasterizer orders each tile's list itself (no gaussian_ids).
+    bool lazy = false;
     uint32_t* bitmap = nullptr;
     float4* rgba = nullptr;
     float* final_t = nullptr;
@@ -282,7 +285,7 @@ int finish_prepare(sf_scratch s, sf_isects* out);
 
 // Binned intersection build (sf_bin.cu) after the projection: count, column
 // scan, tile scan, one sync for the total, place, per-tile sorts.
-int prepare_binned(sf_scratch s, uint32_t n, uint32_t tiles, cudaStream_t st, bool want_tile_ids) {
+int prepare_binned(sf_scratch s, uint32_t n, uint32_t tiles, cudaStream_t st, bool want_tile_ids, bool lazy) {
     uint32_t* words = s->words;
     unsigned long long* total_dev = reinterpret_cast<unsigned long long*>(words + 4);
     SF_CK(launch_bin_count(s->bbox, n, s->tiles_x, tiles, s->bin_chunks, s->bin_hist, st));
@@ -306,19 +309,27 @@ int prepare_binned(sf_scratch s, uint32_t n, uint32_t tiles, cudaStream_t st, bo
     uint2* pairs = reinterpret_cast<uint2*>(s->tid_a);
     SF_CK(launch_bin_place(s->bbox, s->depth_keys, n, s->tiles_x, tiles, s->bin_chunks, s->bin_hist,
                            s->tile_start, (uint32_t)s->cap, pairs, words + 1, st));
-    const uint32_t grids[4] = {hw[8], hw[9], hw[10], hw[7]};
-    SF_CK(launch_tile_sorts(grids, s->bin_lists, words, tiles, s->tile_start, (uint32_t)s->cap, pairs, s->gid_e,
-                            want_tile_ids ? s->tid_e : nullptr, s->tid_e, s->ctx->sm_count, st));
-    s->tids = want_tile_ids ? s->tid_e : nullptr;
-    s->gids = s->gid_e;
+    s->lazy = lazy;
+    if (lazy) {
+        s->tids = s->gids = nullptr;
+    } else {
+        const uint32_t grids[4] = {hw[8], hw[9], hw[10], hw[7]};
+        SF_CK(launch_tile_sorts(grids, s->bin_lists, words, tiles, s->tile_start, (uint32_t)s->cap, pairs,
+                                s->gid_e, want_tile_ids ? s->tid_e : nullptr, s->tid_e, s->ctx->sm_count, st));
+        s->tids = want_tile_ids ? s->tid_e : nullptr;
+        s->gids = s->gid_e;
+    }
     s->num_isects = (uint32_t)total;
     s->binned = true;
     return SF_OK;
 }
 
 // prepare_isects (src/render.rs:274-364).
+// lazy: the caller only rasterizes this frame (no sorted lists handed out,
+// no adjoint state), so the binned build may leave each tile's order to the
+// rasterizer (tuning.raster_order).
 int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32_t h,
-            cudaStream_t st, sf_isects* out) {
+            cudaStream_t st, sf_isects* out, bool lazy = false) {
     if (!sp || !s || !cam) return fail(SF_ERR_ARG, "null argument");
     if (w == 0 || h == 0 || w > 65535 * 16 || h > 65535 * 16) return fail(SF_ERR_SHAPE, "bad image size");
     SF_CK(use_device(s->ctx->device));
@@ -335,8 +346,10 @@ int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32
     const uint32_t tiles = s->tiles_x * s->tiles_y;
     s->order = nullptr;
     s->tids = s->gids = nullptr;
+    s->lazy = false;
     if (s->tuning.isect_build == SF_ISECTS_BINNED && s->bin_hist) {
-        const int rc = prepare_binned(s, n, tiles, st, out != nullptr);
+        const int rc = prepare_binned(s, n, tiles, st, out != nullptr,
+                                      lazy && out == nullptr && s->tuning.raster_order == SF_ORDER_IN_RASTER);
         if (rc != SF_OK) return rc;
         return finish_prepare(s, out);
     }
@@ -404,6 +417,7 @@ RasterArgs raster_args(sf_scratch s, const sf_isects* is) {
     a.row_stride = s->row_stride;
     a.tile_start = is ? is->tile_start : s->tile_start;
     a.gaussian_ids = is ? is->gaussian_ids : s->gids;
+    a.pairs = (!is && s->lazy) ? reinterpret_cast<const uint2*>(s->tid_a) : nullptr;
     a.geo0 = s->geo0;
     a.geo1 = s->geo1;
     a.color = s->color;
@@ -652,6 +666,7 @@ int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t) {
     if (!s || !t) return fail(SF_ERR_ARG, "null argument");
     if (t->raster_cull > 1 || t->raster_detail > 1) return fail(SF_ERR_ARG, "raster flags must be 0 or 1");
     if (t->isect_build > SF_ISECTS_DEPTH_SORTED) return fail(SF_ERR_ARG, "unknown isect_build");
+    if (t->raster_order > SF_ORDER_IN_RASTER) return fail(SF_ERR_ARG, "unknown raster_order");
     s->tuning = *t;
     return SF_OK;
 }
@@ -686,7 +701,7 @@ int sf_finalize_rgb(sf_splats s, sf_scratch scratch, const sf_isects* isects, ui
 int sf_render_with(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
                    sf_stream stream, const uint32_t** bitmap, uint32_t* row_stride) {
     SF_TRY({
-        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr);
+        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr, true);
         if (rc != SF_OK) return rc;
         rc = finalize_rgb(scratch, nullptr, false, S(stream));
         if (rc != SF_OK) return rc;
@@ -703,7 +718,7 @@ int sf_render_posterior(sf_splats s, sf_scratch scratch, sf_beta beta, const sf_
         // A posterior of another size (model swapped mid-run): the plain
         // colour render, as the reference degrades (src/seg/paint.rs:30-32).
         if (!beta || beta->n != s->n) return sf_render_with(s, scratch, cam, w, h, stream, bitmap, row_stride);
-        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr);
+        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr, true);
         if (rc != SF_OK) return rc;
         SF_CK(launch_paint_posterior(beta->a, beta->b, s->n, scratch->color, S(stream)));
         rc = finalize_rgb(scratch, nullptr, false, S(stream));
@@ -745,7 +760,7 @@ int sf_splats_restore_colors(sf_splats s, const float* src, sf_stream stream) {
 int sf_render_float(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
                     sf_stream stream, const float** rgba) {
     SF_TRY({
-        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr);
+        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr, true);
         if (rc != SF_OK) return rc;
         rc = finalize_rgb(scratch, nullptr, true, S(stream));
         if (rc != SF_OK) return rc;
@@ -811,7 +826,7 @@ int sf_render_to_host(sf_splats s, sf_scratch scratch, const sf_camera* cam, uin
                       sf_stream stream, uint32_t* out) {
     SF_TRY({
         if (!out) return fail(SF_ERR_ARG, "null out");
-        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr);
+        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr, true);
         if (rc != SF_OK) return rc;
         rc = finalize_rgb(scratch, nullptr, false, S(stream));
         if (rc != SF_OK) return rc;
@@ -988,7 +1003,7 @@ int sf_render_responsibility(sf_splats s, sf_scratch scratch, sf_accum acc, cons
                              uint32_t w, uint32_t h, sf_stream stream) {
     SF_TRY({
         if (!acc) return fail(SF_ERR_ARG, "null accumulator");
-        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr);
+        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr, true);
         if (rc != SF_OK) return rc;
         return accumulate(scratch, nullptr, w, h, acc, nullptr, S(stream));
     })

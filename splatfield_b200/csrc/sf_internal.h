@@ -58,6 +58,9 @@ struct RasterArgs {
     uint32_t w, h, tiles_x, tiles_y, row_stride;
     const uint32_t* tile_start;
     const uint32_t* gaussian_ids;
+    // Unsorted placed (depth key, splat id) pairs of the binned build; when
+    // set, the rasterizer orders each tile's list itself (gaussian_ids unused).
+    const uint2* pairs;
     const float4* geo0;
     const float4* geo1;
     const float4* color;

@@ -316,91 +316,107 @@ __device__ __forceinline__ uint32_t warp_mask(float mx, float my, float2 e, uint
 // Responsibility/evidence words are reduced per warp (redux.sync), then per
 // tile in shared memory, then added to global memory once per (tile, splat):
 // integer sums, so the words equal the reference's per-pixel atomics exactly.
-template <int MODE, bool CULL, bool DETAIL>
-__global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
-    __shared__ float4 s_g0[256];
-    __shared__ float4 s_g1[256];
-    __shared__ float4 s_col[MODE == 0 ? 256 : 1];
-    __shared__ uint32_t s_gid[MODE == 0 ? 1 : 256];
-    __shared__ uint32_t s_acc0[MODE == 0 ? 1 : 256];
-    __shared__ uint32_t s_acc1[MODE == 2 ? 256 : 1];
-    __shared__ uint8_t s_mask[256];
+//
+// LAZY: the tile's list comes unsorted — the binned build's placed (depth
+// key, splat id) pairs — and is put in order here, slab by slab, only as far
+// as the tile needs: a 256-bin histogram over the 64-bit (key, id) values
+// left picks the longest run of bins holding at most kSlab entries (narrowing
+// the key interval while even the first bin holds more), those entries are
+// gathered and bitonic-sorted in shared memory and composited, and the next
+// slab starts after the last bin taken. (key, id) values are distinct and
+// slabs end on bin boundaries, so the composite order is exactly the sorted
+// list's; most tiles saturate inside their first slab, so most of the list is
+// never sorted. The stored per-pixel last-contributor index counts positions
+// in that order.
 
-    const uint32_t tile = blockIdx.x;
-    const uint32_t tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+constexpr uint32_t kSlab = 2048;
+constexpr uint32_t kFirstSlab = 256;
+
+struct RasterSmem {
+    float4* g0;
+    float4* g1;
+    float4* col;
+    uint32_t* gid;
+    uint32_t* acc0;
+    uint32_t* acc1;
+    uint8_t* mask;
+};
+
+struct PixelState {
+    float T, pr, pg, pb;
+    uint32_t last;
+    bool done;
+    uint32_t n_eval, n_hit, n_proc, visited;
+};
+
+// Composites list entries [0, count) in order; id(i) gives entry i's splat
+// id, list_off the entry's offset in the tile's whole sorted list. Returns
+// true once every pixel of the tile is saturated (uniform).
+template <int MODE, bool CULL, bool DETAIL, typename IdOf>
+__device__ bool composite_list(const RasterArgs& a, const RasterSmem& sm, IdOf id, uint32_t count,
+                               uint32_t list_off, uint32_t tx, uint32_t ty, float fx, float fy, uint32_t inside,
+                               PixelState& ps) {
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    const uint32_t px = tx * 16 + (warp & 1u) * 8 + (lane & 7u);
-    const uint32_t py = ty * 16 + (warp >> 1) * 4 + (lane >> 3);
-    const bool in_bounds = px < a.w && py < a.h;
-    const float fx = (float)px + 0.5f, fy = (float)py + 0.5f;
-    uint32_t inside = 0;
-    if (MODE == 2 && in_bounds) inside = (a.mask[px / 32 + py * a.mask_wpr] >> (px % 32)) & 1u;
-    const uint32_t start = a.tile_start[tile], end = a.tile_start[tile + 1];
     const float inv255 = 1.0f / 255.0f;
-    float T = 1.0f, pr = 0.0f, pg = 0.0f, pb = 0.0f;
-    uint32_t last = 0;
-    bool done = !in_bounds;
-    uint32_t n_eval = 0, n_hit = 0, n_proc = 0, visited = 0;
-
-    for (uint32_t chunk = start; chunk < end; chunk += 256) {
+    for (uint32_t chunk = 0; chunk < count; chunk += 256) {
         __syncthreads();
         const uint32_t idx = chunk + tid;
-        if (idx < end) {
-            const uint32_t g = a.gaussian_ids[idx];
+        if (idx < count) {
+            const uint32_t g = id(idx);
             const float4 g0 = a.geo0[g], g1 = a.geo1[g];
-            s_g0[tid] = g0;
-            s_g1[tid] = g1;
-            if (CULL) s_mask[tid] = (uint8_t)warp_mask(g0.x, g0.y, a.ext[g], tx, ty);
+            sm.g0[tid] = g0;
+            sm.g1[tid] = g1;
+            if (CULL) sm.mask[tid] = (uint8_t)warp_mask(g0.x, g0.y, a.ext[g], tx, ty);
             if (MODE == 0) {
-                s_col[tid] = a.color[g];
+                sm.col[tid] = a.color[g];
             } else {
-                s_gid[tid] = g;
-                s_acc0[tid] = 0u;
-                if (MODE == 2) s_acc1[tid] = 0u;
+                sm.gid[tid] = g;
+                sm.acc0[tid] = 0u;
+                if (MODE == 2) sm.acc1[tid] = 0u;
             }
         }
-        if (__syncthreads_count(done) == 256) break;
-        const uint32_t cnt = min(256u, end - chunk);
-        visited += cnt;
+        if (__syncthreads_count(ps.done) == 256) return true;
+        const uint32_t cnt = min(256u, count - chunk);
+        ps.visited += cnt;
         // One (warp, entry) step: every lane of the warp runs it together.
         auto step = [&](uint32_t j) {
-            if (DETAIL) ++n_proc;
+            if (DETAIL) ++ps.n_proc;
             uint32_t q = 0;
-            if (!done) {
-                const float4 g0 = s_g0[j];
-                const float4 g1 = s_g1[j];
+            if (!ps.done) {
+                const float4 g0 = sm.g0[j];
+                const float4 g1 = sm.g1[j];
                 const float dx = g0.x - fx, dy = g0.y - fy;
                 const float power = fma_(g0.z * dx, dx, fma_(g1.x * dy, dy, (g0.w * dx) * dy));
                 if (!(power > g1.z)) {
-                    if (DETAIL) ++n_eval;
+                    if (DETAIL) ++ps.n_eval;
                     const float alpha = fminf(g1.y * exp_neg_(-power), 0.999f);
                     if (alpha >= inv255) {
-                        if (DETAIL) ++n_hit;
-                        const float vis = alpha * T;
+                        if (DETAIL) ++ps.n_hit;
+                        const float vis = alpha * ps.T;
                         if (MODE == 0) {
-                            const float4 c = s_col[j];
-                            pr = fma_(c.x, vis, pr);
-                            pg = fma_(c.y, vis, pg);
-                            pb = fma_(c.z, vis, pb);
+                            const float4 c = sm.col[j];
+                            ps.pr = fma_(c.x, vis, ps.pr);
+                            ps.pg = fma_(c.y, vis, ps.pg);
+                            ps.pb = fma_(c.z, vis, ps.pb);
                         } else {
                             q = sat_u32(vis * a.scale);
                         }
-                        T = T * (1.0f - alpha);
-                        last = chunk - start + j + 1;
-                        if (T < inv255) done = true;
+                        ps.T = ps.T * (1.0f - alpha);
+                        ps.last = list_off + chunk + j + 1;
+                        if (ps.T < inv255) ps.done = true;
                     }
                 }
             }
             if (MODE == 1) {
                 const uint32_t s = __reduce_add_sync(0xffffffffu, q);
-                if (lane == 0 && s) atomicAdd(&s_acc0[j], s);
+                if (lane == 0 && s) atomicAdd(&sm.acc0[j], s);
             } else if (MODE == 2) {
                 const uint32_t qf = inside ? q : 0u;
                 const uint32_t sf = __reduce_add_sync(0xffffffffu, qf);
                 const uint32_t sb = __reduce_add_sync(0xffffffffu, q - qf);
                 if (lane == 0) {
-                    if (sf) atomicAdd(&s_acc0[j], sf);
-                    if (sb) atomicAdd(&s_acc1[j], sb);
+                    if (sf) atomicAdd(&sm.acc0[j], sf);
+                    if (sb) atomicAdd(&sm.acc1[j], sb);
                 }
             }
         };
@@ -408,9 +424,9 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
             // This warp's entries of the chunk, 32 candidates per ballot;
             // only entries with the warp's bit are walked, in list order.
             for (uint32_t g32 = 0; g32 < cnt; g32 += 32) {
-                if (__all_sync(0xffffffffu, done)) break;
+                if (__all_sync(0xffffffffu, ps.done)) break;
                 uint32_t word = __ballot_sync(0xffffffffu,
-                                              g32 + lane < cnt && ((s_mask[g32 + lane] >> warp) & 1u));
+                                              g32 + lane < cnt && ((sm.mask[g32 + lane] >> warp) & 1u));
                 while (word) {
                     const uint32_t j = g32 + (uint32_t)(__ffs(word) - 1);
                     word &= word - 1u;
@@ -423,43 +439,254 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
         if (MODE != 0) {
             __syncthreads();
             if (tid < cnt) {
-                const uint32_t g = s_gid[tid];
+                const uint32_t g = sm.gid[tid];
                 if (MODE == 1) {
-                    if (s_acc0[tid]) atomicAdd(a.resp + g, s_acc0[tid]);
+                    if (sm.acc0[tid]) atomicAdd(a.resp + g, sm.acc0[tid]);
                 } else {
-                    if (s_acc0[tid]) atomicAdd(a.fg + g, s_acc0[tid]);
-                    if (s_acc1[tid]) atomicAdd(a.bg + g, s_acc1[tid]);
+                    if (sm.acc0[tid]) atomicAdd(a.fg + g, sm.acc0[tid]);
+                    if (sm.acc1[tid]) atomicAdd(a.bg + g, sm.acc1[tid]);
                 }
+            }
+        }
+    }
+    return false;
+}
+
+__device__ __forceinline__ unsigned long long pair_value(uint2 p) {
+    return ((unsigned long long)p.x << 32) | p.y;
+}
+
+// Block min / max of 64-bit values (uniform); s64 holds 2 * 8 words.
+__device__ void block_minmax64(unsigned long long lo, unsigned long long hi, unsigned long long* s64,
+                               unsigned long long& mn, unsigned long long& mx) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (uint32_t d = 16; d > 0; d >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, d));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, d));
+    }
+    __syncthreads();
+    if (lane == 0) {
+        s64[warp] = lo;
+        s64[8 + warp] = hi;
+    }
+    __syncthreads();
+    mn = s64[0];
+    mx = s64[8];
+    for (uint32_t w = 1; w < 8; ++w) {
+        mn = min(mn, s64[w]);
+        mx = max(mx, s64[8 + w]);
+    }
+    __syncthreads();
+}
+
+// Bitonic sort of v[0, m) ascending in shared memory (m <= kSlab), padded to
+// a power of two with the largest value.
+__device__ void bitonic_sort64(unsigned long long* v, uint32_t m) {
+    uint32_t p = 1;
+    while (p < m) p <<= 1;
+    for (uint32_t i = m + threadIdx.x; i < p; i += 256) v[i] = ~0ull;
+    __syncthreads();
+    for (uint32_t k = 2; k <= p; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < p; i += 256) {
+                const uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    const unsigned long long x = v[i], y = v[ixj];
+                    const bool up = (i & k) == 0;
+                    if ((x > y) == up) {
+                        v[i] = y;
+                        v[ixj] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <int MODE, bool CULL, bool DETAIL, bool LAZY>
+__global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
+    __shared__ float4 s_g0[256];
+    __shared__ float4 s_g1[256];
+    __shared__ float4 s_col[MODE == 0 ? 256 : 1];
+    __shared__ uint32_t s_gid[MODE == 0 ? 1 : 256];
+    __shared__ uint32_t s_acc0[MODE == 0 ? 1 : 256];
+    __shared__ uint32_t s_acc1[MODE == 2 ? 256 : 1];
+    __shared__ uint8_t s_mask[256];
+    __shared__ unsigned long long s_slab[LAZY ? kSlab : 1];
+    __shared__ uint32_t s_hist[LAZY ? 256 : 1];
+    __shared__ unsigned long long s_64[16];
+    __shared__ uint32_t s_ctl[4];
+
+    const uint32_t tile = blockIdx.x;
+    const uint32_t tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u;
+    const uint32_t warp = tid >> 5;
+    const uint32_t px = tx * 16 + (warp & 1u) * 8 + (lane & 7u);
+    const uint32_t py = ty * 16 + (warp >> 1) * 4 + (lane >> 3);
+    const bool in_bounds = px < a.w && py < a.h;
+    const float fx = (float)px + 0.5f, fy = (float)py + 0.5f;
+    uint32_t inside = 0;
+    if (MODE == 2 && in_bounds) inside = (a.mask[px / 32 + py * a.mask_wpr] >> (px % 32)) & 1u;
+    const uint32_t start = a.tile_start[tile], end = a.tile_start[tile + 1];
+    const RasterSmem sm{s_g0, s_g1, s_col, s_gid, s_acc0, s_acc1, s_mask};
+    PixelState ps{1.0f, 0.0f, 0.0f, 0.0f, 0u, !in_bounds, 0u, 0u, 0u, 0u};
+
+    if (!LAZY) {
+        const uint32_t* ids = a.gaussian_ids + start;
+        composite_list<MODE, CULL, DETAIL>(
+            a, sm, [&](uint32_t i) { return ids[i]; }, end - start, 0, tx, ty, fx, fy, inside, ps);
+    } else if (end > start) {
+        const uint2* pairs = a.pairs + start;
+        const uint32_t n = end - start;
+        unsigned long long lo = ~0ull, hi = 0;
+        for (uint32_t i = tid; i < n; i += 256) {
+            const unsigned long long v = pair_value(pairs[i]);
+            lo = min(lo, v);
+            hi = max(hi, v);
+        }
+        unsigned long long vmin, vmax;
+        block_minmax64(lo, hi, s_64, vmin, vmax);
+        auto slab_id = [&](uint32_t i) { return (uint32_t)s_slab[i]; };
+        if (n <= kFirstSlab) {
+            for (uint32_t i = tid; i < n; i += 256) s_slab[i] = pair_value(pairs[i]);
+            __syncthreads();
+            bitonic_sort64(s_slab, n);
+            composite_list<MODE, CULL, DETAIL>(a, sm, slab_id, n, 0, tx, ty, fx, fy, inside, ps);
+        } else {
+            unsigned long long cur = vmin;
+            uint32_t pos = 0;
+            // The first slab aims at kFirstSlab entries (most tiles saturate
+            // well inside it), later ones at the full kSlab.
+            uint32_t target = kFirstSlab;
+            for (;;) {
+                // Pick [cur, sel] holding at most `target` of the values left
+                // (one whole bin of up to kSlab when the first bin alone is
+                // past the target).
+                unsigned long long top = vmax, sel = vmax;
+                for (;;) {
+                    const unsigned long long width = top - cur;
+                    const uint32_t wbits = width == 0 ? 0u : 64u - (uint32_t)__clzll(width);
+                    const uint32_t shift = wbits > 8 ? wbits - 8 : 0u;
+                    s_hist[tid] = 0;
+                    __syncthreads();
+                    for (uint32_t i = tid; i < n; i += 256) {
+                        const unsigned long long v = pair_value(pairs[i]);
+                        if (v >= cur && v <= top) atomicAdd(&s_hist[(uint32_t)((v - cur) >> shift)], 1u);
+                    }
+                    __syncthreads();
+                    if (tid < 32) {
+                        // Warp 0: prefix over the 256 bins (8 per lane), the
+                        // last bin whose running total stays within target.
+                        const uint32_t nb = (uint32_t)(width >> shift) + 1u;
+                        uint32_t c[8], run = 0;
+#pragma unroll
+                        for (uint32_t q = 0; q < 8; ++q) {
+                            const uint32_t b = lane * 8 + q;
+                            c[q] = b < nb ? s_hist[b] : 0u;
+                            run += c[q];
+                        }
+                        uint32_t incl = run;
+#pragma unroll
+                        for (uint32_t d = 1; d < 32; d <<= 1) {
+                            const uint32_t x = __shfl_up_sync(0xffffffffu, incl, d);
+                            if (lane >= d) incl += x;
+                        }
+                        uint32_t acc = incl - run, best = 0u;
+                        bool any = false;
+#pragma unroll
+                        for (uint32_t q = 0; q < 8; ++q) {
+                            acc += c[q];
+                            const uint32_t b = lane * 8 + q;
+                            if (b < nb && acc <= target) {
+                                best = b;
+                                any = true;
+                            }
+                        }
+                        const uint32_t e = __reduce_max_sync(0xffffffffu, any ? best + 1u : 0u);
+                        if (lane == 0) {
+                            const uint32_t h0 = s_hist[0];
+                            // e == 0: even bin 0 is past the target.
+                            s_ctl[0] = e > 0 ? 1u : (h0 <= kSlab ? 1u : 0u);
+                            s_ctl[1] = e > 0 ? e - 1u : 0u;
+                            s_ctl[2] = nb;
+                        }
+                    }
+                    __syncthreads();
+                    const uint32_t e = s_ctl[1], bins = s_ctl[2];
+                    if (!s_ctl[0]) {
+                        // The first bin holds more than kSlab: narrow to it.
+                        top = cur + ((1ull << shift) - 1ull);
+                        continue;
+                    }
+                    sel = (e + 1 >= bins) ? top : cur + (((unsigned long long)(e + 1)) << shift) - 1ull;
+                    break;
+                }
+                if (tid == 0) s_ctl[3] = 0;
+                __syncthreads();
+                for (uint32_t i = tid; i < n; i += 256) {
+                    const unsigned long long v = pair_value(pairs[i]);
+                    if (v >= cur && v <= sel) s_slab[atomicAdd(&s_ctl[3], 1u)] = v;
+                }
+                __syncthreads();
+                const uint32_t m = s_ctl[3];
+                bitonic_sort64(s_slab, m);
+                if (composite_list<MODE, CULL, DETAIL>(a, sm, slab_id, m, pos, tx, ty, fx, fy, inside, ps))
+                    break;
+                pos += m;
+                if (sel == vmax) break;
+                cur = sel + 1;
+                target = kSlab;
+                __syncthreads();
             }
         }
     }
     if (a.stats) {
         if (DETAIL) {
-            const uint32_t e = __reduce_add_sync(0xffffffffu, n_eval);
-            const uint32_t c = __reduce_add_sync(0xffffffffu, n_hit);
-            const uint32_t pr_ = __reduce_add_sync(0xffffffffu, n_proc);
+            const uint32_t e = __reduce_add_sync(0xffffffffu, ps.n_eval);
+            const uint32_t c = __reduce_add_sync(0xffffffffu, ps.n_hit);
+            const uint32_t pr_ = __reduce_add_sync(0xffffffffu, ps.n_proc);
             if (lane == 0) {
                 atomicAdd(a.stats + 1, (unsigned long long)e);
                 atomicAdd(a.stats + 2, (unsigned long long)c);
                 atomicAdd(a.stats + 3, (unsigned long long)pr_);
             }
         }
-        if (tid == 0) atomicAdd(a.stats, 256ull * visited);
+        // Algorithmic pairs: 256 per entry of the sorted list that a walk
+        // in 256-entry chunks covers until every pixel is saturated — the
+        // entry that saturates the tile's last pixel, rounded up to a chunk
+        // (the whole list if a pixel never saturates). The same count for
+        // either list order.
+        const uint32_t n_list = end - start;
+        uint32_t e = ps.done ? ps.last : n_list;
+        e = __reduce_max_sync(0xffffffffu, e);
+        __syncthreads();
+        if (tid == 0) s_ctl[0] = 0;
+        __syncthreads();
+        if (lane == 0) atomicMax(&s_ctl[0], e);
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t emax = s_ctl[0];
+            const uint64_t chunks = ((uint64_t)emax + 255u) / 256u * 256u;
+            const uint64_t walked = chunks < n_list ? chunks : (uint64_t)n_list;
+            atomicAdd(a.stats, 256ull * walked);
+        }
     }
     if (!in_bounds) return;
     const size_t pix = (size_t)py * a.w + px;
     if (MODE == 0) {
         if (a.bitmap) {
-            const uint32_t r = sat_u32(clamp_(pr * 255.0f, 0.0f, 255.0f));
-            const uint32_t g = sat_u32(clamp_(pg * 255.0f, 0.0f, 255.0f));
-            const uint32_t b = sat_u32(clamp_(pb * 255.0f, 0.0f, 255.0f));
-            const uint32_t al = sat_u32(clamp_((1.0f - T) * 255.0f, 0.0f, 255.0f));
+            const uint32_t r = sat_u32(clamp_(ps.pr * 255.0f, 0.0f, 255.0f));
+            const uint32_t g = sat_u32(clamp_(ps.pg * 255.0f, 0.0f, 255.0f));
+            const uint32_t b = sat_u32(clamp_(ps.pb * 255.0f, 0.0f, 255.0f));
+            const uint32_t al = sat_u32(clamp_((1.0f - ps.T) * 255.0f, 0.0f, 255.0f));
             a.bitmap[(size_t)py * a.row_stride + px] = r | (g << 8) | (b << 16) | (al << 24);
         }
-        if (a.rgba) a.rgba[pix] = make_float4(pr, pg, pb, 1.0f - T);
+        if (a.rgba) a.rgba[pix] = make_float4(ps.pr, ps.pg, ps.pb, 1.0f - ps.T);
     }
-    if (a.final_t) a.final_t[pix] = T;
-    if (a.n_contrib) a.n_contrib[pix] = last;
+    if (a.final_t) a.final_t[pix] = ps.T;
+    if (a.n_contrib) a.n_contrib[pix] = ps.last;
 }
 
 __global__ void export_rows_kernel(const float4* __restrict__ geo0, const float4* __restrict__ geo1,
@@ -520,15 +747,21 @@ cudaError_t launch_tile_starts(const uint32_t* sorted_tile_ids, uint32_t num_ise
     return cudaGetLastError();
 }
 
+template <int MODE, bool LAZY>
+void raster_dispatch2(const RasterArgs& a, uint32_t tiles, cudaStream_t stream) {
+    if (a.cull) {
+        if (a.detail) raster_kernel<MODE, true, true, LAZY><<<tiles, 256, 0, stream>>>(a);
+        else raster_kernel<MODE, true, false, LAZY><<<tiles, 256, 0, stream>>>(a);
+    } else {
+        if (a.detail) raster_kernel<MODE, false, true, LAZY><<<tiles, 256, 0, stream>>>(a);
+        else raster_kernel<MODE, false, false, LAZY><<<tiles, 256, 0, stream>>>(a);
+    }
+}
+
 template <int MODE>
 void raster_dispatch(const RasterArgs& a, uint32_t tiles, cudaStream_t stream) {
-    if (a.cull) {
-        if (a.detail) raster_kernel<MODE, true, true><<<tiles, 256, 0, stream>>>(a);
-        else raster_kernel<MODE, true, false><<<tiles, 256, 0, stream>>>(a);
-    } else {
-        if (a.detail) raster_kernel<MODE, false, true><<<tiles, 256, 0, stream>>>(a);
-        else raster_kernel<MODE, false, false><<<tiles, 256, 0, stream>>>(a);
-    }
+    if (a.pairs) raster_dispatch2<MODE, true>(a, tiles, stream);
+    else raster_dispatch2<MODE, false>(a, tiles, stream);
 }
 
 cudaError_t launch_raster(int mode, const RasterArgs& a, cudaStream_t stream) {

@@ -130,7 +130,7 @@ struct sf_round_t {
     const void* g_splats = nullptr;
     const void* g_beta = nullptr;
     int g_mode = -1;
-    uint32_t g_lanes = 0, g_cull = 0, g_build = 0;
+    uint32_t g_lanes = 0, g_cull = 0, g_build = 0, g_order = 0;
     uint32_t chunks = 1;
     std::vector<const sf_mask_t*> g_masks;
 };
@@ -233,7 +233,8 @@ cudaError_t depth_sorted_isects(sf_round_t* r, RoundLane& L, uint32_t n, uint32_
 
 // Responsibility (or evidence) raster of view v and its EIG.
 cudaError_t raster_and_eig(sf_round_t* r, RoundLane& L, uint32_t v, uint32_t tx, uint32_t ty, const uint32_t* gids,
-                           const float* beta_a, const float* beta_b, const float* lut, int mode, cudaStream_t st) {
+                           const uint2* pairs, const float* beta_a, const float* beta_b, const float* lut, int mode,
+                           cudaStream_t st) {
     cudaError_t e;
     const uint32_t n = r->n;
     const uint32_t w = r->w[v], h = r->h[v];
@@ -248,6 +249,7 @@ cudaError_t raster_and_eig(sf_round_t* r, RoundLane& L, uint32_t v, uint32_t tx,
     a.tiles_y = ty;
     a.tile_start = L.tile_start;
     a.gaussian_ids = gids;
+    a.pairs = pairs;
     a.geo0 = L.geo0;
     a.geo1 = L.geo1;
     a.ext = L.ext;
@@ -289,6 +291,7 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
     sf_view dummy{};
     if ((e = launch_project(dummy, sp.attr, sp.sh, n, sp.K, po, st, r->views_dev + v)) != cudaSuccess) return e;
     const uint32_t *tids = nullptr, *gids = nullptr;
+    const uint2* lazy_pairs = nullptr;
     if (r->tuning.isect_build == SF_ISECTS_BINNED && L.hist) {
         // Binned build with device-side counts: the sorts take every tile as
         // the bound of each class and read the class sizes on the device.
@@ -305,16 +308,20 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
             return e;
         clamp_starts_kernel<<<(tiles + 1 + 255) / 256, 256, 0, st>>>(L.tile_start, tiles + 1, (uint32_t)L.cap);
         note_launches(1);
-        const uint32_t grids[4] = {tiles, tiles, tiles, tiles};
-        if ((e = launch_tile_sorts(grids, L.lists, words, tiles, L.tile_start, (uint32_t)L.cap, pairs, L.gid_e,
-                                   nullptr, L.tid_e, r->sm_count, st)) != cudaSuccess)
-            return e;
-        gids = L.gid_e;
+        if (r->tuning.raster_order == SF_ORDER_IN_RASTER) {
+            lazy_pairs = pairs;
+        } else {
+            const uint32_t grids[4] = {tiles, tiles, tiles, tiles};
+            if ((e = launch_tile_sorts(grids, L.lists, words, tiles, L.tile_start, (uint32_t)L.cap, pairs, L.gid_e,
+                                       nullptr, L.tid_e, r->sm_count, st)) != cudaSuccess)
+                return e;
+            gids = L.gid_e;
+        }
     } else {
         if ((e = depth_sorted_isects(r, L, n, tx, tiles, words, total, st, &tids, &gids)) != cudaSuccess)
             return e;
     }
-    return raster_and_eig(r, L, v, tx, ty, gids, beta_a, beta_b, lut, mode, st);
+    return raster_and_eig(r, L, v, tx, ty, gids, lazy_pairs, beta_a, beta_b, lut, mode, st);
 }
 
 }  // namespace
@@ -380,6 +387,7 @@ int build_graph(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, int
     r->g_lanes = (uint32_t)r->lanes.size();
     r->g_cull = r->tuning.raster_cull;
     r->g_build = r->tuning.isect_build;
+    r->g_order = r->tuning.raster_order;
     r->g_masks = r->masks;
     return SF_OK;
 }
@@ -394,7 +402,8 @@ int run_round(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, const
             RF_CK(lanes_build(r, lanes, std::max<uint64_t>(r->want_cap, r->lanes.empty() ? 1024 : r->lanes[0].cap)));
         }
         if (!r->exec || r->g_splats != sp || r->g_beta != beta || r->g_mode != mode ||
-            r->g_cull != r->tuning.raster_cull || r->g_build != r->tuning.isect_build || r->g_masks != r->masks) {
+            r->g_cull != r->tuning.raster_cull || r->g_build != r->tuning.isect_build ||
+            r->g_order != r->tuning.raster_order || r->g_masks != r->masks) {
             const int rc = build_graph(r, sp, beta, mode);
             if (rc != SF_OK) return rc;
         }
@@ -498,7 +507,8 @@ int sf_round_destroy(sf_round r) {
 
 int sf_round_set_tuning(sf_round r, const sf_round_tuning* t) {
     if (!r || !t) return rfail(SF_ERR_ARG, "null argument");
-    if (t->raster_cull > 1 || t->lanes > 64 || t->isect_build > SF_ISECTS_DEPTH_SORTED)
+    if (t->raster_cull > 1 || t->lanes > 64 || t->isect_build > SF_ISECTS_DEPTH_SORTED ||
+        t->raster_order > SF_ORDER_IN_RASTER)
         return rfail(SF_ERR_ARG, "bad tuning");
     r->tuning = *t;
     return SF_OK;

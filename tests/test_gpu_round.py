@@ -26,9 +26,11 @@ def cams_on_sphere(k, radius, seed):
     return synth.sphere_cameras(k, radius, seed, sf.look_at)
 
 
-@pytest.mark.parametrize("lanes,cull,build", [(1, 0, sf.ISECTS_BINNED), (3, 0, sf.ISECTS_DEPTH_SORTED),
-                                              (4, 1, sf.ISECTS_BINNED), (2, 1, sf.ISECTS_DEPTH_SORTED)])
-def test_round_matches_plain_per_view(ctx, lanes, cull, build):
+@pytest.mark.parametrize("lanes,cull,build,order", [
+    (1, 0, sf.ISECTS_BINNED, sf.ORDER_IN_RASTER), (3, 0, sf.ISECTS_DEPTH_SORTED, sf.ORDER_IN_RASTER),
+    (4, 1, sf.ISECTS_BINNED, sf.ORDER_SORTED), (2, 1, sf.ISECTS_DEPTH_SORTED, sf.ORDER_SORTED),
+    (2, 1, sf.ISECTS_BINNED, sf.ORDER_IN_RASTER)])
+def test_round_matches_plain_per_view(ctx, lanes, cull, build, order):
     n = 30000
     attr, sh = synth.scene_clustered(n, 4, seed=3, clusters=4, sigma=0.25, extent=1.0)
     a, b = synth.beta_posterior(n, seed=3)
@@ -37,7 +39,7 @@ def test_round_matches_plain_per_view(ctx, lanes, cull, build):
     sizes = [(64, 48), (128, 128), (96, 160), (70, 70), (33, 17)]
     cams = cams_on_sphere(len(sizes), 3.0, 5)
     rnd = sf.Round(n, sizes)
-    rnd.set_tuning(lanes=lanes, raster_cull=cull, isect_build=build)
+    rnd.set_tuning(lanes=lanes, raster_cull=cull, isect_build=build, raster_order=order)
     for mode in (sf.EIG_LUT_F32, sf.EIG_FP64):
         eig = rnd.eig(splats, beta, cams, mode)
         want = plain(splats, beta, cams, sizes, mode)
@@ -65,8 +67,10 @@ def test_round_graph_replays_with_new_cameras(ctx):
             assert eig[v] == want[v][2]
 
 
-@pytest.mark.parametrize("build", [sf.ISECTS_BINNED, sf.ISECTS_DEPTH_SORTED])
-def test_round_capacity_grows_and_reruns(ctx, build):
+@pytest.mark.parametrize("build,order", [(sf.ISECTS_BINNED, sf.ORDER_IN_RASTER),
+                                         (sf.ISECTS_BINNED, sf.ORDER_SORTED),
+                                         (sf.ISECTS_DEPTH_SORTED, sf.ORDER_SORTED)])
+def test_round_capacity_grows_and_reruns(ctx, build, order):
     """Large splats push the intersections past the first-round capacity
     (min(tiles * n, 2^22)); the round grows and re-runs, results unchanged."""
     n = 60000
@@ -78,7 +82,7 @@ def test_round_capacity_grows_and_reruns(ctx, build):
     sizes = [(512, 512), (256, 256)]
     cams = [sf.look_at((0.0, 0.0, -3.0), (0, 0, 0)), sf.look_at((0.5, 0.3, -3.0), (0, 0, 0))]
     rnd = sf.Round(n, sizes)
-    rnd.set_tuning(isect_build=build)
+    rnd.set_tuning(isect_build=build, raster_order=order)
     rnd.eig(splats, None, cams)
     _, _, nis, _ = rnd.responsibility(0)
     assert nis > (1 << 22)
