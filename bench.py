@@ -51,6 +51,11 @@ WORKLOAD = ("frame: 1M splats SH3 (8 Gaussian clusters sigma 0.3 in [-2,2]^3), 1
             "30-camera radius-4 orbit")
 METRIC = "1080p frames/s @1M splats"
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 lanes x FMA x 1.965 GHz
+# DRAM bytes (read + write) of one rasterizer launch of this workload, from an
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, orbit camera 3:
+# 47.40 MB + 1.59 MB). Traffic far above the gathered records would mean
+# re-reads; here it is the walked entries' records and ids.
+RASTER_TRAFFIC_BYTES = 48.99e6
 RASTER_FLOPS_PER_PAIR = 24
 
 
@@ -308,7 +313,7 @@ def run_ours(args, rank, world):
     import torch
 
     import splatfield_b200 as sf
-    from splatfield_b200 import _lib
+    from splatfield_b200 import _lib, replicas
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -322,7 +327,7 @@ def run_ours(args, rank, world):
     splats = sf.Splats(attr, sh, ctx)
     scratch = sf.RenderScratch(N_SPLATS, (WIDTH, HEIGHT), ctx)
     cams = orbit(sf.look_at)
-    my_cams = [cams[(rank + world * i) % N_CAMS] for i in range(N_CAMS)]
+    my_cams = replicas.replica_share(cams, rank, world)
     stream = torch.cuda.current_stream()
     size = (WIDTH, HEIGHT)
 
@@ -352,11 +357,7 @@ def run_ours(args, rank, world):
         end.record(stream)
         torch.cuda.synchronize()
     launches = _lib.lib().sf_kernel_launches() - launches0
-    ms = start.elapsed_time(end)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(start.elapsed_time(end), dist)
     fps = world * args.steps / (ms / 1e3)
 
     # ---- per-stage split: prepare (everything before the rasterizer) vs rasterizer
@@ -406,11 +407,7 @@ def run_ours(args, rank, world):
     t0 = time.perf_counter()
     for i in range(args.steps):
         splats.render_to_host(scratch, my_cams[i % N_CAMS], size, out=host_out, stream=stream)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dist)
     if pin is not None:
         _lib.lib().sf_host_free(pin)
     e2e_fps = world * args.steps / e2e_s
@@ -436,7 +433,9 @@ def run_ours(args, rank, world):
                 "path": "sf_render_to_host (camera by value, RGBA8 image to pinned host memory)"},
         "roofline": {"kernel": "raster_kernel<RGB>", "bound": "fp32", "achieved": achieved,
                      "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_TFLOPS,
-                     "traffic": None, "pairs_per_frame": pairs,
+                     "traffic": RASTER_TRAFFIC_BYTES,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch, camera 3",
+                     "pairs_per_frame": pairs,
                      "flops_per_pair": RASTER_FLOPS_PER_PAIR,
                      "pairs_processed_per_frame": detail["pairs_processed"] / n_split,
                      "accounting": "algorithmic pairs = 256 per tile-list entry walked before the "
