@@ -163,7 +163,9 @@ typedef struct {
      * sf_render_responsibility, the round), binned build only:
      *   SF_ORDER_SORTED (default): every tile list is sorted first;
      *   SF_ORDER_IN_RASTER: the rasterizer orders each tile's placed pairs
-     *     slab by slab, only as far as the tile saturates.
+     *     slab by slab, only as far as the tile saturates;
+     *   SF_ORDER_HYBRID: lists of up to 12288 entries are sorted, longer
+     *     ones are ordered in the rasterizer.
      * Same results either way. sf_prepare_isects and sf_render_forward always
      * sort (their lists are handed out or replayed). */
     uint32_t raster_order;
@@ -173,6 +175,7 @@ typedef struct {
 #define SF_ISECTS_DEPTH_SORTED 1u
 #define SF_ORDER_SORTED 0u
 #define SF_ORDER_IN_RASTER 1u
+#define SF_ORDER_HYBRID 2u
 int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t);
 int sf_scratch_get_tuning(sf_scratch s, sf_tuning* t);
 
@@ -366,7 +369,8 @@ int sf_round_evidence(sf_round r, sf_splats s, sf_beta beta, const sf_camera* ca
                       const sf_mask* masks, int mode, sf_stream stream, double* eig);
 /* View `view` of the last evidence round: device fg and bg words [total]. */
 int sf_round_evidence_words(sf_round r, uint32_t view, const uint32_t** fg, const uint32_t** bg);
-/* Autotuner: times the round over lanes {1,2,4,8} x raster_cull {0,1}, keeps
+/* Autotuner: times the round over lanes {1,2,4,8} x raster_cull {0,1} (x
+ * raster_order {sorted, in-raster, hybrid} with the binned build), keeps
  * the fastest on the round and in a process-wide cache keyed by (device,
  * splats, view sizes); a cached shape is not re-timed unless best_ms is
  * requested. */

@@ -27,7 +27,7 @@ READ_TILE_IDS, READ_GAUSSIAN_IDS, READ_TILE_START, READ_BITMAP, READ_RGBA, READ_
 
 EIG_LUT_F32, EIG_FP64 = 0, 1
 ISECTS_BINNED, ISECTS_DEPTH_SORTED = 0, 1
-ORDER_SORTED, ORDER_IN_RASTER = 0, 1
+ORDER_SORTED, ORDER_IN_RASTER, ORDER_HYBRID = 0, 1, 2
 
 
 class SplatfieldError(RuntimeError):

@@ -26,12 +26,12 @@ __all__ = [
     "RenderScratch", "TileIsects", "Accumulators", "Mask", "BetaState", "map_labels", "bits_for",
     "RadixScratch", "ScanScratch", "exclusive_scan_gather", "exclusive_scan_buf", "entropy_table",
     "table_entropy", "fractional_bits", "row_stride_for", "EIG_LUT_F32", "EIG_FP64", "Round",
-    "ISECTS_BINNED", "ISECTS_DEPTH_SORTED", "ORDER_IN_RASTER", "ORDER_SORTED", "ply_inspect", "load_ply",
+    "ISECTS_BINNED", "ISECTS_DEPTH_SORTED", "ORDER_IN_RASTER", "ORDER_SORTED", "ORDER_HYBRID", "ply_inspect", "load_ply",
 ]
 
 EIG_LUT_F32, EIG_FP64 = L.EIG_LUT_F32, L.EIG_FP64
 ISECTS_BINNED, ISECTS_DEPTH_SORTED = L.ISECTS_BINNED, L.ISECTS_DEPTH_SORTED
-ORDER_IN_RASTER, ORDER_SORTED = L.ORDER_IN_RASTER, L.ORDER_SORTED
+ORDER_IN_RASTER, ORDER_SORTED, ORDER_HYBRID = L.ORDER_IN_RASTER, L.ORDER_SORTED, L.ORDER_HYBRID
 BASE_FOV = 0.8  # Camera::BASE_FOV (src/camera.rs:86)
 
 
@@ -451,7 +451,7 @@ class RenderScratch:
         """Kernel forms (results are identical across forms): raster_cull 0/1,
         isect_build ISECTS_BINNED (default) or ISECTS_DEPTH_SORTED,
         raster_detail 1 to count the per-pair diagnostics of ``stats``,
-        raster_order ORDER_SORTED (default) or ORDER_IN_RASTER."""
+        raster_order ORDER_SORTED (default), ORDER_IN_RASTER or ORDER_HYBRID."""
         t = L.Tuning()
         t.raster_cull = int(raster_cull)
         t.isect_build = int(isect_build)

@@ -135,6 +135,7 @@ struct sf_scratch_t {
     // The last prepare left the binned build's placed pairs unsorted: the
     // rasterizer orders each tile's list itself (no gaussian_ids).
     bool lazy = false;
+    uint32_t lazy_min = 0;  // lists longer than this are ordered in the raster
     uint32_t* bitmap = nullptr;
     float4* rgba = nullptr;
     float* final_t = nullptr;
@@ -285,7 +286,9 @@ int finish_prepare(sf_scratch s, sf_isects* out);
 
 // Binned intersection build (sf_bin.cu) after the projection: count, column
 // scan, tile scan, one sync for the total, place, per-tile sorts.
-int prepare_binned(sf_scratch s, uint32_t n, uint32_t tiles, cudaStream_t st, bool want_tile_ids, bool lazy) {
+// order: SF_ORDER_SORTED sorts every list; SF_ORDER_IN_RASTER none;
+// SF_ORDER_HYBRID all but the longest (left to the rasterizer).
+int prepare_binned(sf_scratch s, uint32_t n, uint32_t tiles, cudaStream_t st, bool want_tile_ids, uint32_t order) {
     uint32_t* words = s->words;
     unsigned long long* total_dev = reinterpret_cast<unsigned long long*>(words + 4);
     SF_CK(launch_bin_count(s->bbox, n, s->tiles_x, tiles, s->bin_chunks, s->bin_hist, st));
@@ -309,11 +312,12 @@ int prepare_binned(sf_scratch s, uint32_t n, uint32_t tiles, cudaStream_t st, bo
     uint2* pairs = reinterpret_cast<uint2*>(s->tid_a);
     SF_CK(launch_bin_place(s->bbox, s->depth_keys, n, s->tiles_x, tiles, s->bin_chunks, s->bin_hist,
                            s->tile_start, (uint32_t)s->cap, pairs, words + 1, st));
-    s->lazy = lazy;
-    if (lazy) {
+    s->lazy = order != SF_ORDER_SORTED;
+    s->lazy_min = order == SF_ORDER_HYBRID ? kBinSharedMax : 0u;
+    if (order == SF_ORDER_IN_RASTER) {
         s->tids = s->gids = nullptr;
     } else {
-        const uint32_t grids[4] = {hw[8], hw[9], hw[10], hw[7]};
+        const uint32_t grids[4] = {hw[8], hw[9], hw[10], order == SF_ORDER_HYBRID ? 0u : hw[7]};
         SF_CK(launch_tile_sorts(grids, s->bin_lists, words, tiles, s->tile_start, (uint32_t)s->cap, pairs,
                                 s->gid_e, want_tile_ids ? s->tid_e : nullptr, s->tid_e, s->ctx->sm_count, st));
         s->tids = want_tile_ids ? s->tid_e : nullptr;
@@ -349,7 +353,7 @@ int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32
     s->lazy = false;
     if (s->tuning.isect_build == SF_ISECTS_BINNED && s->bin_hist) {
         const int rc = prepare_binned(s, n, tiles, st, out != nullptr,
-                                      lazy && out == nullptr && s->tuning.raster_order == SF_ORDER_IN_RASTER);
+                                      (lazy && out == nullptr) ? s->tuning.raster_order : SF_ORDER_SORTED);
         if (rc != SF_OK) return rc;
         return finish_prepare(s, out);
     }
@@ -418,6 +422,7 @@ RasterArgs raster_args(sf_scratch s, const sf_isects* is) {
     a.tile_start = is ? is->tile_start : s->tile_start;
     a.gaussian_ids = is ? is->gaussian_ids : s->gids;
     a.pairs = (!is && s->lazy) ? reinterpret_cast<const uint2*>(s->tid_a) : nullptr;
+    a.lazy_min = s->lazy_min;
     a.geo0 = s->geo0;
     a.geo1 = s->geo1;
     a.color = s->color;
@@ -666,7 +671,7 @@ int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t) {
     if (!s || !t) return fail(SF_ERR_ARG, "null argument");
     if (t->raster_cull > 1 || t->raster_detail > 1) return fail(SF_ERR_ARG, "raster flags must be 0 or 1");
     if (t->isect_build > SF_ISECTS_DEPTH_SORTED) return fail(SF_ERR_ARG, "unknown isect_build");
-    if (t->raster_order > SF_ORDER_IN_RASTER) return fail(SF_ERR_ARG, "unknown raster_order");
+    if (t->raster_order > SF_ORDER_HYBRID) return fail(SF_ERR_ARG, "unknown raster_order");
     s->tuning = *t;
     return SF_OK;
 }

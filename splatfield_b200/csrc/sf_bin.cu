@@ -595,7 +595,7 @@ constexpr size_t sort_smem() {
 
 // Size classes of the shared-form sort (entries, buckets, threads); longer
 // lists take the global form.
-constexpr uint32_t kClass0 = 2048, kClass1 = 6144, kClass2 = 12288;
+constexpr uint32_t kClass0 = 2048, kClass1 = 6144, kClass2 = kBinSharedMax;
 constexpr uint32_t kBins0 = 4096, kBins1 = 8192, kBins2 = 16384, kBinsGiant = 32768;
 constexpr uint32_t kThreads0 = 256, kThreads1 = 512, kThreads2 = 1024;
 static_assert(sort_smem<kClass2, kBins2, kThreads2>() <= 227 * 1024, "per-tile sort exceeds shared memory");

@@ -59,8 +59,10 @@ struct RasterArgs {
     const uint32_t* tile_start;
     const uint32_t* gaussian_ids;
     // Unsorted placed (depth key, splat id) pairs of the binned build; when
-    // set, the rasterizer orders each tile's list itself (gaussian_ids unused).
+    // set, the rasterizer orders itself every tile list longer than
+    // lazy_min entries (the others come sorted in gaussian_ids).
     const uint2* pairs;
+    uint32_t lazy_min;
     const float4* geo0;
     const float4* geo1;
     const float4* color;
@@ -133,6 +135,9 @@ cudaError_t exclusive_scan(const uint32_t* gids, const uint32_t* counts, uint32_
 constexpr uint32_t kBinMaxTiles = 49152;
 uint32_t bin_chunks(uint32_t n, int sm_count);
 uint32_t bin_class_limit(int k);  // largest tile list sorted by size class k (0..2)
+// Longest list the shared-memory classes sort; longer lists go to the global
+// form (or, with the hybrid order, to the rasterizer).
+constexpr uint32_t kBinSharedMax = 12288;
 // hist: [chunks][tiles] counts, then (after colscan) per-chunk exclusive
 // prefixes. cnt: [tiles + 1] per-tile totals (cnt[tiles] = 0). lists:
 // [4][tiles] tiles of each size class. words: [6] max tile total, [7] tiles
@@ -146,7 +151,8 @@ cudaError_t launch_bin_place(const uint2* bbox, const uint32_t* depth_keys, uint
                              uint32_t tiles, uint32_t chunks, const uint32_t* hist, const uint32_t* tile_start,
                              uint32_t capacity, uint2* pairs, uint32_t* err, cudaStream_t st);
 // grids[k]: CTAs launched for class k (the class count when the host knows
-// it, else `tiles`; CTAs past the device count exit).
+// it, else `tiles`; CTAs past the device count exit); grids[3] = 0 leaves
+// the longest lists unsorted.
 // pairs: the placed (depth key, splat id) per slot (overwritten for the
 // longest lists); ids / tids_out receive the sorted splat ids / tile ids
 // (tids_out may be null); keys_tmp: capacity u32 of scratch (may alias

@@ -533,7 +533,7 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
     const RasterSmem sm{s_g0, s_g1, s_col, s_gid, s_acc0, s_acc1, s_mask};
     PixelState ps{1.0f, 0.0f, 0.0f, 0.0f, 0u, !in_bounds, 0u, 0u, 0u, 0u};
 
-    if (!LAZY) {
+    if (!LAZY || end - start <= a.lazy_min) {
         const uint32_t* ids = a.gaussian_ids + start;
         composite_list<MODE, CULL, DETAIL>(
             a, sm, [&](uint32_t i) { return ids[i]; }, end - start, 0, tx, ty, fx, fy, inside, ps);

@@ -250,6 +250,7 @@ cudaError_t raster_and_eig(sf_round_t* r, RoundLane& L, uint32_t v, uint32_t tx,
     a.tile_start = L.tile_start;
     a.gaussian_ids = gids;
     a.pairs = pairs;
+    a.lazy_min = r->tuning.raster_order == SF_ORDER_HYBRID ? kBinSharedMax : 0u;
     a.geo0 = L.geo0;
     a.geo1 = L.geo1;
     a.ext = L.ext;
@@ -308,10 +309,10 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
             return e;
         clamp_starts_kernel<<<(tiles + 1 + 255) / 256, 256, 0, st>>>(L.tile_start, tiles + 1, (uint32_t)L.cap);
         note_launches(1);
-        if (r->tuning.raster_order == SF_ORDER_IN_RASTER) {
-            lazy_pairs = pairs;
-        } else {
-            const uint32_t grids[4] = {tiles, tiles, tiles, tiles};
+        const uint32_t order = r->tuning.raster_order;
+        if (order != SF_ORDER_SORTED) lazy_pairs = pairs;
+        if (order != SF_ORDER_IN_RASTER) {
+            const uint32_t grids[4] = {tiles, tiles, tiles, order == SF_ORDER_HYBRID ? 0u : tiles};
             if ((e = launch_tile_sorts(grids, L.lists, words, tiles, L.tile_start, (uint32_t)L.cap, pairs, L.gid_e,
                                        nullptr, L.tid_e, r->sm_count, st)) != cudaSuccess)
                 return e;
@@ -508,7 +509,7 @@ int sf_round_destroy(sf_round r) {
 int sf_round_set_tuning(sf_round r, const sf_round_tuning* t) {
     if (!r || !t) return rfail(SF_ERR_ARG, "null argument");
     if (t->raster_cull > 1 || t->lanes > 64 || t->isect_build > SF_ISECTS_DEPTH_SORTED ||
-        t->raster_order > SF_ORDER_IN_RASTER)
+        t->raster_order > SF_ORDER_HYBRID)
         return rfail(SF_ERR_ARG, "bad tuning");
     r->tuning = *t;
     return SF_OK;
@@ -607,12 +608,15 @@ int sf_round_autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* ca
         float winner_ms = 1e30f;
         std::vector<double> eig(r->views);
         const uint32_t lane_options[] = {1, 2, 4, 8};
+        const uint32_t orders = r->tuning.isect_build == SF_ISECTS_BINNED ? 3u : 1u;
+        for (uint32_t order = 0; order < orders; ++order)
         for (uint32_t cull = 0; cull <= 1; ++cull)
             for (uint32_t lanes : lane_options) {
                 if (lanes > r->views) continue;
                 sf_round_tuning t = r->tuning;
                 t.lanes = lanes;
                 t.raster_cull = cull;
+                if (orders == 3) t.raster_order = order;
                 r->tuning = t;
                 int rc = sf_round_eig(r, s, beta, cams, mode, stream, eig.data());  // warm-up / build
                 if (rc != SF_OK) return rc;

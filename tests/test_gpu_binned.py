@@ -107,9 +107,10 @@ def scene_for(kind):
     return opaque(pos), zero_sh(n), 1, 64, 64
 
 
+@pytest.mark.parametrize("order", [sf.ORDER_IN_RASTER, sf.ORDER_HYBRID])
 @pytest.mark.parametrize("cull", [0, 1])
 @pytest.mark.parametrize("kind", ["clustered", "ties", "one_spot", "one_spot_ties"])
-def test_in_raster_order_matches_sorted_lists(ctx, oracle_mod, kind, cull):
+def test_in_raster_order_matches_sorted_lists(ctx, oracle_mod, kind, cull, order):
     """The rasterizer's own slab ordering of the unsorted placed pairs gives
     the same image, float plane and responsibility / evidence words as the
     sorted lists, and the oracle's image (tiles up to 20,000 entries, with
@@ -120,7 +121,7 @@ def test_in_raster_order_matches_sorted_lists(ctx, oracle_mod, kind, cull):
     cam = sf.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
     cam.fov[0], cam.fov[1] = synth.fov_for(w, h)
     lazy, sorted_ = sf.RenderScratch(n, (w, h)), sf.RenderScratch(n, (w, h))
-    lazy.set_tuning(raster_cull=cull, raster_order=sf.ORDER_IN_RASTER)
+    lazy.set_tuning(raster_cull=cull, raster_order=order)
     sorted_.set_tuning(raster_cull=cull, raster_order=sf.ORDER_SORTED)
     img_l = splats.render_with(lazy, cam, (w, h)).read()
     img_s = splats.render_with(sorted_, cam, (w, h)).read()

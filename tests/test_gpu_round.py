@@ -29,7 +29,7 @@ def cams_on_sphere(k, radius, seed):
 @pytest.mark.parametrize("lanes,cull,build,order", [
     (1, 0, sf.ISECTS_BINNED, sf.ORDER_IN_RASTER), (3, 0, sf.ISECTS_DEPTH_SORTED, sf.ORDER_IN_RASTER),
     (4, 1, sf.ISECTS_BINNED, sf.ORDER_SORTED), (2, 1, sf.ISECTS_DEPTH_SORTED, sf.ORDER_SORTED),
-    (2, 1, sf.ISECTS_BINNED, sf.ORDER_IN_RASTER)])
+    (2, 1, sf.ISECTS_BINNED, sf.ORDER_IN_RASTER), (3, 0, sf.ISECTS_BINNED, sf.ORDER_HYBRID)])
 def test_round_matches_plain_per_view(ctx, lanes, cull, build, order):
     n = 30000
     attr, sh = synth.scene_clustered(n, 4, seed=3, clusters=4, sigma=0.25, extent=1.0)
@@ -68,6 +68,7 @@ def test_round_graph_replays_with_new_cameras(ctx):
 
 
 @pytest.mark.parametrize("build,order", [(sf.ISECTS_BINNED, sf.ORDER_IN_RASTER),
+                                         (sf.ISECTS_BINNED, sf.ORDER_HYBRID),
                                          (sf.ISECTS_BINNED, sf.ORDER_SORTED),
                                          (sf.ISECTS_DEPTH_SORTED, sf.ORDER_SORTED)])
 def test_round_capacity_grows_and_reruns(ctx, build, order):
