@@ -136,6 +136,21 @@ struct sf_scratch_t {
     // rasterizer orders each tile's list itself (no gaussian_ids).
     bool lazy = false;
     uint32_t lazy_min = 0;  // lists longer than this are ordered in the raster
+    SortStreams sort_streams;  // concurrent per-tile sort classes inside the frame graph
+    // Frame graph (binned RGB frames): one capture per (splats, size,
+    // capacity, tuning), replayed with the camera copied in by its first node.
+    struct FrameGraph {
+        cudaGraphExec_t exec = nullptr;
+        cudaStream_t stream = nullptr;  // capture stream
+        sf_view* view_dev = nullptr;
+        sf_view* view_host = nullptr;   // pinned
+        const void* splats = nullptr;
+        const float* attr = nullptr;
+        const float* sh = nullptr;
+        uint32_t K = 0, n = 0, w = 0, h = 0;
+        uint64_t cap = 0;
+        sf_tuning tuning{};
+    } fg;
     uint32_t* bitmap = nullptr;
     float4* rgba = nullptr;
     float* final_t = nullptr;
@@ -477,6 +492,168 @@ int accumulate(sf_scratch s, const sf_isects* is, uint32_t w, uint32_t h, sf_acc
     return SF_OK;
 }
 
+// ---------------------------------------------------------- frame graph
+//
+// A binned RGB frame with no host step in the middle: projection, counts,
+// scans, placement against the current capacity (device-side guard, tile
+// starts clamped), per-tile sorts as persistent kernels reading their class
+// sizes on the device (the classes on side streams), raster, and the status
+// words back to pinned memory — captured once and replayed with one launch
+// per frame on the caller's stream. The host reads the words after the
+// frame; a frame that outgrew the capacity grows it and runs again (the
+// graph is captured anew).
+
+// frame_render's answer when the frame graph does not apply (the caller
+// takes the step-by-step path).
+constexpr int kNoFrameGraph = -2;
+
+bool frame_graph_usable(sf_splats sp, sf_scratch s) {
+    return s->bin_hist && sp->n == s->total && s->tuning.isect_build == SF_ISECTS_BINNED &&
+           !s->tuning.raster_detail;
+}
+
+int frame_graph_capture(sf_splats sp, sf_scratch s) {
+    auto& g = s->fg;
+    if (g.exec) {
+        cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    }
+    if (!g.stream) SF_CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+    if (!g.view_dev) SF_CK(dalloc(&g.view_dev, 1));
+    if (!g.view_host) SF_CK(cudaMallocHost(reinterpret_cast<void**>(&g.view_host), sizeof(sf_view)));
+    if (!s->sort_streams.s[0]) SF_CK(sort_streams_create(&s->sort_streams));
+    const uint32_t n = sp->n;
+    const uint32_t tiles = s->tiles_x * s->tiles_y;
+    const uint32_t cap = (uint32_t)s->cap;
+    const uint32_t order = s->tuning.raster_order;
+    uint32_t* words = s->words;
+    auto* total = reinterpret_cast<unsigned long long*>(words + 4);
+    cudaStream_t st = g.stream;
+    SF_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaMemcpyAsync(g.view_dev, g.view_host, sizeof(sf_view), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(words, 0, 64, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->stats, 0, 32, st);
+    ProjOut po{s->depth_keys, s->tile_counts, s->bbox, s->geo0, s->geo1, s->color, words, s->ext};
+    sf_view dummy{};
+    if (e == cudaSuccess) e = launch_project(dummy, sp->attr, sp->sh, n, sp->K, po, st, g.view_dev);
+    if (e == cudaSuccess) e = launch_bin_count(s->bbox, n, s->tiles_x, tiles, s->bin_chunks, s->bin_hist, st);
+    if (e == cudaSuccess)
+        e = launch_bin_colscan(s->bin_hist, s->bin_chunks, tiles, s->bin_cnt, s->bin_lists, words, st);
+    if (e == cudaSuccess)
+        e = exclusive_scan(nullptr, s->bin_cnt, s->tile_start, tiles + 1, nullptr, tiles + 1, s->scan_tmp, total,
+                           words + 1, st);
+    if (e == cudaSuccess) e = launch_clamp_count(total, cap, words + 2, words + 1, st);
+    uint2* pairs = reinterpret_cast<uint2*>(s->tid_a);
+    if (e == cudaSuccess)
+        e = launch_bin_place(s->bbox, s->depth_keys, n, s->tiles_x, tiles, s->bin_chunks, s->bin_hist,
+                             s->tile_start, cap, pairs, words + 1, st);
+    if (e == cudaSuccess) e = launch_clamp_starts(s->tile_start, tiles + 1, cap, st);
+    if (e == cudaSuccess && order != SF_ORDER_IN_RASTER) {
+        const uint32_t grids[4] = {tiles, tiles, tiles, order == SF_ORDER_HYBRID ? 0u : tiles};
+        e = launch_tile_sorts(grids, s->bin_lists, words, tiles, s->tile_start, cap, pairs, s->gid_e, nullptr,
+                              s->tid_e, s->ctx->sm_count, st, &s->sort_streams);
+    }
+    if (e == cudaSuccess) {
+        RasterArgs a{};
+        a.w = s->w;
+        a.h = s->h;
+        a.tiles_x = s->tiles_x;
+        a.tiles_y = s->tiles_y;
+        a.row_stride = s->row_stride;
+        a.tile_start = s->tile_start;
+        a.gaussian_ids = order == SF_ORDER_IN_RASTER ? nullptr : s->gid_e;
+        a.pairs = order == SF_ORDER_SORTED ? nullptr : pairs;
+        a.lazy_min = order == SF_ORDER_HYBRID ? kBinSharedMax : 0u;
+        a.geo0 = s->geo0;
+        a.geo1 = s->geo1;
+        a.color = s->color;
+        a.ext = s->ext;
+        a.cull = s->tuning.raster_cull;
+        a.stats = s->stats;
+        a.bitmap = s->bitmap;
+        e = launch_raster(0, a, st);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->host_words, words, 64, cudaMemcpyDeviceToHost, st);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return fail(SF_ERR_CUDA,
+                    std::string("frame graph capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        g.exec = nullptr;
+        return fail(SF_ERR_CUDA, std::string("frame graph instantiate: ") + cudaGetErrorString(e));
+    }
+    g.splats = sp;
+    g.attr = sp->attr;
+    g.sh = sp->sh;
+    g.K = sp->K;
+    g.n = sp->n;
+    g.w = s->w;
+    g.h = s->h;
+    g.cap = s->cap;
+    g.tuning = s->tuning;
+    return SF_OK;
+}
+
+// One RGB frame through the frame graph on stream st; the image is in
+// s->bitmap and, when host_out is given, copied there. Syncs once.
+int frame_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32_t h,
+                       cudaStream_t st, uint32_t* host_out) {
+    auto& g = s->fg;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        if (!g.exec || g.splats != sp || g.attr != sp->attr || g.sh != sp->sh || g.K != sp->K || g.n != sp->n ||
+            g.w != w || g.h != h || g.cap != s->cap || std::memcmp(&g.tuning, &s->tuning, sizeof(sf_tuning)) != 0) {
+            const int rc = frame_graph_capture(sp, s);
+            if (rc != SF_OK) return rc;
+        }
+        view_for_camera(*cam, w, h, g.view_host);
+        SF_CK(cudaGraphLaunch(g.exec, st));
+        if (host_out)
+            SF_CK(cudaMemcpy2DAsync(host_out, (size_t)w * 4, s->bitmap, (size_t)s->row_stride * 4, (size_t)w * 4,
+                                    h, cudaMemcpyDeviceToHost, st));
+        SF_CK(cudaStreamSynchronize(st));
+        const uint32_t* hw = s->host_words;
+        if (hw[1] & SF_DEV_ERR_TIMEOUT) return fail(SF_ERR_TIMEOUT, "device look-back wait timed out");
+        uint64_t total = 0;
+        std::memcpy(&total, hw + 4, 8);
+        s->num_visible = hw[0];
+        s->last_isects_raw = total;
+        if (total > kMaxIsects) return fail(SF_ERR_CAPACITY, "intersection count exceeds 2^30-1");
+        if (total <= s->cap) {
+            const uint32_t order = s->tuning.raster_order;
+            s->num_isects = (uint32_t)total;
+            s->binned = true;
+            s->lazy = order != SF_ORDER_SORTED;
+            s->lazy_min = order == SF_ORDER_HYBRID ? kBinSharedMax : 0u;
+            s->order = nullptr;
+            s->tids = nullptr;
+            s->gids = order == SF_ORDER_IN_RASTER ? nullptr : s->gid_e;
+            s->prepared = true;
+            s->has_forward = false;
+            return SF_OK;
+        }
+        std::fprintf(stderr, "splatfield_b200: intersection capacity %llu reached (%llu needed); growing\n",
+                     (unsigned long long)s->cap, (unsigned long long)total);
+        SF_CK(grow_isects(s, total));
+    }
+    return fail(SF_ERR_CAPACITY, "frame capacity did not settle");
+}
+
+int frame_render(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32_t h, cudaStream_t st,
+                 uint32_t* host_out) {
+    if (!sp || !s || !cam) return fail(SF_ERR_ARG, "null argument");
+    if (w == 0 || h == 0 || w > 65535 * 16 || h > 65535 * 16) return fail(SF_ERR_SHAPE, "bad image size");
+    SF_CK(use_device(s->ctx->device));
+    if (s->total != sp->n || s->w != w || s->h != h) SF_CK(scratch_build(s, sp->n, w, h));
+    if (!frame_graph_usable(sp, s)) return kNoFrameGraph;
+    return frame_graph_render(sp, s, cam, w, h, st, host_out);
+}
+
 }  // namespace
 
 // ================================================================ C ABI
@@ -663,6 +840,11 @@ int sf_scratch_destroy(sf_scratch s) {
     dfree(s->words);
     dfree(s->stats);
     if (s->host_words) cudaFreeHost(s->host_words);
+    sort_streams_destroy(&s->sort_streams);
+    if (s->fg.exec) cudaGraphExecDestroy(s->fg.exec);
+    if (s->fg.stream) cudaStreamDestroy(s->fg.stream);
+    dfree(s->fg.view_dev);
+    if (s->fg.view_host) cudaFreeHost(s->fg.view_host);
     delete s;
     return SF_OK;
 }
@@ -706,7 +888,14 @@ int sf_finalize_rgb(sf_splats s, sf_scratch scratch, const sf_isects* isects, ui
 int sf_render_with(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
                    sf_stream stream, const uint32_t** bitmap, uint32_t* row_stride) {
     SF_TRY({
-        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr, true);
+        int rc = frame_render(s, scratch, cam, w, h, S(stream), nullptr);
+        if (rc != kNoFrameGraph) {
+            if (rc != SF_OK) return rc;
+            if (bitmap) *bitmap = scratch->bitmap;
+            if (row_stride) *row_stride = scratch->row_stride;
+            return SF_OK;
+        }
+        rc = prepare(s, scratch, cam, w, h, S(stream), nullptr, true);
         if (rc != SF_OK) return rc;
         rc = finalize_rgb(scratch, nullptr, false, S(stream));
         if (rc != SF_OK) return rc;
@@ -831,7 +1020,9 @@ int sf_render_to_host(sf_splats s, sf_scratch scratch, const sf_camera* cam, uin
                       sf_stream stream, uint32_t* out) {
     SF_TRY({
         if (!out) return fail(SF_ERR_ARG, "null out");
-        int rc = prepare(s, scratch, cam, w, h, S(stream), nullptr, true);
+        int rc = frame_render(s, scratch, cam, w, h, S(stream), out);
+        if (rc != kNoFrameGraph) return rc;
+        rc = prepare(s, scratch, cam, w, h, S(stream), nullptr, true);
         if (rc != SF_OK) return rc;
         rc = finalize_rgb(scratch, nullptr, false, S(stream));
         if (rc != SF_OK) return rc;

@@ -666,28 +666,97 @@ cudaError_t launch_bin_place(const uint2* bbox, const uint32_t* depth_keys, uint
     return cudaGetLastError();
 }
 
+namespace {
+
+__global__ void clamp_count_kernel(const unsigned long long* total, uint32_t cap, uint32_t* n32, uint32_t* err) {
+    const unsigned long long t = *total;
+    if (t > cap) atomicOr(err, SF_DEV_ERR_CAPACITY);
+    *n32 = (uint32_t)(t < cap ? t : cap);
+}
+
+__global__ void clamp_starts_kernel(uint32_t* tile_start, uint32_t count, uint32_t cap) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count && tile_start[i] > cap) tile_start[i] = cap;
+}
+
+}  // namespace
+
+cudaError_t launch_clamp_count(const unsigned long long* total, uint32_t cap, uint32_t* n32, uint32_t* err,
+                               cudaStream_t st) {
+    clamp_count_kernel<<<1, 1, 0, st>>>(total, cap, n32, err);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_clamp_starts(uint32_t* tile_start, uint32_t count, uint32_t cap, cudaStream_t st) {
+    clamp_starts_kernel<<<(count + 255) / 256, 256, 0, st>>>(tile_start, count, cap);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t sort_streams_create(SortStreams* ss) {
+    for (int k = 0; k < 3; ++k) {
+        cudaError_t e = cudaStreamCreateWithFlags(&ss->s[k], cudaStreamNonBlocking);
+        if (e != cudaSuccess) return e;
+    }
+    for (int k = 0; k < 4; ++k) {
+        cudaError_t e = cudaEventCreateWithFlags(&ss->e[k], cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+void sort_streams_destroy(SortStreams* ss) {
+    for (int k = 0; k < 3; ++k) {
+        if (ss->s[k]) cudaStreamDestroy(ss->s[k]);
+        ss->s[k] = nullptr;
+    }
+    for (int k = 0; k < 4; ++k) {
+        if (ss->e[k]) cudaEventDestroy(ss->e[k]);
+        ss->e[k] = nullptr;
+    }
+}
+
 cudaError_t launch_tile_sorts(const uint32_t grids[4], const uint32_t* lists, const uint32_t* words,
                               uint32_t tiles, const uint32_t* tile_start, uint32_t capacity, uint2* pairs,
                               uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, int sm_count,
-                              cudaStream_t st) {
+                              cudaStream_t st, const SortStreams* side) {
     cudaError_t e;
-    // Each form reads and overwrites only its own tiles' ranges.
+    // Each form reads and overwrites only its own tiles' ranges, so the
+    // classes may run concurrently.
+    cudaStream_t s1 = st, s2 = st, s3 = st;
+    if (side && side->s[0]) {
+        if ((e = cudaEventRecord(side->e[0], st)) != cudaSuccess) return e;
+        for (int k = 0; k < 3; ++k)
+            if ((e = cudaStreamWaitEvent(side->s[k], side->e[0], 0)) != cudaSuccess) return e;
+        s1 = side->s[0];
+        s2 = side->s[1];
+        s3 = side->s[2];
+    }
     e = launch_sort_kernel(tile_sort_global_kernel<kBinsGiant, 512>, 512, (kBinsGiant + 64) * 4, grids[3],
                            sm_count, lists + 3 * (size_t)tiles, words + 7, tile_start, capacity, pairs, ids,
-                           tids_out, keys_tmp, st);
+                           tids_out, keys_tmp, s3);
+    if (e != cudaSuccess) return e;
+    e = launch_sort_kernel(tile_sort_kernel<kClass1, kBins1, kThreads1>, kThreads1,
+                           sort_smem<kClass1, kBins1, kThreads1>(), grids[1], sm_count, lists + tiles, words + 9,
+                           tile_start, capacity, pairs, ids, tids_out, keys_tmp, s1);
+    if (e != cudaSuccess) return e;
+    e = launch_sort_kernel(tile_sort_kernel<kClass2, kBins2, kThreads2>, kThreads2,
+                           sort_smem<kClass2, kBins2, kThreads2>(), grids[2], sm_count,
+                           lists + 2 * (size_t)tiles, words + 10, tile_start, capacity, pairs, ids, tids_out,
+                           keys_tmp, s2);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClass0, kBins0, kThreads0>, kThreads0,
                            sort_smem<kClass0, kBins0, kThreads0>(), grids[0], sm_count, lists, words + 8,
                            tile_start, capacity, pairs, ids, tids_out, keys_tmp, st);
     if (e != cudaSuccess) return e;
-    e = launch_sort_kernel(tile_sort_kernel<kClass1, kBins1, kThreads1>, kThreads1,
-                           sort_smem<kClass1, kBins1, kThreads1>(), grids[1], sm_count, lists + tiles, words + 9,
-                           tile_start, capacity, pairs, ids, tids_out, keys_tmp, st);
-    if (e != cudaSuccess) return e;
-    return launch_sort_kernel(tile_sort_kernel<kClass2, kBins2, kThreads2>, kThreads2,
-                              sort_smem<kClass2, kBins2, kThreads2>(), grids[2], sm_count,
-                              lists + 2 * (size_t)tiles, words + 10, tile_start, capacity, pairs, ids, tids_out,
-                              keys_tmp, st);
+    if (side && side->s[0]) {
+        for (int k = 0; k < 3; ++k) {
+            if ((e = cudaEventRecord(side->e[1 + k], side->s[k])) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(st, side->e[1 + k], 0)) != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
 }
 
 }  // namespace sfk

@@ -153,6 +153,25 @@ cudaError_t launch_bin_place(const uint2* bbox, const uint32_t* depth_keys, uint
 // grids[k]: CTAs launched for class k (the class count when the host knows
 // it, else `tiles`; CTAs past the device count exit); grids[3] = 0 leaves
 // the longest lists unsorted.
+// Device-side capacity handling when the intersection total is not read
+// on the host first: n32 = min(total, cap) with SF_DEV_ERR_CAPACITY set past
+// it, and tile starts cut back to the capacity (every slot below it holds a
+// placed pair, so the sorts and the raster stay inside the buffers).
+cudaError_t launch_clamp_count(const unsigned long long* total, uint32_t cap, uint32_t* n32, uint32_t* err,
+                               cudaStream_t st);
+cudaError_t launch_clamp_starts(uint32_t* tile_start, uint32_t count, uint32_t cap, cudaStream_t st);
+
+// Side streams the per-tile sort classes run on concurrently inside a
+// captured graph (the tail of one class overlaps the others); null runs them
+// in turn on one stream (outside a graph the extra event calls cost more
+// host time than the overlap gains).
+struct SortStreams {
+    cudaStream_t s[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+cudaError_t sort_streams_create(SortStreams* ss);
+void sort_streams_destroy(SortStreams* ss);
+
 // pairs: the placed (depth key, splat id) per slot (overwritten for the
 // longest lists); ids / tids_out receive the sorted splat ids / tile ids
 // (tids_out may be null); keys_tmp: capacity u32 of scratch (may alias
@@ -161,7 +180,7 @@ cudaError_t launch_bin_place(const uint2* bbox, const uint32_t* depth_keys, uint
 cudaError_t launch_tile_sorts(const uint32_t grids[4], const uint32_t* lists, const uint32_t* words,
                               uint32_t tiles, const uint32_t* tile_start, uint32_t capacity, uint2* pairs,
                               uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, int sm_count,
-                              cudaStream_t st);
+                              cudaStream_t st, const SortStreams* side = nullptr);
 
 // ---- segmentation (sf_seg.cu)
 constexpr int kGridPts = 445;

@@ -75,7 +75,7 @@ __device__ __forceinline__ void sh_to_rgb(V3 d, const float (&c)[3 * K], float& 
 // project_splats (src/project.rs:235-327), one thread per splat. Field-major
 // planes make every plane load a coalesced 128-byte warp access.
 template <int K>
-__global__ __launch_bounds__(256) void project_kernel(sf_view v_arg, const sf_view* __restrict__ v_dev,
+__global__ __launch_bounds__(256, 3) void project_kernel(sf_view v_arg, const sf_view* __restrict__ v_dev,
                                                       const float* __restrict__ attr,
                                                       const float* __restrict__ shs, uint32_t n,
                                                       ProjOut o) {

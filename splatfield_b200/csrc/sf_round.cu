@@ -29,22 +29,6 @@
 namespace sfk {
 namespace {
 
-__global__ void clamp_count_kernel(const unsigned long long* total, uint32_t cap, uint32_t* n32,
-                                   uint32_t* err) {
-    const unsigned long long t = *total;
-    if (t > cap) atomicOr(err, SF_DEV_ERR_CAPACITY);
-    *n32 = (uint32_t)(t < cap ? t : cap);
-}
-
-// Tile starts past the capacity (a view whose intersections outgrew it) are
-// cut back to it, so that the sorts and the raster only read slots below the
-// capacity, all of which the placement filled. The round then grows and
-// re-runs the view.
-__global__ void clamp_starts_kernel(uint32_t* tile_start, uint32_t count, uint32_t cap) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count && tile_start[i] > cap) tile_start[i] = cap;
-}
-
 uint32_t bits_for(uint32_t max_exclusive) {
     const uint32_t m = max_exclusive > 0 ? max_exclusive - 1 : 0;
     return m == 0 ? 0u : 32u - (uint32_t)__builtin_clz(m);
@@ -97,6 +81,7 @@ struct RoundLane {
     uint32_t* hist = nullptr;
     uint32_t* cnt = nullptr;
     uint32_t* lists = nullptr;
+    SortStreams sort_streams;
 };
 
 }  // namespace sfk
@@ -147,6 +132,7 @@ void lane_free(RoundLane& L) {
     L.gid_a = nullptr;
     dfree(L.tile_start); dfree(L.partials);
     dfree(L.hist); dfree(L.cnt); dfree(L.lists);
+    sort_streams_destroy(&L.sort_streams);
     if (L.stream) cudaStreamDestroy(L.stream);
     if (L.join) cudaEventDestroy(L.join);
     L.stream = nullptr;
@@ -174,6 +160,7 @@ cudaError_t lane_alloc(sf_round_t* r, RoundLane& L, uint64_t cap) {
     const size_t st = std::max(radix_temp_bytes(n, 4), radix_temp_bytes((uint32_t)cap, 4));
     if ((e = cudaMalloc(&L.sort_tmp, st)) != cudaSuccess) return e;
     if ((e = cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    if ((e = sort_streams_create(&L.sort_streams)) != cudaSuccess) return e;
     if ((e = cudaEventCreateWithFlags(&L.join, cudaEventDisableTiming)) != cudaSuccess) return e;
     L.cap = cap;
     return cudaSuccess;
@@ -212,8 +199,7 @@ cudaError_t depth_sorted_isects(sf_round_t* r, RoundLane& L, uint32_t n, uint32_
     if ((e = launch_emit(order, L.bbox, L.offsets, n, tx, (uint32_t)L.cap, L.tid_e, L.gid_e, words + 1, st)) !=
         cudaSuccess)
         return e;
-    clamp_count_kernel<<<1, 1, 0, st>>>(total, (uint32_t)L.cap, words + 2, words + 1);
-    note_launches(1);
+    if ((e = launch_clamp_count(total, (uint32_t)L.cap, words + 2, words + 1, st)) != cudaSuccess) return e;
     const uint32_t tbits = bits_for(tiles);
     const uint32_t *tids = L.tid_e, *gids = L.gid_e;
     if (tbits > 0) {
@@ -301,20 +287,18 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
         if ((e = exclusive_scan(nullptr, L.cnt, L.tile_start, tiles + 1, nullptr, tiles + 1, L.scan_tmp, total,
                                 words + 1, st)) != cudaSuccess)
             return e;
-        clamp_count_kernel<<<1, 1, 0, st>>>(total, (uint32_t)L.cap, words + 2, words + 1);
-        note_launches(1);
+        if ((e = launch_clamp_count(total, (uint32_t)L.cap, words + 2, words + 1, st)) != cudaSuccess) return e;
         uint2* pairs = reinterpret_cast<uint2*>(L.tid_a);
         if ((e = launch_bin_place(L.bbox, L.keys, n, tx, tiles, r->chunks, L.hist, L.tile_start, (uint32_t)L.cap,
                                   pairs, words + 1, st)) != cudaSuccess)
             return e;
-        clamp_starts_kernel<<<(tiles + 1 + 255) / 256, 256, 0, st>>>(L.tile_start, tiles + 1, (uint32_t)L.cap);
-        note_launches(1);
+        if ((e = launch_clamp_starts(L.tile_start, tiles + 1, (uint32_t)L.cap, st)) != cudaSuccess) return e;
         const uint32_t order = r->tuning.raster_order;
         if (order != SF_ORDER_SORTED) lazy_pairs = pairs;
         if (order != SF_ORDER_IN_RASTER) {
             const uint32_t grids[4] = {tiles, tiles, tiles, order == SF_ORDER_HYBRID ? 0u : tiles};
             if ((e = launch_tile_sorts(grids, L.lists, words, tiles, L.tile_start, (uint32_t)L.cap, pairs, L.gid_e,
-                                       nullptr, L.tid_e, r->sm_count, st)) != cudaSuccess)
+                                       nullptr, L.tid_e, r->sm_count, st, &L.sort_streams)) != cudaSuccess)
                 return e;
             gids = L.gid_e;
         }

@@ -298,3 +298,30 @@ def test_raster_detail_counters_change_nothing(ctx, cull):
     assert plain["pairs_visited"] == detail["pairs_visited"] > 0
     assert plain["exp_evaluated"] == 0 and detail["exp_evaluated"] >= detail["contributing"] > 0
     assert detail["pairs_processed"] <= detail["pairs_visited"]
+
+
+@pytest.mark.parametrize("order", [sf.ORDER_SORTED, sf.ORDER_HYBRID, sf.ORDER_IN_RASTER])
+def test_frame_graph_grows_capacity_and_matches_oracle(ctx, oracle_mod, order):
+    """sf_render_with / sf_render_to_host run the binned frame as one graph
+    with device-side capacity guards: a first frame past the initial
+    capacity grows it, re-runs, and still equals the oracle; later frames of
+    other cameras replay the graph."""
+    from splatfield_b200 import synth
+
+    n, w, h = 60000, 512, 512
+    attr, sh = synth.scene_uniform(n, 1, 11)
+    attr = attr.reshape(11, n)
+    attr[7:10] += 2.5
+    attr = attr.reshape(-1)
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    scratch.set_tuning(raster_order=order)
+    for pos in [(0.0, 0.0, -3.0), (0.4, 0.2, -3.2), (0.0, 0.0, -3.0)]:
+        cam = sf.look_at(pos, (0.0, 0.0, 0.0))
+        got = splats.render_with(scratch, cam, (w, h)).read()
+        host = splats.render_to_host(scratch, cam, (w, h))
+        prep = oracle_mod.prepare(oracle_mod.look_at(pos, (0.0, 0.0, 0.0)), w, h, attr, sh, 1)
+        want = oracle_mod.rasterize(prep, 0)["bitmap"]
+        np.testing.assert_array_equal(got, want)
+        np.testing.assert_array_equal(host, want[:, :w])
+    assert scratch.capacity() > (1 << 22)
