@@ -156,7 +156,7 @@ struct sf_scratch_t {
     float* final_t = nullptr;
     uint32_t* n_contrib = nullptr;
     // device words: [0] visible, [1] error bits, [2..3] spare, [4..5] u64
-    // total, [6..10] binned-build tile statistics (sf_internal.h)
+    // total, [6..13] binned-build tile statistics (sf_internal.h)
     uint32_t* words = nullptr;
     uint32_t* host_words = nullptr;  // pinned mirror
     unsigned long long* stats = nullptr;  // raster pair statistics of the last finalize
@@ -277,7 +277,7 @@ cudaError_t scratch_build(sf_scratch s, uint32_t total, uint32_t w, uint32_t h) 
         s->bin_chunks = bin_chunks(total, s->ctx->sm_count);
         SF_AL(s->bin_hist, (size_t)s->bin_chunks * tiles);
         SF_AL(s->bin_cnt, tiles + 1);
-        SF_AL(s->bin_lists, 4 * tiles);
+        SF_AL(s->bin_lists, (size_t)kSortClasses * tiles);
     }
     SF_AL(s->bitmap, (size_t)h * s->row_stride);
 #undef SF_AL
@@ -332,7 +332,9 @@ int prepare_binned(sf_scratch s, uint32_t n, uint32_t tiles, cudaStream_t st, bo
     if (order == SF_ORDER_IN_RASTER) {
         s->tids = s->gids = nullptr;
     } else {
-        const uint32_t grids[4] = {hw[8], hw[9], hw[10], order == SF_ORDER_HYBRID ? 0u : hw[7]};
+        uint32_t grids[kSortClasses];
+        for (int k = 0; k < kSortClasses; ++k) grids[k] = hw[8 + k];
+        if (order == SF_ORDER_HYBRID) grids[kSortClasses - 1] = 0;
         SF_CK(launch_tile_sorts(grids, s->bin_lists, words, tiles, s->tile_start, (uint32_t)s->cap, pairs,
                                 s->gid_e, want_tile_ids ? s->tid_e : nullptr, s->tid_e, s->ctx->sm_count, st));
         s->tids = want_tile_ids ? s->tid_e : nullptr;
@@ -549,7 +551,9 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
                              s->tile_start, cap, pairs, words + 1, st);
     if (e == cudaSuccess) e = launch_clamp_starts(s->tile_start, tiles + 1, cap, st);
     if (e == cudaSuccess && order != SF_ORDER_IN_RASTER) {
-        const uint32_t grids[4] = {tiles, tiles, tiles, order == SF_ORDER_HYBRID ? 0u : tiles};
+        uint32_t grids[kSortClasses];
+        for (int k = 0; k < kSortClasses; ++k) grids[k] = tiles;
+        if (order == SF_ORDER_HYBRID) grids[kSortClasses - 1] = 0;
         e = launch_tile_sorts(grids, s->bin_lists, words, tiles, s->tile_start, cap, pairs, s->gid_e, nullptr,
                               s->tid_e, s->ctx->sm_count, st, &s->sort_streams);
     }

@@ -108,14 +108,18 @@ __global__ __launch_bounds__(kBinThreads) void bin_count_kernel(const uint2* __r
     for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) row[t] = s_hist[t];
 }
 
+struct ClassLimits {
+    uint32_t max_n[kSortClasses - 1];  // longest list of each class but the last
+};
+
 // Block (32, 32): x = tile within the block's 32, y = a group of chunks.
-// words: [6] max tile count (atomicMax), [7] tiles longer than the shared
-// classes (lists[3 * tiles + i]), [8 + k] tiles in shared class k
-// (lists[k * tiles + i]).
+// words: [6] max tile count (atomicMax), [8 + k] tiles in size class k
+// (lists[k * tiles + i]); the last class holds the lists longer than every
+// shared-memory class.
 __global__ __launch_bounds__(1024) void bin_colscan_kernel(uint32_t* __restrict__ hist, uint32_t chunks,
                                                            uint32_t tiles, uint32_t* __restrict__ cnt,
                                                            uint32_t* __restrict__ lists, uint32_t* words,
-                                                           uint32_t class0, uint32_t class1, uint32_t class2) {
+                                                           ClassLimits lim) {
     __shared__ uint32_t s_part[32][33];
     const uint32_t tx = threadIdx.x, ty = threadIdx.y;
     const uint32_t t = blockIdx.x * 32u + tx;
@@ -138,17 +142,19 @@ __global__ __launch_bounds__(1024) void bin_colscan_kernel(uint32_t* __restrict_
         if (blockIdx.x == 0 && tx == 0) cnt[tiles] = 0;
         // Size classes (warp-aggregated appends; the list order is free).
         const uint32_t total = valid ? run : 0u;
-        const uint32_t cls = total == 0 ? 4u : total <= class0 ? 0u : total <= class1 ? 1u
-                           : total <= class2 ? 2u : 3u;
+        uint32_t cls = total == 0 ? kSortClasses : kSortClasses - 1;
+        if (total > 0)
+            for (int k = kSortClasses - 2; k >= 0; --k)
+                if (total <= lim.max_n[k]) cls = (uint32_t)k;
         const uint32_t mx = __reduce_max_sync(0xffffffffu, total);
         if (tx == 0 && mx) atomicMax(words + 6, mx);
 #pragma unroll
-        for (uint32_t k = 0; k < 4; ++k) {
+        for (uint32_t k = 0; k < kSortClasses; ++k) {
             const uint32_t m = __ballot_sync(0xffffffffu, cls == k);
             if (!m) continue;
             const uint32_t leader = __ffs(m) - 1;
             uint32_t base = 0;
-            if (tx == leader) base = atomicAdd(words + (k == 3 ? 7u : 8u + k), __popc(m));
+            if (tx == leader) base = atomicAdd(words + 8u + k, __popc(m));
             base = __shfl_sync(0xffffffffu, base, leader);
             if (cls == k) lists[k * tiles + base + __popc(m & lanemask_lt())] = t;
         }
@@ -588,17 +594,74 @@ __global__ __launch_bounds__(THREADS, 1) void tile_sort_global_kernel(const uint
     }
 }
 
+// Lists of up to 64 entries: one warp per tile, the 64-bit (key, id) values
+// two per lane, a bitonic network over lanes (shuffles) and the lane's two
+// slots; 8 tiles per 256-thread CTA, persistent over the class's tiles.
+__global__ __launch_bounds__(256) void tile_sort_warp_kernel(const uint32_t* __restrict__ list,
+                                                             const uint32_t* list_n,
+                                                             const uint32_t* __restrict__ tile_start,
+                                                             uint32_t capacity, uint2* pairs, uint32_t* ids,
+                                                             uint32_t* tids_out, uint32_t*) {
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint32_t count = *list_n;
+    for (uint32_t idx = blockIdx.x * 8u + wib; idx < count; idx += gridDim.x * 8u) {
+        const uint32_t t = list[idx];
+        const uint32_t start = tile_start[t], end = tile_start[t + 1];
+        const uint32_t n = end - start;
+        // The class and the capacity clamp keep these false (warp-uniform).
+        if (n > 64 || end > capacity || end < start) continue;
+        unsigned long long v0 = ~0ull, v1 = ~0ull;
+        if (lane < n) {
+            const uint2 p = pairs[start + lane];
+            v0 = ((unsigned long long)p.x << 32) | p.y;
+        }
+        if (lane + 32 < n) {
+            const uint2 p = pairs[start + lane + 32];
+            v1 = ((unsigned long long)p.x << 32) | p.y;
+        }
+#pragma unroll
+        for (uint32_t k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                if (j == 32) {
+                    // Element lane against element lane + 32, ascending.
+                    const unsigned long long lo = min(v0, v1), hi = max(v0, v1);
+                    v0 = lo;
+                    v1 = hi;
+                } else {
+                    const unsigned long long p0 = __shfl_xor_sync(0xffffffffu, v0, j);
+                    const unsigned long long p1 = __shfl_xor_sync(0xffffffffu, v1, j);
+                    const bool lower = (lane & j) == 0;
+                    const bool asc0 = (lane & k) == 0, asc1 = ((lane + 32u) & k) == 0;
+                    v0 = (lower == asc0) ? min(v0, p0) : max(v0, p0);
+                    v1 = (lower == asc1) ? min(v1, p1) : max(v1, p1);
+                }
+            }
+        }
+        if (lane < n) {
+            ids[start + lane] = (uint32_t)v0;
+            if (tids_out) tids_out[start + lane] = t;
+        }
+        if (lane + 32 < n) {
+            ids[start + lane + 32] = (uint32_t)v1;
+            if (tids_out) tids_out[start + lane + 32] = t;
+        }
+    }
+}
+
 template <uint32_t MAXN, uint32_t BINS, uint32_t THREADS>
 constexpr size_t sort_smem() {
     return (2ull * MAXN + BINS + 4 * (THREADS / 32)) * 4;
 }
 
-// Size classes of the shared-form sort (entries, buckets, threads); longer
-// lists take the global form.
-constexpr uint32_t kClass0 = 2048, kClass1 = 6144, kClass2 = kBinSharedMax;
-constexpr uint32_t kBins0 = 4096, kBins1 = 8192, kBins2 = 16384, kBinsGiant = 32768;
-constexpr uint32_t kThreads0 = 256, kThreads1 = 512, kThreads2 = 1024;
+// Size classes (longest list): a warp per tile up to 64 entries, then the
+// shared-memory bucket sorts (entries, buckets, threads); longer lists take
+// the global form.
+constexpr uint32_t kClassWarp = 64, kClassS = 512, kClass0 = 2048, kClass1 = 6144, kClass2 = kBinSharedMax;
+constexpr uint32_t kBinsS = 2304, kBins0 = 4096, kBins1 = 8192, kBins2 = 16384, kBinsGiant = 32768;
+constexpr uint32_t kThreadsS = 256, kThreads0 = 256, kThreads1 = 512, kThreads2 = 1024;
 static_assert(sort_smem<kClass2, kBins2, kThreads2>() <= 227 * 1024, "per-tile sort exceeds shared memory");
+static_assert(kSortClasses == 6, "class table");
 
 // grid: the class's tile count when the host knows it, else an upper bound;
 // capped at the CTAs resident at once (the kernels loop over their tiles).
@@ -634,7 +697,10 @@ uint32_t bin_chunks(uint32_t n, int sm_count) {
 
 uint32_t bin_chunk_size(uint32_t n, uint32_t chunks) { return ((n + chunks - 1) / chunks + 31) / 32 * 32; }
 
-uint32_t bin_class_limit(int k) { return k == 0 ? kClass0 : k == 1 ? kClass1 : kClass2; }
+uint32_t bin_class_limit(int k) {
+    const uint32_t lim[kSortClasses - 1] = {kClassWarp, kClassS, kClass0, kClass1, kClass2};
+    return k >= 0 && k < kSortClasses - 1 ? lim[k] : 0xffffffffu;
+}
 
 cudaError_t launch_bin_count(const uint2* bbox, uint32_t n, uint32_t tiles_x, uint32_t tiles, uint32_t chunks,
                              uint32_t* hist, cudaStream_t st) {
@@ -648,8 +714,8 @@ cudaError_t launch_bin_count(const uint2* bbox, uint32_t n, uint32_t tiles_x, ui
 
 cudaError_t launch_bin_colscan(uint32_t* hist, uint32_t chunks, uint32_t tiles, uint32_t* cnt, uint32_t* lists,
                                uint32_t* words, cudaStream_t st) {
-    bin_colscan_kernel<<<(tiles + 31) / 32, dim3(32, 32), 0, st>>>(hist, chunks, tiles, cnt, lists, words,
-                                                                   kClass0, kClass1, kClass2);
+    const ClassLimits lim{{kClassWarp, kClassS, kClass0, kClass1, kClass2}};
+    bin_colscan_kernel<<<(tiles + 31) / 32, dim3(32, 32), 0, st>>>(hist, chunks, tiles, cnt, lists, words, lim);
     note_launches(1);
     return cudaGetLastError();
 }
@@ -717,7 +783,7 @@ void sort_streams_destroy(SortStreams* ss) {
     }
 }
 
-cudaError_t launch_tile_sorts(const uint32_t grids[4], const uint32_t* lists, const uint32_t* words,
+cudaError_t launch_tile_sorts(const uint32_t grids[kSortClasses], const uint32_t* lists, const uint32_t* words,
                               uint32_t tiles, const uint32_t* tile_start, uint32_t capacity, uint2* pairs,
                               uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, int sm_count,
                               cudaStream_t st, const SortStreams* side) {
@@ -733,22 +799,29 @@ cudaError_t launch_tile_sorts(const uint32_t grids[4], const uint32_t* lists, co
         s2 = side->s[1];
         s3 = side->s[2];
     }
-    e = launch_sort_kernel(tile_sort_global_kernel<kBinsGiant, 512>, 512, (kBinsGiant + 64) * 4, grids[3],
-                           sm_count, lists + 3 * (size_t)tiles, words + 7, tile_start, capacity, pairs, ids,
-                           tids_out, keys_tmp, s3);
+    auto L = [&](int k) { return lists + (size_t)k * tiles; };
+    auto N = [&](int k) { return words + 8 + k; };
+    e = launch_sort_kernel(tile_sort_global_kernel<kBinsGiant, 512>, 512, (kBinsGiant + 64) * 4, grids[5],
+                           sm_count, L(5), N(5), tile_start, capacity, pairs, ids, tids_out, keys_tmp, s3);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClass1, kBins1, kThreads1>, kThreads1,
-                           sort_smem<kClass1, kBins1, kThreads1>(), grids[1], sm_count, lists + tiles, words + 9,
-                           tile_start, capacity, pairs, ids, tids_out, keys_tmp, s1);
+                           sort_smem<kClass1, kBins1, kThreads1>(), grids[3], sm_count, L(3), N(3), tile_start,
+                           capacity, pairs, ids, tids_out, keys_tmp, s1);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClass2, kBins2, kThreads2>, kThreads2,
-                           sort_smem<kClass2, kBins2, kThreads2>(), grids[2], sm_count,
-                           lists + 2 * (size_t)tiles, words + 10, tile_start, capacity, pairs, ids, tids_out,
-                           keys_tmp, s2);
+                           sort_smem<kClass2, kBins2, kThreads2>(), grids[4], sm_count, L(4), N(4), tile_start,
+                           capacity, pairs, ids, tids_out, keys_tmp, s2);
+    if (e != cudaSuccess) return e;
+    e = launch_sort_kernel(tile_sort_warp_kernel, 256, 0, (grids[0] + 7) / 8, sm_count, L(0), N(0), tile_start, capacity,
+                           pairs, ids, tids_out, keys_tmp, s2);
+    if (e != cudaSuccess) return e;
+    e = launch_sort_kernel(tile_sort_kernel<kClassS, kBinsS, kThreadsS>, kThreadsS,
+                           sort_smem<kClassS, kBinsS, kThreadsS>(), grids[1], sm_count, L(1), N(1), tile_start,
+                           capacity, pairs, ids, tids_out, keys_tmp, s3);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClass0, kBins0, kThreads0>, kThreads0,
-                           sort_smem<kClass0, kBins0, kThreads0>(), grids[0], sm_count, lists, words + 8,
-                           tile_start, capacity, pairs, ids, tids_out, keys_tmp, st);
+                           sort_smem<kClass0, kBins0, kThreads0>(), grids[2], sm_count, L(2), N(2), tile_start,
+                           capacity, pairs, ids, tids_out, keys_tmp, st);
     if (e != cudaSuccess) return e;
     if (side && side->s[0]) {
         for (int k = 0; k < 3; ++k) {

@@ -134,15 +134,17 @@ cudaError_t exclusive_scan(const uint32_t* gids, const uint32_t* counts, uint32_
 // per tile in the count and place kernels).
 constexpr uint32_t kBinMaxTiles = 49152;
 uint32_t bin_chunks(uint32_t n, int sm_count);
-uint32_t bin_class_limit(int k);  // largest tile list sorted by size class k (0..2)
+// Per-tile sort size classes: k = 0 .. kSortClasses - 2 hold lists of up to
+// bin_class_limit(k) entries; the last class holds the longer lists.
+constexpr int kSortClasses = 6;
+uint32_t bin_class_limit(int k);
 // Longest list the shared-memory classes sort; longer lists go to the global
 // form (or, with the hybrid order, to the rasterizer).
 constexpr uint32_t kBinSharedMax = 12288;
 // hist: [chunks][tiles] counts, then (after colscan) per-chunk exclusive
 // prefixes. cnt: [tiles + 1] per-tile totals (cnt[tiles] = 0). lists:
-// [4][tiles] tiles of each size class. words: [6] max tile total, [7] tiles
-// longer than the shared-memory classes, [8..10] tiles per shared class (all
-// zero on entry).
+// [kSortClasses][tiles] tiles of each size class. words: [6] max tile total,
+// [8 + k] tiles in class k (all zero on entry).
 cudaError_t launch_bin_count(const uint2* bbox, uint32_t n, uint32_t tiles_x, uint32_t tiles, uint32_t chunks,
                              uint32_t* hist, cudaStream_t st);
 cudaError_t launch_bin_colscan(uint32_t* hist, uint32_t chunks, uint32_t tiles, uint32_t* cnt, uint32_t* lists,
@@ -175,9 +177,9 @@ void sort_streams_destroy(SortStreams* ss);
 // pairs: the placed (depth key, splat id) per slot (overwritten for the
 // longest lists); ids / tids_out receive the sorted splat ids / tile ids
 // (tids_out may be null); keys_tmp: capacity u32 of scratch (may alias
-// tids_out). grids[0..2]: shared classes, grids[3]: longer lists (each the
-// class's tile count, or an upper bound when the counts are on the device).
-cudaError_t launch_tile_sorts(const uint32_t grids[4], const uint32_t* lists, const uint32_t* words,
+// tids_out). grids[k]: the tile count of size class k, or an upper bound
+// when the counts are on the device (0 skips the class).
+cudaError_t launch_tile_sorts(const uint32_t grids[kSortClasses], const uint32_t* lists, const uint32_t* words,
                               uint32_t tiles, const uint32_t* tile_start, uint32_t capacity, uint2* pairs,
                               uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, int sm_count,
                               cudaStream_t st, const SortStreams* side = nullptr);

@@ -99,7 +99,7 @@ struct sf_round_t {
     std::vector<RoundLane> lanes;
     sf_view* views_dev = nullptr;
     sf_view* views_host = nullptr;  // pinned
-    uint32_t* words = nullptr;      // [views][16]: 0 visible, 1 err, 2 n32, 4..5 total u64, 6..10 binned stats
+    uint32_t* words = nullptr;      // [views][16]: 0 visible, 1 err, 2 n32, 4..5 total u64, 6..13 binned stats
     uint32_t* words_host = nullptr; // pinned
     double* eig_dev = nullptr;
     double* eig_host = nullptr;     // pinned
@@ -153,7 +153,7 @@ cudaError_t lane_alloc(sf_round_t* r, RoundLane& L, uint64_t cap) {
     if (r->max_tiles <= kBinMaxTiles) {
         RA(L.hist, (size_t)r->chunks * r->max_tiles);
         RA(L.cnt, (size_t)r->max_tiles + 1);
-        RA(L.lists, 4 * (size_t)r->max_tiles);
+        RA(L.lists, (size_t)kSortClasses * r->max_tiles);
     }
 #undef RA
     if ((e = cudaMalloc(&L.scan_tmp, scan_temp_bytes(std::max(n, r->max_tiles + 1)))) != cudaSuccess) return e;
@@ -296,7 +296,9 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
         const uint32_t order = r->tuning.raster_order;
         if (order != SF_ORDER_SORTED) lazy_pairs = pairs;
         if (order != SF_ORDER_IN_RASTER) {
-            const uint32_t grids[4] = {tiles, tiles, tiles, order == SF_ORDER_HYBRID ? 0u : tiles};
+            uint32_t grids[kSortClasses];
+            for (int k = 0; k < kSortClasses; ++k) grids[k] = tiles;
+            if (order == SF_ORDER_HYBRID) grids[kSortClasses - 1] = 0;
             if ((e = launch_tile_sorts(grids, L.lists, words, tiles, L.tile_start, (uint32_t)L.cap, pairs, L.gid_e,
                                        nullptr, L.tid_e, r->sm_count, st, &L.sort_streams)) != cudaSuccess)
                 return e;
