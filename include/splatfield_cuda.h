@@ -206,6 +206,16 @@ int sf_render_float(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint3
  * written to host memory `out`; syncs. */
 int sf_render_to_host(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w,
                       uint32_t h, sf_stream stream, uint32_t* out);
+/* `count` frames, camera cams[i] to out + i * w * h (packed RGBA8 rows
+ * [h][w], as sf_render_to_host writes them); syncs once at the end. Each
+ * image leaves the device (from a staging copy, on a stream of its own)
+ * while the next frame renders, so the read-backs overlap the rendering when
+ * `out` is pinned host memory. The images equal `count` sf_render_to_host
+ * calls; frames past the intersection capacity are rendered again after it
+ * has grown. The scratch is left holding the last frame. A camera path over
+ * the reference's per-frame render_with (src/render.rs:371-380). */
+int sf_render_frames_to_host(sf_splats s, sf_scratch scratch, const sf_camera* cams, uint32_t count,
+                             uint32_t w, uint32_t h, sf_stream stream, uint32_t* out);
 /* Adjoint (no counterpart in the reference, which renders forward only).
  * sf_render_forward: sf_render_float that also keeps, per pixel, the final
  * transmittance and the position of the last contributor, for the backward.

@@ -113,6 +113,7 @@ SIGNATURES = {
         "sf_splats_restore_colors": (i32, [P, P, P]),
         "sf_render_float": (i32, [P, P, P, u32, u32, P, PP]),
         "sf_render_to_host": (i32, [P, P, P, u32, u32, P, P]),
+        "sf_render_frames_to_host": (i32, [P, P, P, u32, u32, u32, P, P]),
         "sf_render_forward": (i32, [P, P, P, u32, u32, P, PP]),
         "sf_render_backward": (i32, [P, P, P, u32, u32, P, P, P, P, P]),
         "sf_prepare_isects": (i32, [P, P, P, u32, u32, P, P]),

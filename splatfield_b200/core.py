@@ -27,12 +27,51 @@ __all__ = [
     "RadixScratch", "ScanScratch", "exclusive_scan_gather", "exclusive_scan_buf", "entropy_table",
     "table_entropy", "fractional_bits", "row_stride_for", "EIG_LUT_F32", "EIG_FP64", "Round",
     "ISECTS_BINNED", "ISECTS_DEPTH_SORTED", "ORDER_IN_RASTER", "ORDER_SORTED", "ORDER_HYBRID", "ply_inspect", "load_ply",
+    "pinned_empty",
 ]
 
 EIG_LUT_F32, EIG_FP64 = L.EIG_LUT_F32, L.EIG_FP64
 ISECTS_BINNED, ISECTS_DEPTH_SORTED = L.ISECTS_BINNED, L.ISECTS_DEPTH_SORTED
 ORDER_IN_RASTER, ORDER_SORTED, ORDER_HYBRID = L.ORDER_IN_RASTER, L.ORDER_SORTED, L.ORDER_HYBRID
 BASE_FOV = 0.8  # Camera::BASE_FOV (src/camera.rs:86)
+
+
+class _PinnedOwner:
+    """Frees one sf_host_alloc block when the last array viewing it goes."""
+
+    def __init__(self, nbytes: int):
+        p = C.c_void_p()
+        check(lib().sf_host_alloc(max(nbytes, 1), C.byref(p)))
+        self.ptr = p
+
+    def __del__(self):
+        if self.ptr is not None:
+            try:
+                lib().sf_host_free(self.ptr)
+            except Exception:  # interpreter shutdown
+                pass
+            self.ptr = None
+
+
+class _PinnedArray(np.ndarray):
+    _pin = None
+
+    def __array_finalize__(self, obj):
+        self._pin = getattr(obj, "_pin", None)
+
+
+def pinned_empty(shape, dtype=np.uint32) -> np.ndarray:
+    """An uninitialised array in page-locked host memory (copies to and from
+    it run asynchronously); the memory lives as long as the array or any view
+    of it."""
+    dtype = np.dtype(dtype)
+    shape = tuple(int(x) for x in (shape if isinstance(shape, (tuple, list)) else (shape,)))
+    nbytes = int(np.prod(shape, dtype=np.int64)) * dtype.itemsize
+    owner = _PinnedOwner(nbytes)
+    raw = (C.c_uint8 * max(nbytes, 1)).from_address(owner.ptr.value)
+    arr = np.frombuffer(raw, np.uint8, nbytes).view(dtype).reshape(shape).view(_PinnedArray)
+    arr._pin = owner
+    return arr
 
 
 def _vp(x) -> C.c_void_p:
@@ -376,6 +415,20 @@ class Splats:
             out = np.empty((h, w), np.uint32)
         check(lib().sf_render_to_host(self.handle, scratch.handle, C.byref(camera), w, h, _stream(stream),
                                       _vp(out)))
+        return out
+
+    def render_frames_to_host(self, scratch: "RenderScratch", cameras, img_size, out=None, stream=None):
+        """One RGBA8 image per camera, [count, h, w] words in host memory
+        (``out``: pinned memory lets each image's read-back overlap the next
+        frame; see ``pinned_empty``)."""
+        w, h = img_size
+        cams = (Camera * len(cameras))(*cameras)
+        if out is None:
+            out = np.empty((len(cameras), h, w), np.uint32)
+        if out.dtype != np.uint32 or not out.flags.c_contiguous or out.size < len(cameras) * w * h:
+            raise ValueError("out must be a C-contiguous uint32 array of count * h * w words")
+        check(lib().sf_render_frames_to_host(self.handle, scratch.handle, cams, len(cameras), w, h,
+                                             _stream(stream), _vp(out)))
         return out
 
     def prepare_isects(self, scratch: "RenderScratch", camera: Camera, img_size, stream=None) -> "TileIsects":

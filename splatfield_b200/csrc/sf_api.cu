@@ -150,6 +150,16 @@ struct sf_scratch_t {
         uint32_t K = 0, n = 0, w = 0, h = 0;
         uint64_t cap = 0;
         sf_tuning tuning{};
+        // Frames to host memory in a batch: each image is copied out of the
+        // bitmap into one of two staging images, whose device-to-host copy
+        // (copy stream) runs while the next frame renders.
+        cudaStream_t copy = nullptr;
+        cudaEvent_t ready[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+        uint32_t* stage[2] = {nullptr, nullptr};
+        size_t stage_words = 0;
+        sf_view* views = nullptr;     // pinned, one per frame of the batch
+        uint32_t* frame_words = nullptr;  // pinned, 16 per frame
+        uint32_t batch_cap = 0;
     } fg;
     uint32_t* bitmap = nullptr;
     float4* rgba = nullptr;
@@ -531,9 +541,10 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
     uint32_t* words = s->words;
     auto* total = reinterpret_cast<unsigned long long*>(words + 4);
     cudaStream_t st = g.stream;
+    // The camera's view is copied to g.view_dev before each launch (from a
+    // pinned slot of the caller's choosing), outside the graph.
     SF_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaMemcpyAsync(g.view_dev, g.view_host, sizeof(sf_view), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(words, 0, 64, st);
+    cudaError_t e = cudaMemsetAsync(words, 0, 64, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->stats, 0, 32, st);
     ProjOut po{s->depth_keys, s->tile_counts, s->bbox, s->geo0, s->geo1, s->color, words, s->ext};
     sf_view dummy{};
@@ -604,18 +615,43 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
     return SF_OK;
 }
 
+// (Re)captures the frame graph when the splats, image size, capacity or
+// tuning it was captured for changed.
+int frame_graph_ready(sf_splats sp, sf_scratch s, uint32_t w, uint32_t h) {
+    auto& g = s->fg;
+    if (!g.exec || g.splats != sp || g.attr != sp->attr || g.sh != sp->sh || g.K != sp->K || g.n != sp->n ||
+        g.w != w || g.h != h || g.cap != s->cap || std::memcmp(&g.tuning, &s->tuning, sizeof(sf_tuning)) != 0)
+        return frame_graph_capture(sp, s);
+    return SF_OK;
+}
+
+// The scratch's prepared-frame state after a frame whose device words are
+// hw (total <= capacity).
+void frame_graph_settle(sf_scratch s, const uint32_t* hw, uint64_t total) {
+    const uint32_t order = s->tuning.raster_order;
+    s->num_visible = hw[0];
+    s->last_isects_raw = total;
+    s->num_isects = (uint32_t)total;
+    s->binned = true;
+    s->lazy = order != SF_ORDER_SORTED;
+    s->lazy_min = order == SF_ORDER_HYBRID ? kBinSharedMax : 0u;
+    s->order = nullptr;
+    s->tids = nullptr;
+    s->gids = order == SF_ORDER_IN_RASTER ? nullptr : s->gid_e;
+    s->prepared = true;
+    s->has_forward = false;
+}
+
 // One RGB frame through the frame graph on stream st; the image is in
 // s->bitmap and, when host_out is given, copied there. Syncs once.
 int frame_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32_t h,
                        cudaStream_t st, uint32_t* host_out) {
     auto& g = s->fg;
     for (int attempt = 0; attempt < 4; ++attempt) {
-        if (!g.exec || g.splats != sp || g.attr != sp->attr || g.sh != sp->sh || g.K != sp->K || g.n != sp->n ||
-            g.w != w || g.h != h || g.cap != s->cap || std::memcmp(&g.tuning, &s->tuning, sizeof(sf_tuning)) != 0) {
-            const int rc = frame_graph_capture(sp, s);
-            if (rc != SF_OK) return rc;
-        }
+        const int rc = frame_graph_ready(sp, s, w, h);
+        if (rc != SF_OK) return rc;
         view_for_camera(*cam, w, h, g.view_host);
+        SF_CK(cudaMemcpyAsync(g.view_dev, g.view_host, sizeof(sf_view), cudaMemcpyHostToDevice, st));
         SF_CK(cudaGraphLaunch(g.exec, st));
         if (host_out)
             SF_CK(cudaMemcpy2DAsync(host_out, (size_t)w * 4, s->bitmap, (size_t)s->row_stride * 4, (size_t)w * 4,
@@ -629,16 +665,7 @@ int frame_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_
         s->last_isects_raw = total;
         if (total > kMaxIsects) return fail(SF_ERR_CAPACITY, "intersection count exceeds 2^30-1");
         if (total <= s->cap) {
-            const uint32_t order = s->tuning.raster_order;
-            s->num_isects = (uint32_t)total;
-            s->binned = true;
-            s->lazy = order != SF_ORDER_SORTED;
-            s->lazy_min = order == SF_ORDER_HYBRID ? kBinSharedMax : 0u;
-            s->order = nullptr;
-            s->tids = nullptr;
-            s->gids = order == SF_ORDER_IN_RASTER ? nullptr : s->gid_e;
-            s->prepared = true;
-            s->has_forward = false;
+            frame_graph_settle(s, hw, total);
             return SF_OK;
         }
         std::fprintf(stderr, "splatfield_b200: intersection capacity %llu reached (%llu needed); growing\n",
@@ -646,6 +673,109 @@ int frame_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_
         SF_CK(grow_isects(s, total));
     }
     return fail(SF_ERR_CAPACITY, "frame capacity did not settle");
+}
+
+cudaError_t frames_batch_resources(sf_scratch s, uint32_t count, size_t image_words) {
+    auto& g = s->fg;
+    cudaError_t e;
+    if (!g.copy && (e = cudaStreamCreateWithFlags(&g.copy, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    for (int k = 0; k < 2; ++k) {
+        if (!g.ready[k] && (e = cudaEventCreateWithFlags(&g.ready[k], cudaEventDisableTiming)) != cudaSuccess)
+            return e;
+        if (!g.copied[k] && (e = cudaEventCreateWithFlags(&g.copied[k], cudaEventDisableTiming)) != cudaSuccess)
+            return e;
+    }
+    if (g.stage_words < image_words) {
+        for (int k = 0; k < 2; ++k) {
+            dfree(g.stage[k]);
+            g.stage[k] = nullptr;
+        }
+        g.stage_words = 0;
+        for (int k = 0; k < 2; ++k)
+            if ((e = dalloc(&g.stage[k], image_words)) != cudaSuccess) return e;
+        g.stage_words = image_words;
+    }
+    if (g.batch_cap < count) {
+        if (g.views) cudaFreeHost(g.views);
+        if (g.frame_words) cudaFreeHost(g.frame_words);
+        g.views = nullptr;
+        g.frame_words = nullptr;
+        g.batch_cap = 0;
+        if ((e = cudaMallocHost(reinterpret_cast<void**>(&g.views), sizeof(sf_view) * count)) != cudaSuccess)
+            return e;
+        if ((e = cudaMallocHost(reinterpret_cast<void**>(&g.frame_words), 64 * (size_t)count)) != cudaSuccess)
+            return e;
+        g.batch_cap = count;
+    }
+    return cudaSuccess;
+}
+
+// `count` frames through the frame graph, frame i's image to
+// host_out + i * w * h. The device-to-host copy of frame i (copy stream,
+// from a staging image) overlaps frame i + 1 on st. Frames whose
+// intersections passed the capacity are rendered again, one by one, after
+// the capacity has grown. Syncs at the end.
+int frames_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cams, uint32_t count, uint32_t w,
+                        uint32_t h, cudaStream_t st, uint32_t* host_out) {
+    auto& g = s->fg;
+    const size_t img = (size_t)w * h;
+    int rc = frame_graph_ready(sp, s, w, h);
+    if (rc != SF_OK) return rc;
+    SF_CK(frames_batch_resources(s, count, img));
+    for (uint32_t i = 0; i < count; ++i) view_for_camera(cams[i], w, h, g.views + i);
+    // The copy stream may still hold another batch's copies of the staging
+    // images: the first two frames of this one wait for them.
+    SF_CK(cudaEventRecord(g.ready[0], g.copy));
+    SF_CK(cudaStreamWaitEvent(st, g.ready[0], 0));
+    for (uint32_t i = 0; i < count; ++i) {
+        const int slot = (int)(i & 1u);
+        SF_CK(cudaMemcpyAsync(g.view_dev, g.views + i, sizeof(sf_view), cudaMemcpyHostToDevice, st));
+        SF_CK(cudaGraphLaunch(g.exec, st));
+        SF_CK(cudaMemcpyAsync(g.frame_words + 16 * (size_t)i, s->words, 64, cudaMemcpyDeviceToHost, st));
+        if (i >= 2) SF_CK(cudaStreamWaitEvent(st, g.copied[slot], 0));
+        SF_CK(cudaMemcpy2DAsync(g.stage[slot], (size_t)w * 4, s->bitmap, (size_t)s->row_stride * 4,
+                                (size_t)w * 4, h, cudaMemcpyDeviceToDevice, st));
+        SF_CK(cudaEventRecord(g.ready[slot], st));
+        SF_CK(cudaStreamWaitEvent(g.copy, g.ready[slot], 0));
+        SF_CK(cudaMemcpyAsync(host_out + i * img, g.stage[slot], img * 4, cudaMemcpyDeviceToHost, g.copy));
+        SF_CK(cudaEventRecord(g.copied[slot], g.copy));
+    }
+    SF_CK(cudaStreamSynchronize(g.copy));
+    SF_CK(cudaStreamSynchronize(st));
+    uint64_t need = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const uint32_t* hw = g.frame_words + 16 * (size_t)i;
+        if (hw[1] & SF_DEV_ERR_TIMEOUT) return fail(SF_ERR_TIMEOUT, "device look-back wait timed out");
+        uint64_t total = 0;
+        std::memcpy(&total, hw + 4, 8);
+        if (total > kMaxIsects) return fail(SF_ERR_CAPACITY, "intersection count exceeds 2^30-1");
+        if (total > need) need = total;
+    }
+    if (need > s->cap) {
+        // Frames past the capacity (their images were drawn from clamped
+        // lists) are rendered again after one growth.
+        std::vector<uint32_t> redo;
+        for (uint32_t i = 0; i < count; ++i) {
+            uint64_t total = 0;
+            std::memcpy(&total, g.frame_words + 16 * (size_t)i + 4, 8);
+            if (total > s->cap) redo.push_back(i);
+        }
+        std::fprintf(stderr, "splatfield_b200: intersection capacity %llu reached (%llu needed); growing\n",
+                     (unsigned long long)s->cap, (unsigned long long)need);
+        SF_CK(grow_isects(s, need));
+        for (uint32_t i : redo) {
+            rc = frame_graph_render(sp, s, cams + i, w, h, st, host_out + i * img);
+            if (rc != SF_OK) return rc;
+        }
+        if (!redo.empty() && redo.back() == count - 1) return SF_OK;
+        // The scratch's state is the last frame's (rendered again below).
+        return frame_graph_render(sp, s, cams + count - 1, w, h, st, nullptr);
+    }
+    const uint32_t* last = g.frame_words + 16 * (size_t)(count - 1);
+    uint64_t total = 0;
+    std::memcpy(&total, last + 4, 8);
+    frame_graph_settle(s, last, total);
+    return SF_OK;
 }
 
 int frame_render(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32_t h, cudaStream_t st,
@@ -849,6 +979,17 @@ int sf_scratch_destroy(sf_scratch s) {
     if (s->fg.stream) cudaStreamDestroy(s->fg.stream);
     dfree(s->fg.view_dev);
     if (s->fg.view_host) cudaFreeHost(s->fg.view_host);
+    if (s->fg.copy) {
+        cudaStreamSynchronize(s->fg.copy);
+        cudaStreamDestroy(s->fg.copy);
+    }
+    for (int k = 0; k < 2; ++k) {
+        if (s->fg.ready[k]) cudaEventDestroy(s->fg.ready[k]);
+        if (s->fg.copied[k]) cudaEventDestroy(s->fg.copied[k]);
+        dfree(s->fg.stage[k]);
+    }
+    if (s->fg.views) cudaFreeHost(s->fg.views);
+    if (s->fg.frame_words) cudaFreeHost(s->fg.frame_words);
     delete s;
     return SF_OK;
 }
@@ -1033,6 +1174,24 @@ int sf_render_to_host(sf_splats s, sf_scratch scratch, const sf_camera* cam, uin
         SF_CK(cudaMemcpy2DAsync(out, (size_t)w * 4, scratch->bitmap, (size_t)scratch->row_stride * 4,
                                 (size_t)w * 4, h, cudaMemcpyDeviceToHost, S(stream)));
         SF_CK(cudaStreamSynchronize(S(stream)));
+        return SF_OK;
+    })
+}
+
+int sf_render_frames_to_host(sf_splats s, sf_scratch scratch, const sf_camera* cams, uint32_t count,
+                             uint32_t w, uint32_t h, sf_stream stream, uint32_t* out) {
+    SF_TRY({
+        if (!s || !scratch || (count && (!cams || !out))) return fail(SF_ERR_ARG, "null argument");
+        if (count == 0) return SF_OK;
+        if (w == 0 || h == 0 || w > 65535 * 16 || h > 65535 * 16) return fail(SF_ERR_SHAPE, "bad image size");
+        cudaStream_t st = S(stream);
+        SF_CK(use_device(scratch->ctx->device));
+        if (scratch->total != s->n || scratch->w != w || scratch->h != h) SF_CK(scratch_build(scratch, s->n, w, h));
+        if (frame_graph_usable(s, scratch)) return frames_graph_render(s, scratch, cams, count, w, h, st, out);
+        for (uint32_t i = 0; i < count; ++i) {
+            const int rc = sf_render_to_host(s, scratch, cams + i, w, h, stream, out + (size_t)i * w * h);
+            if (rc != SF_OK) return rc;
+        }
         return SF_OK;
     })
 }

@@ -325,3 +325,38 @@ def test_frame_graph_grows_capacity_and_matches_oracle(ctx, oracle_mod, order):
         np.testing.assert_array_equal(got, want)
         np.testing.assert_array_equal(host, want[:, :w])
     assert scratch.capacity() > (1 << 22)
+
+
+def test_frames_to_host_equal_single_frames_and_oracle(ctx, oracle_mod):
+    """sf_render_frames_to_host: a camera path in one call (read-backs from
+    two staging images overlapping the next frames) gives, frame for frame,
+    the images of sf_render_to_host and of the oracle. The first batch starts
+    below the capacity its frames need, so the frames past it are rendered
+    again after the growth; a second batch into the same pinned buffer
+    replays the graph."""
+    from splatfield_b200 import synth
+
+    n, w, h = 60000, 320, 240
+    attr, sh = synth.scene_uniform(n, 1, 11)
+    attr = attr.reshape(11, n)
+    attr[7:10] += 2.5
+    attr = attr.reshape(-1)
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    poses = [(0.0, 0.0, -3.0), (0.4, 0.2, -3.2), (-0.5, 0.1, -2.6), (0.0, 0.6, -3.5), (0.2, -0.3, -2.9)]
+    cams = [sf.look_at(p, (0.0, 0.0, 0.0)) for p in poses]
+    out = sf.pinned_empty((len(cams), h, w), np.uint32)
+    splats.render_frames_to_host(scratch, cams, (w, h), out=out)
+    assert scratch.capacity() > (1 << 22)
+    for i, p in enumerate(poses):
+        prep = oracle_mod.prepare(oracle_mod.look_at(p, (0.0, 0.0, 0.0)), w, h, attr, sh, 1)
+        want = oracle_mod.rasterize(prep, 0)["bitmap"][:, :w]
+        np.testing.assert_array_equal(out[i], want)
+    again = sf.pinned_empty((len(cams), h, w), np.uint32)
+    splats.render_frames_to_host(scratch, cams[::-1], (w, h), out=again)
+    for i in range(len(cams)):
+        np.testing.assert_array_equal(again[i], out[len(cams) - 1 - i])
+        np.testing.assert_array_equal(splats.render_to_host(scratch, cams[i], (w, h)), out[i])
+    # Pageable output memory works too (the copies then do not overlap).
+    plain = splats.render_frames_to_host(scratch, cams[:2], (w, h))
+    np.testing.assert_array_equal(plain, out[:2])
