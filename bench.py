@@ -2,10 +2,11 @@
 
 Headline workload ("frame"): 1M splats, SH degree 3 (16 coefficients per
 channel), means from 8 Gaussian clusters, 1920x1080, cameras on a 30-view
-radius-4 orbit. A step renders one frame through the reference-facing API
-(Splats::render_with: project, binned intersection build (per-tile counts,
-placement, per-tile sort by depth), rasterize, with its one host sync for the
-intersection total).
+radius-4 orbit. A step renders one frame (project, binned intersection build:
+per-tile counts, placement, per-tile sort by depth; rasterize) through
+sf_render_frames, the orbit's 30 cameras per call: the frames are enqueued
+back to back and each frame's intersection total is checked at the call's
+one host sync.
 
   value   frames/s, all ranks, device-timed with CUDA events on the launch
           stream, inputs resident in HBM (236 MB of splat planes > 126 MB L2,
@@ -363,10 +364,14 @@ def run_ours(args, rank, world):
         dist.barrier()
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    path = [my_cams[i % N_CAMS] for i in range(N_CAMS)]
     with ClockSampler(local) as clocks:
         start.record(stream)
-        for i in range(args.steps):
-            splats.render_with(scratch, my_cams[i % N_CAMS], size, stream=stream)
+        done = 0
+        while done < args.steps:
+            k = min(N_CAMS, args.steps - done)
+            splats.render_frames(scratch, path[:k], size, stream=stream)
+            done += k
         end.record(stream)
         torch.cuda.synchronize()
     launches = _lib.lib().sf_kernel_launches() - launches0

@@ -169,13 +169,21 @@ typedef struct {
      * Same results either way. sf_prepare_isects and sf_render_forward always
      * sort (their lists are handed out or replayed). */
     uint32_t raster_order;
-    uint32_t reserved[4];
+    /* Block schedule of the rasterizer for binned RGB frames
+     * (sf_render_with / _to_host, sf_render_frames / _frames_to_host):
+     *   SF_SCHEDULE_LONGEST (default): blocks take the tiles by list size
+     *     class, longest first, so the longest walks do not trail the grid;
+     *   SF_SCHEDULE_TILES: block i takes tile i. */
+    uint32_t raster_schedule;
+    uint32_t reserved[3];
 } sf_tuning;
 #define SF_ISECTS_BINNED 0u
 #define SF_ISECTS_DEPTH_SORTED 1u
 #define SF_ORDER_SORTED 0u
 #define SF_ORDER_IN_RASTER 1u
 #define SF_ORDER_HYBRID 2u
+#define SF_SCHEDULE_LONGEST 0u
+#define SF_SCHEDULE_TILES 1u
 int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t);
 int sf_scratch_get_tuning(sf_scratch s, sf_tuning* t);
 
@@ -216,6 +224,12 @@ int sf_render_to_host(sf_splats s, sf_scratch scratch, const sf_camera* cam, uin
  * the reference's per-frame render_with (src/render.rs:371-380). */
 int sf_render_frames_to_host(sf_splats s, sf_scratch scratch, const sf_camera* cams, uint32_t count,
                              uint32_t w, uint32_t h, sf_stream stream, uint32_t* out);
+/* `count` frames, as `count` sf_render_with calls, enqueued back to back
+ * with one sync at the end (each frame's intersection total is checked
+ * then; frames past the capacity are rendered again after it has grown).
+ * The last frame's image is the scratch's bitmap (sf_scratch_buffers). */
+int sf_render_frames(sf_splats s, sf_scratch scratch, const sf_camera* cams, uint32_t count, uint32_t w,
+                     uint32_t h, sf_stream stream);
 /* Adjoint (no counterpart in the reference, which renders forward only).
  * sf_render_forward: sf_render_float that also keeps, per pixel, the final
  * transmittance and the position of the last contributor, for the backward.

@@ -28,6 +28,7 @@ READ_TILE_IDS, READ_GAUSSIAN_IDS, READ_TILE_START, READ_BITMAP, READ_RGBA, READ_
 EIG_LUT_F32, EIG_FP64 = 0, 1
 ISECTS_BINNED, ISECTS_DEPTH_SORTED = 0, 1
 ORDER_SORTED, ORDER_IN_RASTER, ORDER_HYBRID = 0, 1, 2
+SCHEDULE_LONGEST, SCHEDULE_TILES = 0, 1
 
 
 class SplatfieldError(RuntimeError):
@@ -54,7 +55,7 @@ class Tuning(C.Structure):
     """sf_tuning: kernel forms of a scratch (results are identical across forms)."""
 
     _fields_ = [("raster_cull", C.c_uint32), ("isect_build", C.c_uint32), ("raster_detail", C.c_uint32),
-                ("raster_order", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+                ("raster_order", C.c_uint32), ("raster_schedule", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class RoundTuning(C.Structure):
@@ -114,6 +115,7 @@ SIGNATURES = {
         "sf_render_float": (i32, [P, P, P, u32, u32, P, PP]),
         "sf_render_to_host": (i32, [P, P, P, u32, u32, P, P]),
         "sf_render_frames_to_host": (i32, [P, P, P, u32, u32, u32, P, P]),
+        "sf_render_frames": (i32, [P, P, P, u32, u32, u32, P]),
         "sf_render_forward": (i32, [P, P, P, u32, u32, P, PP]),
         "sf_render_backward": (i32, [P, P, P, u32, u32, P, P, P, P, P]),
         "sf_prepare_isects": (i32, [P, P, P, u32, u32, P, P]),

@@ -26,13 +26,14 @@ __all__ = [
     "RenderScratch", "TileIsects", "Accumulators", "Mask", "BetaState", "map_labels", "bits_for",
     "RadixScratch", "ScanScratch", "exclusive_scan_gather", "exclusive_scan_buf", "entropy_table",
     "table_entropy", "fractional_bits", "row_stride_for", "EIG_LUT_F32", "EIG_FP64", "Round",
-    "ISECTS_BINNED", "ISECTS_DEPTH_SORTED", "ORDER_IN_RASTER", "ORDER_SORTED", "ORDER_HYBRID", "ply_inspect", "load_ply",
+    "ISECTS_BINNED", "ISECTS_DEPTH_SORTED", "ORDER_IN_RASTER", "ORDER_SORTED", "ORDER_HYBRID", "SCHEDULE_LONGEST", "SCHEDULE_TILES", "ply_inspect", "load_ply",
     "pinned_empty",
 ]
 
 EIG_LUT_F32, EIG_FP64 = L.EIG_LUT_F32, L.EIG_FP64
 ISECTS_BINNED, ISECTS_DEPTH_SORTED = L.ISECTS_BINNED, L.ISECTS_DEPTH_SORTED
 ORDER_IN_RASTER, ORDER_SORTED, ORDER_HYBRID = L.ORDER_IN_RASTER, L.ORDER_SORTED, L.ORDER_HYBRID
+SCHEDULE_TILES, SCHEDULE_LONGEST = L.SCHEDULE_TILES, L.SCHEDULE_LONGEST
 BASE_FOV = 0.8  # Camera::BASE_FOV (src/camera.rs:86)
 
 
@@ -417,6 +418,14 @@ class Splats:
                                       _vp(out)))
         return out
 
+    def render_frames(self, scratch: "RenderScratch", cameras, img_size, stream=None) -> DeviceView:
+        """``len(cameras)`` frames enqueued back to back with one sync at the
+        end; returns the last frame's image (device view, [h][row_stride])."""
+        w, h = img_size
+        cams = (Camera * len(cameras))(*cameras)
+        check(lib().sf_render_frames(self.handle, scratch.handle, cams, len(cameras), w, h, _stream(stream)))
+        return DeviceView(scratch.bitmap_ptr(), np.uint32, (h, row_stride_for(w)), scratch)
+
     def render_frames_to_host(self, scratch: "RenderScratch", cameras, img_size, out=None, stream=None):
         """One RGBA8 image per camera, [count, h, w] words in host memory
         (``out``: pinned memory lets each image's read-back overlap the next
@@ -500,23 +509,26 @@ class RenderScratch:
         return int(c.value)
 
     def set_tuning(self, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED, raster_detail: int = 0,
-                   raster_order: int = L.ORDER_SORTED) -> None:
+                   raster_order: int = L.ORDER_SORTED, raster_schedule: int = L.SCHEDULE_LONGEST) -> None:
         """Kernel forms (results are identical across forms): raster_cull 0/1,
         isect_build ISECTS_BINNED (default) or ISECTS_DEPTH_SORTED,
         raster_detail 1 to count the per-pair diagnostics of ``stats``,
-        raster_order ORDER_SORTED (default), ORDER_IN_RASTER or ORDER_HYBRID."""
+        raster_order ORDER_SORTED (default), ORDER_IN_RASTER or ORDER_HYBRID,
+        raster_schedule SCHEDULE_LONGEST (default) or SCHEDULE_TILES."""
         t = L.Tuning()
         t.raster_cull = int(raster_cull)
         t.isect_build = int(isect_build)
         t.raster_detail = int(raster_detail)
         t.raster_order = int(raster_order)
+        t.raster_schedule = int(raster_schedule)
         check(lib().sf_scratch_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:
         t = L.Tuning()
         check(lib().sf_scratch_get_tuning(self.handle, C.byref(t)))
         return {"raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build),
-                "raster_detail": int(t.raster_detail), "raster_order": int(t.raster_order)}
+                "raster_detail": int(t.raster_detail), "raster_order": int(t.raster_order),
+                "raster_schedule": int(t.raster_schedule)}
 
     def read(self, what: int, count: int, dtype=np.uint32, stream=None) -> np.ndarray:
         out = np.empty(count, dtype)

@@ -141,6 +141,7 @@ struct sf_scratch_t {
     // capacity, tuning), replayed with the camera copied in by its first node.
     struct FrameGraph {
         cudaGraphExec_t exec = nullptr;
+        uint32_t kernels = 0;           // kernel nodes of exec
         cudaStream_t stream = nullptr;  // capture stream
         sf_view* view_dev = nullptr;
         sf_view* view_host = nullptr;   // pinned
@@ -166,7 +167,7 @@ struct sf_scratch_t {
     float* final_t = nullptr;
     uint32_t* n_contrib = nullptr;
     // device words: [0] visible, [1] error bits, [2..3] spare, [4..5] u64
-    // total, [6..13] binned-build tile statistics (sf_internal.h)
+    // total, [6..14] binned-build tile statistics (sf_internal.h)
     uint32_t* words = nullptr;
     uint32_t* host_words = nullptr;  // pinned mirror
     unsigned long long* stats = nullptr;  // raster pair statistics of the last finalize
@@ -287,7 +288,7 @@ cudaError_t scratch_build(sf_scratch s, uint32_t total, uint32_t w, uint32_t h) 
         s->bin_chunks = bin_chunks(total, s->ctx->sm_count);
         SF_AL(s->bin_hist, (size_t)s->bin_chunks * tiles);
         SF_AL(s->bin_cnt, tiles + 1);
-        SF_AL(s->bin_lists, (size_t)kSortClasses * tiles);
+        SF_AL(s->bin_lists, (size_t)(kSortClasses + 1) * tiles);
     }
     SF_AL(s->bitmap, (size_t)h * s->row_stride);
 #undef SF_AL
@@ -543,6 +544,7 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
     cudaStream_t st = g.stream;
     // The camera's view is copied to g.view_dev before each launch (from a
     // pinned slot of the caller's choosing), outside the graph.
+    const uint64_t launches0 = launches();
     SF_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaMemsetAsync(words, 0, 64, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->stats, 0, 32, st);
@@ -586,11 +588,17 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
         a.cull = s->tuning.raster_cull;
         a.stats = s->stats;
         a.bitmap = s->bitmap;
+        if (s->tuning.raster_schedule == SF_SCHEDULE_LONGEST && order != SF_ORDER_IN_RASTER) {
+            a.class_lists = s->bin_lists;
+            a.class_n = words + 8;
+        }
         e = launch_raster(0, a, st);
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(s->host_words, words, 64, cudaMemcpyDeviceToHost, st);
     cudaGraph_t graph = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+    g.kernels = (uint32_t)(launches() - launches0);
+    forget_launches(g.kernels);
     if (e != cudaSuccess || e2 != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
@@ -653,6 +661,7 @@ int frame_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_
         view_for_camera(*cam, w, h, g.view_host);
         SF_CK(cudaMemcpyAsync(g.view_dev, g.view_host, sizeof(sf_view), cudaMemcpyHostToDevice, st));
         SF_CK(cudaGraphLaunch(g.exec, st));
+        note_launches(g.kernels);
         if (host_out)
             SF_CK(cudaMemcpy2DAsync(host_out, (size_t)w * 4, s->bitmap, (size_t)s->row_stride * 4, (size_t)w * 4,
                                     h, cudaMemcpyDeviceToHost, st));
@@ -711,7 +720,8 @@ cudaError_t frames_batch_resources(sf_scratch s, uint32_t count, size_t image_wo
 }
 
 // `count` frames through the frame graph, frame i's image to
-// host_out + i * w * h. The device-to-host copy of frame i (copy stream,
+// host_out + i * w * h (host_out null: the images stay on the device, the
+// last one in the scratch). The device-to-host copy of frame i (copy stream,
 // from a staging image) overlaps frame i + 1 on st. Frames whose
 // intersections passed the capacity are rendered again, one by one, after
 // the capacity has grown. Syncs at the end.
@@ -721,7 +731,7 @@ int frames_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cams, uint3
     const size_t img = (size_t)w * h;
     int rc = frame_graph_ready(sp, s, w, h);
     if (rc != SF_OK) return rc;
-    SF_CK(frames_batch_resources(s, count, img));
+    SF_CK(frames_batch_resources(s, count, host_out ? img : 0));
     for (uint32_t i = 0; i < count; ++i) view_for_camera(cams[i], w, h, g.views + i);
     // The copy stream may still hold another batch's copies of the staging
     // images: the first two frames of this one wait for them.
@@ -731,7 +741,9 @@ int frames_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cams, uint3
         const int slot = (int)(i & 1u);
         SF_CK(cudaMemcpyAsync(g.view_dev, g.views + i, sizeof(sf_view), cudaMemcpyHostToDevice, st));
         SF_CK(cudaGraphLaunch(g.exec, st));
+        note_launches(g.kernels);
         SF_CK(cudaMemcpyAsync(g.frame_words + 16 * (size_t)i, s->words, 64, cudaMemcpyDeviceToHost, st));
+        if (!host_out) continue;
         if (i >= 2) SF_CK(cudaStreamWaitEvent(st, g.copied[slot], 0));
         SF_CK(cudaMemcpy2DAsync(g.stage[slot], (size_t)w * 4, s->bitmap, (size_t)s->row_stride * 4,
                                 (size_t)w * 4, h, cudaMemcpyDeviceToDevice, st));
@@ -764,7 +776,7 @@ int frames_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cams, uint3
                      (unsigned long long)s->cap, (unsigned long long)need);
         SF_CK(grow_isects(s, need));
         for (uint32_t i : redo) {
-            rc = frame_graph_render(sp, s, cams + i, w, h, st, host_out + i * img);
+            rc = frame_graph_render(sp, s, cams + i, w, h, st, host_out ? host_out + i * img : nullptr);
             if (rc != SF_OK) return rc;
         }
         if (!redo.empty() && redo.back() == count - 1) return SF_OK;
@@ -999,6 +1011,7 @@ int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t) {
     if (t->raster_cull > 1 || t->raster_detail > 1) return fail(SF_ERR_ARG, "raster flags must be 0 or 1");
     if (t->isect_build > SF_ISECTS_DEPTH_SORTED) return fail(SF_ERR_ARG, "unknown isect_build");
     if (t->raster_order > SF_ORDER_HYBRID) return fail(SF_ERR_ARG, "unknown raster_order");
+    if (t->raster_schedule > SF_SCHEDULE_TILES) return fail(SF_ERR_ARG, "unknown raster_schedule");
     s->tuning = *t;
     return SF_OK;
 }
@@ -1174,6 +1187,24 @@ int sf_render_to_host(sf_splats s, sf_scratch scratch, const sf_camera* cam, uin
         SF_CK(cudaMemcpy2DAsync(out, (size_t)w * 4, scratch->bitmap, (size_t)scratch->row_stride * 4,
                                 (size_t)w * 4, h, cudaMemcpyDeviceToHost, S(stream)));
         SF_CK(cudaStreamSynchronize(S(stream)));
+        return SF_OK;
+    })
+}
+
+int sf_render_frames(sf_splats s, sf_scratch scratch, const sf_camera* cams, uint32_t count, uint32_t w,
+                     uint32_t h, sf_stream stream) {
+    SF_TRY({
+        if (!s || !scratch || (count && !cams)) return fail(SF_ERR_ARG, "null argument");
+        if (count == 0) return SF_OK;
+        if (w == 0 || h == 0 || w > 65535 * 16 || h > 65535 * 16) return fail(SF_ERR_SHAPE, "bad image size");
+        cudaStream_t st = S(stream);
+        SF_CK(use_device(scratch->ctx->device));
+        if (scratch->total != s->n || scratch->w != w || scratch->h != h) SF_CK(scratch_build(scratch, s->n, w, h));
+        if (frame_graph_usable(s, scratch)) return frames_graph_render(s, scratch, cams, count, w, h, st, nullptr);
+        for (uint32_t i = 0; i < count; ++i) {
+            const int rc = sf_render_with(s, scratch, cams + i, w, h, stream, nullptr, nullptr);
+            if (rc != SF_OK) return rc;
+        }
         return SF_OK;
     })
 }

@@ -49,20 +49,31 @@ __device__ __forceinline__ void for_each_pair(uint32_t begin, uint32_t end, cons
                                               const uint32_t* __restrict__ payload, uint32_t tiles_x, F&& f) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = threadIdx.x >> 5;
-    const uint32_t nwarps = blockDim.x >> 5;
-    for (uint32_t g0 = begin + warp * 32u; g0 < end; g0 += nwarps * 32u) {
-        const uint32_t r = g0 + lane;
-        uint32_t min_x = 0, min_y = 0, width = 1, cnt = 0, pay = 0;
-        if (r < end) {
-            const uint2 bb = bbox[r];
-            if (payload) pay = payload[r];
-            min_x = bb.x & 0xffffu;
-            min_y = bb.x >> 16;
-            const uint32_t max_x = bb.y & 0xffffu, max_y = bb.y >> 16;
-            if (max_x > min_x && max_y > min_y) {
-                width = max_x - min_x;
-                cnt = width * (max_y - min_y);
-            }
+    const uint32_t stride = (blockDim.x >> 5) * 32u;
+    // The next group's box and payload are loaded while this group's pairs
+    // are handed out (a zero box has no pairs).
+    uint2 bb_next = make_uint2(0u, 0u);
+    uint32_t pay_next = 0;
+    uint32_t g0 = begin + warp * 32u;
+    if (g0 + lane < end) {
+        bb_next = bbox[g0 + lane];
+        if (payload) pay_next = payload[g0 + lane];
+    }
+    for (; g0 < end; g0 += stride) {
+        const uint2 bb = bb_next;
+        const uint32_t pay = pay_next;
+        const uint32_t rn = g0 + stride + lane;
+        bb_next = make_uint2(0u, 0u);
+        pay_next = 0;
+        if (rn < end) {
+            bb_next = bbox[rn];
+            if (payload) pay_next = payload[rn];
+        }
+        uint32_t min_x = bb.x & 0xffffu, min_y = bb.x >> 16, width = 1, cnt = 0;
+        const uint32_t max_x = bb.y & 0xffffu, max_y = bb.y >> 16;
+        if (max_x > min_x && max_y > min_y) {
+            width = max_x - min_x;
+            cnt = width * (max_y - min_y);
         }
         uint32_t incl = cnt;
 #pragma unroll
@@ -86,8 +97,20 @@ __device__ __forceinline__ void for_each_pair(uint32_t begin, uint32_t end, cons
             const uint32_t oy = __shfl_sync(0xffffffffu, min_y, o);
             const uint32_t opay = __shfl_sync(0xffffffffu, pay, o);
             if (p < total) {
+                // Row and column of pair k in the owner's box: a float
+                // quotient (k < 2^16, so it is off by at most one) and an
+                // exact integer correction.
                 const uint32_t k = p - (oend - ocnt);
-                f(g0 + o, (ox + k % ow) + (oy + k / ow) * tiles_x, opay);
+                uint32_t row = (uint32_t)((float)k * __fdividef(1.0f, (float)ow));
+                int32_t col = (int32_t)(k - row * ow);
+                if (col < 0) {
+                    --row;
+                    col += (int32_t)ow;
+                } else if (col >= (int32_t)ow) {
+                    ++row;
+                    col -= (int32_t)ow;
+                }
+                f(g0 + o, (ox + (uint32_t)col) + (oy + row) * tiles_x, opay);
             }
         }
     }
@@ -114,8 +137,8 @@ struct ClassLimits {
 
 // Block (32, 32): x = tile within the block's 32, y = a group of chunks.
 // words: [6] max tile count (atomicMax), [8 + k] tiles in size class k
-// (lists[k * tiles + i]); the last class holds the lists longer than every
-// shared-memory class.
+// (lists[k * tiles + i]); class kSortClasses - 1 holds the lists longer than
+// every shared-memory class, "class" kSortClasses the empty tiles.
 __global__ __launch_bounds__(1024) void bin_colscan_kernel(uint32_t* __restrict__ hist, uint32_t chunks,
                                                            uint32_t tiles, uint32_t* __restrict__ cnt,
                                                            uint32_t* __restrict__ lists, uint32_t* words,
@@ -142,15 +165,15 @@ __global__ __launch_bounds__(1024) void bin_colscan_kernel(uint32_t* __restrict_
         if (blockIdx.x == 0 && tx == 0) cnt[tiles] = 0;
         // Size classes (warp-aggregated appends; the list order is free).
         const uint32_t total = valid ? run : 0u;
-        uint32_t cls = total == 0 ? kSortClasses : kSortClasses - 1;
+        uint32_t cls = total == 0 ? kSortClasses : kSortClasses - 1;  // kSortClasses: the empty tiles
         if (total > 0)
             for (int k = kSortClasses - 2; k >= 0; --k)
                 if (total <= lim.max_n[k]) cls = (uint32_t)k;
         const uint32_t mx = __reduce_max_sync(0xffffffffu, total);
         if (tx == 0 && mx) atomicMax(words + 6, mx);
 #pragma unroll
-        for (uint32_t k = 0; k < kSortClasses; ++k) {
-            const uint32_t m = __ballot_sync(0xffffffffu, cls == k);
+        for (uint32_t k = 0; k <= kSortClasses; ++k) {
+            const uint32_t m = __ballot_sync(0xffffffffu, valid && cls == k);
             if (!m) continue;
             const uint32_t leader = __ffs(m) - 1;
             uint32_t base = 0;
@@ -805,15 +828,15 @@ cudaError_t launch_tile_sorts(const uint32_t grids[kSortClasses], const uint32_t
                            sm_count, L(5), N(5), tile_start, capacity, pairs, ids, tids_out, keys_tmp, s3);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClass1, kBins1, kThreads1>, kThreads1,
-                           sort_smem<kClass1, kBins1, kThreads1>(), grids[3], sm_count, L(3), N(3), tile_start,
-                           capacity, pairs, ids, tids_out, keys_tmp, s1);
+                           sort_smem<kClass1, kBins1, kThreads1>(), grids[3], sm_count, L(3), N(3),
+                           tile_start, capacity, pairs, ids, tids_out, keys_tmp, s1);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClass2, kBins2, kThreads2>, kThreads2,
-                           sort_smem<kClass2, kBins2, kThreads2>(), grids[4], sm_count, L(4), N(4), tile_start,
-                           capacity, pairs, ids, tids_out, keys_tmp, s2);
+                           sort_smem<kClass2, kBins2, kThreads2>(), grids[4], sm_count, L(4), N(4),
+                           tile_start, capacity, pairs, ids, tids_out, keys_tmp, s2);
     if (e != cudaSuccess) return e;
-    e = launch_sort_kernel(tile_sort_warp_kernel, 256, 0, (grids[0] + 7) / 8, sm_count, L(0), N(0), tile_start, capacity,
-                           pairs, ids, tids_out, keys_tmp, s2);
+    e = launch_sort_kernel(tile_sort_warp_kernel, 256, 0, (grids[0] + 7) / 8, sm_count, L(0), N(0), tile_start,
+                           capacity, pairs, ids, tids_out, keys_tmp, s2);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClassS, kBinsS, kThreadsS>, kThreadsS,
                            sort_smem<kClassS, kBinsS, kThreadsS>(), grids[1], sm_count, L(1), N(1), tile_start,

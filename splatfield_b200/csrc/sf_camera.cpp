@@ -88,5 +88,6 @@ namespace {
 std::atomic<uint64_t> g_launches{0};
 }
 void note_launches(uint32_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+void forget_launches(uint64_t k) { g_launches.fetch_sub(k, std::memory_order_relaxed); }
 uint64_t launches() { return g_launches.load(std::memory_order_relaxed); }
 }  // namespace sfk

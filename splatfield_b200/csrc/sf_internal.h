@@ -15,6 +15,9 @@ namespace sfk {
 
 // Process-wide count of kernels launched by this library.
 void note_launches(uint32_t k);
+// A stream capture enqueues kernels without running them: the capture takes
+// its count back (forget_launches) and each graph launch notes it again.
+void forget_launches(uint64_t k);
 uint64_t launches();
 
 // Per-splat projected record, split so that the responsibility modes read 32
@@ -86,6 +89,11 @@ struct RasterArgs {
     // (256 per tile-list entry walked before the tile's early exit), [1]
     // exponentials evaluated, [2] contributing pairs (alpha >= 1/255).
     unsigned long long* stats;
+    // Block schedule (optional, one block per tile): the binned build's
+    // class lists, longest lists first (class_lists[k * tiles + i], counts
+    // class_n[k], k = kSortClasses - 1 .. 0, then the empty tiles).
+    const uint32_t* class_lists;
+    const uint32_t* class_n;
 };
 // mode 0 = RGB, 1 = total responsibility, 2 = evidence.
 cudaError_t launch_raster(int mode, const RasterArgs& a, cudaStream_t stream);
@@ -143,8 +151,9 @@ uint32_t bin_class_limit(int k);
 constexpr uint32_t kBinSharedMax = 12288;
 // hist: [chunks][tiles] counts, then (after colscan) per-chunk exclusive
 // prefixes. cnt: [tiles + 1] per-tile totals (cnt[tiles] = 0). lists:
-// [kSortClasses][tiles] tiles of each size class. words: [6] max tile total,
-// [8 + k] tiles in class k (all zero on entry).
+// [kSortClasses + 1][tiles] tiles of each size class, then the empty tiles.
+// words: [6] max tile total, [8 + k] tiles in class k, k <= kSortClasses
+// (all zero on entry).
 cudaError_t launch_bin_count(const uint2* bbox, uint32_t n, uint32_t tiles_x, uint32_t tiles, uint32_t chunks,
                              uint32_t* hist, cudaStream_t st);
 cudaError_t launch_bin_colscan(uint32_t* hist, uint32_t chunks, uint32_t tiles, uint32_t* cnt, uint32_t* lists,

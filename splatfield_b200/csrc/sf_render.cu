@@ -505,8 +505,9 @@ __device__ void bitonic_sort64(unsigned long long* v, uint32_t m) {
     }
 }
 
+// One tile (block-uniform); the shared arrays are the kernel's.
 template <int MODE, bool CULL, bool DETAIL, bool LAZY>
-__global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
+__device__ __forceinline__ void raster_tile(const RasterArgs& a, const uint32_t tile) {
     __shared__ float4 s_g0[256];
     __shared__ float4 s_g1[256];
     __shared__ float4 s_col[MODE == 0 ? 256 : 1];
@@ -519,7 +520,6 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
     __shared__ unsigned long long s_64[16];
     __shared__ uint32_t s_ctl[4];
 
-    const uint32_t tile = blockIdx.x;
     const uint32_t tx = tile % a.tiles_x, ty = tile / a.tiles_x;
     const uint32_t tid = threadIdx.x, lane = tid & 31u;
     const uint32_t warp = tid >> 5;
@@ -687,6 +687,26 @@ __global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
     }
     if (a.final_t) a.final_t[pix] = ps.T;
     if (a.n_contrib) a.n_contrib[pix] = ps.last;
+}
+
+// One block per tile: block i takes tile i, or with class lists the i-th
+// tile in longest-list-first order.
+template <int MODE, bool CULL, bool DETAIL, bool LAZY>
+__global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
+    uint32_t tile = blockIdx.x;
+    if (a.class_lists) {
+        const uint32_t tiles = a.tiles_x * a.tiles_y;
+        uint32_t j = blockIdx.x;
+        int k = kSortClasses - 1;
+        for (; k >= 0; --k) {
+            const uint32_t c = a.class_n[k];
+            if (j < c) break;
+            j -= c;
+        }
+        // k < 0: the empty tiles (the counts sum to the tile count).
+        tile = a.class_lists[(size_t)(k < 0 ? kSortClasses : k) * tiles + j];
+    }
+    raster_tile<MODE, CULL, DETAIL, LAZY>(a, tile);
 }
 
 __global__ void export_rows_kernel(const float4* __restrict__ geo0, const float4* __restrict__ geo1,

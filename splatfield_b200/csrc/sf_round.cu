@@ -99,7 +99,7 @@ struct sf_round_t {
     std::vector<RoundLane> lanes;
     sf_view* views_dev = nullptr;
     sf_view* views_host = nullptr;  // pinned
-    uint32_t* words = nullptr;      // [views][16]: 0 visible, 1 err, 2 n32, 4..5 total u64, 6..13 binned stats
+    uint32_t* words = nullptr;      // [views][16]: 0 visible, 1 err, 2 n32, 4..5 total u64, 6..14 binned stats
     uint32_t* words_host = nullptr; // pinned
     double* eig_dev = nullptr;
     double* eig_host = nullptr;     // pinned
@@ -112,6 +112,7 @@ struct sf_round_t {
     cudaStream_t main = nullptr;
     cudaEvent_t fork = nullptr;
     cudaGraphExec_t exec = nullptr;
+    uint32_t graph_kernels = 0;  // kernel nodes of exec
     const void* g_splats = nullptr;
     const void* g_beta = nullptr;
     int g_mode = -1;
@@ -153,7 +154,7 @@ cudaError_t lane_alloc(sf_round_t* r, RoundLane& L, uint64_t cap) {
     if (r->max_tiles <= kBinMaxTiles) {
         RA(L.hist, (size_t)r->chunks * r->max_tiles);
         RA(L.cnt, (size_t)r->max_tiles + 1);
-        RA(L.lists, (size_t)kSortClasses * r->max_tiles);
+        RA(L.lists, (size_t)(kSortClasses + 1) * r->max_tiles);
     }
 #undef RA
     if ((e = cudaMalloc(&L.scan_tmp, scan_temp_bytes(std::max(n, r->max_tiles + 1)))) != cudaSuccess) return e;
@@ -335,6 +336,7 @@ cudaError_t use_dev(int dev) {
 // Capture the whole round into r->exec.
 int build_graph(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, int mode) {
     graph_drop(r);
+    const uint64_t launches0 = launches();
     RF_CK(cudaStreamBeginCapture(r->main, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaMemcpyAsync(r->views_dev, r->views_host, sizeof(sf_view) * r->views,
                                     cudaMemcpyHostToDevice, r->main);
@@ -356,6 +358,8 @@ int build_graph(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, int
         e = cudaMemcpyAsync(r->eig_host, r->eig_dev, 8 * r->views, cudaMemcpyDeviceToHost, r->main);
     cudaGraph_t graph = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(r->main, &graph);
+    r->graph_kernels = (uint32_t)(launches() - launches0);
+    forget_launches(r->graph_kernels);
     if (e != cudaSuccess || e2 != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
@@ -401,6 +405,7 @@ int run_round(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, const
         RF_CK(cudaStreamWaitEvent(r->main, ev, 0));
         cudaEventDestroy(ev);
         RF_CK(cudaGraphLaunch(r->exec, r->main));
+        note_launches(r->graph_kernels);
         RF_CK(cudaStreamSynchronize(r->main));
         uint64_t worst = 0;
         bool over = false;

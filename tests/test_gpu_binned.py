@@ -141,3 +141,26 @@ def test_in_raster_order_matches_sorted_lists(ctx, oracle_mod, kind, cull, order
     np.testing.assert_array_equal(acc_l.bits.read(), acc_s.bits.read())
     # Stats count the same walked entries either way.
     assert lazy.stats()["pairs_visited"] == sorted_.stats()["pairs_visited"]
+
+
+
+@pytest.mark.parametrize("kind", ["clustered", "one_spot", "ties"])
+def test_raster_schedules_match_oracle(ctx, oracle_mod, kind):
+    """The rasterizer's block schedules (longest lists first, the default;
+    tile order) give the same frame as each other and the oracle, with the
+    same walked-pair count, through sf_render_with and sf_render_frames."""
+    attr, sh, k, w, h = scene_for(kind)
+    n = attr.size // 11
+    splats = sf.Splats(attr, sh)
+    cam = sf.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    cam.fov[0], cam.fov[1] = synth.fov_for(w, h)
+    longest, tiles = sf.RenderScratch(n, (w, h)), sf.RenderScratch(n, (w, h))
+    assert longest.get_tuning()["raster_schedule"] == sf.SCHEDULE_LONGEST
+    tiles.set_tuning(raster_schedule=sf.SCHEDULE_TILES)
+    got = splats.render_with(longest, cam, (w, h)).read()
+    np.testing.assert_array_equal(got, splats.render_with(tiles, cam, (w, h)).read())
+    assert longest.stats()["pairs_visited"] == tiles.stats()["pairs_visited"]
+    cam_o = oracle_mod.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    cam_o.fov[0], cam_o.fov[1] = synth.fov_for(w, h)
+    np.testing.assert_array_equal(got, oracle_mod.rasterize(oracle_mod.prepare(cam_o, w, h, attr, sh, k), 0)["bitmap"])
+    np.testing.assert_array_equal(splats.render_frames(longest, [cam, cam], (w, h)).read(), got)

@@ -360,3 +360,25 @@ def test_frames_to_host_equal_single_frames_and_oracle(ctx, oracle_mod):
     # Pageable output memory works too (the copies then do not overlap).
     plain = splats.render_frames_to_host(scratch, cams[:2], (w, h))
     np.testing.assert_array_equal(plain, out[:2])
+
+
+def test_render_frames_equals_render_with_and_counts_replays(ctx, oracle_mod):
+    """sf_render_frames (frames enqueued back to back, one sync) leaves the
+    last frame's image, equal to sf_render_with's and the oracle's; each
+    graph replay is counted in sf_kernel_launches."""
+    from splatfield_b200 import _lib, synth
+
+    n, w, h = 30000, 256, 192
+    attr, sh = synth.scene_uniform(n, 1, 21)
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    poses = [(0.0, 0.0, -3.0), (0.3, 0.1, -2.8), (-0.2, 0.4, -3.3)]
+    cams = [sf.look_at(p, (0.0, 0.0, 0.0)) for p in poses]
+    splats.render_frames(scratch, cams, (w, h))  # captures the graph
+    k0 = _lib.lib().sf_kernel_launches()
+    last = splats.render_frames(scratch, cams, (w, h)).read()
+    per_frame = (_lib.lib().sf_kernel_launches() - k0) / len(cams)
+    assert per_frame >= 8 and per_frame == int(per_frame)
+    np.testing.assert_array_equal(last, splats.render_with(scratch, cams[-1], (w, h)).read())
+    prep = oracle_mod.prepare(oracle_mod.look_at(poses[-1], (0.0, 0.0, 0.0)), w, h, attr, sh, 1)
+    np.testing.assert_array_equal(last, oracle_mod.rasterize(prep, 0)["bitmap"])
