@@ -119,6 +119,8 @@ __device__ __forceinline__ void for_each_pair(uint32_t begin, uint32_t end, cons
 __global__ __launch_bounds__(kBinThreads) void bin_count_kernel(const uint2* __restrict__ bbox, uint32_t n,
                                                                 uint32_t chunk, uint32_t tiles_x,
                                                                 uint32_t tiles, uint32_t* __restrict__ hist) {
+    pdl_trigger();
+    pdl_wait();
     extern __shared__ uint32_t s_hist[];
     for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) s_hist[t] = 0;
     __syncthreads();
@@ -143,6 +145,8 @@ __global__ __launch_bounds__(1024) void bin_colscan_kernel(uint32_t* __restrict_
                                                            uint32_t tiles, uint32_t* __restrict__ cnt,
                                                            uint32_t* __restrict__ lists, uint32_t* words,
                                                            ClassLimits lim) {
+    pdl_trigger();
+    pdl_wait();
     __shared__ uint32_t s_part[32][33];
     const uint32_t tx = threadIdx.x, ty = threadIdx.y;
     const uint32_t t = blockIdx.x * 32u + tx;
@@ -198,6 +202,8 @@ __global__ __launch_bounds__(kBinThreads) void bin_place_kernel(
     const uint2* __restrict__ bbox, const uint32_t* __restrict__ depth_keys, uint32_t n, uint32_t chunk,
     uint32_t tiles_x, uint32_t tiles, const uint32_t* __restrict__ hist, const uint32_t* __restrict__ tile_start,
     uint32_t capacity, uint2* __restrict__ pairs, uint32_t* err) {
+    pdl_trigger();
+    pdl_wait();
     extern __shared__ uint32_t s_cur[];
     const uint32_t* row = hist + (size_t)blockIdx.x * tiles;
     for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) s_cur[t] = tile_start[t] + row[t];
@@ -730,17 +736,19 @@ cudaError_t launch_bin_count(const uint2* bbox, uint32_t n, uint32_t tiles_x, ui
     const size_t smem = (size_t)tiles * 4;
     cudaError_t e = smem_opt_in((const void*)bin_count_kernel, smem);
     if (e != cudaSuccess) return e;
-    bin_count_kernel<<<chunks, kBinThreads, smem, st>>>(bbox, n, bin_chunk_size(n, chunks), tiles_x, tiles, hist);
+    e = launch_pdl(bin_count_kernel, chunks, kBinThreads, smem, st, bbox, n, bin_chunk_size(n, chunks), tiles_x,
+                   tiles, hist);
     note_launches(1);
-    return cudaGetLastError();
+    return e;
 }
 
 cudaError_t launch_bin_colscan(uint32_t* hist, uint32_t chunks, uint32_t tiles, uint32_t* cnt, uint32_t* lists,
                                uint32_t* words, cudaStream_t st) {
     const ClassLimits lim{{kClassWarp, kClassS, kClass0, kClass1, kClass2}};
-    bin_colscan_kernel<<<(tiles + 31) / 32, dim3(32, 32), 0, st>>>(hist, chunks, tiles, cnt, lists, words, lim);
+    const cudaError_t e =
+        launch_pdl(bin_colscan_kernel, (tiles + 31) / 32, dim3(32, 32), 0, st, hist, chunks, tiles, cnt, lists, words, lim);
     note_launches(1);
-    return cudaGetLastError();
+    return e;
 }
 
 cudaError_t launch_bin_place(const uint2* bbox, const uint32_t* depth_keys, uint32_t n, uint32_t tiles_x,
@@ -749,21 +757,25 @@ cudaError_t launch_bin_place(const uint2* bbox, const uint32_t* depth_keys, uint
     const size_t smem = (size_t)tiles * 4;
     cudaError_t e = smem_opt_in((const void*)bin_place_kernel, smem);
     if (e != cudaSuccess) return e;
-    bin_place_kernel<<<chunks, kBinThreads, smem, st>>>(bbox, depth_keys, n, bin_chunk_size(n, chunks), tiles_x,
-                                                        tiles, hist, tile_start, capacity, pairs, err);
+    e = launch_pdl(bin_place_kernel, chunks, kBinThreads, smem, st, bbox, depth_keys, n, bin_chunk_size(n, chunks),
+                   tiles_x, tiles, hist, tile_start, capacity, pairs, err);
     note_launches(1);
-    return cudaGetLastError();
+    return e;
 }
 
 namespace {
 
 __global__ void clamp_count_kernel(const unsigned long long* total, uint32_t cap, uint32_t* n32, uint32_t* err) {
+    pdl_trigger();
+    pdl_wait();
     const unsigned long long t = *total;
     if (t > cap) atomicOr(err, SF_DEV_ERR_CAPACITY);
     *n32 = (uint32_t)(t < cap ? t : cap);
 }
 
 __global__ void clamp_starts_kernel(uint32_t* tile_start, uint32_t count, uint32_t cap) {
+    pdl_trigger();
+    pdl_wait();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < count && tile_start[i] > cap) tile_start[i] = cap;
 }
@@ -772,15 +784,15 @@ __global__ void clamp_starts_kernel(uint32_t* tile_start, uint32_t count, uint32
 
 cudaError_t launch_clamp_count(const unsigned long long* total, uint32_t cap, uint32_t* n32, uint32_t* err,
                                cudaStream_t st) {
-    clamp_count_kernel<<<1, 1, 0, st>>>(total, cap, n32, err);
+    const cudaError_t e = launch_pdl(clamp_count_kernel, 1, 1, 0, st, total, cap, n32, err);
     note_launches(1);
-    return cudaGetLastError();
+    return e;
 }
 
 cudaError_t launch_clamp_starts(uint32_t* tile_start, uint32_t count, uint32_t cap, cudaStream_t st) {
-    clamp_starts_kernel<<<(count + 255) / 256, 256, 0, st>>>(tile_start, count, cap);
+    const cudaError_t e = launch_pdl(clamp_starts_kernel, (count + 255) / 256, 256, 0, st, tile_start, count, cap);
     note_launches(1);
-    return cudaGetLastError();
+    return e;
 }
 
 cudaError_t sort_streams_create(SortStreams* ss) {

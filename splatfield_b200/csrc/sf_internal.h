@@ -15,6 +15,30 @@ namespace sfk {
 
 // Process-wide count of kernels launched by this library.
 void note_launches(uint32_t k);
+
+// Programmatic dependent launch: a kernel launched by launch_pdl may be
+// scheduled while the kernel before it on the stream drains (that kernel's
+// blocks call pdl_trigger as they start); it calls pdl_wait before its first
+// memory access, which returns once the previous kernel has completed and
+// its writes are visible. Both are no-ops for a kernel launched without the
+// attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
 // A stream capture enqueues kernels without running them: the capture takes
 // its count back (forget_launches) and each graph launch notes it again.
 void forget_launches(uint64_t k);

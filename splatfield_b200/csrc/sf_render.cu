@@ -79,6 +79,7 @@ __global__ __launch_bounds__(256, 3) void project_kernel(sf_view v_arg, const sf
                                                       const float* __restrict__ attr,
                                                       const float* __restrict__ shs, uint32_t n,
                                                       ProjOut o) {
+    pdl_trigger();  // the kernel after it may be scheduled in its last wave
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     // The view comes by value, or (for captured graphs re-run with new

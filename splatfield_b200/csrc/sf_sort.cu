@@ -326,6 +326,8 @@ __global__ __launch_bounds__(kThreads) void scan_kernel(
     const uint32_t* __restrict__ gids, const uint32_t* counts, uint32_t* out, const uint32_t* n_dev,
     uint32_t n_static, unsigned long long* lookback, uint32_t* ticket,
     unsigned long long* total_out, uint32_t* err) {
+    pdl_trigger();
+    pdl_wait();
     __shared__ uint32_t s_part;
     __shared__ unsigned long long s_warp[kWarps];
     __shared__ unsigned long long s_prefix;
