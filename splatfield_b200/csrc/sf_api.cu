@@ -374,7 +374,7 @@ int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32
     unsigned long long* total_dev = reinterpret_cast<unsigned long long*>(words + 4);
     SF_CK(cudaMemsetAsync(words, 0, 64, st));
     ProjOut po{s->depth_keys, s->tile_counts, s->bbox, s->geo0, s->geo1, s->color, words, s->ext};
-    SF_CK(launch_project(view, sp->attr, sp->sh, n, sp->K, po, st));
+    SF_CK(launch_project(view, sp->attr, sp->geom, sp->sh, n, sp->K, po, st));
     const uint32_t tiles = s->tiles_x * s->tiles_y;
     s->order = nullptr;
     s->tids = s->gids = nullptr;
@@ -550,7 +550,7 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
     if (e == cudaSuccess) e = cudaMemsetAsync(s->stats, 0, 32, st);
     ProjOut po{s->depth_keys, s->tile_counts, s->bbox, s->geo0, s->geo1, s->color, words, s->ext};
     sf_view dummy{};
-    if (e == cudaSuccess) e = launch_project(dummy, sp->attr, sp->sh, n, sp->K, po, st, g.view_dev);
+    if (e == cudaSuccess) e = launch_project(dummy, sp->attr, sp->geom, sp->sh, n, sp->K, po, st, g.view_dev);
     if (e == cudaSuccess) e = launch_bin_count(s->bbox, n, s->tiles_x, tiles, s->bin_chunks, s->bin_hist, st);
     if (e == cudaSuccess)
         e = launch_bin_colscan(s->bin_hist, s->bin_chunks, tiles, s->bin_cnt, s->bin_lists, words, st);
@@ -918,11 +918,15 @@ int sf_splats_create(sf_ctx ctx, const float* attributes, const float* sh, uint3
         s->K = sh_per_ch;
         cudaError_t e = dalloc(&s->attr, (size_t)11 * n);
         if (e == cudaSuccess) e = dalloc(&s->sh, (size_t)3 * sh_per_ch * n);
+        if (e == cudaSuccess) e = dalloc(&s->geom, (size_t)kGeomPlanes * n);
         if (e == cudaSuccess) e = cudaMemcpy(s->attr, attributes, (size_t)11 * n * 4, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(s->sh, sh, (size_t)3 * sh_per_ch * n * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = launch_splat_geom(s->attr, n, s->geom, nullptr);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
         if (e != cudaSuccess) {
             dfree(s->attr);
             dfree(s->sh);
+            dfree(s->geom);
             delete s;
             return fail(e == cudaErrorMemoryAllocation ? SF_ERR_NOMEM : SF_ERR_CUDA, cudaGetErrorString(e));
         }
@@ -943,6 +947,7 @@ int sf_splats_destroy(sf_splats s) {
     use_device(s->ctx->device);
     dfree(s->attr);
     dfree(s->sh);
+    dfree(s->geom);
     delete s;
     return SF_OK;
 }

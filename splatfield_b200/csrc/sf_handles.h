@@ -15,6 +15,7 @@ struct sf_splats_t {
     uint32_t n = 0, K = 1;
     float* attr = nullptr;
     float* sh = nullptr;
+    float* geom = nullptr;  // [kGeomPlanes][n] camera-independent projection terms of attr
     float bounds[6] = {0, 0, 0, 0, 0, 0};
 };
 

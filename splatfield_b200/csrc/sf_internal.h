@@ -67,8 +67,13 @@ inline uint32_t sh_degree_coeffs(uint32_t sh_per_ch) {
     return sh_per_ch >= 16 ? 16u : sh_per_ch >= 9 ? 9u : sh_per_ch >= 4 ? 4u : 1u;
 }
 
+// Per-splat camera-independent projection terms, [kGeomPlanes][n]: the
+// rows of M = R(q) diag(exp(log_scale)) (9), opacity, extent cutoff,
+// power_max. Computed once per splat set (launch_splat_geom).
+constexpr int kGeomPlanes = 12;
+cudaError_t launch_splat_geom(const float* attr, uint32_t n, float* geom, cudaStream_t stream);
 // view_dev (optional) supplies the view from device memory instead.
-cudaError_t launch_project(const sf_view& view, const float* attr, const float* sh, uint32_t n,
+cudaError_t launch_project(const sf_view& view, const float* attr, const float* geom, const float* sh, uint32_t n,
                            uint32_t sh_per_ch, const ProjOut& out, cudaStream_t stream,
                            const sf_view* view_dev = nullptr);
 

@@ -238,6 +238,7 @@ int sf_ply_load(sf_ctx ctx, const void* bytes, size_t len, sf_splats* out) {
         if (e == cudaSuccess) e = cudaMalloc(&rows, row_bytes);
         if (e == cudaSuccess) e = cudaMalloc(&s->attr, (size_t)11 * n * 4);
         if (e == cudaSuccess) e = cudaMalloc(&s->sh, (size_t)3 * h.lay.k * n * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&s->geom, (size_t)kGeomPlanes * n * 4);
         if (e == cudaSuccess) e = cudaMalloc(&bounds_u, 6 * 4);
         if (e == cudaSuccess)
             e = cudaMemcpy(rows, static_cast<const uint8_t*>(bytes) + h.data_off, row_bytes, cudaMemcpyHostToDevice);
@@ -248,6 +249,7 @@ int sf_ply_load(sf_ctx ctx, const void* bytes, size_t len, sf_splats* out) {
             note_launches(1);
             e = cudaGetLastError();
         }
+        if (e == cudaSuccess) e = launch_splat_geom(s->attr, n, s->geom, nullptr);
         uint32_t bu[6] = {0, 0, 0, 0, 0, 0};
         if (e == cudaSuccess) e = cudaMemcpy(bu, bounds_u, sizeof(bu), cudaMemcpyDeviceToHost);
         if (rows) cudaFree(rows);
@@ -255,6 +257,7 @@ int sf_ply_load(sf_ctx ctx, const void* bytes, size_t len, sf_splats* out) {
         if (e != cudaSuccess) {
             if (s->attr) cudaFree(s->attr);
             if (s->sh) cudaFree(s->sh);
+            if (s->geom) cudaFree(s->geom);
             delete s;
             return set_error(e == cudaErrorMemoryAllocation ? SF_ERR_NOMEM : SF_ERR_CUDA, cudaGetErrorString(e));
         }

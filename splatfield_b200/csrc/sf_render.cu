@@ -72,11 +72,43 @@ __device__ __forceinline__ void sh_to_rgb(V3 d, const float (&c)[3 * K], float& 
     }
 }
 
-// project_splats (src/project.rs:235-327), one thread per splat. Field-major
+// The camera-independent terms of project_splats (src/project.rs:235-327),
+// once per splat when the splats are created, in the f32 operations the
+// projection would spend on them every frame: M = R(q) diag(exp(log_scale))
+// (rows m0, m1, m2), opacity = sigmoid(logit), the extent cutoff
+// log(opacity / (10/255)) and power_max = log(255 opacity) + margin.
+// geom planes [kGeomPlanes][n]: m0.xyz, m1.xyz, m2.xyz, opacity, cutoff,
+// power_max.
+__global__ void splat_geom_kernel(const float* __restrict__ attr, uint32_t n, float* __restrict__ geom) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t N = n;
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = attr[(3 + k) * N + i];
+    const float qw = a[0], qx = a[1], qy = a[2], qz = a[3];
+    const V3 s{exp_(a[4]), exp_(a[5]), exp_(a[6])};
+    const float opacity = sigmoid_(a[7]);
+    const float x2 = qx * qx, y2 = qy * qy, z2 = qz * qz;
+    const float xy = qx * qy, xz = qx * qz, yz = qy * qz;
+    const float wx = qw * qx, wy = qw * qy, wz = qw * qz;
+    const V3 r0{1.0f - 2.0f * (y2 + z2), 2.0f * (xy - wz), 2.0f * (xz + wy)};
+    const V3 r1{2.0f * (xy + wz), 1.0f - 2.0f * (x2 + z2), 2.0f * (yz - wx)};
+    const V3 r2{2.0f * (xz - wy), 2.0f * (yz + wx), 1.0f - 2.0f * (x2 + y2)};
+    const float g[kGeomPlanes] = {r0.x * s.x, r0.y * s.y, r0.z * s.z, r1.x * s.x, r1.y * s.y, r1.z * s.z,
+                                  r2.x * s.x, r2.y * s.y, r2.z * s.z, opacity, log_(opacity / kAlphaCutoff),
+                                  log_(255.0f * opacity) + kPowerMargin};
+#pragma unroll
+    for (int k = 0; k < kGeomPlanes; ++k) geom[k * N + i] = g[k];
+}
+
+// project_splats (src/project.rs:235-327), one thread per splat, with the
+// camera-independent terms read from geom (splat_geom_kernel). Field-major
 // planes make every plane load a coalesced 128-byte warp access.
 template <int K>
 __global__ __launch_bounds__(256, 3) void project_kernel(sf_view v_arg, const sf_view* __restrict__ v_dev,
                                                       const float* __restrict__ attr,
+                                                      const float* __restrict__ geom,
                                                       const float* __restrict__ shs, uint32_t n,
                                                       ProjOut o) {
     pdl_trigger();  // the kernel after it may be scheduled in its last wave
@@ -88,16 +120,18 @@ __global__ __launch_bounds__(256, 3) void project_kernel(sf_view v_arg, const sf
     const size_t N = n;
     // Every load is issued before any use (all planes in flight at once);
     // culled splats (a few percent) read their colour planes for nothing.
-    float a[11];
+    float a[3], gm[kGeomPlanes];
 #pragma unroll
-    for (int k = 0; k < 11; ++k) a[k] = __ldg(attr + k * N + i);
+    for (int k = 0; k < 3; ++k) a[k] = __ldg(attr + k * N + i);
+#pragma unroll
+    for (int k = 0; k < kGeomPlanes; ++k) gm[k] = __ldg(geom + k * N + i);
     float c[3 * K];
     const bool want_color = o.color != nullptr;
     if (want_color) {
 #pragma unroll
         for (int k = 0; k < 3 * K; ++k) c[k] = __ldg(shs + k * N + i);
     }
-    const float opacity = sigmoid_(a[10]);
+    const float opacity = gm[9];
     const V3 mean{a[0], a[1], a[2]};
     const V3 rot0{v.rot0[0], v.rot0[1], v.rot0[2]};
     const V3 rot1{v.rot1[0], v.rot1[1], v.rot1[2]};
@@ -111,19 +145,10 @@ __global__ __launch_bounds__(256, 3) void project_kernel(sf_view v_arg, const sf
     }
     const float cam_x = dot3(rot0, mean) + v.trans[0];
     const float cam_y = dot3(rot1, mean) + v.trans[1];
-    const float qw = a[3], qx = a[4], qy = a[5], qz = a[6];
-    const V3 s{exp_(a[7]), exp_(a[8]), exp_(a[9])};
     const float inv_z = 1.0f / cam_z;
-
-    const float x2 = qx * qx, y2 = qy * qy, z2 = qz * qz;
-    const float xy = qx * qy, xz = qx * qz, yz = qy * qz;
-    const float wx = qw * qx, wy = qw * qy, wz = qw * qz;
-    const V3 r0{1.0f - 2.0f * (y2 + z2), 2.0f * (xy - wz), 2.0f * (xz + wy)};
-    const V3 r1{2.0f * (xy + wz), 1.0f - 2.0f * (x2 + z2), 2.0f * (yz - wx)};
-    const V3 r2{2.0f * (xz - wy), 2.0f * (yz + wx), 1.0f - 2.0f * (x2 + y2)};
-    const V3 m0{r0.x * s.x, r0.y * s.y, r0.z * s.z};
-    const V3 m1{r1.x * s.x, r1.y * s.y, r1.z * s.z};
-    const V3 m2{r2.x * s.x, r2.y * s.y, r2.z * s.z};
+    const V3 m0{gm[0], gm[1], gm[2]};
+    const V3 m1{gm[3], gm[4], gm[5]};
+    const V3 m2{gm[6], gm[7], gm[8]};
     const float lim_x = (1.3f * v.img[0]) / (2.0f * v.focal[0]);
     const float lim_y = (1.3f * v.img[1]) / (2.0f * v.focal[1]);
     const float u = clamp_(cam_x * inv_z, -lim_x, lim_x);
@@ -158,7 +183,7 @@ __global__ __launch_bounds__(256, 3) void project_kernel(sf_view v_arg, const sf
         sh_to_rgb<K>(dir, c, r, g, b);
         o.color[i] = make_float4(r + 0.5f, g + 0.5f, b + 0.5f, 0.0f);
     }
-    const float cutoff = log_(opacity / kAlphaCutoff);
+    const float cutoff = gm[10];
     const float ext_x = sqrtf((2.0f * cutoff) * ca);
     const float ext_y = sqrtf((2.0f * cutoff) * cc);
     const float inv_tile = 1.0f / 16.0f;
@@ -166,7 +191,7 @@ __global__ __launch_bounds__(256, 3) void project_kernel(sf_view v_arg, const sf
     const uint32_t min_y = sat_u32(clamp_((my - ext_y) * inv_tile, 0.0f, v.tile_bounds[1]));
     const uint32_t max_x = sat_u32(clamp_((mx + ext_x) * inv_tile + 1.0f, 0.0f, v.tile_bounds[0]));
     const uint32_t max_y = sat_u32(clamp_((my + ext_y) * inv_tile + 1.0f, 0.0f, v.tile_bounds[1]));
-    const float power_max = log_(255.0f * opacity) + kPowerMargin;
+    const float power_max = gm[11];
 
     o.depth_keys[i] = f2u(cam_z);
     o.tile_counts[i] = (max_x - min_x) * (max_y - min_y);
@@ -729,7 +754,14 @@ __global__ void export_rows_kernel(const float4* __restrict__ geo0, const float4
 
 }  // namespace
 
-cudaError_t launch_project(const sf_view& view, const float* attr, const float* sh, uint32_t n,
+cudaError_t launch_splat_geom(const float* attr, uint32_t n, float* geom, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    splat_geom_kernel<<<(n + 255) / 256, 256, 0, stream>>>(attr, n, geom);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_project(const sf_view& view, const float* attr, const float* geom, const float* sh, uint32_t n,
                            uint32_t sh_per_ch, const ProjOut& out, cudaStream_t stream,
                            const sf_view* view_dev) {
     if (n == 0) return cudaSuccess;
@@ -738,10 +770,10 @@ cudaError_t launch_project(const sf_view& view, const float* attr, const float* 
     // fewest registers (more warps in flight for the attribute loads).
     sh_per_ch = out.color ? sh_degree_coeffs(sh_per_ch) : 1u;
     switch (sh_per_ch) {
-        case 1: project_kernel<1><<<grid, 256, 0, stream>>>(view, view_dev, attr, sh, n, out); break;
-        case 4: project_kernel<4><<<grid, 256, 0, stream>>>(view, view_dev, attr, sh, n, out); break;
-        case 9: project_kernel<9><<<grid, 256, 0, stream>>>(view, view_dev, attr, sh, n, out); break;
-        case 16: project_kernel<16><<<grid, 256, 0, stream>>>(view, view_dev, attr, sh, n, out); break;
+        case 1: project_kernel<1><<<grid, 256, 0, stream>>>(view, view_dev, attr, geom, sh, n, out); break;
+        case 4: project_kernel<4><<<grid, 256, 0, stream>>>(view, view_dev, attr, geom, sh, n, out); break;
+        case 9: project_kernel<9><<<grid, 256, 0, stream>>>(view, view_dev, attr, geom, sh, n, out); break;
+        case 16: project_kernel<16><<<grid, 256, 0, stream>>>(view, view_dev, attr, geom, sh, n, out); break;
         default: return cudaErrorInvalidValue;
     }
     note_launches(1);

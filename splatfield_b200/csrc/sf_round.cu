@@ -277,7 +277,7 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
     if ((e = cudaMemsetAsync(words, 0, 64, st)) != cudaSuccess) return e;
     ProjOut po{L.keys, L.counts, L.bbox, L.geo0, L.geo1, nullptr, words, r->tuning.raster_cull ? L.ext : nullptr};
     sf_view dummy{};
-    if ((e = launch_project(dummy, sp.attr, sp.sh, n, sp.K, po, st, r->views_dev + v)) != cudaSuccess) return e;
+    if ((e = launch_project(dummy, sp.attr, sp.geom, sp.sh, n, sp.K, po, st, r->views_dev + v)) != cudaSuccess) return e;
     const uint32_t *tids = nullptr, *gids = nullptr;
     const uint2* lazy_pairs = nullptr;
     if (r->tuning.isect_build == SF_ISECTS_BINNED && L.hist) {
