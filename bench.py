@@ -61,6 +61,7 @@ FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 lanes x FMA x
 # re-reads; here it is the walked entries' records and ids.
 RASTER_TRAFFIC_BYTES = 48.99e6
 RASTER_FLOPS_PER_PAIR = 24
+RESERVE_ISECTS = 1 << 24
 
 
 def measured_peaks():
@@ -340,6 +341,9 @@ def run_ours(args, rank, world):
     attr, sh = make_scene()
     splats = sf.Splats(attr, sh, ctx)
     scratch = sf.RenderScratch(N_SPLATS, (WIDTH, HEIGHT), ctx)
+    # Intersection capacity sized up front (the orbit's frames need up to
+    # about 8.4M), so no reallocation falls inside a timed region.
+    scratch.reserve(RESERVE_ISECTS)
     cams = orbit(sf.look_at)
     my_cams = replicas.replica_share(cams, rank, world)
     stream = torch.cuda.current_stream()

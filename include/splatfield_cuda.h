@@ -141,6 +141,10 @@ int sf_scratch_create(sf_ctx ctx, uint32_t total, uint32_t w, uint32_t h, sf_scr
 int sf_scratch_destroy(sf_scratch s);
 /* Current intersection capacity (entries). */
 int sf_scratch_capacity(sf_scratch s, uint64_t* capacity);
+/* Grows the intersection capacity ahead of time to at least `isects`
+ * entries (the next power of two), so frames up to that size never
+ * reallocate; the capacity never shrinks. */
+int sf_scratch_reserve(sf_scratch s, uint64_t isects);
 
 /* Kernel forms a scratch launches; all forms give identical results (the
  * autotuner picks by measured time). */

@@ -116,6 +116,7 @@ SIGNATURES = {
         "sf_render_to_host": (i32, [P, P, P, u32, u32, P, P]),
         "sf_render_frames_to_host": (i32, [P, P, P, u32, u32, u32, P, P]),
         "sf_render_frames": (i32, [P, P, P, u32, u32, u32, P]),
+        "sf_scratch_reserve": (i32, [P, C.c_uint64]),
         "sf_render_forward": (i32, [P, P, P, u32, u32, P, PP]),
         "sf_render_backward": (i32, [P, P, P, u32, u32, P, P, P, P, P]),
         "sf_prepare_isects": (i32, [P, P, P, u32, u32, P, P]),

@@ -508,6 +508,10 @@ class RenderScratch:
         check(lib().sf_scratch_capacity(self.handle, C.byref(c)))
         return int(c.value)
 
+    def reserve(self, isects: int) -> None:
+        """Grow the intersection capacity to at least ``isects`` up front."""
+        check(lib().sf_scratch_reserve(self.handle, int(isects)))
+
     def set_tuning(self, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED, raster_detail: int = 0,
                    raster_order: int = L.ORDER_SORTED, raster_schedule: int = L.SCHEDULE_LONGEST) -> None:
         """Kernel forms (results are identical across forms): raster_cull 0/1,

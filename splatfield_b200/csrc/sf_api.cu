@@ -1033,6 +1033,16 @@ int sf_scratch_capacity(sf_scratch s, uint64_t* capacity) {
     return SF_OK;
 }
 
+int sf_scratch_reserve(sf_scratch s, uint64_t isects) {
+    SF_TRY({
+        if (!s) return fail(SF_ERR_ARG, "null scratch");
+        if (isects > kMaxIsects) return fail(SF_ERR_CAPACITY, "intersection count exceeds 2^30-1");
+        SF_CK(use_device(s->ctx->device));
+        SF_CK(grow_isects(s, isects));
+        return SF_OK;
+    })
+}
+
 int sf_prepare_isects(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
                       sf_stream stream, sf_isects* out) {
     SF_TRY({ return prepare(s, scratch, cam, w, h, S(stream), out); })

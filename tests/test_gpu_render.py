@@ -197,6 +197,25 @@ def test_scratch_stops_allocating_after_first_frame(ctx):
         assert scratch.capacity() == cap
 
 
+def test_scratch_reserve_grows_once_and_keeps_frames_exact(ctx, oracle_mod):
+    """sf_scratch_reserve sizes the capacity up front (next power of two, never
+    shrinking); frames under it neither grow it nor change."""
+    attr = sine_attributes(300, 0.07, 0.4)
+    splats = sf.Splats(attr, zero_sh(300))
+    cam = sf.make_camera(position=(0.0, -1.2, 0.0))
+    scratch = sf.RenderScratch(300, (96, 64))
+    scratch.reserve(3_000_000)
+    assert scratch.capacity() == 1 << 22
+    scratch.reserve(1000)
+    assert scratch.capacity() == 1 << 22
+    img = splats.render_with(scratch, cam, (96, 64)).read()
+    assert scratch.capacity() == 1 << 22
+    cam_o = oracle_mod.camera(position=(0.0, -1.2, 0.0))
+    np.testing.assert_array_equal(img, oracle_mod.render(cam_o, 96, 64, attr, zero_sh(300), 1)["bitmap"])
+    with pytest.raises(sf.SplatfieldError):
+        scratch.reserve(1 << 31)
+
+
 def test_capacity_grows_instead_of_truncating(ctx, oracle_mod):
     """The reference truncates past capacity and grows next frame
     (src/raster.rs:38-46, src/render.rs:171-197); here the first frame is
