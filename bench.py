@@ -324,6 +324,38 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_round_only(args):
+    """Profiling mode: the eig_round workload's batched round alone, with the
+    tuning the autotuner picks for it fixed, timed on the host clock."""
+    import torch
+
+    import splatfield_b200 as sf
+    from splatfield_b200 import synth
+
+    torch.cuda.set_device(0)
+    ctx = sf.Context(0)
+    attr, sh = make_scene()
+    splats = sf.Splats(attr, sh, ctx)
+    size = (ROUND_SIDE, ROUND_SIDE)
+    a, b = synth.beta_posterior(N_SPLATS, seed=1)
+    beta = sf.BetaState.from_host(a, b, ctx)
+    cams = synth.sphere_cameras(ROUND_VIEWS, ROUND_RADIUS, 2, sf.look_at)
+    rnd = sf.Round(N_SPLATS, [size] * ROUND_VIEWS, ctx)
+    rnd.set_tuning(lanes=8, raster_cull=1, raster_order=sf.ORDER_HYBRID)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        rnd.eig(splats, beta, cams, sf.EIG_LUT_F32, stream=stream)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        rnd.eig(splats, beta, cams, sf.EIG_LUT_F32, stream=stream)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * float(np.median(times))
+    print(json.dumps({"round_only": args.steps, "ms_per_round": ms, "views_per_s": ROUND_VIEWS / (ms / 1e3)}))
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -492,6 +524,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames-only", action="store_true",
                     help="render warmup + steps frames and exit (for profilers)")
+    ap.add_argument("--round-only", action="store_true",
+                    help="run warmup + steps batched segmentation rounds (8 lanes, culling, hybrid order) "
+                         "and exit (for profilers)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -506,6 +541,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.round_only:
+            run_round_only(args)
         else:
             run_ours(args, rank, world)
     finally:

@@ -686,11 +686,12 @@ constexpr size_t sort_smem() {
 // Size classes (longest list): a warp per tile up to 64 entries, then the
 // shared-memory bucket sorts (entries, buckets, threads); longer lists take
 // the global form.
-constexpr uint32_t kClassWarp = 64, kClassS = 512, kClass0 = 2048, kClass1 = 6144, kClass2 = kBinSharedMax;
-constexpr uint32_t kBinsS = 2304, kBins0 = 4096, kBins1 = 8192, kBins2 = 16384, kBinsGiant = 32768;
-constexpr uint32_t kThreadsS = 256, kThreads0 = 256, kThreads1 = 512, kThreads2 = 1024;
+constexpr uint32_t kClassWarp = 64, kClassS = 512, kClass0 = 2048, kClassM = 4096, kClass1 = 6144,
+                   kClass2 = kBinSharedMax;
+constexpr uint32_t kBinsS = 2304, kBins0 = 4096, kBinsM = 8192, kBins1 = 8192, kBins2 = 16384, kBinsGiant = 32768;
+constexpr uint32_t kThreadsS = 256, kThreads0 = 256, kThreadsM = 512, kThreads1 = 512, kThreads2 = 1024;
 static_assert(sort_smem<kClass2, kBins2, kThreads2>() <= 227 * 1024, "per-tile sort exceeds shared memory");
-static_assert(kSortClasses == 6, "class table");
+static_assert(kSortClasses == 7, "class table");
 
 // grid: the class's tile count when the host knows it, else an upper bound;
 // capped at the CTAs resident at once (the kernels loop over their tiles).
@@ -727,7 +728,7 @@ uint32_t bin_chunks(uint32_t n, int sm_count) {
 uint32_t bin_chunk_size(uint32_t n, uint32_t chunks) { return ((n + chunks - 1) / chunks + 31) / 32 * 32; }
 
 uint32_t bin_class_limit(int k) {
-    const uint32_t lim[kSortClasses - 1] = {kClassWarp, kClassS, kClass0, kClass1, kClass2};
+    const uint32_t lim[kSortClasses - 1] = {kClassWarp, kClassS, kClass0, kClassM, kClass1, kClass2};
     return k >= 0 && k < kSortClasses - 1 ? lim[k] : 0xffffffffu;
 }
 
@@ -744,7 +745,7 @@ cudaError_t launch_bin_count(const uint2* bbox, uint32_t n, uint32_t tiles_x, ui
 
 cudaError_t launch_bin_colscan(uint32_t* hist, uint32_t chunks, uint32_t tiles, uint32_t* cnt, uint32_t* lists,
                                uint32_t* words, cudaStream_t st) {
-    const ClassLimits lim{{kClassWarp, kClassS, kClass0, kClass1, kClass2}};
+    const ClassLimits lim{{kClassWarp, kClassS, kClass0, kClassM, kClass1, kClass2}};
     const cudaError_t e =
         launch_pdl(bin_colscan_kernel, (tiles + 31) / 32, dim3(32, 32), 0, st, hist, chunks, tiles, cnt, lists, words, lim);
     note_launches(1);
@@ -796,11 +797,11 @@ cudaError_t launch_clamp_starts(uint32_t* tile_start, uint32_t count, uint32_t c
 }
 
 cudaError_t sort_streams_create(SortStreams* ss) {
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 4; ++k) {
         cudaError_t e = cudaStreamCreateWithFlags(&ss->s[k], cudaStreamNonBlocking);
         if (e != cudaSuccess) return e;
     }
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 5; ++k) {
         cudaError_t e = cudaEventCreateWithFlags(&ss->e[k], cudaEventDisableTiming);
         if (e != cudaSuccess) return e;
     }
@@ -808,11 +809,11 @@ cudaError_t sort_streams_create(SortStreams* ss) {
 }
 
 void sort_streams_destroy(SortStreams* ss) {
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 4; ++k) {
         if (ss->s[k]) cudaStreamDestroy(ss->s[k]);
         ss->s[k] = nullptr;
     }
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 5; ++k) {
         if (ss->e[k]) cudaEventDestroy(ss->e[k]);
         ss->e[k] = nullptr;
     }
@@ -825,27 +826,32 @@ cudaError_t launch_tile_sorts(const uint32_t grids[kSortClasses], const uint32_t
     cudaError_t e;
     // Each form reads and overwrites only its own tiles' ranges, so the
     // classes may run concurrently.
-    cudaStream_t s1 = st, s2 = st, s3 = st;
+    cudaStream_t s1 = st, s2 = st, s3 = st, s4 = st;
     if (side && side->s[0]) {
         if ((e = cudaEventRecord(side->e[0], st)) != cudaSuccess) return e;
-        for (int k = 0; k < 3; ++k)
+        for (int k = 0; k < 4; ++k)
             if ((e = cudaStreamWaitEvent(side->s[k], side->e[0], 0)) != cudaSuccess) return e;
         s1 = side->s[0];
         s2 = side->s[1];
         s3 = side->s[2];
+        s4 = side->s[3];
     }
     auto L = [&](int k) { return lists + (size_t)k * tiles; };
     auto N = [&](int k) { return words + 8 + k; };
-    e = launch_sort_kernel(tile_sort_global_kernel<kBinsGiant, 512>, 512, (kBinsGiant + 64) * 4, grids[5],
-                           sm_count, L(5), N(5), tile_start, capacity, pairs, ids, tids_out, keys_tmp, s3);
+    e = launch_sort_kernel(tile_sort_global_kernel<kBinsGiant, 512>, 512, (kBinsGiant + 64) * 4, grids[6],
+                           sm_count, L(6), N(6), tile_start, capacity, pairs, ids, tids_out, keys_tmp, s3);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClass1, kBins1, kThreads1>, kThreads1,
-                           sort_smem<kClass1, kBins1, kThreads1>(), grids[3], sm_count, L(3), N(3),
-                           tile_start, capacity, pairs, ids, tids_out, keys_tmp, s1);
+                           sort_smem<kClass1, kBins1, kThreads1>(), grids[4], sm_count, L(4), N(4), tile_start,
+                           capacity, pairs, ids, tids_out, keys_tmp, s1);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClass2, kBins2, kThreads2>, kThreads2,
-                           sort_smem<kClass2, kBins2, kThreads2>(), grids[4], sm_count, L(4), N(4),
-                           tile_start, capacity, pairs, ids, tids_out, keys_tmp, s2);
+                           sort_smem<kClass2, kBins2, kThreads2>(), grids[5], sm_count, L(5), N(5), tile_start,
+                           capacity, pairs, ids, tids_out, keys_tmp, s2);
+    if (e != cudaSuccess) return e;
+    e = launch_sort_kernel(tile_sort_kernel<kClassM, kBinsM, kThreadsM>, kThreadsM,
+                           sort_smem<kClassM, kBinsM, kThreadsM>(), grids[3], sm_count, L(3), N(3), tile_start,
+                           capacity, pairs, ids, tids_out, keys_tmp, s4);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_warp_kernel, 256, 0, (grids[0] + 7) / 8, sm_count, L(0), N(0), tile_start,
                            capacity, pairs, ids, tids_out, keys_tmp, s2);
@@ -859,7 +865,7 @@ cudaError_t launch_tile_sorts(const uint32_t grids[kSortClasses], const uint32_t
                            capacity, pairs, ids, tids_out, keys_tmp, st);
     if (e != cudaSuccess) return e;
     if (side && side->s[0]) {
-        for (int k = 0; k < 3; ++k) {
+        for (int k = 0; k < 4; ++k) {
             if ((e = cudaEventRecord(side->e[1 + k], side->s[k])) != cudaSuccess) return e;
             if ((e = cudaStreamWaitEvent(st, side->e[1 + k], 0)) != cudaSuccess) return e;
         }

@@ -173,7 +173,7 @@ constexpr uint32_t kBinMaxTiles = 49152;
 uint32_t bin_chunks(uint32_t n, int sm_count);
 // Per-tile sort size classes: k = 0 .. kSortClasses - 2 hold lists of up to
 // bin_class_limit(k) entries; the last class holds the longer lists.
-constexpr int kSortClasses = 6;
+constexpr int kSortClasses = 7;
 uint32_t bin_class_limit(int k);
 // Longest list the shared-memory classes sort; longer lists go to the global
 // form (or, with the hybrid order, to the rasterizer).
@@ -206,8 +206,8 @@ cudaError_t launch_clamp_starts(uint32_t* tile_start, uint32_t count, uint32_t c
 // in turn on one stream (outside a graph the extra event calls cost more
 // host time than the overlap gains).
 struct SortStreams {
-    cudaStream_t s[3] = {nullptr, nullptr, nullptr};
-    cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t s[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t e[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 cudaError_t sort_streams_create(SortStreams* ss);
 void sort_streams_destroy(SortStreams* ss);

@@ -102,21 +102,14 @@ __global__ void splat_geom_kernel(const float* __restrict__ attr, uint32_t n, fl
     for (int k = 0; k < kGeomPlanes; ++k) geom[k * N + i] = g[k];
 }
 
-// project_splats (src/project.rs:235-327), one thread per splat, with the
+// project_splats (src/project.rs:235-327) for splat i, with the
 // camera-independent terms read from geom (splat_geom_kernel). Field-major
-// planes make every plane load a coalesced 128-byte warp access.
+// planes make every plane load a coalesced 128-byte warp access. Returns
+// whether the splat is visible (not culled).
 template <int K>
-__global__ __launch_bounds__(256, 3) void project_kernel(sf_view v_arg, const sf_view* __restrict__ v_dev,
-                                                      const float* __restrict__ attr,
-                                                      const float* __restrict__ geom,
-                                                      const float* __restrict__ shs, uint32_t n,
-                                                      ProjOut o) {
-    pdl_trigger();  // the kernel after it may be scheduled in its last wave
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    // The view comes by value, or (for captured graphs re-run with new
-    // cameras) from device memory.
-    const sf_view v = v_dev ? *v_dev : v_arg;
+__device__ __forceinline__ bool project_one(const sf_view& v, const float* __restrict__ attr,
+                                            const float* __restrict__ geom, const float* __restrict__ shs,
+                                            uint32_t n, const ProjOut& o, uint32_t i) {
     const size_t N = n;
     // Every load is issued before any use (all planes in flight at once);
     // culled splats (a few percent) read their colour planes for nothing.
@@ -141,7 +134,7 @@ __global__ __launch_bounds__(256, 3) void project_kernel(sf_view v_arg, const sf
         o.depth_keys[i] = 0xffffffffu;
         o.tile_counts[i] = 0u;
         o.bbox[i] = make_uint2(0u, 0u);
-        return;
+        return false;
     }
     const float cam_x = dot3(rot0, mean) + v.trans[0];
     const float cam_y = dot3(rot1, mean) + v.trans[1];
@@ -214,8 +207,34 @@ __global__ __launch_bounds__(256, 3) void project_kernel(sf_view v_arg, const sf
         }
         o.ext[i] = make_float2(ex, ey);
     }
-    if (o.visible) {
-        // Warp-aggregated visible count.
+    return true;
+}
+
+// One thread per splat. The visible count goes to one counter: the
+// colour-free form (K = 1, a short kernel) sums it per block, since one
+// atomic per warp on a single address serialises in L2 and bounded that
+// kernel; the colour forms add it per warp (a block-wide count costs them
+// registers).
+template <int K>
+__global__ __launch_bounds__(256, 3) void project_kernel(sf_view v_arg, const sf_view* __restrict__ v_dev,
+                                                      const float* __restrict__ attr,
+                                                      const float* __restrict__ geom,
+                                                      const float* __restrict__ shs, uint32_t n,
+                                                      ProjOut o) {
+    pdl_trigger();  // the kernel after it may be scheduled in its last wave
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    // The view comes by value, or (for captured graphs re-run with new
+    // cameras) from device memory.
+    if (K == 1 && o.visible) {
+        bool vis = false;
+        if (i < n) vis = project_one<K>(v_dev ? *v_dev : v_arg, attr, geom, shs, n, o, i);
+        const int c = __syncthreads_count(vis);
+        if (threadIdx.x == 0 && c) atomicAdd(o.visible, (uint32_t)c);
+        return;
+    }
+    if (i >= n) return;
+    const sf_view v = v_dev ? *v_dev : v_arg;
+    if (project_one<K>(v, attr, geom, shs, n, o, i) && o.visible) {
         const uint32_t active = __activemask();
         if ((threadIdx.x & 31u) == (uint32_t)(__ffs(active) - 1)) atomicAdd(o.visible, __popc(active));
     }

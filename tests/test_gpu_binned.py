@@ -46,14 +46,14 @@ def check(got, want, img, want_img):
 
 def test_binned_covers_every_sort_class(ctx, oracle_mod):
     """A dense cluster: tile lists from a handful to ~9k entries, so the
-    warp sort (up to 64 entries) and the 512-, 2048-, 6144- and 12288-entry
-    sorts all run."""
+    warp sort (up to 64 entries) and the 512-, 2048-, 4096-, 6144- and
+    12288-entry sorts all run."""
     n, w, h = 40000, 256, 256
     attr, sh = synth.scene_clustered(n, 4, seed=31, clusters=1, sigma=0.25, extent=1.0)
     got, want, img, want_img = build_both(oracle_mod, attr, sh, 4, w, h)
     lens = np.diff(got["tile_start"])
     assert lens.max() > 6144 and lens.max() <= 12288, lens.max()
-    for lo, hi in [(0, 64), (64, 512), (512, 2048), (2048, 6144)]:
+    for lo, hi in [(0, 64), (64, 512), (512, 2048), (2048, 4096), (4096, 6144)]:
         assert ((lens > lo) & (lens <= hi)).any(), (lo, hi)
     check(got, want, img, want_img)
 
