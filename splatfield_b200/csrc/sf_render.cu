@@ -427,12 +427,15 @@ __device__ bool composite_list(const RasterArgs& a, const RasterSmem& sm, IdOf i
         auto step = [&](uint32_t j) {
             if (DETAIL) ++ps.n_proc;
             uint32_t q = 0;
-            if (!ps.done) {
+            // CULL: a warp whose pixels are all done has left the chunk, so
+            // the power is formed unconditionally and one branch tests both.
+            // Otherwise a done warp skips the loads and arithmetic.
+            if (CULL || !ps.done) {
                 const float4 g0 = sm.g0[j];
                 const float4 g1 = sm.g1[j];
                 const float dx = g0.x - fx, dy = g0.y - fy;
                 const float power = fma_(g0.z * dx, dx, fma_(g1.x * dy, dy, (g0.w * dx) * dy));
-                if (!(power > g1.z)) {
+                if ((!CULL || !ps.done) && !(power > g1.z)) {
                     if (DETAIL) ++ps.n_eval;
                     const float alpha = fminf(g1.y * exp_neg_(-power), 0.999f);
                     if (alpha >= inv255) {
