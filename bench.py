@@ -212,10 +212,11 @@ def time_eig_round(sf, splats, ctx, stream, args):
             total) then sf_beta_eig (one sync for the sum);
     batched sf_round_eig: all views in one CUDA graph, one sync per round
             (lanes and raster form chosen by sf_round_autotune, untimed).
-    The evidence form renders each view's fg / bg words under a 1-3 ellipse
-    mask (prepare + masked sf_accumulate_prepared per view vs
+    The evidence + EIG form (the C2 round) lifts each view's fg / bg words
+    under a 1-3 ellipse mask and reduces its EIG over fg + bg (prepare +
+    masked sf_accumulate_prepared + sf_beta_eig per view vs
     sf_round_evidence); the words stay on the device in both arms and are
-    compared once after timing.
+    compared once after timing, the EIGs every round.
     Rounds are timed on the host clock around a synchronised round (the plain
     path's host syncs are part of its cost); results must agree exactly."""
     import torch
@@ -240,7 +241,8 @@ def time_eig_round(sf, splats, ctx, stream, args):
                 isects = splats.prepare_isects(scratch, cams[v], size, stream=stream)
                 splats.accumulate_prepared(scratch, isects, size, acc, masks[v], stream=stream)
                 if keep is not None:
-                    keep.append(acc.fg.read(stream))
+                    keep.append((acc.fg.read(stream), acc.bg.read(stream)))
+                out.append(beta.eig(acc, mode, stream=stream))
             else:
                 splats.render_responsibility(scratch, acc, cams[v], size, stream=stream)
                 out.append(beta.eig(acc, mode, stream=stream))
@@ -248,8 +250,7 @@ def time_eig_round(sf, splats, ctx, stream, args):
 
     def batched_round(mode, evidence):
         if evidence:
-            rnd.evidence(splats, None, cams, masks, mode, stream=stream)
-            return None
+            return rnd.evidence(splats, beta, cams, masks, mode, stream=stream)
         return rnd.eig(splats, beta, cams, mode, stream=stream)
 
     def timed(fn, *a):
@@ -269,22 +270,125 @@ def time_eig_round(sf, splats, ctx, stream, args):
               "tuning": tuning, "reps": reps}
     for name, mode, evidence in (("responsibility_lut_f32", sf.EIG_LUT_F32, False),
                                  ("responsibility_fp64", sf.EIG_FP64, False),
-                                 ("evidence", sf.EIG_LUT_F32, True)):
+                                 ("evidence_eig_lut_f32", sf.EIG_LUT_F32, True)):
         tp, ep = timed(plain_round, mode, evidence)
         tb, eb = timed(batched_round, mode, evidence)
+        entry = {"plain_views_per_s": ROUND_VIEWS / tp, "batched_views_per_s": ROUND_VIEWS / tb,
+                 "plain_ms_per_round": 1e3 * tp, "batched_ms_per_round": 1e3 * tb, "speedup": tp / tb,
+                 "eig_identical": bool(np.array_equal(ep, eb))}
         if evidence:
-            # Checked once, outside the timed rounds: every view's fg words.
+            # Checked once, outside the timed rounds: every view's fg and bg
+            # words (the masked evidence lift of the C2 round).
             kept = []
             plain_round(mode, True, kept)
-            rnd.evidence(splats, None, cams, masks, mode, stream=stream)
-            same = all(np.array_equal(kept[v], rnd.evidence_words(v)[0].read(stream)) for v in range(ROUND_VIEWS))
-        else:
-            same = bool(np.array_equal(ep, eb))
-        result[name] = {
-            "plain_views_per_s": ROUND_VIEWS / tp, "batched_views_per_s": ROUND_VIEWS / tb,
-            "plain_ms_per_round": 1e3 * tp, "batched_ms_per_round": 1e3 * tb, "speedup": tp / tb,
-            ("words_identical" if evidence else "eig_identical"): bool(same)}
+            rnd.evidence(splats, beta, cams, masks, mode, stream=stream)
+            entry["words_identical"] = all(
+                np.array_equal(kept[v][0], rnd.evidence_words(v)[0].read(stream))
+                and np.array_equal(kept[v][1], rnd.evidence_words(v)[1].read(stream)) for v in range(ROUND_VIEWS))
+        result[name] = entry
     return result
+
+
+UNEVEN_SPLATS, UNEVEN_SH, UNEVEN_VIEWS, UNEVEN_SIDES = 3_000_000, 4, 64, (256, 384, 512, 768, 1024)
+
+
+def time_uneven_round(sf, ctx, stream, args):
+    """The uneven batched lift (C4): 3M splats with SH degree 1 (clustered as
+    the frame scene), 64 views whose sides are drawn from 256..1024, each
+    with a 1-3 ellipse mask; per view the masked evidence lift and its FP64
+    EIG (over fg + bg), as one batched graph (sf_round_evidence) against the
+    plain per-view calls (one scratch per side, so the plain arm never
+    reallocates). Responsibilities are the u32 lift; the adjoint's per-splat
+    feature gradient is checked against it in the tests."""
+    import torch
+
+    from splatfield_b200 import synth
+
+    attr, sh = synth.scene_clustered(UNEVEN_SPLATS, UNEVEN_SH, seed=7)
+    splats = sf.Splats(attr, sh, ctx)
+    del attr, sh
+    rng = np.random.default_rng(11)
+    sides = [int(x) for x in rng.choice(UNEVEN_SIDES, UNEVEN_VIEWS)]
+    cams = synth.sphere_cameras(UNEVEN_VIEWS, ROUND_RADIUS, 9, sf.look_at)
+    masks = [sf.Mask.from_bytes((s, s), synth.ellipse_mask(s, s, seed=300 + v), ctx) for v, s in enumerate(sides)]
+    a, b = synth.beta_posterior(UNEVEN_SPLATS, seed=5)
+    beta = sf.BetaState.from_host(a, b, ctx)
+    acc = sf.Accumulators(UNEVEN_SPLATS, ctx)
+    scratches = {s: sf.RenderScratch(UNEVEN_SPLATS, (s, s), ctx) for s in UNEVEN_SIDES}
+    rnd = sf.Round(UNEVEN_SPLATS, [(s, s) for s in sides], ctx)
+    rnd.set_tuning(lanes=8, raster_cull=1, raster_order=sf.ORDER_HYBRID)
+    reps = 3
+
+    def plain():
+        out = []
+        for v, s in enumerate(sides):
+            isects = splats.prepare_isects(scratches[s], cams[v], (s, s), stream=stream)
+            splats.accumulate_prepared(scratches[s], isects, (s, s), acc, masks[v], stream=stream)
+            out.append(beta.eig(acc, sf.EIG_FP64, stream=stream))
+        return np.array(out)
+
+    def batched():
+        return rnd.evidence(splats, beta, cams, masks, sf.EIG_FP64, stream=stream)
+
+    def timed(fn):
+        fn()
+        times, out = [], None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        return float(np.median(times)), out
+
+    tp, ep = timed(plain)
+    tb, eb = timed(batched)
+    sizes = {str(s): sides.count(s) for s in UNEVEN_SIDES}
+    return {"workload": f"uneven round: {UNEVEN_SPLATS // 1_000_000}M splats SH1 (8 Gaussian clusters), "
+                        f"{UNEVEN_VIEWS} views with sides in {list(UNEVEN_SIDES)}, ellipse masks, "
+                        "evidence lift + FP64 EIG per view",
+            "views_per_side": sizes, "reps": reps,
+            "plain_views_per_s": UNEVEN_VIEWS / tp, "batched_views_per_s": UNEVEN_VIEWS / tb,
+            "plain_ms_per_round": 1e3 * tp, "batched_ms_per_round": 1e3 * tb, "speedup": tp / tb,
+            "eig_identical": bool(np.array_equal(ep, eb))}
+
+
+def cpu_other_configs(attr, sh, budget_s=25.0):
+    """The CPU oracle on the other configs' plain paths, on the host's cores:
+    one C0 frame (100k SH0 splats uniform in [-1,1]^3, 512x512, fov 60 deg)
+    and the C2 round (per view: prepare, masked evidence lift, LUT EIG over
+    fg + bg), as many of its 20 views as fit the budget."""
+    import oracle as O
+
+    from splatfield_b200 import synth
+
+    a0, s0 = synth.scene_uniform(100_000, 1, 0)
+    cam0 = O.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    cam0.fov[0], cam0.fov[1] = synth.fov_for(512, 512)
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        O.rasterize(O.prepare(cam0, 512, 512, a0, s0, 1), 0, want_float=False)
+        times.append(time.perf_counter() - t0)
+    c0_ms = 1e3 * float(np.median(times))
+    size = (ROUND_SIDE, ROUND_SIDE)
+    a, b = synth.beta_posterior(N_SPLATS, seed=1)
+    cams = synth.sphere_cameras(ROUND_VIEWS, ROUND_RADIUS, 2, O.look_at)
+    scale = O.scale_for(*size)
+    t0 = time.perf_counter()
+    done = 0
+    for v in range(ROUND_VIEWS):
+        prep = O.prepare(cams[v], ROUND_SIDE, ROUND_SIDE, attr, sh, SH_PER_CH)
+        fg, bg = O.evidence(prep, synth.ellipse_mask(ROUND_SIDE, ROUND_SIDE, seed=100 + v))
+        O.eig(a, b, fg + bg, scale, 0)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    per_view = (time.perf_counter() - t0) / done
+    return {"kind": "port", "cores": O.num_threads(),
+            "c0_frame": {"ms": c0_ms, "sample": "3 frames of 100k SH0 splats at 512x512, median"},
+            "c2_round": {"views_per_s": 1.0 / per_view, "ms_per_round": 1e3 * per_view * ROUND_VIEWS,
+                         "sample": f"{done} of the round's {ROUND_VIEWS} views (evidence lift + LUT EIG)"}}
 
 
 def run_reference(args, rank, world):
@@ -472,10 +576,13 @@ def run_ours(args, rank, world):
 
     bwd = time_backward(sf, splats, scratch, attr, sh, my_cams[0], stream, args)
     eig_round = time_eig_round(sf, splats, ctx, stream, args)
+    del scratch
+    uneven = time_uneven_round(sf, ctx, stream, args)
 
     if rank != 0:
         return
     cpu_s, cpu_frames, cores = cpu_frame_time(attr, sh)
+    cpu_more = cpu_other_configs(attr, sh)
     clk = clocks.summary()
     peaks, which = measured_peaks()
     line = {
@@ -507,8 +614,10 @@ def run_ours(args, rank, world):
         "raster_stats": {k: v / n_split for k, v in detail.items()},
         "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "frames/s", "cores": cores, "kind": "port",
                          "sample": f"{cpu_frames} full frame(s) of the workload, median"},
+        "cpu_other_configs": cpu_more,
         "backward": bwd,
         "eig_round": eig_round,
+        "uneven_round": uneven,
         "clocks": clk,
         "gpu_launches": int(launches),
         "peaks": {"source": which, "hbm_gbs": peaks.get("hbm_gbs")},

@@ -332,7 +332,9 @@ int sf_beta_destroy(sf_beta beta);
 int sf_beta_read(sf_beta beta, float* a, float* b, sf_stream stream);
 int sf_beta_info(sf_beta beta, uint32_t* n, float** a_dev, float** b_dev);
 /* BetaState::eig (src/seg/beta.rs:241-268): EIG = sum_i dH_i for the accumulator's
- * responsibility. mode SF_EIG_LUT_F32 reads the f32 445x445 log-spaced LUT
+ * responsibility: its ε words, or fg + bg when its last fill was a masked
+ * sf_accumulate_prepared (the same words, src/seg/tests.rs:208-227).
+ * mode SF_EIG_LUT_F32 reads the f32 445x445 log-spaced LUT
  * (beta.rs:128-201); SF_EIG_FP64 evaluates the f64 lgamma/digamma entropy on
  * the GPU. Reduced on the device in f64 (no partials read-back); syncs. */
 int sf_beta_eig(sf_beta beta, sf_accum acc, int mode, sf_stream stream, double* eig);

@@ -487,6 +487,7 @@ int accumulate(sf_scratch s, const sf_isects* is, uint32_t w, uint32_t h, sf_acc
     acc->scale = (float)((uint64_t)1 << frac_bits(w, h));
     RasterArgs a = raster_args(s, is);
     a.scale = acc->scale;
+    acc->evidence = mask != nullptr;
     SF_CK(cudaMemsetAsync(s->stats, 0, 32, st));
     if (!mask) {
         SF_CK(cudaMemsetAsync(acc->resp, 0, (size_t)acc->total * 4, st));
@@ -1512,8 +1513,10 @@ int sf_beta_eig_async(sf_beta b, sf_accum acc, int mode, double* eig_dev, sf_str
         if (mode != SF_EIG_LUT_F32 && mode != SF_EIG_FP64) return fail(SF_ERR_ARG, "bad EIG mode");
         if (acc->total != b->n) return fail(SF_ERR_SHAPE, "accumulator and posterior sizes differ");
         SF_CK(use_device(b->ctx->device));
-        SF_CK(launch_eig(mode, b->a, b->b, acc->resp, b->n, acc->scale, b->ctx->lut, b->partials,
-                         b->blocks, eig_dev, S(stream)));
+        // After a masked split the responsibility is fg + bg (word for word
+        // the unmasked ε).
+        SF_CK(launch_eig(mode, b->a, b->b, acc->evidence ? acc->fg : acc->resp, b->n, acc->scale, b->ctx->lut,
+                         b->partials, b->blocks, eig_dev, S(stream), acc->evidence ? acc->bg : nullptr));
         return SF_OK;
     })
 }

@@ -24,6 +24,7 @@ struct sf_accum_t {
     uint32_t total = 0;
     uint32_t *resp = nullptr, *fg = nullptr, *bg = nullptr;
     float scale = 1.0f;
+    bool evidence = false;  // the last fill was a masked split (fg, bg), not resp
 };
 
 struct sf_mask_t {

@@ -149,3 +149,27 @@ def test_batched_scoring_equals_plain_per_view_scoring(ctx):
     for cam, e in zip(cams, batched):
         segmenter.splats.render_responsibility(scratch, acc, cam, (256, 256))
         assert segmenter.state.eig(acc, sf.EIG_LUT_F32) == e
+
+
+def test_eig_after_masked_accumulate_equals_responsibility_eig(ctx):
+    """sf_beta_eig over an accumulator whose last fill was a masked split
+    reads fg + bg, which equals the unmasked ε word for word
+    (src/seg/tests.rs:208-227), so its EIG equals the responsibility EIG."""
+    from splatfield_b200 import synth
+
+    n, w, h = 20000, 128, 96
+    attr, sh = synth.scene_uniform(n, 1, 5)
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    cam = sf.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    a, b = synth.beta_posterior(n, seed=2)
+    beta = sf.BetaState.from_host(a, b)
+    acc = sf.Accumulators(n)
+    splats.render_responsibility(scratch, acc, cam, (w, h))
+    want = {m: beta.eig(acc, m) for m in (sf.EIG_LUT_F32, sf.EIG_FP64)}
+    mask = sf.Mask.from_bytes((w, h), synth.ellipse_mask(w, h, seed=4))
+    isects = splats.prepare_isects(scratch, cam, (w, h))
+    splats.accumulate_prepared(scratch, isects, (w, h), acc, mask)
+    assert acc.fg.read().sum() > 0 and acc.bg.read().sum() > 0
+    for m, v in want.items():
+        assert beta.eig(acc, m) == v
