@@ -159,7 +159,12 @@ struct sf_scratch_t {
         uint32_t* stage[2] = {nullptr, nullptr};
         size_t stage_words = 0;
         sf_view* views = nullptr;     // pinned, one per frame of the batch
-        uint32_t* frame_words = nullptr;  // pinned, 16 per frame
+        uint32_t* frame_words = nullptr;  // pinned, 16 per frame of the batch
+        // Device ring the graph's last node saves each frame's words to
+        // (slot = *ring_counter, which it then increments), read back once a
+        // run of frames has finished.
+        uint32_t* ring = nullptr;
+        uint32_t* ring_counter = nullptr;
         uint32_t batch_cap = 0;
     } fg;
     uint32_t* bitmap = nullptr;
@@ -512,10 +517,10 @@ int accumulate(sf_scratch s, const sf_isects* is, uint32_t w, uint32_t h, sf_acc
 // scans, placement against the current capacity (device-side guard, tile
 // starts clamped), per-tile sorts as persistent kernels reading their class
 // sizes on the device (the classes on side streams), raster, and the status
-// words back to pinned memory — captured once and replayed with one launch
-// per frame on the caller's stream. The host reads the words after the
-// frame; a frame that outgrew the capacity grows it and runs again (the
-// graph is captured anew).
+// words saved to a device ring — captured once and replayed with one launch
+// per frame on the caller's stream. The host reads the words after the frame
+// (or after a run of frames); a frame that outgrew the capacity grows it and
+// runs again (the graph is captured anew).
 
 // frame_render's answer when the frame graph does not apply (the caller
 // takes the step-by-step path).
@@ -526,6 +531,8 @@ bool frame_graph_usable(sf_splats sp, sf_scratch s) {
            !s->tuning.raster_detail;
 }
 
+constexpr uint32_t kFrameRing = 4096;  // frames whose status words the ring holds
+
 int frame_graph_capture(sf_splats sp, sf_scratch s) {
     auto& g = s->fg;
     if (g.exec) {
@@ -534,6 +541,8 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
     }
     if (!g.stream) SF_CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
     if (!g.view_dev) SF_CK(dalloc(&g.view_dev, 1));
+    if (!g.ring) SF_CK(dalloc(&g.ring, 16 * (size_t)kFrameRing));
+    if (!g.ring_counter) SF_CK(dalloc(&g.ring_counter, 1));
     if (!g.view_host) SF_CK(cudaMallocHost(reinterpret_cast<void**>(&g.view_host), sizeof(sf_view)));
     if (!s->sort_streams.s[0]) SF_CK(sort_streams_create(&s->sort_streams));
     const uint32_t n = sp->n;
@@ -595,7 +604,7 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
         }
         e = launch_raster(0, a, st);
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(s->host_words, words, 64, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = launch_save_words(words, g.ring, g.ring_counter, kFrameRing, st);
     cudaGraph_t graph = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
     g.kernels = (uint32_t)(launches() - launches0);
@@ -663,6 +672,7 @@ int frame_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_
         SF_CK(cudaMemcpyAsync(g.view_dev, g.view_host, sizeof(sf_view), cudaMemcpyHostToDevice, st));
         SF_CK(cudaGraphLaunch(g.exec, st));
         note_launches(g.kernels);
+        SF_CK(cudaMemcpyAsync(s->host_words, s->words, 64, cudaMemcpyDeviceToHost, st));
         if (host_out)
             SF_CK(cudaMemcpy2DAsync(host_out, (size_t)w * 4, s->bitmap, (size_t)s->row_stride * 4, (size_t)w * 4,
                                     h, cudaMemcpyDeviceToHost, st));
@@ -715,6 +725,7 @@ cudaError_t frames_batch_resources(sf_scratch s, uint32_t count, size_t image_wo
             return e;
         if ((e = cudaMallocHost(reinterpret_cast<void**>(&g.frame_words), 64 * (size_t)count)) != cudaSuccess)
             return e;
+
         g.batch_cap = count;
     }
     return cudaSuccess;
@@ -740,10 +751,20 @@ int frames_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cams, uint3
     SF_CK(cudaStreamWaitEvent(st, g.ready[0], 0));
     for (uint32_t i = 0; i < count; ++i) {
         const int slot = (int)(i & 1u);
+        // Each run of up to kFrameRing frames saves its words to the device
+        // ring, read back once after the run has finished (a read-back after
+        // every frame cost 2% of the frame rate).
+        if (i % kFrameRing == 0) {
+            if (i > 0) {
+                SF_CK(cudaStreamSynchronize(st));
+                SF_CK(cudaMemcpy(g.frame_words + 16 * (size_t)(i - kFrameRing), g.ring, 64 * (size_t)kFrameRing,
+                                 cudaMemcpyDeviceToHost));
+            }
+            SF_CK(cudaMemsetAsync(g.ring_counter, 0, 4, st));
+        }
         SF_CK(cudaMemcpyAsync(g.view_dev, g.views + i, sizeof(sf_view), cudaMemcpyHostToDevice, st));
         SF_CK(cudaGraphLaunch(g.exec, st));
         note_launches(g.kernels);
-        SF_CK(cudaMemcpyAsync(g.frame_words + 16 * (size_t)i, s->words, 64, cudaMemcpyDeviceToHost, st));
         if (!host_out) continue;
         if (i >= 2) SF_CK(cudaStreamWaitEvent(st, g.copied[slot], 0));
         SF_CK(cudaMemcpy2DAsync(g.stage[slot], (size_t)w * 4, s->bitmap, (size_t)s->row_stride * 4,
@@ -755,6 +776,11 @@ int frames_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cams, uint3
     }
     SF_CK(cudaStreamSynchronize(g.copy));
     SF_CK(cudaStreamSynchronize(st));
+    {
+        const uint32_t first = (count - 1) / kFrameRing * kFrameRing;
+        SF_CK(cudaMemcpy(g.frame_words + 16 * (size_t)first, g.ring, 64 * (size_t)(count - first),
+                         cudaMemcpyDeviceToHost));
+    }
     uint64_t need = 0;
     for (uint32_t i = 0; i < count; ++i) {
         const uint32_t* hw = g.frame_words + 16 * (size_t)i;
@@ -1008,6 +1034,8 @@ int sf_scratch_destroy(sf_scratch s) {
     }
     if (s->fg.views) cudaFreeHost(s->fg.views);
     if (s->fg.frame_words) cudaFreeHost(s->fg.frame_words);
+    dfree(s->fg.ring);
+    dfree(s->fg.ring_counter);
     delete s;
     return SF_OK;
 }

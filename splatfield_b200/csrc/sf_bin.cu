@@ -774,6 +774,14 @@ __global__ void clamp_count_kernel(const unsigned long long* total, uint32_t cap
     *n32 = (uint32_t)(t < cap ? t : cap);
 }
 
+__global__ void save_words_kernel(const uint32_t* __restrict__ words, uint32_t* __restrict__ ring,
+                                  uint32_t* counter, uint32_t ring_frames) {
+    const uint32_t idx = *counter;
+    if (idx < ring_frames)
+        for (uint32_t k = 0; k < 16; ++k) ring[(size_t)idx * 16 + k] = words[k];
+    *counter = idx + 1;
+}
+
 __global__ void clamp_starts_kernel(uint32_t* tile_start, uint32_t count, uint32_t cap) {
     pdl_trigger();
     pdl_wait();
@@ -788,6 +796,13 @@ cudaError_t launch_clamp_count(const unsigned long long* total, uint32_t cap, ui
     const cudaError_t e = launch_pdl(clamp_count_kernel, 1, 1, 0, st, total, cap, n32, err);
     note_launches(1);
     return e;
+}
+
+cudaError_t launch_save_words(const uint32_t* words, uint32_t* ring, uint32_t* counter, uint32_t ring_frames,
+                              cudaStream_t st) {
+    save_words_kernel<<<1, 1, 0, st>>>(words, ring, counter, ring_frames);
+    note_launches(1);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_clamp_starts(uint32_t* tile_start, uint32_t count, uint32_t cap, cudaStream_t st) {

@@ -199,6 +199,11 @@ cudaError_t launch_bin_place(const uint2* bbox, const uint32_t* depth_keys, uint
 // placed pair, so the sorts and the raster stay inside the buffers).
 cudaError_t launch_clamp_count(const unsigned long long* total, uint32_t cap, uint32_t* n32, uint32_t* err,
                                cudaStream_t st);
+// A frame's 16 status words to slot *counter of a device ring (when it is
+// below ring_frames), then ++*counter: the last node of the frame graph, so
+// frames enqueued back to back keep their words on the device.
+cudaError_t launch_save_words(const uint32_t* words, uint32_t* ring, uint32_t* counter, uint32_t ring_frames,
+                              cudaStream_t st);
 cudaError_t launch_clamp_starts(uint32_t* tile_start, uint32_t count, uint32_t cap, cudaStream_t st);
 
 // Side streams the per-tile sort classes run on concurrently inside a
