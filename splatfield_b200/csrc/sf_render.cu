@@ -391,7 +391,7 @@ struct PixelState {
     float T, pr, pg, pb;
     uint32_t last;
     bool done;
-    uint32_t n_eval, n_hit, n_proc, visited;
+    uint32_t n_eval, n_hit, n_proc;
 };
 
 // Composites list entries [0, count) in order; id(i) gives entry i's splat
@@ -422,7 +422,6 @@ __device__ bool composite_list(const RasterArgs& a, const RasterSmem& sm, IdOf i
         }
         if (__syncthreads_count(ps.done) == 256) return true;
         const uint32_t cnt = min(256u, count - chunk);
-        ps.visited += cnt;
         // One (warp, entry) step: every lane of the warp runs it together.
         auto step = [&](uint32_t j) {
             if (DETAIL) ++ps.n_proc;
@@ -579,7 +578,7 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, const uint32_t 
     if (MODE == 2 && in_bounds) inside = (a.mask[px / 32 + py * a.mask_wpr] >> (px % 32)) & 1u;
     const uint32_t start = a.tile_start[tile], end = a.tile_start[tile + 1];
     const RasterSmem sm{s_g0, s_g1, s_col, s_gid, s_acc0, s_acc1, s_mask};
-    PixelState ps{1.0f, 0.0f, 0.0f, 0.0f, 0u, !in_bounds, 0u, 0u, 0u, 0u};
+    PixelState ps{1.0f, 0.0f, 0.0f, 0.0f, 0u, !in_bounds, 0u, 0u, 0u};
 
     if (!LAZY || end - start <= a.lazy_min) {
         const uint32_t* ids = a.gaussian_ids + start;
