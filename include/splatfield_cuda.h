@@ -434,7 +434,9 @@ int sf_radix_destroy(sf_radix r);
  * Outputs are device pointers into the scratch (or the inputs themselves when
  * n <= 1 or bits == 0, as the reference returns). write_keys = 0 leaves the
  * returned keys stale (values are always sorted). Onesweep: 8-bit digits, one
- * upfront histogram, one decoupled-look-back pass per digit. */
+ * upfront histogram, one decoupled-look-back pass per digit. The call waits
+ * for the stream and reads the sort's device error word: a look-back wait
+ * that ran out returns SF_ERR_TIMEOUT (the outputs are then not valid). */
 int sf_radix_argsort(sf_radix r, const uint32_t* keys, const uint32_t* vals, uint32_t n,
                      uint32_t bits, int write_keys, sf_stream stream, const uint32_t** keys_out,
                      const uint32_t** vals_out);
@@ -443,7 +445,8 @@ int sf_scan_create(sf_ctx ctx, uint32_t max_elems, sf_scan* out);
 int sf_scan_destroy(sf_scan s);
 /* exclusive_scan_gather (crates/sort/src/scan.rs:219-255):
  * offsets[i] = sum_{j<i} counts[gids[j]], single-pass decoupled look-back;
- * n = 0 writes nothing. */
+ * n = 0 writes nothing. Like sf_radix_argsort, the call waits for the stream
+ * and returns SF_ERR_TIMEOUT if a look-back wait ran out. */
 int sf_exclusive_scan_gather(sf_scan s, const uint32_t* gids, const uint32_t* counts,
                              uint32_t* offsets, uint32_t n, sf_stream stream);
 /* exclusive_scan_buf (crates/sort/src/scan.rs:185-213): in place. */
@@ -456,10 +459,25 @@ int sf_exclusive_scan(sf_scan s, uint32_t* buf, uint32_t n, sf_stream stream);
  * calling thread's current device; n > SF_SCAN_NOALLOC_MAX_ELEMS (2^24) is
  * rejected with SF_ERR_SHAPE before any CUDA call. Every call on a device
  * shares the one array: calls that overlap on the GPU race, so order them
- * (one stream). */
+ * (one stream). The first call on a device finds the array's device address
+ * (cudaGetSymbolAddress) and keeps it; a cudaDeviceReset invalidates it. The
+ * call waits for the stream, reads the error word into a host stack variable
+ * and returns SF_ERR_TIMEOUT if a look-back wait ran out. */
 #define SF_SCAN_NOALLOC_MAX_ELEMS (1u << 24)
 int sf_exclusive_scan_gather_noalloc(const uint32_t* gids, const uint32_t* counts,
                                      uint32_t* offsets, uint32_t n, sf_stream stream);
+
+/* ------------------------------------------------------- test hooks */
+/* No counterpart in the reference. Knobs of the bounded look-back waits of
+ * the scan and the radix sort, for tests of the timeout path: spin_limit caps
+ * the polls of one wait (0 restores the default); withhold = 1 keeps the first
+ * partition of every scan and digit pass from publishing its status, so the
+ * waits after it run out and the calls return SF_ERR_TIMEOUT instead of
+ * hanging. Process-wide host state; call (0, 0) afterwards. Only
+ * sf_radix_argsort, sf_exclusive_scan_gather, sf_exclusive_scan and
+ * sf_exclusive_scan_gather_noalloc pass the knobs to their kernels; the
+ * frame, round and backward paths never see them. */
+int sf_debug_lookback(uint32_t spin_limit, int withhold);
 
 #ifdef __cplusplus
 }

@@ -55,7 +55,10 @@ extern "C" double sfo_lgamma(double x) {
 }
 
 // digamma: recurrence to x >= 6, then the asymptotic series (beta.rs:77-86).
+// Departure: x <= 0 and NaN return NaN (Beta parameters are positive); the
+// reference's recurrence would run about |x| steps there, forever below -2^53.
 extern "C" double sfo_digamma(double x) {
+    if (!(x > 0.0)) return std::nan("");
     double r = 0.0;
     while (x < 6.0) { r -= 1.0 / x; x += 1.0; }
     const double inv = 1.0 / x, inv2 = inv * inv;

@@ -168,6 +168,7 @@ SIGNATURES = {
         "sf_exclusive_scan_gather": (i32, [P, P, P, P, u32, P]),
         "sf_exclusive_scan": (i32, [P, P, u32, P]),
         "sf_exclusive_scan_gather_noalloc": (i32, [P, P, P, u32, P]),
+        "sf_debug_lookback": (i32, [u32, i32]),
 }
 del P, u32, i32, sz, PP
 

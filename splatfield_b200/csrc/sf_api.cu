@@ -1497,6 +1497,13 @@ int sf_beta_create(sf_ctx ctx, const float* a, const float* bb, uint32_t n, sf_b
     SF_TRY({
         if (!ctx || !a || !bb || !out) return fail(SF_ERR_ARG, "null argument");
         *out = nullptr;
+        // Beta parameters are positive and finite; anything else is refused
+        // here, before any CUDA call, rather than reaching the EIG kernels.
+        for (uint32_t i = 0; i < n; ++i) {
+            if (!(a[i] > 0.0f && a[i] < INFINITY) || !(bb[i] > 0.0f && bb[i] < INFINITY))
+                return fail(SF_ERR_ARG, "Beta parameters must be positive and finite (splat " +
+                                            std::to_string(i) + ")");
+        }
         SF_CK(use_device(ctx->device));
         sf_beta b = nullptr;
         int rc = beta_alloc(ctx, n, &b);
@@ -1620,6 +1627,20 @@ int sf_table_entropy(sf_ctx ctx, const float* a, const float* b, uint32_t n, flo
 
 // ------------------------------------------------------------ sort / scan
 
+// Waits for the stream, reads a look-back error word and clears it: a wait
+// that ran out returns SF_ERR_TIMEOUT (the results are then not valid).
+static int read_timeout_word(uint32_t* err_dev, cudaStream_t st) {
+    uint32_t word = 0;
+    SF_CK(cudaMemcpyAsync(&word, err_dev, 4, cudaMemcpyDeviceToHost, st));
+    SF_CK(cudaStreamSynchronize(st));
+    if (word & SF_DEV_ERR_TIMEOUT) {
+        SF_CK(cudaMemsetAsync(err_dev, 0, 4, st));
+        SF_CK(cudaStreamSynchronize(st));
+        return fail(SF_ERR_TIMEOUT, "device look-back wait timed out");
+    }
+    return SF_OK;
+}
+
 uint32_t sf_bits_for(uint32_t max_exclusive) { return bits_for_u32(max_exclusive); }
 
 int sf_radix_create(sf_ctx ctx, uint32_t max_elems, sf_radix* out) {
@@ -1677,10 +1698,10 @@ int sf_radix_argsort(sf_radix r, const uint32_t* keys, const uint32_t* vals, uin
         int in_b = 0;
         SF_CK(radix_sort_pairs(keys, vals, r->ka, r->va, r->kb, r->vb, n, nullptr, n, bits,
                                write_keys != 0, vals == nullptr, r->tmp, r->err, r->ctx->sm_count,
-                               S(stream), &in_b));
+                               S(stream), &in_b, lookback_test_knobs()));
         *keys_out = in_b ? r->kb : r->ka;
         *vals_out = in_b ? r->vb : r->va;
-        return SF_OK;
+        return read_timeout_word(r->err, S(stream));
     })
 }
 
@@ -1726,8 +1747,9 @@ int sf_exclusive_scan_gather(sf_scan s, const uint32_t* gids, const uint32_t* co
             return fail(SF_ERR_SHAPE, "offsets undersized: scanned " + std::to_string(n) +
                                           " elements, capacity " + std::to_string(s->max));
         SF_CK(use_device(s->ctx->device));
-        SF_CK(exclusive_scan(gids, counts, offsets, n, nullptr, n, s->tmp, s->total, s->err, S(stream)));
-        return SF_OK;
+        SF_CK(exclusive_scan(gids, counts, offsets, n, nullptr, n, s->tmp, s->total, s->err, S(stream),
+                             lookback_test_knobs()));
+        return read_timeout_word(s->err, S(stream));
     })
 }
 

@@ -151,6 +151,15 @@ cudaError_t launch_export_rows(const float4* geo0, const float4* geo1, const flo
                                cudaStream_t stream);
 
 // ---- sort / scan (sf_sort.cu)
+// Test knobs of the bounded look-back waits (sf_debug_lookback): spin_limit
+// caps the polls of one wait (0: the default), withhold = 1 keeps partition 0
+// from publishing so the later waits run out. Zero in every internal call;
+// only the standalone sort and scan entry points pass lookback_test_knobs().
+struct LookbackKnobs {
+    uint32_t spin_limit;
+    uint32_t withhold;
+};
+LookbackKnobs lookback_test_knobs();
 uint32_t radix_passes(uint32_t bits);
 size_t radix_temp_bytes(uint32_t max_elems, uint32_t max_passes);
 // Sorts keys_in/vals_in by the low `bits` bits into the (a, b) ping-pong
@@ -160,11 +169,12 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
                              uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, uint32_t n,
                              const uint32_t* n_dev, uint32_t max_n, uint32_t bits, bool write_keys,
                              bool vals_iota, void* temp, uint32_t* err, int sm_count,
-                             cudaStream_t stream, int* out_in_b);
+                             cudaStream_t stream, int* out_in_b, LookbackKnobs knobs = {0u, 0u});
 size_t scan_temp_bytes(uint32_t max_elems);
 cudaError_t exclusive_scan(const uint32_t* gids, const uint32_t* counts, uint32_t* out, uint32_t n,
                            const uint32_t* n_dev, uint32_t max_n, void* temp,
-                           unsigned long long* total_out, uint32_t* err, cudaStream_t stream);
+                           unsigned long long* total_out, uint32_t* err, cudaStream_t stream,
+                           LookbackKnobs knobs = {0u, 0u});
 
 // ---- binned intersection build (sf_bin.cu)
 // Tiles per frame the binned build handles (one u32 shared-memory counter

@@ -34,7 +34,10 @@ constexpr size_t kNoAllocBytes = kNoAllocTotalsBytes + kNoAllocScanBytes;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-// Device address of g_noalloc_scratch per device, found once per device.
+// Device address of g_noalloc_scratch per device, found once per device by
+// the first call on it. A cudaDeviceReset unloads the module that holds the
+// array, so the cached address is not valid across one: callers that reset a
+// device must not use this entry point afterwards in the same process.
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[kMaxDevices] = {};
@@ -87,9 +90,16 @@ int sf_exclusive_scan_gather_noalloc(const uint32_t* gids, const uint32_t* count
         e = cudaMemsetAsync(base, 0, kNoAllocTotalsBytes, st);
         if (e == cudaSuccess)
             e = sfk::exclusive_scan(gids, counts, offsets, n, nullptr, n, base + kNoAllocTotalsBytes, total,
-                                    err, st);
+                                    err, st, sfk::lookback_test_knobs());
+        // The error word comes back into a host stack variable (no pinned
+        // buffer is allocated); a look-back wait that ran out is reported.
+        uint32_t word = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&word, err, 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess)
             return na_fail(SF_ERR_CUDA, std::string("static-scratch scan: ") + cudaGetErrorString(e));
+        if (word & SF_DEV_ERR_TIMEOUT)
+            return na_fail(SF_ERR_TIMEOUT, "static-scratch scan: device look-back wait timed out");
         return SF_OK;
     } catch (const std::bad_alloc&) {
         return na_fail(SF_ERR_NOMEM, "host allocation failed");

@@ -6,6 +6,7 @@
 // sum is an f64 two-level reduction on the device in a fixed order, so the
 // result is deterministic and a batched round needs no host sync per view.
 #include <cmath>
+#include <math_constants.h>
 #include <cstdint>
 #include "sf_internal.h"
 #include "sf_math.cuh"
@@ -24,7 +25,12 @@ double lgamma_h(double x) {
     const double t = z + 7.5;
     return 0.5 * std::log(2.0 * 3.141592653589793) + (z + 0.5) * std::log(t) - t + std::log(series);
 }
+// The recurrence runs at most six steps for x > 0. Beta parameters are
+// positive, so x <= 0 and NaN return NaN instead of recurring (the
+// reference's loop, beta.rs:77-86, would take about |x| steps there and never
+// end for x <= -2^53).
 double digamma_h(double x) {
+    if (!(x > 0.0)) return NAN;
     double r = 0.0;
     while (x < 6.0) { r -= 1.0 / x; x += 1.0; }
     const double inv = 1.0 / x, inv2 = inv * inv;
@@ -66,7 +72,10 @@ __device__ __forceinline__ double lgamma_d(double x) {
     const double t = z + 7.5;
     return 0.5 * log(2.0 * 3.141592653589793) + (z + 0.5) * log(t) - t + log(series);
 }
+// As digamma_h: x <= 0 and NaN give NaN, so the recurrence is at most six
+// steps for every input (a posterior word of -inf cannot hold the kernel).
 __device__ __forceinline__ double digamma_d(double x) {
+    if (!(x > 0.0)) return CUDART_NAN;
     double r = 0.0;
     while (x < 6.0) { r -= 1.0 / x; x += 1.0; }
     const double inv = 1.0 / x, inv2 = inv * inv;

@@ -17,7 +17,8 @@
 // SF_DEV_ERR_TIMEOUT in the error word and carries on, so a lost predecessor
 // can corrupt the result but never hang the GPU.
 #include <cstdint>
-#include "sf_internal.h"
+#include <string>
+#include "sf_handles.h"
 
 namespace sfk {
 
@@ -33,6 +34,16 @@ constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kCountMask = (1u << 30) - 1u;
 constexpr uint32_t kSpinLimit = 1u << 22;
+
+// Test knobs of the look-back waits, set by sf_debug_lookback and passed to
+// the kernels only by the standalone sort and scan entry points (the frame
+// and round paths always pass zeros). spin_limit caps the polls of one wait
+// (0: kSpinLimit). withhold = 1 keeps partition 0 of the scan and of every
+// digit pass from publishing its status, a flag that nothing then sets: every
+// later partition's wait runs out after spin_limit polls, records
+// SF_DEV_ERR_TIMEOUT and returns, and the host reports SF_ERR_TIMEOUT. Every
+// access stays inside the buffers either way; only the values are wrong.
+LookbackKnobs g_test_knobs = {0u, 0u};
 
 __device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
     uint32_t v;
@@ -65,10 +76,11 @@ __device__ __forceinline__ unsigned long long ld_status(const unsigned long long
 constexpr int kWindow = 8;
 template <typename W>
 __device__ __forceinline__ W lookback_window(const W* stat, size_t stride, uint32_t part, W flag_prefix,
-                                             W value_mask, uint32_t* err) {
+                                             W value_mask, uint32_t* err, uint32_t spin_limit) {
     W excl = 0;
     int64_t p = (int64_t)part - 1;
     uint32_t spins = 0;
+    const uint32_t limit = spin_limit ? spin_limit : kSpinLimit;
     while (p >= 0) {
         W s[kWindow];
 #pragma unroll
@@ -86,7 +98,7 @@ __device__ __forceinline__ W lookback_window(const W* stat, size_t stride, uint3
             }
         }
         if (found) break;
-        if (used == 0 && ++spins > kSpinLimit) {
+        if (used == 0 && ++spins > limit) {
             atomicOr(err, SF_DEV_ERR_TIMEOUT);
             break;
         }
@@ -173,7 +185,7 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, const uint32_t* n_dev,
     uint32_t n_static, uint32_t shift, uint32_t digit_mask, const uint32_t* __restrict__ pass_hist,
-    uint32_t* lookback, uint32_t* ticket, uint32_t* err, int vals_iota, int write_keys) {
+    uint32_t* lookback, uint32_t* ticket, uint32_t* err, int vals_iota, int write_keys, LookbackKnobs knobs) {
     __shared__ uint32_t s_part;
     __shared__ uint32_t s_warp_hist[kWarps][kRadix];
     __shared__ uint32_t s_local_start[kRadix];
@@ -230,7 +242,8 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
             sum += c;
         }
         digit_total = sum;
-        st_relaxed(&lookback[(size_t)part * kRadix + tid], (part == 0 ? kFlagPrefix : kFlagAgg) | sum);
+        if (part > 0 || !knobs.withhold)
+            st_relaxed(&lookback[(size_t)part * kRadix + tid], (part == 0 ? kFlagPrefix : kFlagAgg) | sum);
     }
     // Block exclusive scan of digit totals (digit order) -> local starts.
     {
@@ -283,7 +296,8 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
     if (tid < kRadix) {
         uint32_t excl = 0;
         if (part > 0) {
-            excl = lookback_window<uint32_t>(lookback + tid, kRadix, part, kFlagPrefix, kCountMask, err);
+            excl = lookback_window<uint32_t>(lookback + tid, kRadix, part, kFlagPrefix, kCountMask, err,
+                                            knobs.spin_limit);
             st_relaxed(&lookback[(size_t)part * kRadix + tid], kFlagPrefix | ((excl + digit_total) & kCountMask));
         }
         s_global_base[tid] = gstart + excl - s_local_start[tid];
@@ -325,7 +339,7 @@ constexpr unsigned long long kScanValMask = (1ull << 62) - 1ull;
 __global__ __launch_bounds__(kThreads) void scan_kernel(
     const uint32_t* __restrict__ gids, const uint32_t* counts, uint32_t* out, const uint32_t* n_dev,
     uint32_t n_static, unsigned long long* lookback, uint32_t* ticket,
-    unsigned long long* total_out, uint32_t* err) {
+    unsigned long long* total_out, uint32_t* err, LookbackKnobs knobs) {
     pdl_trigger();
     pdl_wait();
     __shared__ uint32_t s_part;
@@ -382,10 +396,11 @@ __global__ __launch_bounds__(kThreads) void scan_kernel(
     if (tid == 0) {
         unsigned long long excl = 0;
         if (part == 0) {
-            st_relaxed64(&lookback[0], kScanFlagPrefix | block_total);
+            if (!knobs.withhold) st_relaxed64(&lookback[0], kScanFlagPrefix | block_total);
         } else {
             st_relaxed64(&lookback[part], kScanFlagAgg | block_total);
-            excl = lookback_window<unsigned long long>(lookback, 1, part, kScanFlagPrefix, kScanValMask, err);
+            excl = lookback_window<unsigned long long>(lookback, 1, part, kScanFlagPrefix, kScanValMask, err,
+                                                      knobs.spin_limit);
             st_relaxed64(&lookback[part], kScanFlagPrefix | (excl + block_total));
         }
         s_prefix = excl;
@@ -422,7 +437,7 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
                              uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, uint32_t n,
                              const uint32_t* n_dev, uint32_t max_n, uint32_t bits, bool write_keys,
                              bool vals_iota, void* temp, uint32_t* err, int sm_count,
-                             cudaStream_t stream, int* out_in_b) {
+                             cudaStream_t stream, int* out_in_b, LookbackKnobs knobs) {
     const uint32_t passes = radix_passes(bits);
     const uint32_t grid_n = n_dev ? max_n : n;
     uint8_t* t = static_cast<uint8_t*>(temp);
@@ -449,7 +464,7 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
         onesweep_pass_kernel<<<(uint32_t)parts, kThreads, 0, stream>>>(
             kin, vin, kout, vout, n_dev, n, shift, (1u << w) - 1u, hist + p * kRadix,
             lookback + (size_t)p * parts * kRadix, tickets + p, err, (vals_iota && p == 0) ? 1 : 0,
-            wk ? 1 : 0);
+            wk ? 1 : 0, knobs);
         kin = kout;
         vin = vout;
         in_b = (p % 2 == 1);
@@ -466,7 +481,8 @@ size_t scan_temp_bytes(uint32_t max_elems) {
 
 cudaError_t exclusive_scan(const uint32_t* gids, const uint32_t* counts, uint32_t* out, uint32_t n,
                            const uint32_t* n_dev, uint32_t max_n, void* temp,
-                           unsigned long long* total_out, uint32_t* err, cudaStream_t stream) {
+                           unsigned long long* total_out, uint32_t* err, cudaStream_t stream,
+                           LookbackKnobs knobs) {
     const uint32_t grid_n = n_dev ? max_n : n;
     const size_t parts = std::max<size_t>((grid_n + kScanTile - 1) / kScanTile, 1);
     uint8_t* t = static_cast<uint8_t*>(temp);
@@ -475,9 +491,18 @@ cudaError_t exclusive_scan(const uint32_t* gids, const uint32_t* counts, uint32_
     cudaError_t e = cudaMemsetAsync(temp, 0, 64 + parts * 8, stream);
     if (e != cudaSuccess) return e;
     scan_kernel<<<(uint32_t)parts, kThreads, 0, stream>>>(gids, counts, out, n_dev, n, lookback,
-                                                           ticket, total_out, err);
+                                                           ticket, total_out, err, knobs);
     note_launches(1);
     return cudaGetLastError();
 }
 
 }  // namespace sfk
+
+namespace sfk {
+LookbackKnobs lookback_test_knobs() { return g_test_knobs; }
+}  // namespace sfk
+
+extern "C" int sf_debug_lookback(uint32_t spin_limit, int withhold) {
+    sfk::g_test_knobs = sfk::LookbackKnobs{spin_limit, withhold ? 1u : 0u};
+    return SF_OK;
+}

@@ -109,3 +109,35 @@ def test_errors_without_a_device_are_reported_not_raised_in_c(built_lib):
     assert L.sf_radix_argsort(None, None, None, 0, 0, 0, None, None, None) == _lib.SF_ERR_ARG
     assert L.sf_beta_eig(None, None, 0, None, None) == _lib.SF_ERR_ARG
     assert L.sf_map_labels(None, None, 0, None) == _lib.SF_OK
+
+
+@pytest.mark.parametrize("bad", [0.0, -1.0, float("nan"), float("inf"), float("-inf"), -2.0**60])
+def test_beta_create_refuses_bad_parameters_before_any_cuda_call(built_lib, bad):
+    """Non-positive or non-finite Beta parameters are refused with SF_ERR_ARG
+    before the context is touched (a stand-in context pointer suffices), so
+    they can never reach the FP64 entropy kernels."""
+    from splatfield_b200 import _lib
+
+    L = _lib.lib()
+    fake_ctx = C.create_string_buffer(64)
+    good = np.ones(4, np.float32)
+    a = good.copy()
+    a[2] = bad
+    out = C.c_void_p()
+    rc = L.sf_beta_create(C.cast(fake_ctx, C.c_void_p), a.ctypes.data_as(C.c_void_p),
+                          good.ctypes.data_as(C.c_void_p), 4, C.byref(out))
+    assert rc == _lib.SF_ERR_ARG
+    assert b"splat 2" in L.sf_last_error()
+    rc = L.sf_beta_create(C.cast(fake_ctx, C.c_void_p), good.ctypes.data_as(C.c_void_p),
+                          a.ctypes.data_as(C.c_void_p), 4, C.byref(out))
+    assert rc == _lib.SF_ERR_ARG
+    assert not out.value
+
+
+@pytest.mark.parametrize("x", [0.0, -1.0, float("-inf"), float("nan"), -2.0**60])
+def test_digamma_terminates_on_non_positive_input(oracle_mod, x):
+    """The oracle's digamma (the restatement of beta.rs:77-86) returns NaN
+    for x <= 0 and NaN instead of running its recurrence without end; the
+    device and host copies in the library carry the same guard."""
+    assert np.isnan(oracle_mod.digamma(x))
+    assert abs(oracle_mod.digamma(1.0) + 0.5772156649015329) < 1e-8
