@@ -179,7 +179,13 @@ typedef struct {
      *     class, longest first, so the longest walks do not trail the grid;
      *   SF_SCHEDULE_TILES: block i takes tile i. */
     uint32_t raster_schedule;
-    uint32_t reserved[3];
+    /* Rasterizer CTAs per 16x16 tile: 0 or 1 (default), one CTA of 8 warps;
+     * 2 or 4: CTAs of 4 or 2 warps, each walking the tile's whole list for
+     * its part of the pixels (a long unsaturated list is then walked on
+     * several SMs at once). The intersection tiles stay 16x16, so results
+     * are unchanged. */
+    uint32_t raster_split;
+    uint32_t reserved[2];
 } sf_tuning;
 #define SF_ISECTS_BINNED 0u
 #define SF_ISECTS_DEPTH_SORTED 1u
@@ -250,6 +256,19 @@ int sf_render_forward(sf_splats s, sf_scratch scratch, const sf_camera* cam, uin
 int sf_render_backward(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
                        const float* dl_drgba, float* d_attr, float* d_sh, float* d_proj,
                        sf_stream stream);
+/* Adjoint of a per-splat scalar feature (no counterpart in the reference,
+ * whose evidence lift is the u32 rasterizer, src/raster.rs:194-211): for the
+ * feature render F(p) = sum_i f_i alpha_i T_i(p), dL/df_i with dL/dF(p) =
+ * mask(p) into fg[i] and with dL/dF(p) = 1 - mask(p) into bg[i] (device
+ * [n] floats; mask NULL: all of it in fg) — the real-valued mask and
+ * background responsibilities sum_p m_p alpha_i T_i(p), which the u32 lift
+ * truncates per pixel to (u32)(alpha T scale). A transmittance-only forward
+ * keeps each pixel's final T and last contributor; the adjoint replays the
+ * sorted lists back to front from them. Float sums, added in no fixed order.
+ * Syncs once (the intersection total). Overwrites an sf_render_forward's
+ * state on the scratch. */
+int sf_render_feature_adjoint(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                              sf_mask mask, sf_stream stream, float* fg, float* bg);
 
 /* Splats::prepare_isects (src/render.rs:274-364): project, depth sort, gather
  * scan, emit, stable tile sort, tile ranges. Syncs once. */
@@ -342,6 +361,12 @@ int sf_beta_eig(sf_beta beta, sf_accum acc, int mode, sf_stream stream, double* 
 int sf_beta_eig_async(sf_beta beta, sf_accum acc, int mode, double* eig_dev, sf_stream stream);
 /* BetaState::update (src/seg/beta.rs:273-286): a += fg/scale, b += bg/scale. */
 int sf_beta_update(sf_beta beta, sf_accum acc, sf_stream stream);
+/* The EIG (beta.rs:152-201) and the Beta update (beta.rs:206-212) over
+ * real-valued responsibilities (sf_render_feature_adjoint,
+ * sf_round_adjoint_responsibility; device [n] floats): eps = fg + bg (bg
+ * may be NULL for the EIG), a += fg, b += bg. The EIG syncs. */
+int sf_beta_eig_real(sf_beta beta, const float* fg, const float* bg, int mode, sf_stream stream, double* eig);
+int sf_beta_update_real(sf_beta beta, const float* fg, const float* bg, sf_stream stream);
 /* localize (src/seg/views.rs:24-66): weighted centre and mean distance of
  * the foreground set {a > b}, weights m = a / (a + b), positions from the
  * splats' mean planes. *found = 0 (and zeros) while no splat is foreground.
@@ -370,7 +395,8 @@ typedef struct {
     uint32_t raster_cull; /* as sf_tuning.raster_cull */
     uint32_t isect_build; /* as sf_tuning.isect_build */
     uint32_t raster_order; /* as sf_tuning.raster_order */
-    uint32_t reserved[4];
+    uint32_t raster_split; /* as sf_tuning.raster_split */
+    uint32_t reserved[3];
 } sf_round_tuning;
 int sf_round_create(sf_ctx ctx, uint32_t total, uint32_t n_views, const uint32_t* widths,
                     const uint32_t* heights, sf_round* out);
@@ -399,13 +425,35 @@ int sf_round_evidence(sf_round r, sf_splats s, sf_beta beta, const sf_camera* ca
                       const sf_mask* masks, int mode, sf_stream stream, double* eig);
 /* View `view` of the last evidence round: device fg and bg words [total]. */
 int sf_round_evidence_words(sf_round r, uint32_t view, const uint32_t** fg, const uint32_t** bg);
-/* Autotuner: times the round over lanes {1,2,4,8} x raster_cull {0,1} (x
- * raster_order {sorted, in-raster, hybrid} with the binned build), keeps
- * the fastest on the round and in a process-wide cache keyed by (device,
- * splats, view sizes); a cached shape is not re-timed unless best_ms is
- * requested. */
+/* Adjoint evidence round (no counterpart in the reference): every view's
+ * responsibilities from the adjoint of a per-splat scalar feature
+ * (sf_render_feature_adjoint: transmittance-only forward, back-to-front
+ * replay) in the round's graph, real-valued fg / bg per splat (masks NULL,
+ * or a NULL entry: all of the view in fg), and with beta each view's EIG
+ * over fg + bg (sf_beta_eig_real). Syncs once. The lists are sorted for the
+ * replay whatever the tuning's raster_order. */
+int sf_round_evidence_adjoint(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams,
+                              const sf_mask* masks, int mode, sf_stream stream, double* eig);
+/* View `view` of the last adjoint round: device fg and bg floats [total]. */
+int sf_round_adjoint_responsibility(sf_round r, uint32_t view, const float** fg, const float** bg);
+/* Autotuner (the round's kernel forms picked by measured time): a
+ * coordinate search, two sweeps, over lanes {1,2,4,8}, isect_build {binned,
+ * depth-sorted}, raster_order {sorted, in-raster, hybrid} (binned build),
+ * raster_cull {0,1} and raster_split {1,2,4} (rasterizer warps per CTA 8, 4
+ * or 2 on 16x16 tiles), each candidate timed as the best of three rounds
+ * after a warm-up round. The winner stays on the round and in a
+ * process-wide cache keyed by (device, splats, view sizes, kind); a cached
+ * shape is not re-timed unless best_ms is requested. sf_round_autotune
+ * tunes the responsibility round (sf_round_eig); sf_round_autotune_kind the
+ * round of `kind`: SF_ROUND_RESPONSIBILITY, SF_ROUND_EVIDENCE
+ * (sf_round_evidence with `masks`) or SF_ROUND_ADJOINT
+ * (sf_round_evidence_adjoint; `masks` may be NULL). */
+enum { SF_ROUND_RESPONSIBILITY = 0, SF_ROUND_EVIDENCE = 1, SF_ROUND_ADJOINT = 2 };
 int sf_round_autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, int mode,
                       sf_stream stream, sf_round_tuning* best, double* best_ms);
+int sf_round_autotune_kind(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams,
+                           const sf_mask* masks, int kind, int mode, sf_stream stream,
+                           sf_round_tuning* best, double* best_ms);
 
 /* -------------------------------------------------------- PLY scenes */
 /* parse_ply's header rules (src/ply.rs:9-77) on a whole file image: the

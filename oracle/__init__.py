@@ -99,6 +99,10 @@ def lib():
             "sfo_beta_update": (None, [f32, P, P, P, P, u32]),
             "sfo64_render": (i32, [P, u32, u32, P, P, u32, u32, P]),
             "sfo64_render_backward": (i32, [P, u32, u32, P, P, u32, u32, P, P, P]),
+            "sfo64_probe_open": (P, [P, u32, u32, P, P, u32, u32, P]),
+            "sfo64_probe_close": (None, [P]),
+            "sfo64_probe_bbox": (i32, [P, u32, P]),
+            "sfo64_probe_loss": (f64, [P, u32, u32, f64, u32, u32, u32, u32]),
             "sfo_num_threads": (i32, []),
             "sfo_set_num_threads": (None, [i32]),
         }
@@ -356,6 +360,46 @@ def render64_backward(cam: Camera, w: int, h: int, attributes, sh, sh_per_ch: in
     lib().sfo64_render_backward(C.byref(cam), w, h, _p(attributes), _p(sh), n, sh_per_ch, _p(dl),
                                 _p(d_attr), _p(d_sh))
     return d_attr, d_sh
+
+
+class ProbeLoss:
+    """FP64 L2 loss of the forward against a target image over a tile region,
+    with one parameter of one splat replaced (sfo64_probe_*): central
+    differences on scenes too large to render whole per probe. Parameters:
+    0..10 the attribute planes, 11 + k*3 + c the SH coefficient (k, c)."""
+
+    def __init__(self, cam: Camera, w: int, h: int, attributes, sh, sh_per_ch: int, target_rgba):
+        self.attr = _c(attributes, np.float64)
+        self.sh = _c(sh, np.float64)
+        self.n = self.attr.size // 11
+        self.w, self.h = w, h
+        target = _c(target_rgba, np.float64)
+        assert target.size == 4 * w * h
+        self.handle = lib().sfo64_probe_open(C.byref(cam), w, h, _p(self.attr), _p(self.sh), self.n, sh_per_ch,
+                                             _p(target))
+
+    def bbox(self, i: int):
+        """(visible, (min_x, min_y, max_x, max_y)) tile box of splat i."""
+        out = np.zeros(2, np.uint32)
+        vis = lib().sfo64_probe_bbox(self.handle, i, _p(out))
+        return bool(vis), (int(out[0] & 0xFFFF), int(out[0] >> 16), int(out[1] & 0xFFFF), int(out[1] >> 16))
+
+    def base_value(self, i: int, param: int) -> float:
+        if param < 11:
+            return float(self.attr[param * self.n + i])
+        return float(self.sh[(param - 11) * self.n + i])
+
+    def loss(self, i: int, param: int, value: float, region) -> float:
+        tx0, ty0, tx1, ty1 = region
+        return float(lib().sfo64_probe_loss(self.handle, i, param, value, tx0, ty0, tx1, ty1))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().sfo64_probe_close(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
 
 
 def num_threads() -> int:

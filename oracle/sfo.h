@@ -140,6 +140,14 @@ int sfo64_render_backward(const sfo_camera* cam, uint32_t w, uint32_t h,
                           const double* attributes, const double* sh, uint32_t n,
                           uint32_t sh_per_ch, const double* dl_drgba, double* d_attr,
                           double* d_sh);
+/* FP64 L2 loss over a tile region with one parameter of one splat replaced
+ * (central differences on large scenes; sfo_grad.cpp). */
+void* sfo64_probe_open(const sfo_camera* cam, uint32_t w, uint32_t h, const double* attributes,
+                       const double* sh, uint32_t n, uint32_t K, const double* target_rgba);
+void sfo64_probe_close(void* handle);
+int sfo64_probe_bbox(void* handle, uint32_t i, uint32_t out[2]);
+double sfo64_probe_loss(void* handle, uint32_t i, uint32_t param, double value, uint32_t tx0, uint32_t ty0,
+                        uint32_t tx1, uint32_t ty1);
 
 /* threads the OpenMP regions use */
 int sfo_num_threads(void);

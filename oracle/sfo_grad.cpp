@@ -388,3 +388,98 @@ extern "C" int sfo64_render_backward(const sfo_camera* cam, uint32_t w, uint32_t
     }
     return 0;
 }
+
+// ---- FP64 L2 loss over a tile region, for central differences on large
+// scenes (TEST INFRASTRUCTURE). The splat set is projected once
+// (sfo64_probe_open). sfo64_probe_loss re-projects only the probed splat with
+// one parameter replaced, lists the splats whose tile box meets the region
+// in the forward's order (visible splats stably sorted by camera depth, as
+// bin64), and sums (rgba - target)^2 over the region's pixels. A splat only
+// reaches the pixels of its own tile box, so for a region holding the probed
+// splat's boxes at both ends of a difference, L(+h) - L(-h) over the region
+// equals that of the whole image.
+namespace {
+struct ProbeSession {
+    View64 v;
+    uint32_t w = 0, h = 0, n = 0, K = 1;
+    std::vector<double> attr, sh;
+    std::vector<double> target;  // [h][w][4]
+    std::vector<Proj> proj;
+};
+}  // namespace
+
+extern "C" void* sfo64_probe_open(const sfo_camera* cam, uint32_t w, uint32_t h, const double* attributes,
+                                  const double* sh, uint32_t n, uint32_t K, const double* target_rgba) {
+    auto* s = new ProbeSession();
+    s->v = make_view(cam, w, h);
+    s->w = w; s->h = h; s->n = n; s->K = K;
+    s->attr.assign(attributes, attributes + (size_t)11 * n);
+    s->sh.assign(sh, sh + (size_t)3 * K * n);
+    s->target.assign(target_rgba, target_rgba + (size_t)4 * w * h);
+    s->proj.assign(n, Proj());
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i)
+        project64(s->v, s->attr.data(), s->sh.data(), n, K, (uint32_t)i, s->proj[i]);
+    return s;
+}
+
+extern "C" void sfo64_probe_close(void* handle) { delete static_cast<ProbeSession*>(handle); }
+
+// Whether splat i is visible and its packed tile box (min, max) at the base
+// parameters.
+extern "C" int sfo64_probe_bbox(void* handle, uint32_t i, uint32_t out[2]) {
+    const auto* s = static_cast<ProbeSession*>(handle);
+    const Proj& p = s->proj[i];
+    out[0] = p.vis ? p.bb[0] : 0;
+    out[1] = p.vis ? p.bb[1] : 0;
+    return p.vis ? 1 : 0;
+}
+
+// param < 11: attribute plane `param` of splat i; otherwise SH coefficient
+// (param - 11) = k * 3 + c. Region: tiles [tx0, tx1) x [ty0, ty1).
+extern "C" double sfo64_probe_loss(void* handle, uint32_t i, uint32_t param, double value, uint32_t tx0,
+                                   uint32_t ty0, uint32_t tx1, uint32_t ty1) {
+    auto* s = static_cast<ProbeSession*>(handle);
+    const size_t N = s->n;
+    double* slot = param < 11 ? &s->attr[(size_t)param * N + i] : &s->sh[(size_t)(param - 11) * N + i];
+    const double keep = *slot;
+    *slot = value;
+    Proj local;
+    project64(s->v, s->attr.data(), s->sh.data(), s->n, s->K, i, local);
+    *slot = keep;
+    auto P = [&](uint32_t id) -> const Proj& { return id == i ? local : s->proj[id]; };
+    std::vector<uint32_t> ids;
+    for (uint32_t id = 0; id < s->n; ++id) {
+        const Proj& p = P(id);
+        if (!p.vis) continue;
+        const uint32_t bx0 = p.bb[0] & 0xffff, by0 = p.bb[0] >> 16, bx1 = p.bb[1] & 0xffff, by1 = p.bb[1] >> 16;
+        if (bx0 < tx1 && bx1 > tx0 && by0 < ty1 && by1 > ty0) ids.push_back(id);
+    }
+    std::stable_sort(ids.begin(), ids.end(), [&](uint32_t a, uint32_t b) { return P(a).cam[2] < P(b).cam[2]; });
+    Binned bn;
+    bn.proj.reserve(ids.size());
+    for (uint32_t id : ids) bn.proj.push_back(P(id));
+    const uint32_t rw = tx1 - tx0, rh = ty1 - ty0;
+    bn.tiles.assign((size_t)rw * rh, {});
+    for (uint32_t k = 0; k < ids.size(); ++k) {
+        const Proj& p = bn.proj[k];
+        const uint32_t bx0 = std::max(p.bb[0] & 0xffff, tx0), by0 = std::max(p.bb[0] >> 16, ty0);
+        const uint32_t bx1 = std::min(p.bb[1] & 0xffff, tx1), by1 = std::min(p.bb[1] >> 16, ty1);
+        for (uint32_t ty = by0; ty < by1; ++ty)
+            for (uint32_t tx = bx0; tx < bx1; ++tx) bn.tiles[(size_t)(ty - ty0) * rw + (tx - tx0)].push_back(k);
+    }
+    double loss = 0.0;
+    const int64_t pixels = (int64_t)rw * 16 * rh * 16;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : loss)
+    for (int64_t q = 0; q < pixels; ++q) {
+        const uint32_t px = tx0 * 16 + (uint32_t)(q % (rw * 16)), py = ty0 * 16 + (uint32_t)(q / (rw * 16));
+        if (px >= s->w || py >= s->h) continue;
+        const auto& list = bn.tiles[(size_t)(py / 16 - ty0) * rw + (px / 16 - tx0)];
+        double rgb[3];
+        const double T = walk_pixel(bn, list, px + 0.5, py + 0.5, nullptr, rgb);
+        const double* t = &s->target[4 * ((size_t)py * s->w + px)];
+        const double d[4] = {rgb[0] - t[0], rgb[1] - t[1], rgb[2] - t[2], (1.0 - T) - t[3]};
+        loss += d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + d[3] * d[3];
+    }
+    return loss;
+}

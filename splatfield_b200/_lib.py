@@ -26,6 +26,7 @@ READ_DEPTH_KEYS, READ_TILE_COUNTS, READ_BBOX, READ_PROJECTED, READ_ORDER, READ_O
 READ_TILE_IDS, READ_GAUSSIAN_IDS, READ_TILE_START, READ_BITMAP, READ_RGBA, READ_FINAL_T, READ_N_CONTRIB = range(6, 13)
 
 EIG_LUT_F32, EIG_FP64 = 0, 1
+ROUND_RESPONSIBILITY, ROUND_EVIDENCE, ROUND_ADJOINT = 0, 1, 2
 ISECTS_BINNED, ISECTS_DEPTH_SORTED = 0, 1
 ORDER_SORTED, ORDER_IN_RASTER, ORDER_HYBRID = 0, 1, 2
 SCHEDULE_LONGEST, SCHEDULE_TILES = 0, 1
@@ -55,14 +56,15 @@ class Tuning(C.Structure):
     """sf_tuning: kernel forms of a scratch (results are identical across forms)."""
 
     _fields_ = [("raster_cull", C.c_uint32), ("isect_build", C.c_uint32), ("raster_detail", C.c_uint32),
-                ("raster_order", C.c_uint32), ("raster_schedule", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("raster_order", C.c_uint32), ("raster_schedule", C.c_uint32), ("raster_split", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
 
 class RoundTuning(C.Structure):
     """sf_round_tuning."""
 
     _fields_ = [("lanes", C.c_uint32), ("raster_cull", C.c_uint32), ("isect_build", C.c_uint32),
-                ("raster_order", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+                ("raster_order", C.c_uint32), ("raster_split", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class Isects(C.Structure):
@@ -169,6 +171,12 @@ SIGNATURES = {
         "sf_exclusive_scan": (i32, [P, P, u32, P]),
         "sf_exclusive_scan_gather_noalloc": (i32, [P, P, P, u32, P]),
         "sf_debug_lookback": (i32, [u32, i32]),
+        "sf_render_feature_adjoint": (i32, [P, P, P, u32, u32, P, P, P, P]),
+        "sf_beta_eig_real": (i32, [P, P, P, i32, P, P]),
+        "sf_beta_update_real": (i32, [P, P, P, P]),
+        "sf_round_evidence_adjoint": (i32, [P, P, P, P, P, i32, P, P]),
+        "sf_round_adjoint_responsibility": (i32, [P, u32, PP, PP]),
+        "sf_round_autotune_kind": (i32, [P, P, P, P, P, i32, i32, P, P, P]),
 }
 del P, u32, i32, sz, PP
 

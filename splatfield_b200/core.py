@@ -27,13 +27,14 @@ __all__ = [
     "RadixScratch", "ScanScratch", "exclusive_scan_gather", "exclusive_scan_buf", "entropy_table",
     "table_entropy", "fractional_bits", "row_stride_for", "EIG_LUT_F32", "EIG_FP64", "Round",
     "ISECTS_BINNED", "ISECTS_DEPTH_SORTED", "ORDER_IN_RASTER", "ORDER_SORTED", "ORDER_HYBRID", "SCHEDULE_LONGEST", "SCHEDULE_TILES", "ply_inspect", "load_ply",
-    "pinned_empty",
+    "pinned_empty", "ROUND_RESPONSIBILITY", "ROUND_EVIDENCE", "ROUND_ADJOINT",
 ]
 
 EIG_LUT_F32, EIG_FP64 = L.EIG_LUT_F32, L.EIG_FP64
 ISECTS_BINNED, ISECTS_DEPTH_SORTED = L.ISECTS_BINNED, L.ISECTS_DEPTH_SORTED
 ORDER_IN_RASTER, ORDER_SORTED, ORDER_HYBRID = L.ORDER_IN_RASTER, L.ORDER_SORTED, L.ORDER_HYBRID
 SCHEDULE_TILES, SCHEDULE_LONGEST = L.SCHEDULE_TILES, L.SCHEDULE_LONGEST
+ROUND_RESPONSIBILITY, ROUND_EVIDENCE, ROUND_ADJOINT = L.ROUND_RESPONSIBILITY, L.ROUND_EVIDENCE, L.ROUND_ADJOINT
 BASE_FOV = 0.8  # Camera::BASE_FOV (src/camera.rs:86)
 
 
@@ -403,6 +404,19 @@ class Splats:
             out = out + (d_proj.read().reshape(self.n, 9),)
         return out
 
+    def render_feature_adjoint(self, scratch: "RenderScratch", camera: Camera, img_size, mask: "Mask | None" = None,
+                               stream=None):
+        """Real-valued (fg, bg) responsibilities [n] from the adjoint of a
+        per-splat scalar feature (fg weighted by the mask, bg by its
+        complement; no mask: all in fg), as device buffers."""
+        w, h = img_size
+        fg = DeviceBuffer.empty(self.n, np.float32, self.ctx)
+        bg = DeviceBuffer.empty(self.n, np.float32, self.ctx)
+        check(lib().sf_render_feature_adjoint(self.handle, scratch.handle, C.byref(camera), w, h,
+                                              mask.handle if mask is not None else None, _stream(stream),
+                                              _vp(fg), _vp(bg)))
+        return fg, bg
+
     def render_backward_into(self, scratch: "RenderScratch", camera: Camera, img_size, dl_drgba,
                              d_attr, d_sh, d_proj=None, stream=None) -> None:
         """render_backward into caller-owned device buffers; enqueues only."""
@@ -513,18 +527,21 @@ class RenderScratch:
         check(lib().sf_scratch_reserve(self.handle, int(isects)))
 
     def set_tuning(self, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED, raster_detail: int = 0,
-                   raster_order: int = L.ORDER_SORTED, raster_schedule: int = L.SCHEDULE_LONGEST) -> None:
+                   raster_order: int = L.ORDER_SORTED, raster_schedule: int = L.SCHEDULE_LONGEST,
+                   raster_split: int = 1) -> None:
         """Kernel forms (results are identical across forms): raster_cull 0/1,
         isect_build ISECTS_BINNED (default) or ISECTS_DEPTH_SORTED,
         raster_detail 1 to count the per-pair diagnostics of ``stats``,
         raster_order ORDER_SORTED (default), ORDER_IN_RASTER or ORDER_HYBRID,
-        raster_schedule SCHEDULE_LONGEST (default) or SCHEDULE_TILES."""
+        raster_schedule SCHEDULE_LONGEST (default) or SCHEDULE_TILES,
+        raster_split 1 (default), 2 or 4 rasterizer CTAs per tile."""
         t = L.Tuning()
         t.raster_cull = int(raster_cull)
         t.isect_build = int(isect_build)
         t.raster_detail = int(raster_detail)
         t.raster_order = int(raster_order)
         t.raster_schedule = int(raster_schedule)
+        t.raster_split = int(raster_split)
         check(lib().sf_scratch_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:
@@ -532,7 +549,7 @@ class RenderScratch:
         check(lib().sf_scratch_get_tuning(self.handle, C.byref(t)))
         return {"raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build),
                 "raster_detail": int(t.raster_detail), "raster_order": int(t.raster_order),
-                "raster_schedule": int(t.raster_schedule)}
+                "raster_schedule": int(t.raster_schedule), "raster_split": int(t.raster_split) or 1}
 
     def read(self, what: int, count: int, dtype=np.uint32, stream=None) -> np.ndarray:
         out = np.empty(count, dtype)
@@ -715,6 +732,16 @@ class BetaState:
     def update(self, acc: Accumulators, stream=None) -> None:
         check(lib().sf_beta_update(self.handle, acc.handle, _stream(stream)))
 
+    def eig_real(self, fg, bg=None, mode: int = EIG_LUT_F32, stream=None) -> float:
+        """EIG over real-valued responsibilities eps = fg + bg (device arrays)."""
+        out = C.c_double()
+        check(lib().sf_beta_eig_real(self.handle, _vp(fg), _vp(bg), mode, _stream(stream), C.byref(out)))
+        return float(out.value)
+
+    def update_real(self, fg, bg, stream=None) -> None:
+        """a += fg, b += bg (device arrays of real-valued responsibilities)."""
+        check(lib().sf_beta_update_real(self.handle, _vp(fg), _vp(bg), _stream(stream)))
+
     def read(self, stream=None):
         a = np.empty(self.n, np.float32)
         b = np.empty(self.n, np.float32)
@@ -782,16 +809,17 @@ class Round:
         return len(self.sizes)
 
     def set_tuning(self, lanes: int = 4, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED,
-                   raster_order: int = L.ORDER_SORTED) -> None:
+                   raster_order: int = L.ORDER_SORTED, raster_split: int = 1) -> None:
         t = L.RoundTuning()
         t.lanes, t.raster_cull, t.isect_build = int(lanes), int(raster_cull), int(isect_build)
         t.raster_order = int(raster_order)
+        t.raster_split = int(raster_split)
         check(lib().sf_round_set_tuning(self.handle, C.byref(t)))
 
     @staticmethod
     def _tuning_dict(t) -> dict:
         return {"lanes": int(t.lanes), "raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build),
-                "raster_order": int(t.raster_order)}
+                "raster_order": int(t.raster_order), "raster_split": int(t.raster_split) or 1}
 
     def get_tuning(self) -> dict:
         t = L.RoundTuning()
@@ -828,6 +856,29 @@ class Round:
                                       self._cams(cameras), hs, mode, _stream(stream), _vp(out)))
         return out
 
+    def evidence_adjoint(self, splats: Splats, beta: "BetaState | None", cameras, masks=None,
+                         mode: int = EIG_LUT_F32, stream=None) -> np.ndarray:
+        """Every view's real-valued (fg, bg) responsibilities from the adjoint
+        of a per-splat scalar feature (read with ``adjoint_responsibility``)
+        and, with a posterior, each view's EIG over fg + bg."""
+        if len(cameras) != self.views or (masks is not None and len(masks) != self.views):
+            raise SplatfieldError(L.SF_ERR_SHAPE, "one camera (and mask) per view")
+        hs = None
+        if masks is not None:
+            hs = (C.c_void_p * self.views)(*[m.handle if m is not None else None for m in masks])
+            self._masks = list(masks)
+        out = np.zeros(self.views, np.float64)
+        check(lib().sf_round_evidence_adjoint(self.handle, splats.handle, beta.handle if beta else None,
+                                              self._cams(cameras), hs, mode, _stream(stream), _vp(out)))
+        return out
+
+    def adjoint_responsibility(self, view: int) -> tuple:
+        """(fg, bg) device floats of a view of the last adjoint round."""
+        fg, bg = C.c_void_p(), C.c_void_p()
+        check(lib().sf_round_adjoint_responsibility(self.handle, view, C.byref(fg), C.byref(bg)))
+        return (DeviceView(fg.value, np.float32, (self.total,), self),
+                DeviceView(bg.value, np.float32, (self.total,), self))
+
     def evidence_words(self, view: int) -> tuple:
         """(fg, bg) device words of a view of the last evidence round."""
         fg, bg = C.c_void_p(), C.c_void_p()
@@ -846,11 +897,19 @@ class Round:
         return DeviceView(p.value, np.uint32, (self.total,), self), float(scale.value), int(nis.value), int(vis.value)
 
     def autotune(self, splats: Splats, beta: "BetaState | None", cameras, mode: int = EIG_LUT_F32,
-                 stream=None) -> tuple:
+                 stream=None, kind: int = L.ROUND_RESPONSIBILITY, masks=None) -> tuple:
+        """Pick the round's kernel forms by measured time for rounds of
+        `kind` (ROUND_RESPONSIBILITY, ROUND_EVIDENCE with masks, or
+        ROUND_ADJOINT); returns (tuning, best ms per round)."""
         t = L.RoundTuning()
         ms = C.c_double()
-        check(lib().sf_round_autotune(self.handle, splats.handle, beta.handle if beta else None,
-                                      self._cams(cameras), mode, _stream(stream), C.byref(t), C.byref(ms)))
+        hs = None
+        if masks is not None:
+            hs = (C.c_void_p * self.views)(*[m.handle if m is not None else None for m in masks])
+            self._masks = list(masks)
+        check(lib().sf_round_autotune_kind(self.handle, splats.handle, beta.handle if beta else None,
+                                           self._cams(cameras), hs, int(kind), mode, _stream(stream), C.byref(t),
+                                           C.byref(ms)))
         return self._tuning_dict(t), float(ms.value)
 
     def close(self):

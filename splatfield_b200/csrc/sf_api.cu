@@ -461,6 +461,7 @@ RasterArgs raster_args(sf_scratch s, const sf_isects* is) {
     a.color = s->color;
     a.ext = s->ext;
     a.cull = s->tuning.raster_cull;
+    a.split = s->tuning.raster_split;
     a.detail = s->tuning.raster_detail;
     a.stats = s->stats;
     return a;
@@ -596,6 +597,7 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
         a.color = s->color;
         a.ext = s->ext;
         a.cull = s->tuning.raster_cull;
+        a.split = s->tuning.raster_split;
         a.stats = s->stats;
         a.bitmap = s->bitmap;
         if (s->tuning.raster_schedule == SF_SCHEDULE_LONGEST && order != SF_ORDER_IN_RASTER) {
@@ -1046,6 +1048,8 @@ int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t) {
     if (t->isect_build > SF_ISECTS_DEPTH_SORTED) return fail(SF_ERR_ARG, "unknown isect_build");
     if (t->raster_order > SF_ORDER_HYBRID) return fail(SF_ERR_ARG, "unknown raster_order");
     if (t->raster_schedule > SF_SCHEDULE_TILES) return fail(SF_ERR_ARG, "unknown raster_schedule");
+    if (t->raster_split != 0 && t->raster_split != 1 && t->raster_split != 2 && t->raster_split != 4)
+        return fail(SF_ERR_ARG, "raster_split must be 1, 2 or 4");
     s->tuning = *t;
     return SF_OK;
 }
@@ -1214,6 +1218,46 @@ int sf_render_backward(sf_splats s, sf_scratch scratch, const sf_camera* cam, ui
         sf_view view;
         view_for_camera(*cam, w, h, &view);
         SF_CK(launch_project_bwd(view, s->attr, s->sh, s->n, s->K, d2d, d_attr, d_sh, st));
+        return SF_OK;
+    })
+}
+
+int sf_render_feature_adjoint(sf_splats s, sf_scratch scratch, const sf_camera* cam, uint32_t w, uint32_t h,
+                              sf_mask mask, sf_stream stream, float* fg, float* bg) {
+    SF_TRY({
+        if (!s || !scratch || !cam || !fg || !bg) return fail(SF_ERR_ARG, "null argument");
+        if (mask && (mask->w != w || mask->h != h)) return fail(SF_ERR_SHAPE, "mask size does not match the frame");
+        cudaStream_t st = S(stream);
+        // Sorted lists: the adjoint replays them back to front.
+        int rc = prepare(s, scratch, cam, w, h, st, nullptr);
+        if (rc != SF_OK) return rc;
+        const size_t pixels = (size_t)w * h;
+        if (!scratch->final_t) SF_CK(dalloc(&scratch->final_t, pixels));
+        if (!scratch->n_contrib) SF_CK(dalloc(&scratch->n_contrib, pixels));
+        scratch->has_forward = false;  // the RGB adjoint's state is overwritten
+        RasterArgs a = raster_args(scratch, nullptr);
+        a.final_t = scratch->final_t;
+        a.n_contrib = scratch->n_contrib;
+        SF_CK(cudaMemsetAsync(scratch->stats, 0, 32, st));
+        SF_CK(launch_raster(3, a, st));
+        SF_CK(cudaMemsetAsync(fg, 0, (size_t)s->n * 4, st));
+        SF_CK(cudaMemsetAsync(bg, 0, (size_t)s->n * 4, st));
+        FeatureBwdArgs f{};
+        f.w = w;
+        f.h = h;
+        f.tiles_x = scratch->tiles_x;
+        f.tiles_y = scratch->tiles_y;
+        f.tile_start = scratch->tile_start;
+        f.gaussian_ids = scratch->gids;
+        f.geo0 = scratch->geo0;
+        f.geo1 = scratch->geo1;
+        f.final_t = scratch->final_t;
+        f.n_contrib = scratch->n_contrib;
+        f.mask = mask ? mask->bits : nullptr;
+        f.mask_wpr = mask ? mask->wpr : 0u;
+        f.fg = fg;
+        f.bg = bg;
+        SF_CK(launch_feature_bwd(f, st));
         return SF_OK;
     })
 }
@@ -1564,6 +1608,30 @@ int sf_beta_eig(sf_beta b, sf_accum acc, int mode, sf_stream stream, double* eig
         SF_CK(cudaMemcpyAsync(b->host_out, b->out, 8, cudaMemcpyDeviceToHost, S(stream)));
         SF_CK(cudaStreamSynchronize(S(stream)));
         *eig = *b->host_out;
+        return SF_OK;
+    })
+}
+
+int sf_beta_eig_real(sf_beta b, const float* fg, const float* bg, int mode, sf_stream stream, double* eig) {
+    SF_TRY({
+        if (!b || !fg || !eig) return fail(SF_ERR_ARG, "null argument");
+        if (mode != SF_EIG_LUT_F32 && mode != SF_EIG_FP64) return fail(SF_ERR_ARG, "bad EIG mode");
+        SF_CK(use_device(b->ctx->device));
+        SF_CK(ensure_lut(b->ctx));
+        cudaStream_t st = S(stream);
+        SF_CK(launch_eig_real(mode, b->a, b->b, fg, bg, b->n, b->ctx->lut, b->partials, b->blocks, b->out, st));
+        SF_CK(cudaMemcpyAsync(b->host_out, b->out, 8, cudaMemcpyDeviceToHost, st));
+        SF_CK(cudaStreamSynchronize(st));
+        *eig = *b->host_out;
+        return SF_OK;
+    })
+}
+
+int sf_beta_update_real(sf_beta b, const float* fg, const float* bg, sf_stream stream) {
+    SF_TRY({
+        if (!b || !fg || !bg) return fail(SF_ERR_ARG, "null argument");
+        SF_CK(use_device(b->ctx->device));
+        SF_CK(launch_beta_update_real(fg, bg, b->a, b->b, b->n, S(stream)));
         return SF_OK;
     })
 }

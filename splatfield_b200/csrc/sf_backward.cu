@@ -150,6 +150,104 @@ __global__ __launch_bounds__(256) void raster_bwd_kernel(BwdArgs a) {
     }
 }
 
+// Adjoint of a per-splat scalar feature f: the render F(p) = sum_k f_k
+// alpha_k T_k over pixel p's contributors has dF(p)/df_k = alpha_k T_k, so
+// for L = sum_p w(p) F(p) the feature gradient is dL/df_i = sum_p w(p)
+// alpha_i T_i(p): splat i's responsibility weighted by w. Two weights at
+// once, w_fg = mask(p) and w_bg = 1 - mask(p) (all ones without a mask),
+// give the real-valued fg / bg responsibilities that the u32 evidence lift
+// truncates per pixel. The walk is the adjoint replay of raster_bwd_kernel
+// (back to front from the forward's final T and last contributor, T_k =
+// T_{k+1} / (1 - alpha_k)), with nothing but the two feature sums; the
+// forward state comes from the transmittance-only raster mode. Float sums
+// are reduced per warp, per tile in shared memory, then added to global
+// memory once per (tile, splat); their order of addition is not fixed.
+__global__ __launch_bounds__(256) void feature_bwd_kernel(FeatureBwdArgs a) {
+    __shared__ float4 s_g0[256];
+    __shared__ float4 s_g1[256];
+    __shared__ uint32_t s_gid[256];
+    __shared__ float s_fg[256];
+    __shared__ float s_bg[256];
+    __shared__ uint32_t s_max_last;
+
+    const uint32_t tile = blockIdx.x;
+    const uint32_t tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t px = tx * 16 + (warp & 1u) * 8 + (lane & 7u);
+    const uint32_t py = ty * 16 + (warp >> 1) * 4 + (lane >> 3);
+    const bool in_bounds = px < a.w && py < a.h;
+    const uint32_t start = a.tile_start[tile];
+    const float fx = (float)px + 0.5f, fy = (float)py + 0.5f;
+    float T = 1.0f;
+    uint32_t last = 0;
+    float wf = 0.0f, wb = 0.0f;
+    if (in_bounds) {
+        const size_t pix = (size_t)py * a.w + px;
+        T = a.final_t[pix];
+        last = a.n_contrib[pix];
+        const bool inside = a.mask ? ((a.mask[px / 32 + py * a.mask_wpr] >> (px % 32)) & 1u) != 0u : true;
+        wf = inside ? 1.0f : 0.0f;
+        wb = 1.0f - wf;
+    }
+    if (tid == 0) s_max_last = 0;
+    s_fg[tid] = 0.0f;
+    s_bg[tid] = 0.0f;
+    __syncthreads();
+    const uint32_t wmax = __reduce_max_sync(0xffffffffu, last);
+    if (lane == 0) atomicMax(&s_max_last, wmax);
+    __syncthreads();
+    const uint32_t max_last = s_max_last;
+    const float inv255 = 1.0f / 255.0f;
+
+    for (int64_t c0 = (int64_t)((max_last + 255u) / 256u) * 256 - 256; c0 >= 0; c0 -= 256) {
+        __syncthreads();
+        const uint32_t e_stage = (uint32_t)c0 + tid;
+        if (e_stage < max_last) {
+            const uint32_t gid = a.gaussian_ids[start + e_stage];
+            s_gid[tid] = gid;
+            s_g0[tid] = a.geo0[gid];
+            s_g1[tid] = a.geo1[gid];
+        }
+        __syncthreads();
+        const uint32_t cnt = min(256u, max_last - (uint32_t)c0);
+        for (int j = (int)cnt - 1; j >= 0; --j) {
+            const uint32_t e = (uint32_t)c0 + (uint32_t)j;
+            float w = 0.0f;
+            if (e < last) {
+                const float4 g0 = s_g0[j];
+                const float4 g1 = s_g1[j];
+                const float dx = g0.x - fx, dy = g0.y - fy;
+                const float power = fma_(g0.z * dx, dx, fma_(g1.x * dy, dy, (g0.w * dx) * dy));
+                if (!(power > g1.z)) {
+                    const float alpha = fminf(g1.y * exp_neg_(-power), 0.999f);
+                    if (alpha >= inv255) {
+                        const float Tk = T / (1.0f - alpha);
+                        w = alpha * Tk;
+                        T = Tk;
+                    }
+                }
+            }
+            if (__any_sync(0xffffffffu, w != 0.0f)) {
+                const float sf = warp_sum(wf * w);
+                const float sb = warp_sum(wb * w);
+                if (lane == 0) {
+                    if (sf != 0.0f) atomicAdd(&s_fg[j], sf);
+                    if (sb != 0.0f) atomicAdd(&s_bg[j], sb);
+                }
+            }
+        }
+        __syncthreads();
+        if (tid < cnt) {
+            const uint32_t g = s_gid[tid];
+            const float f = s_fg[tid], b = s_bg[tid];
+            if (f != 0.0f) atomicAdd(a.fg + g, f);
+            if (b != 0.0f) atomicAdd(a.bg + g, b);
+            s_fg[tid] = 0.0f;
+            s_bg[tid] = 0.0f;
+        }
+    }
+}
+
 struct V3 { float x, y, z; };
 __device__ __forceinline__ float dot3(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
 
@@ -356,6 +454,14 @@ cudaError_t launch_raster_bwd(const BwdArgs& a, cudaStream_t stream) {
     const uint32_t tiles = a.tiles_x * a.tiles_y;
     if (tiles == 0) return cudaSuccess;
     raster_bwd_kernel<<<tiles, 256, 0, stream>>>(a);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_feature_bwd(const FeatureBwdArgs& a, cudaStream_t stream) {
+    const uint32_t tiles = a.tiles_x * a.tiles_y;
+    if (tiles == 0) return cudaSuccess;
+    feature_bwd_kernel<<<tiles, 256, 0, stream>>>(a);
     note_launches(1);
     return cudaGetLastError();
 }

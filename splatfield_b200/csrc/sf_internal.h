@@ -112,6 +112,9 @@ struct RasterArgs {
     // Raster form: 0 walks every staged entry in every warp, 1 culls per warp
     // block with the power_max boxes (needs ext).
     uint32_t cull;
+    // CTAs per 16x16 tile (0 or 1: one CTA of 8 warps; 2 or 4: CTAs of 4 or
+    // 2 warps, each walking the whole list for its part of the pixels).
+    uint32_t split;
     // 1: also count the per-pair diagnostics stats[1..3] (slower form).
     uint32_t detail;
     // Optional pair statistics, added to: [0] (pixel, splat) pairs visited
@@ -124,7 +127,8 @@ struct RasterArgs {
     const uint32_t* class_lists;
     const uint32_t* class_n;
 };
-// mode 0 = RGB, 1 = total responsibility, 2 = evidence.
+// mode 0 = RGB, 1 = total responsibility, 2 = evidence, 3 = transmittance
+// only (final_t and n_contrib required).
 cudaError_t launch_raster(int mode, const RasterArgs& a, cudaStream_t stream);
 
 // Adjoint (sf_backward.cu).
@@ -141,6 +145,24 @@ struct BwdArgs {
     float* d2d;                // [n][9] accumulated: mean2d xy, conic xyz, rgb, opacity
 };
 cudaError_t launch_raster_bwd(const BwdArgs& a, cudaStream_t stream);
+// Adjoint of a per-splat scalar feature: fg[i] += sum_p mask(p) alpha_i
+// T_i(p), bg[i] += sum_p (1 - mask(p)) alpha_i T_i(p) (mask null: all in
+// fg), replayed from the state of the transmittance-only raster (mode 3)
+// over the same sorted lists.
+struct FeatureBwdArgs {
+    uint32_t w, h, tiles_x, tiles_y;
+    const uint32_t* tile_start;
+    const uint32_t* gaussian_ids;
+    const float4* geo0;
+    const float4* geo1;
+    const float* final_t;
+    const uint32_t* n_contrib;
+    const uint32_t* mask;
+    uint32_t mask_wpr;
+    float* fg;
+    float* bg;
+};
+cudaError_t launch_feature_bwd(const FeatureBwdArgs& a, cudaStream_t stream);
 cudaError_t launch_project_bwd(const sf_view& view, const float* attr, const float* sh, uint32_t n,
                                uint32_t sh_per_ch, const float* d2d, float* d_attr, float* d_sh,
                                cudaStream_t stream);
@@ -259,6 +281,13 @@ cudaError_t launch_localize(const float* attr, const float* a, const float* b, u
                             uint32_t blocks, double* out, cudaStream_t stream);
 cudaError_t launch_beta_update(float scale, const uint32_t* fg, const uint32_t* bg, float* a,
                                float* b, uint32_t n, cudaStream_t stream);
+// EIG and Beta update from real-valued responsibilities (eps = fg + bg; bg
+// may be null for the EIG).
+cudaError_t launch_eig_real(int mode, const float* a, const float* b, const float* fg, const float* bg,
+                            uint32_t n, const float* table, double* partials, uint32_t blocks, double* out,
+                            cudaStream_t stream);
+cudaError_t launch_beta_update_real(const float* fg, const float* bg, float* a, float* b, uint32_t n,
+                                    cudaStream_t stream);
 cudaError_t launch_table_probe(const float* a, const float* b, uint32_t n, const float* table,
                                float* out, cudaStream_t stream);
 

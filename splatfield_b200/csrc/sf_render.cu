@@ -327,435 +327,6 @@ __global__ __launch_bounds__(256) void tile_start_kernel(const uint32_t* __restr
     }
 }
 
-// Bit w set: the box around the splat's {power <= power_max} (half extents
-// `e`, computed with margin by the projection) overlaps the pixel centres of
-// warp w's 8x4 block of tile (tx, ty). A pair outside the box has computed
-// power above power_max, which the per-pixel path skips as well, so dropping
-// it changes nothing.
-__device__ __forceinline__ uint32_t warp_mask(float mx, float my, float2 e, uint32_t tx, uint32_t ty) {
-    const float bx = (float)(tx * 16) + 0.5f, by = (float)(ty * 16) + 0.5f;
-    const float lx = mx - e.x - bx, hxr = mx + e.x - bx;  // box relative to the tile's first centre
-    const float ly = my - e.y - by, hyr = my + e.y - by;
-    // columns [0,7] and [8,15]; rows [0,3], [4,7], [8,11], [12,15]
-    const uint32_t cx = (uint32_t)(lx <= 7.0f && hxr >= 0.0f) | ((uint32_t)(lx <= 15.0f && hxr >= 8.0f) << 1);
-    uint32_t m = 0;
-#pragma unroll
-    for (uint32_t r = 0; r < 4; ++r) {
-        const float y0 = (float)(r * 4);
-        if (ly <= y0 + 3.0f && hyr >= y0) m |= cx << (2 * r);
-    }
-    return m;
-}
-
-// rasterize_kernel (src/raster.rs:88-230). One 256-thread block per 16x16
-// tile; each warp owns an 8x4 pixel block. Chunks of 256 splat records are
-// staged in shared memory. Pairs whose power exceeds the splat's power_max
-// (alpha < 1/255 there, the reference's skip) bypass the exponential. The
-// tile stops once every pixel is saturated (T < 1/255).
-// CULL: each staged splat also gets an 8-bit mask of the warp blocks its
-// power_max box reaches (warp_mask) and a warp walks only its splats (and
-// stops once its own pixels are saturated) — fewer steps, more registers;
-// which form is faster depends on the scene, so both are kept.
-// DETAIL: per-pair diagnostic counters (evaluated / contributing / walked
-// pairs); off in the timed kernels.
-// Responsibility/evidence words are reduced per warp (redux.sync), then per
-// tile in shared memory, then added to global memory once per (tile, splat):
-// integer sums, so the words equal the reference's per-pixel atomics exactly.
-//
-// LAZY: the tile's list comes unsorted — the binned build's placed (depth
-// key, splat id) pairs — and is put in order here, slab by slab, only as far
-// as the tile needs: a 256-bin histogram over the 64-bit (key, id) values
-// left picks the longest run of bins holding at most kSlab entries (narrowing
-// the key interval while even the first bin holds more), those entries are
-// gathered and bitonic-sorted in shared memory and composited, and the next
-// slab starts after the last bin taken. (key, id) values are distinct and
-// slabs end on bin boundaries, so the composite order is exactly the sorted
-// list's; most tiles saturate inside their first slab, so most of the list is
-// never sorted. The stored per-pixel last-contributor index counts positions
-// in that order.
-
-constexpr uint32_t kSlab = 2048;
-constexpr uint32_t kFirstSlab = 256;
-
-struct RasterSmem {
-    float4* g0;
-    float4* g1;
-    float4* col;
-    uint32_t* gid;
-    uint32_t* acc0;
-    uint32_t* acc1;
-    uint8_t* mask;
-};
-
-struct PixelState {
-    float T, pr, pg, pb;
-    uint32_t last;
-    bool done;
-    uint32_t n_eval, n_hit, n_proc;
-};
-
-// Composites list entries [0, count) in order; id(i) gives entry i's splat
-// id, list_off the entry's offset in the tile's whole sorted list. Returns
-// true once every pixel of the tile is saturated (uniform).
-template <int MODE, bool CULL, bool DETAIL, typename IdOf>
-__device__ bool composite_list(const RasterArgs& a, const RasterSmem& sm, IdOf id, uint32_t count,
-                               uint32_t list_off, uint32_t tx, uint32_t ty, float fx, float fy, uint32_t inside,
-                               PixelState& ps) {
-    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    const float inv255 = 1.0f / 255.0f;
-    for (uint32_t chunk = 0; chunk < count; chunk += 256) {
-        __syncthreads();
-        const uint32_t idx = chunk + tid;
-        if (idx < count) {
-            const uint32_t g = id(idx);
-            const float4 g0 = a.geo0[g], g1 = a.geo1[g];
-            sm.g0[tid] = g0;
-            sm.g1[tid] = g1;
-            if (CULL) sm.mask[tid] = (uint8_t)warp_mask(g0.x, g0.y, a.ext[g], tx, ty);
-            if (MODE == 0) {
-                sm.col[tid] = a.color[g];
-            } else {
-                sm.gid[tid] = g;
-                sm.acc0[tid] = 0u;
-                if (MODE == 2) sm.acc1[tid] = 0u;
-            }
-        }
-        if (__syncthreads_count(ps.done) == 256) return true;
-        const uint32_t cnt = min(256u, count - chunk);
-        // One (warp, entry) step: every lane of the warp runs it together.
-        auto step = [&](uint32_t j) {
-            if (DETAIL) ++ps.n_proc;
-            uint32_t q = 0;
-            // CULL: a warp whose pixels are all done has left the chunk, so
-            // the power is formed unconditionally and one branch tests both.
-            // Otherwise a done warp skips the loads and arithmetic.
-            if (CULL || !ps.done) {
-                const float4 g0 = sm.g0[j];
-                const float4 g1 = sm.g1[j];
-                const float dx = g0.x - fx, dy = g0.y - fy;
-                const float power = fma_(g0.z * dx, dx, fma_(g1.x * dy, dy, (g0.w * dx) * dy));
-                if ((!CULL || !ps.done) && !(power > g1.z)) {
-                    if (DETAIL) ++ps.n_eval;
-                    const float alpha = fminf(g1.y * exp_neg_(-power), 0.999f);
-                    if (alpha >= inv255) {
-                        if (DETAIL) ++ps.n_hit;
-                        const float vis = alpha * ps.T;
-                        if (MODE == 0) {
-                            const float4 c = sm.col[j];
-                            ps.pr = fma_(c.x, vis, ps.pr);
-                            ps.pg = fma_(c.y, vis, ps.pg);
-                            ps.pb = fma_(c.z, vis, ps.pb);
-                        } else {
-                            q = sat_u32(vis * a.scale);
-                        }
-                        ps.T = ps.T * (1.0f - alpha);
-                        ps.last = list_off + chunk + j + 1;
-                        if (ps.T < inv255) ps.done = true;
-                    }
-                }
-            }
-            if (MODE == 1) {
-                const uint32_t s = __reduce_add_sync(0xffffffffu, q);
-                if (lane == 0 && s) atomicAdd(&sm.acc0[j], s);
-            } else if (MODE == 2) {
-                const uint32_t qf = inside ? q : 0u;
-                const uint32_t sf = __reduce_add_sync(0xffffffffu, qf);
-                const uint32_t sb = __reduce_add_sync(0xffffffffu, q - qf);
-                if (lane == 0) {
-                    if (sf) atomicAdd(&sm.acc0[j], sf);
-                    if (sb) atomicAdd(&sm.acc1[j], sb);
-                }
-            }
-        };
-        if (CULL) {
-            // This warp's entries of the chunk, 32 candidates per ballot;
-            // only entries with the warp's bit are walked, in list order.
-            for (uint32_t g32 = 0; g32 < cnt; g32 += 32) {
-                if (__all_sync(0xffffffffu, ps.done)) break;
-                uint32_t word = __ballot_sync(0xffffffffu,
-                                              g32 + lane < cnt && ((sm.mask[g32 + lane] >> warp) & 1u));
-                while (word) {
-                    const uint32_t j = g32 + (uint32_t)(__ffs(word) - 1);
-                    word &= word - 1u;
-                    step(j);
-                }
-            }
-        } else {
-            for (uint32_t j = 0; j < cnt; ++j) step(j);
-        }
-        if (MODE != 0) {
-            __syncthreads();
-            if (tid < cnt) {
-                const uint32_t g = sm.gid[tid];
-                if (MODE == 1) {
-                    if (sm.acc0[tid]) atomicAdd(a.resp + g, sm.acc0[tid]);
-                } else {
-                    if (sm.acc0[tid]) atomicAdd(a.fg + g, sm.acc0[tid]);
-                    if (sm.acc1[tid]) atomicAdd(a.bg + g, sm.acc1[tid]);
-                }
-            }
-        }
-    }
-    return false;
-}
-
-__device__ __forceinline__ unsigned long long pair_value(uint2 p) {
-    return ((unsigned long long)p.x << 32) | p.y;
-}
-
-// Block min / max of 64-bit values (uniform); s64 holds 2 * 8 words.
-__device__ void block_minmax64(unsigned long long lo, unsigned long long hi, unsigned long long* s64,
-                               unsigned long long& mn, unsigned long long& mx) {
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (uint32_t d = 16; d > 0; d >>= 1) {
-        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, d));
-        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, d));
-    }
-    __syncthreads();
-    if (lane == 0) {
-        s64[warp] = lo;
-        s64[8 + warp] = hi;
-    }
-    __syncthreads();
-    mn = s64[0];
-    mx = s64[8];
-    for (uint32_t w = 1; w < 8; ++w) {
-        mn = min(mn, s64[w]);
-        mx = max(mx, s64[8 + w]);
-    }
-    __syncthreads();
-}
-
-// Bitonic sort of v[0, m) ascending in shared memory (m <= kSlab), padded to
-// a power of two with the largest value.
-__device__ void bitonic_sort64(unsigned long long* v, uint32_t m) {
-    uint32_t p = 1;
-    while (p < m) p <<= 1;
-    for (uint32_t i = m + threadIdx.x; i < p; i += 256) v[i] = ~0ull;
-    __syncthreads();
-    for (uint32_t k = 2; k <= p; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < p; i += 256) {
-                const uint32_t ixj = i ^ j;
-                if (ixj > i) {
-                    const unsigned long long x = v[i], y = v[ixj];
-                    const bool up = (i & k) == 0;
-                    if ((x > y) == up) {
-                        v[i] = y;
-                        v[ixj] = x;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-}
-
-// One tile (block-uniform); the shared arrays are the kernel's.
-template <int MODE, bool CULL, bool DETAIL, bool LAZY>
-__device__ __forceinline__ void raster_tile(const RasterArgs& a, const uint32_t tile) {
-    __shared__ float4 s_g0[256];
-    __shared__ float4 s_g1[256];
-    __shared__ float4 s_col[MODE == 0 ? 256 : 1];
-    __shared__ uint32_t s_gid[MODE == 0 ? 1 : 256];
-    __shared__ uint32_t s_acc0[MODE == 0 ? 1 : 256];
-    __shared__ uint32_t s_acc1[MODE == 2 ? 256 : 1];
-    __shared__ uint8_t s_mask[256];
-    __shared__ unsigned long long s_slab[LAZY ? kSlab : 1];
-    __shared__ uint32_t s_hist[LAZY ? 256 : 1];
-    __shared__ unsigned long long s_64[16];
-    __shared__ uint32_t s_ctl[4];
-
-    const uint32_t tx = tile % a.tiles_x, ty = tile / a.tiles_x;
-    const uint32_t tid = threadIdx.x, lane = tid & 31u;
-    const uint32_t warp = tid >> 5;
-    const uint32_t px = tx * 16 + (warp & 1u) * 8 + (lane & 7u);
-    const uint32_t py = ty * 16 + (warp >> 1) * 4 + (lane >> 3);
-    const bool in_bounds = px < a.w && py < a.h;
-    const float fx = (float)px + 0.5f, fy = (float)py + 0.5f;
-    uint32_t inside = 0;
-    if (MODE == 2 && in_bounds) inside = (a.mask[px / 32 + py * a.mask_wpr] >> (px % 32)) & 1u;
-    const uint32_t start = a.tile_start[tile], end = a.tile_start[tile + 1];
-    const RasterSmem sm{s_g0, s_g1, s_col, s_gid, s_acc0, s_acc1, s_mask};
-    PixelState ps{1.0f, 0.0f, 0.0f, 0.0f, 0u, !in_bounds, 0u, 0u, 0u};
-
-    if (!LAZY || end - start <= a.lazy_min) {
-        const uint32_t* ids = a.gaussian_ids + start;
-        composite_list<MODE, CULL, DETAIL>(
-            a, sm, [&](uint32_t i) { return ids[i]; }, end - start, 0, tx, ty, fx, fy, inside, ps);
-    } else if (end > start) {
-        const uint2* pairs = a.pairs + start;
-        const uint32_t n = end - start;
-        unsigned long long lo = ~0ull, hi = 0;
-        for (uint32_t i = tid; i < n; i += 256) {
-            const unsigned long long v = pair_value(pairs[i]);
-            lo = min(lo, v);
-            hi = max(hi, v);
-        }
-        unsigned long long vmin, vmax;
-        block_minmax64(lo, hi, s_64, vmin, vmax);
-        auto slab_id = [&](uint32_t i) { return (uint32_t)s_slab[i]; };
-        if (n <= kFirstSlab) {
-            for (uint32_t i = tid; i < n; i += 256) s_slab[i] = pair_value(pairs[i]);
-            __syncthreads();
-            bitonic_sort64(s_slab, n);
-            composite_list<MODE, CULL, DETAIL>(a, sm, slab_id, n, 0, tx, ty, fx, fy, inside, ps);
-        } else {
-            unsigned long long cur = vmin;
-            uint32_t pos = 0;
-            // The first slab aims at kFirstSlab entries (most tiles saturate
-            // well inside it), later ones at the full kSlab.
-            uint32_t target = kFirstSlab;
-            for (;;) {
-                // Pick [cur, sel] holding at most `target` of the values left
-                // (one whole bin of up to kSlab when the first bin alone is
-                // past the target).
-                unsigned long long top = vmax, sel = vmax;
-                for (;;) {
-                    const unsigned long long width = top - cur;
-                    const uint32_t wbits = width == 0 ? 0u : 64u - (uint32_t)__clzll(width);
-                    const uint32_t shift = wbits > 8 ? wbits - 8 : 0u;
-                    s_hist[tid] = 0;
-                    __syncthreads();
-                    for (uint32_t i = tid; i < n; i += 256) {
-                        const unsigned long long v = pair_value(pairs[i]);
-                        if (v >= cur && v <= top) atomicAdd(&s_hist[(uint32_t)((v - cur) >> shift)], 1u);
-                    }
-                    __syncthreads();
-                    if (tid < 32) {
-                        // Warp 0: prefix over the 256 bins (8 per lane), the
-                        // last bin whose running total stays within target.
-                        const uint32_t nb = (uint32_t)(width >> shift) + 1u;
-                        uint32_t c[8], run = 0;
-#pragma unroll
-                        for (uint32_t q = 0; q < 8; ++q) {
-                            const uint32_t b = lane * 8 + q;
-                            c[q] = b < nb ? s_hist[b] : 0u;
-                            run += c[q];
-                        }
-                        uint32_t incl = run;
-#pragma unroll
-                        for (uint32_t d = 1; d < 32; d <<= 1) {
-                            const uint32_t x = __shfl_up_sync(0xffffffffu, incl, d);
-                            if (lane >= d) incl += x;
-                        }
-                        uint32_t acc = incl - run, best = 0u;
-                        bool any = false;
-#pragma unroll
-                        for (uint32_t q = 0; q < 8; ++q) {
-                            acc += c[q];
-                            const uint32_t b = lane * 8 + q;
-                            if (b < nb && acc <= target) {
-                                best = b;
-                                any = true;
-                            }
-                        }
-                        const uint32_t e = __reduce_max_sync(0xffffffffu, any ? best + 1u : 0u);
-                        if (lane == 0) {
-                            const uint32_t h0 = s_hist[0];
-                            // e == 0: even bin 0 is past the target.
-                            s_ctl[0] = e > 0 ? 1u : (h0 <= kSlab ? 1u : 0u);
-                            s_ctl[1] = e > 0 ? e - 1u : 0u;
-                            s_ctl[2] = nb;
-                        }
-                    }
-                    __syncthreads();
-                    const uint32_t e = s_ctl[1], bins = s_ctl[2];
-                    if (!s_ctl[0]) {
-                        // The first bin holds more than kSlab: narrow to it.
-                        top = cur + ((1ull << shift) - 1ull);
-                        continue;
-                    }
-                    sel = (e + 1 >= bins) ? top : cur + (((unsigned long long)(e + 1)) << shift) - 1ull;
-                    break;
-                }
-                if (tid == 0) s_ctl[3] = 0;
-                __syncthreads();
-                for (uint32_t i = tid; i < n; i += 256) {
-                    const unsigned long long v = pair_value(pairs[i]);
-                    if (v >= cur && v <= sel) s_slab[atomicAdd(&s_ctl[3], 1u)] = v;
-                }
-                __syncthreads();
-                const uint32_t m = s_ctl[3];
-                bitonic_sort64(s_slab, m);
-                if (composite_list<MODE, CULL, DETAIL>(a, sm, slab_id, m, pos, tx, ty, fx, fy, inside, ps))
-                    break;
-                pos += m;
-                if (sel == vmax) break;
-                cur = sel + 1;
-                target = kSlab;
-                __syncthreads();
-            }
-        }
-    }
-    if (a.stats) {
-        if (DETAIL) {
-            const uint32_t e = __reduce_add_sync(0xffffffffu, ps.n_eval);
-            const uint32_t c = __reduce_add_sync(0xffffffffu, ps.n_hit);
-            const uint32_t pr_ = __reduce_add_sync(0xffffffffu, ps.n_proc);
-            if (lane == 0) {
-                atomicAdd(a.stats + 1, (unsigned long long)e);
-                atomicAdd(a.stats + 2, (unsigned long long)c);
-                atomicAdd(a.stats + 3, (unsigned long long)pr_);
-            }
-        }
-        // Algorithmic pairs: 256 per entry of the sorted list that a walk
-        // in 256-entry chunks covers until every pixel is saturated — the
-        // entry that saturates the tile's last pixel, rounded up to a chunk
-        // (the whole list if a pixel never saturates). The same count for
-        // either list order.
-        const uint32_t n_list = end - start;
-        uint32_t e = ps.done ? ps.last : n_list;
-        e = __reduce_max_sync(0xffffffffu, e);
-        __syncthreads();
-        if (tid == 0) s_ctl[0] = 0;
-        __syncthreads();
-        if (lane == 0) atomicMax(&s_ctl[0], e);
-        __syncthreads();
-        if (tid == 0) {
-            const uint32_t emax = s_ctl[0];
-            const uint64_t chunks = ((uint64_t)emax + 255u) / 256u * 256u;
-            const uint64_t walked = chunks < n_list ? chunks : (uint64_t)n_list;
-            atomicAdd(a.stats, 256ull * walked);
-        }
-    }
-    if (!in_bounds) return;
-    const size_t pix = (size_t)py * a.w + px;
-    if (MODE == 0) {
-        if (a.bitmap) {
-            const uint32_t r = sat_u32(clamp_(ps.pr * 255.0f, 0.0f, 255.0f));
-            const uint32_t g = sat_u32(clamp_(ps.pg * 255.0f, 0.0f, 255.0f));
-            const uint32_t b = sat_u32(clamp_(ps.pb * 255.0f, 0.0f, 255.0f));
-            const uint32_t al = sat_u32(clamp_((1.0f - ps.T) * 255.0f, 0.0f, 255.0f));
-            a.bitmap[(size_t)py * a.row_stride + px] = r | (g << 8) | (b << 16) | (al << 24);
-        }
-        if (a.rgba) a.rgba[pix] = make_float4(ps.pr, ps.pg, ps.pb, 1.0f - ps.T);
-    }
-    if (a.final_t) a.final_t[pix] = ps.T;
-    if (a.n_contrib) a.n_contrib[pix] = ps.last;
-}
-
-// One block per tile: block i takes tile i, or with class lists the i-th
-// tile in longest-list-first order.
-template <int MODE, bool CULL, bool DETAIL, bool LAZY>
-__global__ __launch_bounds__(256) void raster_kernel(RasterArgs a) {
-    uint32_t tile = blockIdx.x;
-    if (a.class_lists) {
-        const uint32_t tiles = a.tiles_x * a.tiles_y;
-        uint32_t j = blockIdx.x;
-        int k = kSortClasses - 1;
-        for (; k >= 0; --k) {
-            const uint32_t c = a.class_n[k];
-            if (j < c) break;
-            j -= c;
-        }
-        // k < 0: the empty tiles (the counts sum to the tile count).
-        tile = a.class_lists[(size_t)(k < 0 ? kSortClasses : k) * tiles + j];
-    }
-    raster_tile<MODE, CULL, DETAIL, LAZY>(a, tile);
-}
-
 __global__ void export_rows_kernel(const float4* __restrict__ geo0, const float4* __restrict__ geo1,
                                    const float4* __restrict__ color,
                                    const uint32_t* __restrict__ keys, uint32_t n,
@@ -817,36 +388,6 @@ cudaError_t launch_tile_starts(const uint32_t* sorted_tile_ids, uint32_t num_ise
     const uint32_t grid_n = ((num_isects_dev ? max_isects : num_isects) + 1 + kStartItems - 1) / kStartItems;
     tile_start_kernel<<<(grid_n + 255) / 256, 256, 0, stream>>>(sorted_tile_ids, num_isects,
                                                                 num_isects_dev, num_tiles, tile_start);
-    note_launches(1);
-    return cudaGetLastError();
-}
-
-template <int MODE, bool LAZY>
-void raster_dispatch2(const RasterArgs& a, uint32_t tiles, cudaStream_t stream) {
-    if (a.cull) {
-        if (a.detail) raster_kernel<MODE, true, true, LAZY><<<tiles, 256, 0, stream>>>(a);
-        else raster_kernel<MODE, true, false, LAZY><<<tiles, 256, 0, stream>>>(a);
-    } else {
-        if (a.detail) raster_kernel<MODE, false, true, LAZY><<<tiles, 256, 0, stream>>>(a);
-        else raster_kernel<MODE, false, false, LAZY><<<tiles, 256, 0, stream>>>(a);
-    }
-}
-
-template <int MODE>
-void raster_dispatch(const RasterArgs& a, uint32_t tiles, cudaStream_t stream) {
-    if (a.pairs) raster_dispatch2<MODE, true>(a, tiles, stream);
-    else raster_dispatch2<MODE, false>(a, tiles, stream);
-}
-
-cudaError_t launch_raster(int mode, const RasterArgs& a, cudaStream_t stream) {
-    const uint32_t tiles = a.tiles_x * a.tiles_y;
-    if (tiles == 0) return cudaSuccess;
-    switch (mode) {
-        case 0: raster_dispatch<0>(a, tiles, stream); break;
-        case 1: raster_dispatch<1>(a, tiles, stream); break;
-        case 2: raster_dispatch<2>(a, tiles, stream); break;
-        default: return cudaErrorInvalidValue;
-    }
     note_launches(1);
     return cudaGetLastError();
 }

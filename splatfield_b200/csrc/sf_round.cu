@@ -77,6 +77,9 @@ struct RoundLane {
     uint32_t *tid_e = nullptr, *gid_e = nullptr, *tid_a = nullptr, *gid_a = nullptr;  // gid_a: tid_a + cap
     uint32_t* tile_start = nullptr;
     double* partials = nullptr;
+    // Adjoint round: the transmittance-only forward's per-pixel state.
+    float* final_t = nullptr;
+    uint32_t* n_contrib = nullptr;
     // Binned build: [chunks][max_tiles] histogram, per-tile totals, class lists.
     uint32_t* hist = nullptr;
     uint32_t* cnt = nullptr;
@@ -106,6 +109,12 @@ struct sf_round_t {
     uint32_t* resp = nullptr;       // [views][n]: total responsibility, or fg under masks
     uint32_t* bg = nullptr;         // [views][n]: bg under masks (allocated on first use)
     std::vector<const sf_mask_t*> masks;  // this round's per-view masks (empty: responsibility)
+    // Adjoint round: real-valued fg / bg responsibilities [views][n]
+    // (allocated on first use); masks may be null entries (all in fg).
+    bool adjoint = false;
+    float* afg = nullptr;
+    float* abg = nullptr;
+    uint64_t max_pixels = 0;
     uint32_t eig_blocks = 1;
     uint64_t want_cap = 0;
     // graph cache
@@ -116,7 +125,8 @@ struct sf_round_t {
     const void* g_splats = nullptr;
     const void* g_beta = nullptr;
     int g_mode = -1;
-    uint32_t g_lanes = 0, g_cull = 0, g_build = 0, g_order = 0;
+    int g_adjoint = -1;
+    uint32_t g_lanes = 0, g_cull = 0, g_build = 0, g_order = 0, g_split = 0;
     uint32_t chunks = 1;
     std::vector<const sf_mask_t*> g_masks;
 };
@@ -131,7 +141,7 @@ void lane_free(RoundLane& L) {
     L.scan_tmp = L.sort_tmp = nullptr;
     dfree(L.tid_e); dfree(L.gid_e); dfree(L.tid_a);
     L.gid_a = nullptr;
-    dfree(L.tile_start); dfree(L.partials);
+    dfree(L.tile_start); dfree(L.partials); dfree(L.final_t); dfree(L.n_contrib);
     dfree(L.hist); dfree(L.cnt); dfree(L.lists);
     sort_streams_destroy(&L.sort_streams);
     if (L.stream) cudaStreamDestroy(L.stream);
@@ -151,6 +161,8 @@ cudaError_t lane_alloc(sf_round_t* r, RoundLane& L, uint64_t cap) {
     L.gid_a = L.tid_a + cap;
     RA(L.tile_start, (size_t)r->max_tiles + 1);
     RA(L.partials, r->eig_blocks);
+    RA(L.final_t, r->max_pixels);
+    RA(L.n_contrib, r->max_pixels);
     if (r->max_tiles <= kBinMaxTiles) {
         RA(L.hist, (size_t)r->chunks * r->max_tiles);
         RA(L.cnt, (size_t)r->max_tiles + 1);
@@ -242,6 +254,7 @@ cudaError_t raster_and_eig(sf_round_t* r, RoundLane& L, uint32_t v, uint32_t tx,
     a.geo1 = L.geo1;
     a.ext = L.ext;
     a.cull = r->tuning.raster_cull;
+    a.split = r->tuning.raster_split;
     a.scale = (float)((uint64_t)1 << frac_bits(w, h));
     if (bg) {
         // Evidence: the mask splits each pixel's weights into fg / bg.
@@ -260,6 +273,55 @@ cudaError_t raster_and_eig(sf_round_t* r, RoundLane& L, uint32_t v, uint32_t tx,
                             r->eig_dev + v, st, bg)) != cudaSuccess)
             return e;
     }
+    return cudaSuccess;
+}
+
+// Adjoint round, view v: the transmittance-only raster keeps each pixel's
+// final T and last contributor, the feature adjoint replays them into the
+// view's real-valued fg / bg responsibilities, and the EIG reads fg + bg.
+cudaError_t adjoint_and_eig(sf_round_t* r, RoundLane& L, uint32_t v, uint32_t tx, uint32_t ty,
+                            const uint32_t* gids, const float* beta_a, const float* beta_b, const float* lut,
+                            int mode, cudaStream_t st) {
+    cudaError_t e;
+    const uint32_t n = r->n;
+    const uint32_t w = r->w[v], h = r->h[v];
+    float* fg = r->afg + (size_t)v * n;
+    float* bg = r->abg + (size_t)v * n;
+    const sf_mask_t* mask = r->masks.empty() ? nullptr : r->masks[v];
+    RasterArgs a{};
+    a.w = w;
+    a.h = h;
+    a.tiles_x = tx;
+    a.tiles_y = ty;
+    a.tile_start = L.tile_start;
+    a.gaussian_ids = gids;
+    a.geo0 = L.geo0;
+    a.geo1 = L.geo1;
+    a.ext = L.ext;
+    a.cull = r->tuning.raster_cull;
+    a.final_t = L.final_t;
+    a.n_contrib = L.n_contrib;
+    if ((e = launch_raster(3, a, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(fg, 0, (size_t)n * 4, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(bg, 0, (size_t)n * 4, st)) != cudaSuccess) return e;
+    FeatureBwdArgs f{};
+    f.w = w;
+    f.h = h;
+    f.tiles_x = tx;
+    f.tiles_y = ty;
+    f.tile_start = L.tile_start;
+    f.gaussian_ids = gids;
+    f.geo0 = L.geo0;
+    f.geo1 = L.geo1;
+    f.final_t = L.final_t;
+    f.n_contrib = L.n_contrib;
+    f.mask = mask ? mask->bits : nullptr;
+    f.mask_wpr = mask ? mask->wpr : 0u;
+    f.fg = fg;
+    f.bg = bg;
+    if ((e = launch_feature_bwd(f, st)) != cudaSuccess) return e;
+    if (beta_a)
+        return launch_eig_real(mode, beta_a, beta_b, fg, bg, n, lut, L.partials, r->eig_blocks, r->eig_dev + v, st);
     return cudaSuccess;
 }
 
@@ -294,7 +356,8 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
                                   pairs, words + 1, st)) != cudaSuccess)
             return e;
         if ((e = launch_clamp_starts(L.tile_start, tiles + 1, (uint32_t)L.cap, st)) != cudaSuccess) return e;
-        const uint32_t order = r->tuning.raster_order;
+        // The adjoint replays sorted lists: every class is sorted for it.
+        const uint32_t order = r->adjoint ? SF_ORDER_SORTED : r->tuning.raster_order;
         if (order != SF_ORDER_SORTED) lazy_pairs = pairs;
         if (order != SF_ORDER_IN_RASTER) {
             uint32_t grids[kSortClasses];
@@ -309,6 +372,7 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
         if ((e = depth_sorted_isects(r, L, n, tx, tiles, words, total, st, &tids, &gids)) != cudaSuccess)
             return e;
     }
+    if (r->adjoint) return adjoint_and_eig(r, L, v, tx, ty, gids, beta_a, beta_b, lut, mode, st);
     return raster_and_eig(r, L, v, tx, ty, gids, lazy_pairs, beta_a, beta_b, lut, mode, st);
 }
 
@@ -375,10 +439,12 @@ int build_graph(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, int
     r->g_splats = sp;
     r->g_beta = beta;
     r->g_mode = mode;
+    r->g_adjoint = (int)r->adjoint;
     r->g_lanes = (uint32_t)r->lanes.size();
     r->g_cull = r->tuning.raster_cull;
     r->g_build = r->tuning.isect_build;
     r->g_order = r->tuning.raster_order;
+    r->g_split = r->tuning.raster_split;
     r->g_masks = r->masks;
     return SF_OK;
 }
@@ -393,8 +459,10 @@ int run_round(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, const
             RF_CK(lanes_build(r, lanes, std::max<uint64_t>(r->want_cap, r->lanes.empty() ? 1024 : r->lanes[0].cap)));
         }
         if (!r->exec || r->g_splats != sp || r->g_beta != beta || r->g_mode != mode ||
+            r->g_adjoint != (int)r->adjoint ||
             r->g_cull != r->tuning.raster_cull || r->g_build != r->tuning.isect_build ||
-            r->g_order != r->tuning.raster_order || r->g_masks != r->masks) {
+            r->g_order != r->tuning.raster_order || r->g_split != r->tuning.raster_split ||
+            r->g_masks != r->masks) {
             const int rc = build_graph(r, sp, beta, mode);
             if (rc != SF_OK) return rc;
         }
@@ -459,8 +527,10 @@ int sf_round_create(sf_ctx ctx, uint32_t total, uint32_t n_views, const uint32_t
     r->views = n_views;
     r->w.assign(widths, widths + n_views);
     r->h.assign(heights, heights + n_views);
-    for (uint32_t v = 0; v < n_views; ++v)
+    for (uint32_t v = 0; v < n_views; ++v) {
         r->max_tiles = std::max(r->max_tiles, ((widths[v] + 15) / 16) * ((heights[v] + 15) / 16));
+        r->max_pixels = std::max<uint64_t>(r->max_pixels, (uint64_t)widths[v] * heights[v]);
+    }
     r->eig_blocks = eig_blocks(total, ctx->sm_count);
     r->chunks = bin_chunks(total, ctx->sm_count);
     r->tuning.lanes = 4;
@@ -488,6 +558,7 @@ int sf_round_destroy(sf_round r) {
     graph_drop(r);
     for (auto& L : r->lanes) lane_free(L);
     dfree(r->views_dev); dfree(r->words); dfree(r->eig_dev); dfree(r->resp); dfree(r->bg);
+    dfree(r->afg); dfree(r->abg);
     if (r->views_host) cudaFreeHost(r->views_host);
     if (r->words_host) cudaFreeHost(r->words_host);
     if (r->eig_host) cudaFreeHost(r->eig_host);
@@ -500,7 +571,8 @@ int sf_round_destroy(sf_round r) {
 int sf_round_set_tuning(sf_round r, const sf_round_tuning* t) {
     if (!r || !t) return rfail(SF_ERR_ARG, "null argument");
     if (t->raster_cull > 1 || t->lanes > 64 || t->isect_build > SF_ISECTS_DEPTH_SORTED ||
-        t->raster_order > SF_ORDER_HYBRID)
+        t->raster_order > SF_ORDER_HYBRID ||
+        (t->raster_split != 0 && t->raster_split != 1 && t->raster_split != 2 && t->raster_split != 4))
         return rfail(SF_ERR_ARG, "bad tuning");
     r->tuning = *t;
     return SF_OK;
@@ -522,6 +594,7 @@ int sf_round_eig(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, i
         if (beta && !eig) return rfail(SF_ERR_ARG, "null eig output");
         RF_CK(use_dev(r->device));
         r->masks.clear();
+        r->adjoint = false;
         const int rc = run_round(r, s, beta, cams, mode, reinterpret_cast<cudaStream_t>(stream));
         if (rc != SF_OK) return rc;
         if (beta) std::memcpy(eig, r->eig_host, 8 * r->views);
@@ -547,6 +620,7 @@ int sf_round_evidence(sf_round r, sf_splats s, sf_beta beta, const sf_camera* ca
         RF_CK(use_dev(r->device));
         if (!r->bg) RF_CK(dalloc(&r->bg, (size_t)r->views * r->n));
         r->masks.assign(masks, masks + r->views);
+        r->adjoint = false;
         const int rc = run_round(r, s, beta, cams, mode, reinterpret_cast<cudaStream_t>(stream));
         if (rc != SF_OK) return rc;
         if (beta) std::memcpy(eig, r->eig_host, 8 * r->views);
@@ -559,7 +633,7 @@ int sf_round_evidence(sf_round r, sf_splats s, sf_beta beta, const sf_camera* ca
 int sf_round_evidence_words(sf_round r, uint32_t view, const uint32_t** fg, const uint32_t** bg) {
     if (!r) return rfail(SF_ERR_ARG, "null round");
     if (view >= r->views) return rfail(SF_ERR_SHAPE, "no such view");
-    if (r->masks.empty()) return rfail(SF_ERR_ARG, "the last round had no masks");
+    if (r->masks.empty() || r->adjoint) return rfail(SF_ERR_ARG, "the last round was not a u32 evidence round");
     if (fg) *fg = r->resp + (size_t)view * r->n;
     if (bg) *bg = r->bg + (size_t)view * r->n;
     return SF_OK;
@@ -569,6 +643,7 @@ int sf_round_responsibility(sf_round r, uint32_t view, const uint32_t** resp, fl
                             uint64_t* num_isects, uint32_t* num_visible) {
     if (!r) return rfail(SF_ERR_ARG, "null round");
     if (view >= r->views) return rfail(SF_ERR_SHAPE, "no such view");
+    if (resp && r->adjoint) return rfail(SF_ERR_ARG, "the last round was an adjoint round (no words)");
     if (resp) *resp = r->resp + (size_t)view * r->n;
     if (scale) *scale = (float)((uint64_t)1 << frac_bits(r->w[view], r->h[view]));
     const uint32_t* w = r->words_host + 16 * view;
@@ -577,66 +652,162 @@ int sf_round_responsibility(sf_round r, uint32_t view, const uint32_t** resp, fl
     return SF_OK;
 }
 
-int sf_round_autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, int mode,
-                      sf_stream stream, sf_round_tuning* best, double* best_ms) {
+int sf_round_evidence_adjoint(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, const sf_mask* masks,
+                              int mode, sf_stream stream, double* eig) {
     try {
         if (!r || !s || !cams) return rfail(SF_ERR_ARG, "null argument");
+        if (s->n != r->n) return rfail(SF_ERR_SHAPE, "splat count differs from the round's");
+        if (beta && beta->n != r->n) return rfail(SF_ERR_SHAPE, "posterior size differs from the round's");
+        if (beta && mode != SF_EIG_LUT_F32 && mode != SF_EIG_FP64) return rfail(SF_ERR_ARG, "bad EIG mode");
+        if (beta && !eig) return rfail(SF_ERR_ARG, "null eig output");
+        if (masks)
+            for (uint32_t v = 0; v < r->views; ++v)
+                if (masks[v] && (masks[v]->w != r->w[v] || masks[v]->h != r->h[v]))
+                    return rfail(SF_ERR_SHAPE, "mask size does not match its view");
         RF_CK(use_dev(r->device));
-        const std::string key = tune_key(r);
-        {
-            std::lock_guard<std::mutex> g(g_tune_mu);
-            auto it = g_tune_cache.find(key);
-            if (it != g_tune_cache.end() && best_ms == nullptr) {
-                r->tuning = it->second;
-                if (best) *best = it->second;
-                return SF_OK;
-            }
+        if (!r->afg) RF_CK(dalloc(&r->afg, (size_t)r->views * r->n));
+        if (!r->abg) RF_CK(dalloc(&r->abg, (size_t)r->views * r->n));
+        if (masks) r->masks.assign(masks, masks + r->views);
+        else r->masks.clear();
+        r->adjoint = true;
+        const int rc = run_round(r, s, beta, cams, mode, reinterpret_cast<cudaStream_t>(stream));
+        if (rc != SF_OK) return rc;
+        if (beta) std::memcpy(eig, r->eig_host, 8 * r->views);
+        return SF_OK;
+    } catch (const std::bad_alloc&) {
+        return rfail(SF_ERR_NOMEM, "host allocation failed");
+    }
+}
+
+int sf_round_adjoint_responsibility(sf_round r, uint32_t view, const float** fg, const float** bg) {
+    if (!r) return rfail(SF_ERR_ARG, "null round");
+    if (view >= r->views) return rfail(SF_ERR_SHAPE, "no such view");
+    if (!r->adjoint || !r->afg) return rfail(SF_ERR_ARG, "the last round was not an adjoint round");
+    if (fg) *fg = r->afg + (size_t)view * r->n;
+    if (bg) *bg = r->abg + (size_t)view * r->n;
+    return SF_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// One round of the given kind (0 responsibility, 1 u32 evidence, 2 adjoint).
+int round_of_kind(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, const sf_mask* masks, int kind,
+                  int mode, sf_stream stream, double* eig) {
+    if (kind == SF_ROUND_EVIDENCE) return sf_round_evidence(r, s, beta, cams, masks, mode, stream, eig);
+    if (kind == SF_ROUND_ADJOINT) return sf_round_evidence_adjoint(r, s, beta, cams, masks, mode, stream, eig);
+    return sf_round_eig(r, s, beta, cams, mode, stream, eig);
+}
+
+// Coordinate search over the round's kernel forms: each dimension in turn
+// (lanes, intersection build, list order, raster culling, CTAs per tile),
+// each value timed as the best of three rounds after one warm-up round
+// (which also captures the graph), the best kept; two sweeps.
+int autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, const sf_mask* masks, int kind,
+             int mode, sf_stream stream, sf_round_tuning* best, double* best_ms) {
+    if (!r || !s || !cams) return rfail(SF_ERR_ARG, "null argument");
+    if (kind == SF_ROUND_EVIDENCE && !masks) return rfail(SF_ERR_ARG, "an evidence round needs masks");
+    RF_CK(use_dev(r->device));
+    const std::string key = tune_key(r) + "|kind" + std::to_string(kind);
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end() && best_ms == nullptr) {
+            r->tuning = it->second;
+            if (best) *best = it->second;
+            return SF_OK;
         }
-        cudaEvent_t e0, e1;
-        RF_CK(cudaEventCreate(&e0));
-        RF_CK(cudaEventCreate(&e1));
-        sf_round_tuning winner = r->tuning;
-        float winner_ms = 1e30f;
-        std::vector<double> eig(r->views);
-        const uint32_t lane_options[] = {1, 2, 4, 8};
-        const uint32_t orders = r->tuning.isect_build == SF_ISECTS_BINNED ? 3u : 1u;
-        for (uint32_t order = 0; order < orders; ++order)
-        for (uint32_t cull = 0; cull <= 1; ++cull)
-            for (uint32_t lanes : lane_options) {
-                if (lanes > r->views) continue;
-                sf_round_tuning t = r->tuning;
-                t.lanes = lanes;
-                t.raster_cull = cull;
-                if (orders == 3) t.raster_order = order;
-                r->tuning = t;
-                int rc = sf_round_eig(r, s, beta, cams, mode, stream, eig.data());  // warm-up / build
+    }
+    cudaEvent_t e0, e1;
+    RF_CK(cudaEventCreate(&e0));
+    RF_CK(cudaEventCreate(&e1));
+    std::vector<double> eig(r->views);
+    auto time_of = [&](const sf_round_tuning& t, float* out_ms) -> int {
+        r->tuning = t;
+        int rc = round_of_kind(r, s, beta, cams, masks, kind, mode, stream, eig.data());
+        if (rc != SF_OK) return rc;
+        float ms_best = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            RF_CK(cudaEventRecord(e0, r->main));
+            rc = round_of_kind(r, s, beta, cams, masks, kind, mode, stream, eig.data());
+            if (rc != SF_OK) return rc;
+            RF_CK(cudaEventRecord(e1, r->main));
+            RF_CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms_best = std::min(ms_best, ms);
+        }
+        *out_ms = ms_best;
+        return SF_OK;
+    };
+    sf_round_tuning winner = r->tuning;
+    if (winner.lanes == 0) winner.lanes = 4;
+    if (winner.raster_split == 0) winner.raster_split = 1;
+    if (kind == SF_ROUND_ADJOINT) winner.raster_order = SF_ORDER_SORTED;
+    float winner_ms = 1e30f;
+    int rc = time_of(winner, &winner_ms);
+    if (rc != SF_OK) return rc;
+    const std::vector<uint32_t> lanes_v = {1, 2, 4, 8}, build_v = {SF_ISECTS_BINNED, SF_ISECTS_DEPTH_SORTED},
+                                order_v = {SF_ORDER_SORTED, SF_ORDER_IN_RASTER, SF_ORDER_HYBRID}, cull_v = {0, 1},
+                                split_v = {1, 2, 4};
+    for (int sweep = 0; sweep < 2; ++sweep) {
+        for (int dim = 0; dim < 5; ++dim) {
+            const std::vector<uint32_t>& vals =
+                dim == 0 ? lanes_v : dim == 1 ? build_v : dim == 2 ? order_v : dim == 3 ? cull_v : split_v;
+            for (uint32_t val : vals) {
+                sf_round_tuning t = winner;
+                uint32_t* field = dim == 0 ? &t.lanes : dim == 1 ? &t.isect_build : dim == 2 ? &t.raster_order
+                                : dim == 3 ? &t.raster_cull : &t.raster_split;
+                if (*field == val) continue;
+                *field = val;
+                if (dim == 0 && val > r->views) continue;
+                // The orders apply to the binned build; the adjoint replays
+                // sorted lists, and its transmittance pass runs one CTA per tile.
+                if (dim == 2 && (t.isect_build != SF_ISECTS_BINNED || kind == SF_ROUND_ADJOINT)) continue;
+                if (dim == 4 && kind == SF_ROUND_ADJOINT) continue;
+                if (dim == 1 && val == SF_ISECTS_DEPTH_SORTED) t.raster_order = SF_ORDER_SORTED;
+                float ms = 0.f;
+                rc = time_of(t, &ms);
                 if (rc != SF_OK) return rc;
-                float ms_best = 1e30f;
-                for (int rep = 0; rep < 3; ++rep) {
-                    RF_CK(cudaEventRecord(e0, r->main));
-                    rc = sf_round_eig(r, s, beta, cams, mode, stream, eig.data());
-                    if (rc != SF_OK) return rc;
-                    RF_CK(cudaEventRecord(e1, r->main));
-                    RF_CK(cudaEventSynchronize(e1));
-                    float ms = 0.f;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                    ms_best = std::min(ms_best, ms);
-                }
-                if (ms_best < winner_ms) {
-                    winner_ms = ms_best;
+                if (ms < winner_ms) {
+                    winner_ms = ms;
                     winner = t;
                 }
             }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        r->tuning = winner;
-        {
-            std::lock_guard<std::mutex> g(g_tune_mu);
-            g_tune_cache[key] = winner;
         }
-        if (best) *best = winner;
-        if (best_ms) *best_ms = winner_ms;
-        return SF_OK;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    r->tuning = winner;
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        g_tune_cache[key] = winner;
+    }
+    if (best) *best = winner;
+    if (best_ms) *best_ms = winner_ms;
+    return SF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sf_round_autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, int mode,
+                      sf_stream stream, sf_round_tuning* best, double* best_ms) {
+    try {
+        return autotune(r, s, beta, cams, nullptr, SF_ROUND_RESPONSIBILITY, mode, stream, best, best_ms);
+    } catch (const std::bad_alloc&) {
+        return rfail(SF_ERR_NOMEM, "host allocation failed");
+    }
+}
+
+int sf_round_autotune_kind(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, const sf_mask* masks,
+                           int kind, int mode, sf_stream stream, sf_round_tuning* best, double* best_ms) {
+    try {
+        if (kind != SF_ROUND_RESPONSIBILITY && kind != SF_ROUND_EVIDENCE && kind != SF_ROUND_ADJOINT)
+            return rfail(SF_ERR_ARG, "unknown round kind");
+        return autotune(r, s, beta, cams, masks, kind, mode, stream, best, best_ms);
     } catch (const std::bad_alloc&) {
         return rfail(SF_ERR_NOMEM, "host allocation failed");
     }

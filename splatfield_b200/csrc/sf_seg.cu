@@ -151,6 +151,39 @@ __global__ __launch_bounds__(kEigThreads) void eig_kernel(const float* __restric
     if (threadIdx.x == 0) partials[blockIdx.x] = total;
 }
 
+// entropy_delta_kernel over real-valued responsibilities (the adjoint of a
+// per-splat scalar feature, sf_backward.cu): eps = fg + bg directly, with no
+// fixed-point scale; the LUT form adds in f32, the FP64 form in f64.
+template <int MODE>
+__global__ __launch_bounds__(kEigThreads) void eig_real_kernel(const float* __restrict__ a,
+                                                               const float* __restrict__ b,
+                                                               const float* __restrict__ fg,
+                                                               const float* __restrict__ bg, uint32_t n,
+                                                               const float* __restrict__ table,
+                                                               double* __restrict__ partials) {
+    __shared__ double s_warp[kEigThreads / 32];
+    double acc = 0.0;
+    const uint32_t stride = gridDim.x * kEigThreads;
+    for (uint32_t i = blockIdx.x * kEigThreads + threadIdx.x; i < n; i += stride) {
+        const float f = fg[i], g = bg ? bg[i] : 0.0f;
+        if (!(f + g > 0.0f)) continue;
+        const float ai = a[i], bi = b[i];
+        if (MODE == SF_EIG_LUT_F32) {
+            const float k = 1.0f + (f + g) / (ai + bi);
+            const float d = max_(table_entropy_d(ai, bi, table) - table_entropy_d(ai * k, bi * k, table), 0.0f);
+            acc += (double)d;
+        } else {
+            const double eps = (double)f + (double)g;
+            const double ad = ai, bd = bi;
+            const double k = 1.0 + eps / (ad + bd);
+            const double d = beta_entropy_d(ad, bd) - beta_entropy_d(ad * k, bd * k);
+            acc += d > 0.0 ? d : 0.0;
+        }
+    }
+    const double total = block_sum(acc, s_warp);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total;
+}
+
 __global__ __launch_bounds__(kEigThreads) void eig_final_kernel(const double* __restrict__ partials,
                                                                 uint32_t nb, double* out) {
     __shared__ double s_warp[kEigThreads / 32];
@@ -253,6 +286,15 @@ __global__ void beta_update_kernel(float scale, const uint32_t* __restrict__ fg,
     b[i] = b[i] + (float)bg[i] / scale;
 }
 
+// Conjugate update from real-valued responsibilities: a += fg, b += bg.
+__global__ void beta_update_real_kernel(const float* __restrict__ fg, const float* __restrict__ bg,
+                                        float* __restrict__ a, float* __restrict__ b, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    a[i] = a[i] + fg[i];
+    b[i] = b[i] + bg[i];
+}
+
 __global__ void table_probe_kernel(const float* a, const float* b, uint32_t n, const float* table,
                                    float* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -301,6 +343,26 @@ cudaError_t launch_eig(int mode, const float* a, const float* b, const uint32_t*
         eig_kernel<SF_EIG_FP64><<<blocks, kEigThreads, 0, stream>>>(a, b, resp, resp2, n, scale, table, partials);
     eig_final_kernel<<<1, kEigThreads, 0, stream>>>(partials, blocks, out);
     note_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_eig_real(int mode, const float* a, const float* b, const float* fg, const float* bg,
+                            uint32_t n, const float* table, double* partials, uint32_t blocks, double* out,
+                            cudaStream_t stream) {
+    if (mode == SF_EIG_LUT_F32)
+        eig_real_kernel<SF_EIG_LUT_F32><<<blocks, kEigThreads, 0, stream>>>(a, b, fg, bg, n, table, partials);
+    else
+        eig_real_kernel<SF_EIG_FP64><<<blocks, kEigThreads, 0, stream>>>(a, b, fg, bg, n, table, partials);
+    eig_final_kernel<<<1, kEigThreads, 0, stream>>>(partials, blocks, out);
+    note_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_beta_update_real(const float* fg, const float* bg, float* a, float* b, uint32_t n,
+                                    cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    beta_update_real_kernel<<<(n + 255) / 256, 256, 0, stream>>>(fg, bg, a, b, n);
+    note_launches(1);
     return cudaGetLastError();
 }
 

@@ -204,3 +204,39 @@ def opaque_attributes(positions) -> np.ndarray:
     a[7:10] = -2.0
     a[10] = 8.0
     return a.reshape(-1)
+
+
+# ---- the workloads' fixed draws (shared by the benchmark and the tests)
+
+ROUND_VIEWS, ROUND_SIDE, ROUND_RADIUS = 20, 512, 3.5
+
+
+def round_workload(n: int, make_look_at):
+    """The segmentation round on an n-splat scene: posterior a, b (seed 1),
+    20 cameras on a radius-3.5 sphere (seed 2), one 512x512 ellipse-union
+    mask per view (seeds 100 + v, bytes row-major)."""
+    a, b = beta_posterior(n, seed=1)
+    cams = sphere_cameras(ROUND_VIEWS, ROUND_RADIUS, 2, make_look_at)
+    masks = [ellipse_mask(ROUND_SIDE, ROUND_SIDE, seed=100 + v) for v in range(ROUND_VIEWS)]
+    return a, b, cams, masks
+
+
+UNEVEN_SPLATS, UNEVEN_SH, UNEVEN_VIEWS = 3_000_000, 4, 64
+
+
+def uneven_scene():
+    """3M splats, SH degree 1, clustered as the frame scene (seed 7)."""
+    return scene_clustered(UNEVEN_SPLATS, UNEVEN_SH, seed=7)
+
+
+def uneven_workload(make_look_at, views: int = UNEVEN_VIEWS):
+    """The uneven round's draws: per view a side from UNEVEN_SIDES, a camera
+    on the radius-3.5 sphere (seed 9) and an ellipse mask (seeds 300 + v);
+    posterior a, b (seed 5)."""
+    rng = np.random.default_rng(11)
+    sides = [int(x) for x in rng.choice(UNEVEN_SIDES, UNEVEN_VIEWS)][:views]
+    cams = sphere_cameras(UNEVEN_VIEWS, ROUND_RADIUS, 9, make_look_at)[:views]
+    masks = [ellipse_mask(s, s, seed=300 + v) for v, s in enumerate(sides)]
+    a, b = beta_posterior(UNEVEN_SPLATS, seed=5)
+    return sides, cams, masks, a, b
+

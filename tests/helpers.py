@@ -103,3 +103,49 @@ def cluster_scene():
         c, r = CLUSTER_CENTERS[i // PER_CLUSTER]
         pos.append(np.asarray(c, np.float32) + np.float32(1.4 * r) * jitter(i))
     return opaque(pos), CLUSTER_CENTERS
+
+
+# ---- GPU frame capture and comparison (used by the -m gpu modules)
+
+def gpu_frame(splats, scratch, cam, w, h, n):
+    """Every array of one GPU frame (prepare + RGB finalize with the float
+    plane), read back for comparison with the oracle's prepare/rasterize."""
+    import splatfield_b200 as sf
+    from splatfield_b200 import _lib as L
+
+    isects = splats.prepare_isects(scratch, cam, (w, h))
+    bitmap = splats.finalize_rgb(scratch, isects, (w, h), want_float=True).read()
+    rgba_f = sf.DeviceView(scratch.rgba_ptr(), np.float32, (h, w, 4)).read()
+    V, I = isects.num_visible, isects.num_isects
+    tiles = isects.tile_bounds[0] * isects.tile_bounds[1]
+    depth_sorted = scratch.get_tuning()["isect_build"] == sf.ISECTS_DEPTH_SORTED
+    return dict(
+        depth_keys=scratch.read(L.READ_DEPTH_KEYS, n),
+        tile_counts=scratch.read(L.READ_TILE_COUNTS, n),
+        bbox=scratch.read(L.READ_BBOX, 2 * n),
+        projected=scratch.read(L.READ_PROJECTED, 9 * n, np.float32).reshape(n, 9),
+        # The binned build keeps no depth order or offsets (they are not on
+        # its path); the depth-sorted build is checked on them.
+        order=scratch.read(L.READ_ORDER, V) if depth_sorted else None,
+        offsets=scratch.read(L.READ_OFFSETS, V) if depth_sorted else None,
+        tile_ids=isects.tile_ids().read(),
+        gaussian_ids=isects.gaussian_ids().read(),
+        tile_start=scratch.read(L.READ_TILE_START, tiles + 1),
+        bitmap=bitmap, rgba=rgba_f, num_visible=V, num_isects=I)
+
+
+def assert_frame_equal(got, want):
+    np.testing.assert_array_equal(got["depth_keys"], want["depth_keys"])
+    np.testing.assert_array_equal(got["tile_counts"], want["tile_counts"])
+    np.testing.assert_array_equal(got["bbox"], want["bbox"])
+    np.testing.assert_array_equal(got["projected"].view(np.uint32), want["projected"].view(np.uint32))
+    assert got["num_visible"] == want["num_visible"]
+    assert got["num_isects"] == want["num_isects"]
+    if got["order"] is not None:
+        np.testing.assert_array_equal(got["order"], want["order"])
+        np.testing.assert_array_equal(got["offsets"], want["offsets"])
+    np.testing.assert_array_equal(got["tile_ids"], want["tile_ids"])
+    np.testing.assert_array_equal(got["gaussian_ids"], want["gaussian_ids"])
+    ranges = want["ranges"]
+    np.testing.assert_array_equal(got["tile_start"][:-1], ranges[:, 0])
+    np.testing.assert_array_equal(got["tile_start"][1:], ranges[:, 1])

@@ -156,3 +156,100 @@ def test_backward_needs_matching_forward(ctx):
     splats.render_with(scratch, cam, (32, 32))
     with pytest.raises(sf.SplatfieldError):
         splats.render_backward(scratch, cam, (32, 32), dl)
+
+
+def _lift_bounds(real_scaled, words, pixels):
+    """The u32 lift truncates each pixel's share: scale * real - words lies in
+    [0, pixels touched] (f32 sums drift by ~1e-5 relative)."""
+    diff = real_scaled - words.astype(np.float64)
+    assert np.all(diff >= -1e-5 * real_scaled - 1.0)
+    assert np.all(diff <= 1e-5 * real_scaled + pixels + 1.0)
+
+
+def test_feature_adjoint_matches_u32_lift_colour_adjoint_and_fp64(ctx, oracle_mod):
+    """sf_render_feature_adjoint: the real-valued fg / bg responsibilities
+    (i) bound the u32 evidence words of the same frame as the truncation
+    allows, (ii) equal the colour adjoint of sf_render_backward with
+    dL/d(rgba) = (mask, 1 - mask, ., 0), and (iii) match the oracle's FP64
+    adjoint (the SH-DC gradient over the constant C0)."""
+    from splatfield_b200 import synth
+
+    n, w, h = 20000, 256, 192
+    attr, sh = synth.scene_uniform(n, 1, 41)
+    mask_b = synth.ellipse_mask(w, h, 41)
+    mask = mask_b.reshape(h, w).astype(np.float32)
+    pos = (0.2, -0.1, -2.6)
+    cam = sf.look_at(pos, (0.0, 0.0, 0.0))
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    m = sf.Mask.from_bytes((w, h), mask_b)
+    fg_d, bg_d = splats.render_feature_adjoint(scratch, cam, (w, h), m)
+    fg, bg = fg_d.read().astype(np.float64), bg_d.read().astype(np.float64)
+    acc = sf.Accumulators(n)
+    isects = splats.prepare_isects(scratch, cam, (w, h))
+    splats.accumulate_prepared(scratch, isects, (w, h), acc, m)
+    pixels = 256.0 * scratch.read(sf._lib.READ_TILE_COUNTS, n).astype(np.float64)
+    _lift_bounds(fg * acc.scale, acc.fg.read(), pixels)
+    _lift_bounds(bg * acc.scale, acc.bg.read(), pixels)
+    assert fg.sum() > 1.0 and bg.sum() > 1.0
+    # The RGB adjoint's colour entries for the same weights.
+    splats.render_forward(scratch, cam, (w, h))
+    dl = np.stack([mask, 1.0 - mask, np.zeros_like(mask), np.zeros_like(mask)], axis=-1)
+    _, _, proj = splats.render_backward(scratch, cam, (w, h), dl, want_proj=True)
+    np.testing.assert_allclose(fg, proj[:, 5], rtol=1e-4, atol=1e-5)
+    np.testing.assert_allclose(bg, proj[:, 6], rtol=1e-4, atol=1e-5)
+    # FP64 oracle: d L / d sh_dc[c] = C0 * (colour adjoint of channel c).
+    cam_o = oracle_mod.look_at(pos, (0.0, 0.0, 0.0))
+    _, d_sh = oracle_mod.render64_backward(cam_o, w, h, attr.astype(np.float64), sh.astype(np.float64), 1,
+                                           dl.astype(np.float64))
+    d_sh = d_sh.reshape(1, 3, n)
+    c0 = 0.2820948
+    for got, want in ((fg, d_sh[0, 0] / c0), (bg, d_sh[0, 1] / c0)):
+        err = np.linalg.norm(got - want) / np.linalg.norm(want)
+        assert err < 5e-3, err
+
+
+def test_round_adjoint_matches_plain_and_feeds_eig_and_update(ctx, oracle_mod):
+    """sf_round_evidence_adjoint over uneven views equals the plain per-view
+    feature adjoint (float sums: within 1e-5 relative), its EIG equals
+    sf_beta_eig_real of those responsibilities to the same precision, and
+    the FP64 EIG is within 1e-6 nats of the oracle's f64 formulas over the
+    same real eps; the real-valued Beta update adds fg / bg exactly."""
+    from splatfield_b200 import synth
+
+    n = 30000
+    attr, sh = synth.scene_clustered(n, 4, seed=5, clusters=4, sigma=0.25, extent=1.0)
+    a, b = synth.beta_posterior(n, seed=5)
+    splats = sf.Splats(attr, sh)
+    beta = sf.BetaState.from_host(a, b)
+    sizes = [(96, 96), (160, 128), (64, 48), (200, 200)]
+    cams = synth.sphere_cameras(len(sizes), 3.0, 7, sf.look_at)
+    masks = [sf.Mask.from_bytes(s, synth.ellipse_mask(s[0], s[1], 50 + v)) for v, s in enumerate(sizes)]
+    rnd = sf.Round(n, sizes)
+    for lanes, cull in ((1, 0), (3, 1)):
+        rnd.set_tuning(lanes=lanes, raster_cull=cull)
+        eig = rnd.evidence_adjoint(splats, beta, cams, masks, sf.EIG_FP64)
+        for v, s in enumerate(sizes):
+            scratch = sf.RenderScratch(n, s)
+            fg_p, bg_p = splats.render_feature_adjoint(scratch, cams[v], s, masks[v])
+            fg_r, bg_r = rnd.adjoint_responsibility(v)
+            np.testing.assert_allclose(fg_r.read(), fg_p.read(), rtol=1e-5, atol=1e-6)
+            np.testing.assert_allclose(bg_r.read(), bg_p.read(), rtol=1e-5, atol=1e-6)
+            e_plain = beta.eig_real(fg_r, bg_r, sf.EIG_FP64)
+            assert abs(eig[v] - e_plain) <= 1e-9 * max(1.0, abs(e_plain))
+            eps = fg_r.read().astype(np.float64) + bg_r.read().astype(np.float64)
+            want = 0.0
+            for ai, bi, e in zip(a, b, eps):
+                if e > 0:
+                    k = 1.0 + e / (float(ai) + float(bi))
+                    d = oracle_mod.beta_entropy(float(ai), float(bi)) - oracle_mod.beta_entropy(float(ai) * k,
+                                                                                              float(bi) * k)
+                    want += max(d, 0.0)
+            assert abs(eig[v] - want) <= 1e-6, (v, eig[v], want)
+    fg_r, bg_r = rnd.adjoint_responsibility(3)
+    beta.update_real(fg_r, bg_r)
+    a2, b2 = beta.read()
+    np.testing.assert_array_equal(a2, (a + fg_r.read()).astype(np.float32))
+    np.testing.assert_array_equal(b2, (b + bg_r.read()).astype(np.float32))
+    with pytest.raises(sf.SplatfieldError):
+        rnd.evidence_words(0)

@@ -9,51 +9,12 @@ import pytest
 
 import splatfield_b200 as sf
 from splatfield_b200 import _lib as L
-from helpers import (known_answers, opaque, rgba, sine_attributes, stacked_positions,
-                     yawed_rotation, zero_sh)
+from helpers import (assert_frame_equal, gpu_frame, known_answers, opaque, rgba, sine_attributes,
+                     stacked_positions, yawed_rotation, zero_sh)
 
 pytestmark = pytest.mark.gpu
 
 KA = known_answers()
-
-
-def gpu_frame(splats, scratch, cam, w, h, n):
-    isects = splats.prepare_isects(scratch, cam, (w, h))
-    bitmap = splats.finalize_rgb(scratch, isects, (w, h), want_float=True).read()
-    rgba_f = sf.DeviceView(scratch.rgba_ptr(), np.float32, (h, w, 4)).read()
-    V, I = isects.num_visible, isects.num_isects
-    tiles = isects.tile_bounds[0] * isects.tile_bounds[1]
-    depth_sorted = scratch.get_tuning()["isect_build"] == sf.ISECTS_DEPTH_SORTED
-    return dict(
-        depth_keys=scratch.read(L.READ_DEPTH_KEYS, n),
-        tile_counts=scratch.read(L.READ_TILE_COUNTS, n),
-        bbox=scratch.read(L.READ_BBOX, 2 * n),
-        projected=scratch.read(L.READ_PROJECTED, 9 * n, np.float32).reshape(n, 9),
-        # The binned build keeps no depth order or offsets (they are not on
-        # its path); the depth-sorted build is checked on them.
-        order=scratch.read(L.READ_ORDER, V) if depth_sorted else None,
-        offsets=scratch.read(L.READ_OFFSETS, V) if depth_sorted else None,
-        tile_ids=isects.tile_ids().read(),
-        gaussian_ids=isects.gaussian_ids().read(),
-        tile_start=scratch.read(L.READ_TILE_START, tiles + 1),
-        bitmap=bitmap, rgba=rgba_f, num_visible=V, num_isects=I)
-
-
-def assert_frame_equal(got, want):
-    np.testing.assert_array_equal(got["depth_keys"], want["depth_keys"])
-    np.testing.assert_array_equal(got["tile_counts"], want["tile_counts"])
-    np.testing.assert_array_equal(got["bbox"], want["bbox"])
-    np.testing.assert_array_equal(got["projected"].view(np.uint32), want["projected"].view(np.uint32))
-    assert got["num_visible"] == want["num_visible"]
-    assert got["num_isects"] == want["num_isects"]
-    if got["order"] is not None:
-        np.testing.assert_array_equal(got["order"], want["order"])
-        np.testing.assert_array_equal(got["offsets"], want["offsets"])
-    np.testing.assert_array_equal(got["tile_ids"], want["tile_ids"])
-    np.testing.assert_array_equal(got["gaussian_ids"], want["gaussian_ids"])
-    ranges = want["ranges"]
-    np.testing.assert_array_equal(got["tile_start"][:-1], ranges[:, 0])
-    np.testing.assert_array_equal(got["tile_start"][1:], ranges[:, 1])
 
 
 BUILDS = [sf.ISECTS_BINNED, sf.ISECTS_DEPTH_SORTED]
@@ -401,3 +362,44 @@ def test_render_frames_equals_render_with_and_counts_replays(ctx, oracle_mod):
     np.testing.assert_array_equal(last, splats.render_with(scratch, cams[-1], (w, h)).read())
     prep = oracle_mod.prepare(oracle_mod.look_at(poses[-1], (0.0, 0.0, 0.0)), w, h, attr, sh, 1)
     np.testing.assert_array_equal(last, oracle_mod.rasterize(prep, 0)["bitmap"])
+
+
+@pytest.mark.parametrize("split", [2, 4])
+@pytest.mark.parametrize("cull", [0, 1])
+@pytest.mark.parametrize("order", [sf.ORDER_SORTED, sf.ORDER_HYBRID, sf.ORDER_IN_RASTER])
+def test_split_tiles_give_the_same_frame_and_words(ctx, oracle_mod, split, cull, order):
+    """raster_split 2 / 4 (a tile's pixels over 2 or 4 CTAs, each walking the
+    whole list): RGBA8, responsibility and evidence words equal the oracle's
+    bit for bit, for sorted, hybrid and in-raster list order."""
+    from splatfield_b200 import synth
+
+    O = oracle_mod
+    n, w, h = 40000, 200, 136
+    attr, sh = synth.scene_uniform(n, 4, 17)
+    attr = attr.reshape(11, n)
+    attr[7:10] += 1.0  # larger splats: long, partly unsaturated lists
+    attr = attr.reshape(-1)
+    pos = (0.1, -0.2, -2.8)
+    cam, cam_o = sf.look_at(pos, (0.0, 0.0, 0.0)), O.look_at(pos, (0.0, 0.0, 0.0))
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    scratch.set_tuning(raster_cull=cull, raster_order=order, raster_split=split)
+    assert scratch.get_tuning()["raster_split"] == split
+    prep = O.prepare(cam_o, w, h, attr, sh, 4)
+    got = splats.render_with(scratch, cam, (w, h)).read()
+    np.testing.assert_array_equal(got, O.rasterize(prep, 0)["bitmap"])
+    acc = sf.Accumulators(n)
+    splats.render_responsibility(scratch, acc, cam, (w, h))
+    np.testing.assert_array_equal(acc.bits.read(), O.rasterize(prep, 1, scale=O.scale_for(w, h))["resp"])
+    mask = synth.ellipse_mask(w, h, 23)
+    isects = splats.prepare_isects(scratch, cam, (w, h))
+    splats.accumulate_prepared(scratch, isects, (w, h), acc, sf.Mask.from_bytes((w, h), mask))
+    fg, bg = O.evidence(prep, mask)
+    np.testing.assert_array_equal(acc.fg.read(), fg)
+    np.testing.assert_array_equal(acc.bg.read(), bg)
+
+
+def test_split_rejects_other_values(ctx):
+    scratch = sf.RenderScratch(10, (32, 32))
+    with pytest.raises(sf.SplatfieldError):
+        scratch.set_tuning(raster_split=3)

@@ -26,11 +26,11 @@ def cams_on_sphere(k, radius, seed):
     return synth.sphere_cameras(k, radius, seed, sf.look_at)
 
 
-@pytest.mark.parametrize("lanes,cull,build,order", [
-    (1, 0, sf.ISECTS_BINNED, sf.ORDER_IN_RASTER), (3, 0, sf.ISECTS_DEPTH_SORTED, sf.ORDER_IN_RASTER),
-    (4, 1, sf.ISECTS_BINNED, sf.ORDER_SORTED), (2, 1, sf.ISECTS_DEPTH_SORTED, sf.ORDER_SORTED),
-    (2, 1, sf.ISECTS_BINNED, sf.ORDER_IN_RASTER), (3, 0, sf.ISECTS_BINNED, sf.ORDER_HYBRID)])
-def test_round_matches_plain_per_view(ctx, lanes, cull, build, order):
+@pytest.mark.parametrize("lanes,cull,build,order,split", [
+    (1, 0, sf.ISECTS_BINNED, sf.ORDER_IN_RASTER, 1), (3, 0, sf.ISECTS_DEPTH_SORTED, sf.ORDER_IN_RASTER, 2),
+    (4, 1, sf.ISECTS_BINNED, sf.ORDER_SORTED, 4), (2, 1, sf.ISECTS_DEPTH_SORTED, sf.ORDER_SORTED, 1),
+    (2, 1, sf.ISECTS_BINNED, sf.ORDER_IN_RASTER, 4), (3, 0, sf.ISECTS_BINNED, sf.ORDER_HYBRID, 2)])
+def test_round_matches_plain_per_view(ctx, lanes, cull, build, order, split):
     n = 30000
     attr, sh = synth.scene_clustered(n, 4, seed=3, clusters=4, sigma=0.25, extent=1.0)
     a, b = synth.beta_posterior(n, seed=3)
@@ -39,7 +39,7 @@ def test_round_matches_plain_per_view(ctx, lanes, cull, build, order):
     sizes = [(64, 48), (128, 128), (96, 160), (70, 70), (33, 17)]
     cams = cams_on_sphere(len(sizes), 3.0, 5)
     rnd = sf.Round(n, sizes)
-    rnd.set_tuning(lanes=lanes, raster_cull=cull, isect_build=build, raster_order=order)
+    rnd.set_tuning(lanes=lanes, raster_cull=cull, isect_build=build, raster_order=order, raster_split=split)
     for mode in (sf.EIG_LUT_F32, sf.EIG_FP64):
         eig = rnd.eig(splats, beta, cams, mode)
         want = plain(splats, beta, cams, sizes, mode)
@@ -156,3 +156,47 @@ def test_round_evidence_matches_plain_masked_accumulate(ctx, lanes):
         rnd.evidence_words(0)
     with pytest.raises(sf.SplatfieldError):
         rnd.evidence(splats, beta, cams, masks[::-1], sf.EIG_LUT_F32)
+
+
+@pytest.mark.parametrize("kind", [sf.ROUND_RESPONSIBILITY, sf.ROUND_EVIDENCE, sf.ROUND_ADJOINT])
+def test_autotune_each_round_kind_keeps_results(ctx, kind):
+    """The coordinate search over lanes, build, order, culling and CTAs per
+    tile returns a valid tuning for each round kind, caches it, and the
+    tuned round's results equal the untuned round's (words bit for bit;
+    adjoint floats within 1e-5 relative)."""
+    n = 20000
+    attr, sh = synth.scene_clustered(n, 1, seed=9, clusters=3, sigma=0.3, extent=1.0)
+    a, b = synth.beta_posterior(n, seed=9)
+    splats = sf.Splats(attr, sh)
+    beta = sf.BetaState.from_host(a, b)
+    sizes = [(96, 96), (128, 64), (80, 80)]
+    cams = cams_on_sphere(len(sizes), 3.0, 21)
+    masks = [sf.Mask.from_bytes(s, synth.ellipse_mask(s[0], s[1], 70 + v)) for v, s in enumerate(sizes)]
+    rnd = sf.Round(n, sizes)
+
+    def run():
+        if kind == sf.ROUND_EVIDENCE:
+            e = rnd.evidence(splats, beta, cams, masks, sf.EIG_FP64)
+            return e, [np.concatenate([x.read() for x in rnd.evidence_words(v)]) for v in range(len(sizes))]
+        if kind == sf.ROUND_ADJOINT:
+            e = rnd.evidence_adjoint(splats, beta, cams, masks, sf.EIG_FP64)
+            return e, [np.concatenate([x.read() for x in rnd.adjoint_responsibility(v)]) for v in range(len(sizes))]
+        e = rnd.eig(splats, beta, cams, sf.EIG_FP64)
+        return e, [rnd.responsibility(v)[0].read() for v in range(len(sizes))]
+
+    e0, w0 = run()
+    tuning, ms = rnd.autotune(splats, beta, cams, sf.EIG_FP64, kind=kind, masks=masks)
+    assert ms > 0 and tuning["lanes"] in (1, 2, 4, 8) and tuning["raster_split"] in (1, 2, 4)
+    if kind == sf.ROUND_ADJOINT:
+        assert tuning["raster_order"] == sf.ORDER_SORTED
+    assert rnd.get_tuning() == tuning
+    e1, w1 = run()
+    for x, y in zip(w0, w1):
+        if kind == sf.ROUND_ADJOINT:
+            np.testing.assert_allclose(y, x, rtol=1e-5, atol=1e-6)
+        else:
+            np.testing.assert_array_equal(y, x)
+    if kind == sf.ROUND_ADJOINT:
+        np.testing.assert_allclose(e1, e0, rtol=1e-6)
+    else:
+        np.testing.assert_array_equal(e1, e0)

@@ -1,0 +1,241 @@
+"""The benchmark workloads themselves against the oracle, at their full sizes
+(GPU). Each test names the workload it checks:
+
+  small frame     100k SH0 splats uniform in [-1,1]^3, one 512x512 camera at
+                  (0,0,-3) with a 60-degree fov: intersection counts, depth
+                  order, scan offsets, sorted tile / splat ids, tile ranges
+                  and RGBA, bit for bit (both intersection builds); the float
+                  image against the FP64 twin, reported.
+  round           the 1M-splat SH3 scene, 20 views at 512x512 with
+                  ellipse-union masks: every view's fg / bg evidence words
+                  bit for bit, the LUT EIG equal to the oracle's LUT EIG, the
+                  FP64 EIG within 1e-6 nats of the oracle's f64 formulas; the
+                  LUT EIG's distance from the FP64 oracle is reported.
+  adjoint         L2 loss against the render of a perturbed copy: the full
+                  FP64 adjoint of a 10k-splat 128x128 subset, and 256 FP64
+                  central differences (h = 1e-4) on the 1M 1080p scene itself,
+                  each evaluated over the probed splat's tiles only.
+  uneven round    the 3M-splat SH1 scene: views of uneven sides, evidence words
+                  bit for bit and the FP64 EIG within 1e-6 nats.
+
+The oracle restates the reference's kernels (src/project.rs, src/raster.rs,
+src/render.rs, src/seg/mod.rs, src/seg/beta.rs) and is pinned to the
+reference's own known answers in tests/test_oracle_reference.py.
+"""
+import numpy as np
+import pytest
+
+import splatfield_b200 as sf
+from splatfield_b200 import synth
+from helpers import assert_frame_equal, gpu_frame
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def frame_scene():
+    return synth.scene_clustered(1_000_000, 16, seed=0)
+
+
+# ---------------------------------------------------------------- small frame
+
+@pytest.mark.parametrize("build", [sf.ISECTS_BINNED, sf.ISECTS_DEPTH_SORTED])
+def test_small_frame_100k_sh0_512_bit_exact(ctx, oracle_mod, build):
+    O = oracle_mod
+    n, k, w, h = 100_000, 1, 512, 512
+    attr, sh = synth.scene_uniform(n, k, 0)
+    cam_o = O.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    cam_o.fov[0], cam_o.fov[1] = synth.fov_for(w, h)
+    cam = sf.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    cam.fov[0], cam.fov[1] = synth.fov_for(w, h)
+    assert abs(cam.fov[0] - np.radians(60.0)) < 1e-6 and abs(cam.fov[1] - np.radians(60.0)) < 1e-6
+    want = O.prepare(cam_o, w, h, attr, sh, k)
+    wr = O.rasterize(want, 0)
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    scratch.set_tuning(isect_build=build)
+    got = gpu_frame(splats, scratch, cam, w, h, n)
+    assert got["num_isects"] > 100_000
+    assert_frame_equal(got, want)
+    np.testing.assert_array_equal(got["bitmap"], wr["bitmap"])
+    np.testing.assert_array_equal(got["rgba"].view(np.uint32), wr["rgba"].view(np.uint32))
+    # The FP32 image against the FP64 twin of the same forward (reported;
+    # pixels whose alpha / saturation decisions fall differently in f64 are
+    # the only ones past 2e-4).
+    ref = O.render64(cam_o, w, h, attr.astype(np.float64), sh.astype(np.float64), k)
+    err = np.abs(got["rgba"].astype(np.float64) - ref)
+    print(f"small frame vs FP64 twin: max abs {err.max():.3e}, "
+          f"fraction within 2e-4 {np.mean(err <= 2e-4):.6f}")
+    assert np.mean(err <= 2e-4) > 0.999
+
+
+# ---------------------------------------------------------------------- round
+
+def test_round_1m_20_views_512_evidence_and_eig_vs_oracle(ctx, oracle_mod, frame_scene):
+    O = oracle_mod
+    attr, sh = frame_scene
+    n, side = 1_000_000, synth.ROUND_SIDE
+    a, b, cams, mask_bytes = synth.round_workload(n, sf.look_at)
+    cams_o = synth.round_workload(1, O.look_at)[2]
+    splats = sf.Splats(attr, sh)
+    beta = sf.BetaState.from_host(a, b)
+    masks = [sf.Mask.from_bytes((side, side), m) for m in mask_bytes]
+    rnd = sf.Round(n, [(side, side)] * synth.ROUND_VIEWS)
+    rnd.set_tuning(lanes=8, raster_cull=1, raster_order=sf.ORDER_HYBRID)
+    eig_lut = rnd.evidence(splats, beta, cams, masks, sf.EIG_LUT_F32)
+    words = [(rnd.evidence_words(v)[0].read(), rnd.evidence_words(v)[1].read()) for v in range(len(cams))]
+    eig_f64 = rnd.evidence(splats, beta, cams, masks, sf.EIG_FP64)
+    scale = O.scale_for(side, side)
+    lut_vs_f64, f64_err = [], []
+    for v in range(len(cams)):
+        prep = O.prepare(cams_o[v], side, side, attr, sh, 16)
+        fg, bg = O.evidence(prep, mask_bytes[v])
+        np.testing.assert_array_equal(words[v][0], fg, err_msg=f"view {v} fg")
+        np.testing.assert_array_equal(words[v][1], bg, err_msg=f"view {v} bg")
+        eps = fg + bg
+        want_lut = O.eig(a, b, eps, scale, 0)
+        want_f64 = O.eig(a, b, eps, scale, 1)
+        assert abs(eig_lut[v] - want_lut) <= 1e-9 * max(1.0, abs(want_lut)), v
+        f64_err.append(abs(eig_f64[v] - want_f64))
+        lut_vs_f64.append(abs(eig_lut[v] - want_f64))
+    print(f"round EIG vs the FP64 oracle, max over 20 views: FP64 {max(f64_err):.3e} nats, "
+          f"LUT {max(lut_vs_f64):.3e} nats")
+    assert max(f64_err) <= 1e-6
+
+
+# -------------------------------------------------------------------- adjoint
+
+def _l2_grad(attr, sh, k, w, h, cam, target):
+    """GPU forward + adjoint of L = sum (rgba - target)^2."""
+    n = attr.size // 11
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    img = splats.render_forward(scratch, cam, (w, h)).read()
+    dl = (2.0 * (img.astype(np.float64) - target)).astype(np.float32)
+    d_attr, d_sh = splats.render_backward(scratch, cam, (w, h), dl)
+    return img, d_attr, d_sh
+
+
+def _target(attr, sh, n, w, h, cam):
+    """The render of the perturbed copy (means + N(0, 0.01), opacity logits
+    + N(0, 0.2)), the adjoint workload's target."""
+    tgt = sf.Splats(synth.perturbed(attr, n, seed=0), sh)
+    return tgt.render_forward(sf.RenderScratch(n, (w, h)), cam, (w, h)).read().astype(np.float64)
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_adjoint_10k_subset_128_full_fp64_gradient(ctx, oracle_mod, frame_scene):
+    O = oracle_mod
+    attr1m, sh1m = frame_scene
+    n, k, w, h = 10_000, 16, 128, 128
+    # The subset: every 100th splat of the scene, planes kept field-major.
+    attr = np.ascontiguousarray(attr1m.reshape(11, -1)[:, ::100][:, :n]).reshape(-1)
+    sh = np.ascontiguousarray(sh1m.reshape(3 * k, -1)[:, ::100][:, :n]).reshape(-1)
+    pos = (2.2, 0.4, -1.9)
+    cam = sf.look_at(pos, (0.0, 0.0, 0.0))
+    cam_o = O.look_at(pos, (0.0, 0.0, 0.0))
+    target = _target(attr, sh, n, w, h, cam)
+    img, d_attr, d_sh = _l2_grad(attr, sh, k, w, h, cam, target)
+    a64, s64 = attr.astype(np.float64), sh.astype(np.float64)
+    img64 = O.render64(cam_o, w, h, a64, s64, k)
+    ref_attr, ref_sh = O.render64_backward(cam_o, w, h, a64, s64, k, 2.0 * (img64 - target))
+    ref_attr, ref_sh = ref_attr.reshape(11, n), ref_sh.reshape(3 * k, n)
+    assert np.mean(np.abs(img - img64) <= 2e-4) > 0.999
+    groups = {"means": slice(0, 3), "quats": slice(3, 7), "log_scales": slice(7, 10), "opacity": slice(10, 11)}
+    report = {}
+    for name, sl in groups.items():
+        g, r = d_attr[sl], ref_attr[sl]
+        report[name] = rel_l2(g, r)
+        close = np.abs(g - r) <= 1e-3 * np.abs(r) + 1e-4 * np.abs(r).max()
+        assert close.mean() > 0.98, (name, close.mean())
+    report["sh"] = rel_l2(d_sh, ref_sh)
+    print("adjoint 10k subset, relative L2 error vs the FP64 adjoint:",
+          {k_: f"{v:.2e}" for k_, v in report.items()})
+    assert max(report.values()) < 5e-3, report
+    assert np.abs(ref_attr).max() > 1e-3
+
+
+def test_adjoint_1m_1080p_vs_fp64_central_differences(ctx, oracle_mod, frame_scene):
+    """256 random parameters of visible splats of the 1M 1080p scene: the GPU
+    gradient against FP64 central differences (h = 1e-4, stepping down where
+    the two sides disagree, i.e. a threshold lies inside the step) of the
+    oracle's FP64 forward, evaluated over the probed splat's tiles plus a
+    one-tile margin (the only pixels the splat reaches)."""
+    O = oracle_mod
+    attr, sh = frame_scene
+    n, k, w, h = 1_000_000, 16, 1920, 1080
+    cam = synth.orbit_cameras(30, 4.0, w, h, sf.look_at)[0]
+    cam_o = synth.orbit_cameras(30, 4.0, w, h, O.look_at)[0]
+    target = _target(attr, sh, n, w, h, cam)
+    _, d_attr, d_sh = _l2_grad(attr, sh, k, w, h, cam, target)
+    d_attr = d_attr.reshape(11, n)
+    d_sh = d_sh.reshape(3 * k, n)
+    probe = O.ProbeLoss(cam_o, w, h, attr, sh, k, target)
+    tx, ty = (w + 15) // 16, (h + 15) // 16
+    rng = np.random.default_rng(0xADC3)
+    picks = []
+    while len(picks) < 256:
+        i = int(rng.integers(n))
+        vis, bb = probe.bbox(i)
+        if not vis or bb[2] <= bb[0] or bb[3] <= bb[1]:
+            continue
+        picks.append((i, int(rng.integers(11 + 3 * k)), bb))
+    ok = checked = 0
+    worst = []
+    for i, param, bb in picks:
+        region = (max(bb[0] - 1, 0), max(bb[1] - 1, 0), min(bb[2] + 1, tx), min(bb[3] + 1, ty))
+        v0 = probe.base_value(i, param)
+        l0 = probe.loss(i, param, v0, region)
+        fd = None
+        for step in (1e-4, 1e-5, 1e-6):
+            lp = probe.loss(i, param, v0 + step, region)
+            lm = probe.loss(i, param, v0 - step, region)
+            if abs((lp - l0) - (l0 - lm)) <= 1e-3 * max(abs(lp - l0), abs(l0 - lm)) + 1e-12:
+                fd = (lp - lm) / (2 * step)
+                break
+        if fd is None:
+            continue
+        g = float(d_attr[param, i]) if param < 11 else float(d_sh[param - 11, i])
+        checked += 1
+        if abs(g - fd) <= 5e-3 * abs(fd) + 1e-6:
+            ok += 1
+        else:
+            worst.append((i, param, g, fd))
+    probe.close()
+    print(f"adjoint 1M 1080p: {ok} of {checked} probes within 5e-3 relative + 1e-6 of FP64 central "
+          f"differences; misses (splat, param, gpu, fd): {worst[:6]}")
+    assert checked >= 230
+    assert ok >= 0.97 * checked, (ok, checked, worst[:10])
+
+
+# --------------------------------------------------------------- uneven round
+
+def test_uneven_round_3m_sh1_views_vs_oracle(ctx, oracle_mod):
+    O = oracle_mod
+    attr, sh = synth.uneven_scene()
+    n = synth.UNEVEN_SPLATS
+    sides, cams, mask_bytes, a, b = synth.uneven_workload(sf.look_at)
+    cams_o = synth.uneven_workload(O.look_at)[1]
+    # One view of each side.
+    pick = [sides.index(s) for s in synth.UNEVEN_SIDES]
+    splats = sf.Splats(attr, sh)
+    beta = sf.BetaState.from_host(a, b)
+    masks = [sf.Mask.from_bytes((sides[v], sides[v]), mask_bytes[v]) for v in pick]
+    rnd = sf.Round(n, [(sides[v], sides[v]) for v in pick])
+    rnd.set_tuning(lanes=4, raster_cull=1, raster_order=sf.ORDER_HYBRID)
+    eig = rnd.evidence(splats, beta, [cams[v] for v in pick], masks, sf.EIG_FP64)
+    errs = []
+    for j, v in enumerate(pick):
+        s = sides[v]
+        prep = O.prepare(cams_o[v], s, s, attr, sh, synth.UNEVEN_SH)
+        fg, bg = O.evidence(prep, mask_bytes[v])
+        got_fg, got_bg = rnd.evidence_words(j)
+        np.testing.assert_array_equal(got_fg.read(), fg, err_msg=f"side {s} fg")
+        np.testing.assert_array_equal(got_bg.read(), bg, err_msg=f"side {s} bg")
+        errs.append(abs(eig[j] - O.eig(a, b, fg + bg, O.scale_for(s, s), 1)))
+    print(f"uneven round, FP64 EIG vs the FP64 oracle per side {list(synth.UNEVEN_SIDES)}: "
+          f"{[f'{e:.1e}' for e in errs]}")
+    assert max(errs) <= 1e-6
