@@ -441,9 +441,9 @@ int sf_round_adjoint_responsibility(sf_round r, uint32_t view, const float** fg,
  * depth-sorted}, raster_order {sorted, in-raster, hybrid} (binned build),
  * raster_cull {0,1} and raster_split {1,2,4} (rasterizer warps per CTA 8, 4
  * or 2 on 16x16 tiles), each candidate timed as the best of three rounds
- * after a warm-up round. The winner stays on the round and in a
- * process-wide cache keyed by (device, splats, view sizes, kind); a cached
- * shape is not re-timed unless best_ms is requested. sf_round_autotune
+ * after a warm-up round. The winner and its time stay on the round and in
+ * a process-wide cache keyed by (device, splats, view sizes, kind); a cached
+ * shape is not searched again (best_ms then gives the cached time). sf_round_autotune
  * tunes the responsibility round (sf_round_eig); sf_round_autotune_kind the
  * round of `kind`: SF_ROUND_RESPONSIBILITY, SF_ROUND_EVIDENCE
  * (sf_round_evidence with `masks`) or SF_ROUND_ADJOINT
@@ -470,6 +470,26 @@ int sf_ply_load_file(sf_ctx ctx, const char* path, sf_splats* out);
  * reports the byte length in *len; else writes it (cap >= *len). */
 int sf_ply_write(const float* attr, const float* sh, uint32_t n, uint32_t sh_per_ch, void* out,
                  size_t cap, size_t* len);
+
+/* --------------------------------------------------------- SOG scenes */
+/* parse_sog (src/sog.rs:97-198): a SOG archive (zip: meta.json + lossless
+ * WebP planes) to splats, with the reference's checks and messages
+ * ("not a SOG archive", "missing meta.json", "invalid meta.json", "SOG
+ * contains no splats", "missing <file>", "<file>: WxH < N pixels", codebook
+ * sizes, "quats: invalid rotation tag T", "shN.bands B outside 1..=3",
+ * "shN label L >= palette size P"); errors are SF_ERR_ARG. The planes are
+ * decoded on the host (zip stored / deflate entries, WebP lossless) and
+ * dequantised on the device into the field-major attribute and SH planes
+ * (sh_per_ch 1, 4, 9 or 16 for shN bands 0..3). sf_sog_inspect reads only
+ * meta.json (no CUDA call). */
+int sf_sog_inspect(const void* bytes, size_t len, uint32_t* n, uint32_t* sh_per_ch);
+int sf_sog_load(sf_ctx ctx, const void* bytes, size_t len, sf_splats* out);
+int sf_sog_load_file(sf_ctx ctx, const char* path, sf_splats* out);
+/* No counterpart in the reference (its SOG planes go through the `image`
+ * crate): the lossless WebP decoder the SOG loader uses, host only. Writes
+ * *w, *h and, when rgba is non-NULL and cap >= w * h * 4, the RGBA8 pixels
+ * row-major. Lossy WebP is refused (SF_ERR_ARG). */
+int sf_webp_decode(const void* bytes, size_t len, uint32_t* w, uint32_t* h, uint8_t* rgba, size_t cap);
 
 /* ------------------------------------------------------- sort / scan */
 /* bits_for (crates/sort/src/sort.rs:259-261). */

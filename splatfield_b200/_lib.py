@@ -171,6 +171,10 @@ SIGNATURES = {
         "sf_exclusive_scan": (i32, [P, P, u32, P]),
         "sf_exclusive_scan_gather_noalloc": (i32, [P, P, P, u32, P]),
         "sf_debug_lookback": (i32, [u32, i32]),
+        "sf_sog_inspect": (i32, [P, sz, P, P]),
+        "sf_sog_load": (i32, [P, P, sz, PP]),
+        "sf_sog_load_file": (i32, [P, C.c_char_p, PP]),
+        "sf_webp_decode": (i32, [P, sz, P, P, P, sz]),
         "sf_render_feature_adjoint": (i32, [P, P, P, u32, u32, P, P, P, P]),
         "sf_beta_eig_real": (i32, [P, P, P, i32, P, P]),
         "sf_beta_update_real": (i32, [P, P, P, P]),

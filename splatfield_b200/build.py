@@ -77,7 +77,7 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
                 if verbose and msg:
                     print(msg, flush=True)
     if todo or _mtime(LIB) < max(_mtime(o) for o in objs):
-        cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+        cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lz", "-lrt", "-ldl", "-lpthread"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -26,7 +26,7 @@ __all__ = [
     "RenderScratch", "TileIsects", "Accumulators", "Mask", "BetaState", "map_labels", "bits_for",
     "RadixScratch", "ScanScratch", "exclusive_scan_gather", "exclusive_scan_buf", "entropy_table",
     "table_entropy", "fractional_bits", "row_stride_for", "EIG_LUT_F32", "EIG_FP64", "Round",
-    "ISECTS_BINNED", "ISECTS_DEPTH_SORTED", "ORDER_IN_RASTER", "ORDER_SORTED", "ORDER_HYBRID", "SCHEDULE_LONGEST", "SCHEDULE_TILES", "ply_inspect", "load_ply",
+    "ISECTS_BINNED", "ISECTS_DEPTH_SORTED", "ORDER_IN_RASTER", "ORDER_SORTED", "ORDER_HYBRID", "SCHEDULE_LONGEST", "SCHEDULE_TILES", "ply_inspect", "load_ply", "sog_inspect", "load_sog", "webp_decode",
     "pinned_empty", "ROUND_RESPONSIBILITY", "ROUND_EVIDENCE", "ROUND_ADJOINT",
 ]
 
@@ -261,6 +261,38 @@ def load_ply(source, ctx: Context | None = None) -> "Splats":
     return Splats._adopt(h, ctx)
 
 
+def sog_inspect(data: bytes):
+    """parse_sog's meta.json checks (src/sog.rs:97-108, 151-159): (splat
+    count, SH coefficients per channel); raises SplatfieldError with the
+    reference's messages."""
+    buf = np.frombuffer(bytes(data), np.uint8)
+    n, k = C.c_uint32(), C.c_uint32()
+    check(lib().sf_sog_inspect(_vp(buf) if buf.size else None, buf.size, C.byref(n), C.byref(k)))
+    return int(n.value), int(k.value)
+
+
+def load_sog(source, ctx: Context | None = None) -> "Splats":
+    """parse_sog + upload (src/sog.rs:97-198): a path or the archive's bytes."""
+    ctx = ctx or default_context()
+    h = C.c_void_p()
+    if isinstance(source, (bytes, bytearray, memoryview)):
+        buf = np.frombuffer(bytes(source), np.uint8)
+        check(lib().sf_sog_load(ctx.handle, _vp(buf) if buf.size else None, buf.size, C.byref(h)))
+    else:
+        check(lib().sf_sog_load_file(ctx.handle, str(source).encode(), C.byref(h)))
+    return Splats._adopt(h, ctx)
+
+
+def webp_decode(data: bytes) -> np.ndarray:
+    """The lossless WebP decoder of the SOG loader: RGBA8 pixels [h, w, 4]."""
+    buf = np.frombuffer(bytes(data), np.uint8)
+    w, h = C.c_uint32(), C.c_uint32()
+    check(lib().sf_webp_decode(_vp(buf), buf.size, C.byref(w), C.byref(h), None, 0))
+    out = np.zeros((h.value, w.value, 4), np.uint8)
+    check(lib().sf_webp_decode(_vp(buf), buf.size, C.byref(w), C.byref(h), _vp(out), out.size))
+    return out
+
+
 class CpuSplats:
     """Host splat payload, field-major (src/render.rs:20-28)."""
 
@@ -405,13 +437,17 @@ class Splats:
         return out
 
     def render_feature_adjoint(self, scratch: "RenderScratch", camera: Camera, img_size, mask: "Mask | None" = None,
-                               stream=None):
+                               stream=None, out=None):
         """Real-valued (fg, bg) responsibilities [n] from the adjoint of a
         per-splat scalar feature (fg weighted by the mask, bg by its
-        complement; no mask: all in fg), as device buffers."""
+        complement; no mask: all in fg), as device buffers (new ones, or the
+        pair `out`)."""
         w, h = img_size
-        fg = DeviceBuffer.empty(self.n, np.float32, self.ctx)
-        bg = DeviceBuffer.empty(self.n, np.float32, self.ctx)
+        if out is not None:
+            fg, bg = out
+        else:
+            fg = DeviceBuffer.empty(self.n, np.float32, self.ctx)
+            bg = DeviceBuffer.empty(self.n, np.float32, self.ctx)
         check(lib().sf_render_feature_adjoint(self.handle, scratch.handle, C.byref(camera), w, h,
                                               mask.handle if mask is not None else None, _stream(stream),
                                               _vp(fg), _vp(bg)))

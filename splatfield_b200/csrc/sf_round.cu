@@ -496,7 +496,11 @@ int run_round(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, const
 
 // Process-wide autotuning cache: (device, splats, views, sizes) -> tuning.
 std::mutex g_tune_mu;
-std::map<std::string, sf_round_tuning> g_tune_cache;
+struct TuneEntry {
+    sf_round_tuning tuning;
+    float ms;
+};
+std::map<std::string, TuneEntry> g_tune_cache;
 
 std::string tune_key(const sf_round_t* r) {
     cudaDeviceProp prop;
@@ -713,9 +717,10 @@ int autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, const
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         auto it = g_tune_cache.find(key);
-        if (it != g_tune_cache.end() && best_ms == nullptr) {
-            r->tuning = it->second;
-            if (best) *best = it->second;
+        if (it != g_tune_cache.end()) {
+            r->tuning = it->second.tuning;
+            if (best) *best = it->second.tuning;
+            if (best_ms) *best_ms = it->second.ms;
             return SF_OK;
         }
     }
@@ -782,7 +787,7 @@ int autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, const
     r->tuning = winner;
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
-        g_tune_cache[key] = winner;
+        g_tune_cache[key] = TuneEntry{winner, winner_ms};
     }
     if (best) *best = winner;
     if (best_ms) *best_ms = winner_ms;
