@@ -185,7 +185,11 @@ typedef struct {
      * several SMs at once). The intersection tiles stay 16x16, so results
      * are unchanged. */
     uint32_t raster_split;
-    uint32_t reserved[2];
+    /* Digit width of the depth-sorted build's onesweep sorts, 4..8 bits per
+     * pass (0: 8). Same order either way; narrower digits take more passes
+     * with fewer bins each. */
+    uint32_t radix_bits;
+    uint32_t reserved[1];
 } sf_tuning;
 #define SF_ISECTS_BINNED 0u
 #define SF_ISECTS_DEPTH_SORTED 1u
@@ -396,7 +400,8 @@ typedef struct {
     uint32_t isect_build; /* as sf_tuning.isect_build */
     uint32_t raster_order; /* as sf_tuning.raster_order */
     uint32_t raster_split; /* as sf_tuning.raster_split */
-    uint32_t reserved[3];
+    uint32_t radix_bits;   /* as sf_tuning.radix_bits */
+    uint32_t reserved[2];
 } sf_round_tuning;
 int sf_round_create(sf_ctx ctx, uint32_t total, uint32_t n_views, const uint32_t* widths,
                     const uint32_t* heights, sf_round* out);
@@ -439,8 +444,9 @@ int sf_round_adjoint_responsibility(sf_round r, uint32_t view, const float** fg,
 /* Autotuner (the round's kernel forms picked by measured time): a
  * coordinate search, two sweeps, over lanes {1,2,4,8}, isect_build {binned,
  * depth-sorted}, raster_order {sorted, in-raster, hybrid} (binned build),
- * raster_cull {0,1} and raster_split {1,2,4} (rasterizer warps per CTA 8, 4
- * or 2 on 16x16 tiles), each candidate timed as the best of three rounds
+ * raster_cull {0,1}, raster_split {1,2,4} (rasterizer warps per CTA 8, 4
+ * or 2 on 16x16 tiles) and radix_bits {4,6,8} (sort digit width, depth-sorted
+ * build), each candidate timed as the best of three rounds
  * after a warm-up round. The winner and its time stay on the round and in
  * a process-wide cache keyed by (device, splats, view sizes, kind); a cached
  * shape is not searched again (best_ms then gives the cached time). sf_round_autotune
@@ -508,6 +514,10 @@ int sf_radix_destroy(sf_radix r);
 int sf_radix_argsort(sf_radix r, const uint32_t* keys, const uint32_t* vals, uint32_t n,
                      uint32_t bits, int write_keys, sf_stream stream, const uint32_t** keys_out,
                      const uint32_t** vals_out);
+/* Digit width of the scratch's passes, 4..8 bits (default 8; the
+ * reference's RADIX_BITS is 6, crates/sort/src/sort.rs:11-17). The order is
+ * the same at every width. */
+int sf_radix_set_digit_bits(sf_radix r, uint32_t digit_bits);
 /* ScanScratch::new (crates/sort/src/scan.rs:54-59). */
 int sf_scan_create(sf_ctx ctx, uint32_t max_elems, sf_scan* out);
 int sf_scan_destroy(sf_scan s);

@@ -57,14 +57,15 @@ class Tuning(C.Structure):
 
     _fields_ = [("raster_cull", C.c_uint32), ("isect_build", C.c_uint32), ("raster_detail", C.c_uint32),
                 ("raster_order", C.c_uint32), ("raster_schedule", C.c_uint32), ("raster_split", C.c_uint32),
-                ("reserved", C.c_uint32 * 2)]
+                ("radix_bits", C.c_uint32), ("reserved", C.c_uint32 * 1)]
 
 
 class RoundTuning(C.Structure):
     """sf_round_tuning."""
 
     _fields_ = [("lanes", C.c_uint32), ("raster_cull", C.c_uint32), ("isect_build", C.c_uint32),
-                ("raster_order", C.c_uint32), ("raster_split", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("raster_order", C.c_uint32), ("raster_split", C.c_uint32), ("radix_bits", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
 
 class Isects(C.Structure):
@@ -165,6 +166,7 @@ SIGNATURES = {
         "sf_radix_create": (i32, [P, u32, PP]),
         "sf_radix_destroy": (i32, [P]),
         "sf_radix_argsort": (i32, [P, P, P, u32, u32, i32, P, PP, PP]),
+        "sf_radix_set_digit_bits": (i32, [P, u32]),
         "sf_scan_create": (i32, [P, u32, PP]),
         "sf_scan_destroy": (i32, [P]),
         "sf_exclusive_scan_gather": (i32, [P, P, P, P, u32, P]),

@@ -564,13 +564,14 @@ class RenderScratch:
 
     def set_tuning(self, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED, raster_detail: int = 0,
                    raster_order: int = L.ORDER_SORTED, raster_schedule: int = L.SCHEDULE_LONGEST,
-                   raster_split: int = 1) -> None:
+                   raster_split: int = 1, radix_bits: int = 8) -> None:
         """Kernel forms (results are identical across forms): raster_cull 0/1,
         isect_build ISECTS_BINNED (default) or ISECTS_DEPTH_SORTED,
         raster_detail 1 to count the per-pair diagnostics of ``stats``,
         raster_order ORDER_SORTED (default), ORDER_IN_RASTER or ORDER_HYBRID,
         raster_schedule SCHEDULE_LONGEST (default) or SCHEDULE_TILES,
-        raster_split 1 (default), 2 or 4 rasterizer CTAs per tile."""
+        raster_split 1 (default), 2 or 4 rasterizer CTAs per tile,
+        radix_bits 4..8 (default 8) digit width of the depth-sorted build."""
         t = L.Tuning()
         t.raster_cull = int(raster_cull)
         t.isect_build = int(isect_build)
@@ -578,6 +579,7 @@ class RenderScratch:
         t.raster_order = int(raster_order)
         t.raster_schedule = int(raster_schedule)
         t.raster_split = int(raster_split)
+        t.radix_bits = int(radix_bits)
         check(lib().sf_scratch_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:
@@ -585,7 +587,8 @@ class RenderScratch:
         check(lib().sf_scratch_get_tuning(self.handle, C.byref(t)))
         return {"raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build),
                 "raster_detail": int(t.raster_detail), "raster_order": int(t.raster_order),
-                "raster_schedule": int(t.raster_schedule), "raster_split": int(t.raster_split) or 1}
+                "raster_schedule": int(t.raster_schedule), "raster_split": int(t.raster_split) or 1,
+                "radix_bits": int(t.radix_bits) or 8}
 
     def read(self, what: int, count: int, dtype=np.uint32, stream=None) -> np.ndarray:
         out = np.empty(count, dtype)
@@ -845,17 +848,19 @@ class Round:
         return len(self.sizes)
 
     def set_tuning(self, lanes: int = 4, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED,
-                   raster_order: int = L.ORDER_SORTED, raster_split: int = 1) -> None:
+                   raster_order: int = L.ORDER_SORTED, raster_split: int = 1, radix_bits: int = 8) -> None:
         t = L.RoundTuning()
         t.lanes, t.raster_cull, t.isect_build = int(lanes), int(raster_cull), int(isect_build)
         t.raster_order = int(raster_order)
         t.raster_split = int(raster_split)
+        t.radix_bits = int(radix_bits)
         check(lib().sf_round_set_tuning(self.handle, C.byref(t)))
 
     @staticmethod
     def _tuning_dict(t) -> dict:
         return {"lanes": int(t.lanes), "raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build),
-                "raster_order": int(t.raster_order), "raster_split": int(t.raster_split) or 1}
+                "raster_order": int(t.raster_order), "raster_split": int(t.raster_split) or 1,
+                "radix_bits": int(t.radix_bits) or 8}
 
     def get_tuning(self) -> dict:
         t = L.RoundTuning()
@@ -976,6 +981,10 @@ class RadixScratch:
         check(lib().sf_radix_create(self.ctx.handle, max_elems, C.byref(h)))
         self.handle = h
         self.max = max_elems
+
+    def set_digit_bits(self, digit_bits: int) -> None:
+        """Digit width of the passes, 4..8 bits (default 8)."""
+        check(lib().sf_radix_set_digit_bits(self.handle, int(digit_bits)))
 
     def argsort(self, keys, vals, n: int, bits: int, write_keys: bool = True, stream=None):
         ko, vo = C.c_void_p(), C.c_void_p()

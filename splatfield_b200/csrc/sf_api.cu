@@ -190,6 +190,7 @@ struct sf_scratch_t {
 struct sf_radix_t {
     sf_ctx ctx = nullptr;
     uint32_t max = 0;
+    uint32_t digit_bits = 8;
     uint32_t *ka = nullptr, *va = nullptr, *kb = nullptr, *vb = nullptr;
     void* tmp = nullptr;
     uint32_t* err = nullptr;
@@ -393,9 +394,10 @@ int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32
     s->binned = false;
     int in_b = 0;
     SF_CK(ensure_sort_tmp(s, radix_temp_bytes(n, 4)));
+    const uint32_t digit_bits = s->tuning.radix_bits ? s->tuning.radix_bits : 8u;
     SF_CK(radix_sort_pairs(s->depth_keys, nullptr, s->keys_a, s->order_a, s->keys_b, s->order_b, n,
                            nullptr, n, 32, false, true, s->sort_tmp, words + 1, s->ctx->sm_count, st,
-                           &in_b));
+                           &in_b, LookbackKnobs{0u, 0u}, digit_bits));
     s->order = in_b ? s->order_b : s->order_a;
     SF_CK(exclusive_scan(s->order, s->tile_counts, s->offsets, n, nullptr, n, s->scan_tmp, total_dev,
                          words + 1, st));
@@ -421,7 +423,8 @@ int prepare(sf_splats sp, sf_scratch s, const sf_camera* cam, uint32_t w, uint32
         s->gids = s->gid_e;
     } else {
         SF_CK(radix_sort_pairs(s->tid_e, s->gid_e, s->tid_a, s->gid_a, s->tid_e, s->gid_e, I, nullptr, I,
-                               tbits, true, false, s->sort_tmp, words + 1, s->ctx->sm_count, st, &in_b));
+                               tbits, true, false, s->sort_tmp, words + 1, s->ctx->sm_count, st, &in_b,
+                               LookbackKnobs{0u, 0u}, digit_bits));
         s->tids = in_b ? s->tid_e : s->tid_a;
         s->gids = in_b ? s->gid_e : s->gid_a;
     }
@@ -1050,6 +1053,8 @@ int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t) {
     if (t->raster_schedule > SF_SCHEDULE_TILES) return fail(SF_ERR_ARG, "unknown raster_schedule");
     if (t->raster_split != 0 && t->raster_split != 1 && t->raster_split != 2 && t->raster_split != 4)
         return fail(SF_ERR_ARG, "raster_split must be 1, 2 or 4");
+    if (t->radix_bits != 0 && (t->radix_bits < 4 || t->radix_bits > 8))
+        return fail(SF_ERR_ARG, "radix_bits must be 4..8 (0: 8)");
     s->tuning = *t;
     return SF_OK;
 }
@@ -1766,11 +1771,18 @@ int sf_radix_argsort(sf_radix r, const uint32_t* keys, const uint32_t* vals, uin
         int in_b = 0;
         SF_CK(radix_sort_pairs(keys, vals, r->ka, r->va, r->kb, r->vb, n, nullptr, n, bits,
                                write_keys != 0, vals == nullptr, r->tmp, r->err, r->ctx->sm_count,
-                               S(stream), &in_b, lookback_test_knobs()));
+                               S(stream), &in_b, lookback_test_knobs(), r->digit_bits));
         *keys_out = in_b ? r->kb : r->ka;
         *vals_out = in_b ? r->vb : r->va;
         return read_timeout_word(r->err, S(stream));
     })
+}
+
+int sf_radix_set_digit_bits(sf_radix r, uint32_t digit_bits) {
+    if (!r) return fail(SF_ERR_ARG, "null radix scratch");
+    if (digit_bits < 4 || digit_bits > 8) return fail(SF_ERR_ARG, "digit_bits must be 4..8");
+    r->digit_bits = digit_bits;
+    return SF_OK;
 }
 
 int sf_scan_create(sf_ctx ctx, uint32_t max_elems, sf_scan* out) {

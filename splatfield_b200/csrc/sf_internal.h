@@ -182,7 +182,8 @@ struct LookbackKnobs {
     uint32_t withhold;
 };
 LookbackKnobs lookback_test_knobs();
-uint32_t radix_passes(uint32_t bits);
+// Passes of an LSD sort of `bits` key bits at digit_bits per pass (4..8).
+uint32_t radix_passes(uint32_t bits, uint32_t digit_bits = 8);
 size_t radix_temp_bytes(uint32_t max_elems, uint32_t max_passes);
 // Sorts keys_in/vals_in by the low `bits` bits into the (a, b) ping-pong
 // buffers; *out_in_b tells which holds the result. n_dev (optional) supplies
@@ -191,7 +192,8 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
                              uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, uint32_t n,
                              const uint32_t* n_dev, uint32_t max_n, uint32_t bits, bool write_keys,
                              bool vals_iota, void* temp, uint32_t* err, int sm_count,
-                             cudaStream_t stream, int* out_in_b, LookbackKnobs knobs = {0u, 0u});
+                             cudaStream_t stream, int* out_in_b, LookbackKnobs knobs = {0u, 0u},
+                             uint32_t digit_bits = 8);
 size_t scan_temp_bytes(uint32_t max_elems);
 cudaError_t exclusive_scan(const uint32_t* gids, const uint32_t* counts, uint32_t* out, uint32_t n,
                            const uint32_t* n_dev, uint32_t max_n, void* temp,

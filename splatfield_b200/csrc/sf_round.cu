@@ -126,7 +126,7 @@ struct sf_round_t {
     const void* g_beta = nullptr;
     int g_mode = -1;
     int g_adjoint = -1;
-    uint32_t g_lanes = 0, g_cull = 0, g_build = 0, g_order = 0, g_split = 0;
+    uint32_t g_lanes = 0, g_cull = 0, g_build = 0, g_order = 0, g_split = 0, g_radix = 0;
     uint32_t chunks = 1;
     std::vector<const sf_mask_t*> g_masks;
 };
@@ -202,8 +202,10 @@ cudaError_t depth_sorted_isects(sf_round_t* r, RoundLane& L, uint32_t n, uint32_
                                 const uint32_t** tids_out, const uint32_t** gids_out) {
     cudaError_t e;
     int in_b = 0;
+    const uint32_t digit_bits = r->tuning.radix_bits ? r->tuning.radix_bits : 8u;
     if ((e = radix_sort_pairs(L.keys, nullptr, L.keys_a, L.order_a, L.keys_b, L.order_b, n, nullptr, n, 32,
-                              false, true, L.sort_tmp, words + 1, r->sm_count, st, &in_b)) != cudaSuccess)
+                              false, true, L.sort_tmp, words + 1, r->sm_count, st, &in_b, LookbackKnobs{0u, 0u},
+                              digit_bits)) != cudaSuccess)
         return e;
     const uint32_t* order = in_b ? L.order_b : L.order_a;
     if ((e = exclusive_scan(order, L.counts, L.offsets, n, nullptr, n, L.scan_tmp, total, words + 1, st)) !=
@@ -218,7 +220,7 @@ cudaError_t depth_sorted_isects(sf_round_t* r, RoundLane& L, uint32_t n, uint32_
     if (tbits > 0) {
         if ((e = radix_sort_pairs(L.tid_e, L.gid_e, L.tid_a, L.gid_a, L.tid_e, L.gid_e, 0, words + 2,
                                   (uint32_t)L.cap, tbits, true, false, L.sort_tmp, words + 1, r->sm_count, st,
-                                  &in_b)) != cudaSuccess)
+                                  &in_b, LookbackKnobs{0u, 0u}, digit_bits)) != cudaSuccess)
             return e;
         tids = in_b ? L.tid_e : L.tid_a;
         gids = in_b ? L.gid_e : L.gid_a;
@@ -445,6 +447,7 @@ int build_graph(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, int
     r->g_build = r->tuning.isect_build;
     r->g_order = r->tuning.raster_order;
     r->g_split = r->tuning.raster_split;
+    r->g_radix = r->tuning.radix_bits;
     r->g_masks = r->masks;
     return SF_OK;
 }
@@ -462,6 +465,7 @@ int run_round(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, const
             r->g_adjoint != (int)r->adjoint ||
             r->g_cull != r->tuning.raster_cull || r->g_build != r->tuning.isect_build ||
             r->g_order != r->tuning.raster_order || r->g_split != r->tuning.raster_split ||
+            r->g_radix != r->tuning.radix_bits ||
             r->g_masks != r->masks) {
             const int rc = build_graph(r, sp, beta, mode);
             if (rc != SF_OK) return rc;
@@ -576,7 +580,8 @@ int sf_round_set_tuning(sf_round r, const sf_round_tuning* t) {
     if (!r || !t) return rfail(SF_ERR_ARG, "null argument");
     if (t->raster_cull > 1 || t->lanes > 64 || t->isect_build > SF_ISECTS_DEPTH_SORTED ||
         t->raster_order > SF_ORDER_HYBRID ||
-        (t->raster_split != 0 && t->raster_split != 1 && t->raster_split != 2 && t->raster_split != 4))
+        (t->raster_split != 0 && t->raster_split != 1 && t->raster_split != 2 && t->raster_split != 4) ||
+        (t->radix_bits != 0 && (t->radix_bits < 4 || t->radix_bits > 8)))
         return rfail(SF_ERR_ARG, "bad tuning");
     r->tuning = *t;
     return SF_OK;
@@ -753,17 +758,18 @@ int autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, const
     float winner_ms = 1e30f;
     int rc = time_of(winner, &winner_ms);
     if (rc != SF_OK) return rc;
+    if (winner.radix_bits == 0) winner.radix_bits = 8;
     const std::vector<uint32_t> lanes_v = {1, 2, 4, 8}, build_v = {SF_ISECTS_BINNED, SF_ISECTS_DEPTH_SORTED},
                                 order_v = {SF_ORDER_SORTED, SF_ORDER_IN_RASTER, SF_ORDER_HYBRID}, cull_v = {0, 1},
-                                split_v = {1, 2, 4};
+                                split_v = {1, 2, 4}, radix_v = {4, 6, 8};
     for (int sweep = 0; sweep < 2; ++sweep) {
-        for (int dim = 0; dim < 5; ++dim) {
-            const std::vector<uint32_t>& vals =
-                dim == 0 ? lanes_v : dim == 1 ? build_v : dim == 2 ? order_v : dim == 3 ? cull_v : split_v;
+        for (int dim = 0; dim < 6; ++dim) {
+            const std::vector<uint32_t>& vals = dim == 0 ? lanes_v : dim == 1 ? build_v : dim == 2 ? order_v
+                                              : dim == 3 ? cull_v : dim == 4 ? split_v : radix_v;
             for (uint32_t val : vals) {
                 sf_round_tuning t = winner;
                 uint32_t* field = dim == 0 ? &t.lanes : dim == 1 ? &t.isect_build : dim == 2 ? &t.raster_order
-                                : dim == 3 ? &t.raster_cull : &t.raster_split;
+                                : dim == 3 ? &t.raster_cull : dim == 4 ? &t.raster_split : &t.radix_bits;
                 if (*field == val) continue;
                 *field = val;
                 if (dim == 0 && val > r->views) continue;
@@ -771,6 +777,8 @@ int autotune(sf_round r, sf_splats s, sf_beta beta, const sf_camera* cams, const
                 // sorted lists, and its transmittance pass runs one CTA per tile.
                 if (dim == 2 && (t.isect_build != SF_ISECTS_BINNED || kind == SF_ROUND_ADJOINT)) continue;
                 if (dim == 4 && kind == SF_ROUND_ADJOINT) continue;
+                // The digit width applies to the depth-sorted build's sorts.
+                if (dim == 5 && t.isect_build != SF_ISECTS_DEPTH_SORTED) continue;
                 if (dim == 1 && val == SF_ISECTS_DEPTH_SORTED) t.raster_order = SF_ORDER_SORTED;
                 float ms = 0.f;
                 rc = time_of(t, &ms);

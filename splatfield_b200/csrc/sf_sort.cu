@@ -24,8 +24,11 @@ namespace sfk {
 
 namespace {
 
+// Digit width: 4 to 8 bits (a template parameter of the kernels); the
+// scratch is laid out for the widest case, 256 bins, 4 passes of 32 bits.
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
+constexpr int kHistWords = 1024;  // passes x bins <= 1024 for every width
 constexpr int kThreads = 256;
 constexpr int kItems = 16;
 constexpr int kTile = kThreads * kItems;  // 4096 keys per partition
@@ -113,14 +116,16 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
-// Lanes holding the same 8-bit digit (and the same validity) as this lane:
-// one ballot per digit bit, inverted where this lane's bit is clear, ANDed.
-// Fixed cost of nine votes, far cheaper on this part than match.any.
+// Lanes holding the same BITS-bit digit (and the same validity) as this
+// lane: one ballot per digit bit, inverted where this lane's bit is clear,
+// ANDed. Fixed cost of BITS + 1 votes, far cheaper on this part than
+// match.any.
+template <int BITS>
 __device__ __forceinline__ uint32_t match_digit(uint32_t d, bool valid) {
     uint32_t peers = __ballot_sync(0xffffffffu, valid);
     if (!valid) peers = ~peers;
 #pragma unroll
-    for (int b = 0; b < kRadixBits; ++b) {
+    for (int b = 0; b < BITS; ++b) {
         const bool bit = (d >> b) & 1u;
         const uint32_t v = __ballot_sync(0xffffffffu, bit);
         peers &= bit ? v : ~v;
@@ -132,13 +137,15 @@ __device__ __forceinline__ uint32_t load_n(const uint32_t* n_dev, uint32_t n_sta
     return n_dev ? *n_dev : n_static;
 }
 
-// Upfront digit histograms: hist[pass * 256 + digit] over all n keys.
+// Upfront digit histograms: hist[pass * 2^BITS + digit] over all n keys.
+template <int BITS>
 __global__ __launch_bounds__(kThreads) void radix_histogram_kernel(
     const uint32_t* __restrict__ keys, const uint32_t* n_dev, uint32_t n_static,
     uint32_t num_passes, uint32_t bits, uint32_t* __restrict__ hist) {
-    __shared__ uint32_t s_hist[4 * kRadix];
+    constexpr uint32_t R = 1u << BITS;
+    __shared__ uint32_t s_hist[kHistWords];
     const uint32_t n = load_n(n_dev, n_static);
-    for (uint32_t i = threadIdx.x; i < num_passes * kRadix; i += kThreads) s_hist[i] = 0;
+    for (uint32_t i = threadIdx.x; i < num_passes * R; i += kThreads) s_hist[i] = 0;
     __syncthreads();
     // Whole warps iterate together (the bound is rounded up) so that runs of
     // equal digits in neighbouring lanes are merged before the shared atomic:
@@ -161,35 +168,37 @@ __global__ __launch_bounds__(kThreads) void radix_histogram_kernel(
         for (int u = 0; u < 4; ++u) {
             const bool valid = base + u * 32u + lane < n;
             for (uint32_t p = 0; p < num_passes; ++p) {
-                const uint32_t shift = p * kRadixBits;
-                const uint32_t w = bits - shift < (uint32_t)kRadixBits ? bits - shift : kRadixBits;
-                const uint32_t d = valid ? ((kk[u] >> shift) & ((1u << w) - 1u)) : (uint32_t)kRadix;
+                const uint32_t shift = p * BITS;
+                const uint32_t w = bits - shift < (uint32_t)BITS ? bits - shift : (uint32_t)BITS;
+                const uint32_t d = valid ? ((kk[u] >> shift) & ((1u << w) - 1u)) : R;
                 const uint32_t left = __shfl_up_sync(0xffffffffu, d, 1);
                 const bool head = lane == 0 || left != d;
                 const uint32_t heads = __ballot_sync(0xffffffffu, head);
                 if (valid && head) {
                     const uint32_t above = heads & ~((2u << lane) - 1u);
                     const uint32_t next = above ? (uint32_t)(__ffs(above) - 1) : 32u;
-                    atomicAdd(&s_hist[p * kRadix + d], next - lane);
+                    atomicAdd(&s_hist[p * R + d], next - lane);
                 }
             }
         }
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < num_passes * kRadix; i += kThreads)
+    for (uint32_t i = threadIdx.x; i < num_passes * R; i += kThreads)
         if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
 }
 
-// One 8-bit digit pass. `vals_iota` substitutes vals_in[i] = i.
+// One BITS-bit digit pass. `vals_iota` substitutes vals_in[i] = i.
+template <int BITS>
 __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, const uint32_t* n_dev,
     uint32_t n_static, uint32_t shift, uint32_t digit_mask, const uint32_t* __restrict__ pass_hist,
     uint32_t* lookback, uint32_t* ticket, uint32_t* err, int vals_iota, int write_keys, LookbackKnobs knobs) {
+    constexpr uint32_t R = 1u << BITS;
     __shared__ uint32_t s_part;
-    __shared__ uint32_t s_warp_hist[kWarps][kRadix];
-    __shared__ uint32_t s_local_start[kRadix];
-    __shared__ uint32_t s_global_base[kRadix];
+    __shared__ uint32_t s_warp_hist[kWarps][R];
+    __shared__ uint32_t s_local_start[R];
+    __shared__ uint32_t s_global_base[R];
     __shared__ uint32_t s_scan[kWarps];
     __shared__ uint32_t s_keys[kTile];
     __shared__ uint32_t s_vals[kTile];
@@ -198,7 +207,7 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
     const uint32_t n = load_n(n_dev, n_static);
     const uint32_t num_parts = (n + kTile - 1) / kTile;
     if (tid == 0) s_part = atomicAdd(ticket, 1u);
-    for (uint32_t i = tid; i < kWarps * kRadix; i += kThreads) (&s_warp_hist[0][0])[i] = 0;
+    for (uint32_t i = tid; i < kWarps * R; i += kThreads) (&s_warp_hist[0][0])[i] = 0;
     __syncthreads();
     const uint32_t part = s_part;
     if (part >= num_parts) return;
@@ -217,8 +226,8 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
     for (int i = 0; i < kItems; ++i) {
         const uint32_t idx = wbase + i * 32 + lane;
         const bool valid = idx < n;
-        const uint32_t d = valid ? ((k[i] >> shift) & digit_mask) : (uint32_t)kRadix;
-        const uint32_t peers = match_digit(d, valid);
+        const uint32_t d = valid ? ((k[i] >> shift) & digit_mask) : R;
+        const uint32_t peers = match_digit<BITS>(d, valid);
         const uint32_t leader = __ffs(peers) - 1;
         uint32_t prev = 0;
         if (valid && lane == leader) {
@@ -233,7 +242,7 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
 
     // Per digit: exclusive prefix over warps, block total, publish.
     uint32_t digit_total = 0;
-    if (tid < kRadix) {
+    if (tid < R) {
         uint32_t sum = 0;
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) {
@@ -243,7 +252,7 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
         }
         digit_total = sum;
         if (part > 0 || !knobs.withhold)
-            st_relaxed(&lookback[(size_t)part * kRadix + tid], (part == 0 ? kFlagPrefix : kFlagAgg) | sum);
+            st_relaxed(&lookback[(size_t)part * R + tid], (part == 0 ? kFlagPrefix : kFlagAgg) | sum);
     }
     // Block exclusive scan of digit totals (digit order) -> local starts.
     {
@@ -265,12 +274,12 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
             if (tid < (uint32_t)kWarps) s_scan[tid] = w;
         }
         __syncthreads();
-        if (tid < kRadix) s_local_start[tid] = v - digit_total + (warp ? s_scan[warp - 1] : 0u);
+        if (tid < R) s_local_start[tid] = v - digit_total + (warp ? s_scan[warp - 1] : 0u);
     }
     // Global digit offsets of this pass (exclusive over digits of pass_hist).
     uint32_t gstart = 0;
     {
-        const uint32_t h = tid < kRadix ? pass_hist[tid] : 0u;
+        const uint32_t h = tid < R ? pass_hist[tid] : 0u;
         uint32_t v = h;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -293,12 +302,12 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
         gstart = v - h + (warp ? s_scan[warp - 1] : 0u);
     }
     // Decoupled look-back, one digit per thread, kWindow predecessors per step.
-    if (tid < kRadix) {
+    if (tid < R) {
         uint32_t excl = 0;
         if (part > 0) {
-            excl = lookback_window<uint32_t>(lookback + tid, kRadix, part, kFlagPrefix, kCountMask, err,
+            excl = lookback_window<uint32_t>(lookback + tid, R, part, kFlagPrefix, kCountMask, err,
                                             knobs.spin_limit);
-            st_relaxed(&lookback[(size_t)part * kRadix + tid], kFlagPrefix | ((excl + digit_total) & kCountMask));
+            st_relaxed(&lookback[(size_t)part * R + tid], kFlagPrefix | ((excl + digit_total) & kCountMask));
         }
         s_global_base[tid] = gstart + excl - s_local_start[tid];
     }
@@ -425,45 +434,50 @@ __global__ __launch_bounds__(kThreads) void scan_kernel(
 
 }  // namespace
 
-uint32_t radix_passes(uint32_t bits) { return (bits + kRadixBits - 1) / kRadixBits; }
+uint32_t radix_passes(uint32_t bits, uint32_t digit_bits) { return (bits + digit_bits - 1) / digit_bits; }
 
 size_t radix_temp_bytes(uint32_t max_elems, uint32_t max_passes) {
     const size_t parts = (max_elems + kTile - 1) / kTile;
-    // hist [4][256] + tickets [4] + lookback [passes][parts][256]
-    return 4 * kRadix * 4 + 64 + (size_t)max_passes * parts * kRadix * 4;
+    // hist [1024] + tickets [16] + lookback [passes][parts][256]: 32-bit keys
+    // at 8-bit digits (4 passes x 256 bins) need the most, and every narrower
+    // digit (passes x bins <= 1024) fits the same space.
+    return kHistWords * 4 + 64 + (size_t)max_passes * parts * kRadix * 4;
 }
 
-cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_a,
-                             uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, uint32_t n,
-                             const uint32_t* n_dev, uint32_t max_n, uint32_t bits, bool write_keys,
-                             bool vals_iota, void* temp, uint32_t* err, int sm_count,
-                             cudaStream_t stream, int* out_in_b, LookbackKnobs knobs) {
-    const uint32_t passes = radix_passes(bits);
+namespace {
+
+template <int BITS>
+cudaError_t radix_sort_bits(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_a, uint32_t* vals_a,
+                            uint32_t* keys_b, uint32_t* vals_b, uint32_t n, const uint32_t* n_dev, uint32_t max_n,
+                            uint32_t bits, bool write_keys, bool vals_iota, void* temp, uint32_t* err,
+                            int sm_count, cudaStream_t stream, int* out_in_b, LookbackKnobs knobs) {
+    constexpr uint32_t R = 1u << BITS;
+    const uint32_t passes = radix_passes(bits, BITS);
     const uint32_t grid_n = n_dev ? max_n : n;
     uint8_t* t = static_cast<uint8_t*>(temp);
     uint32_t* hist = reinterpret_cast<uint32_t*>(t);
-    uint32_t* tickets = reinterpret_cast<uint32_t*>(t + 4 * kRadix * 4);
-    uint32_t* lookback = reinterpret_cast<uint32_t*>(t + 4 * kRadix * 4 + 64);
+    uint32_t* tickets = reinterpret_cast<uint32_t*>(t + kHistWords * 4);
+    uint32_t* lookback = reinterpret_cast<uint32_t*>(t + kHistWords * 4 + 64);
     const size_t parts = (grid_n + kTile - 1) / kTile;
-    cudaError_t e = cudaMemsetAsync(temp, 0, 4 * kRadix * 4 + 64 + passes * parts * kRadix * 4, stream);
+    cudaError_t e = cudaMemsetAsync(temp, 0, kHistWords * 4 + 64 + passes * parts * R * 4, stream);
     if (e != cudaSuccess) return e;
     if (parts == 0) { *out_in_b = 0; return cudaSuccess; }
     const uint32_t hist_blocks = (uint32_t)std::min<size_t>((grid_n + kThreads * 8 - 1) / (kThreads * 8),
                                                              (size_t)sm_count * 4);
-    radix_histogram_kernel<<<std::max(hist_blocks, 1u), kThreads, 0, stream>>>(
+    radix_histogram_kernel<BITS><<<std::max(hist_blocks, 1u), kThreads, 0, stream>>>(
         keys_in, n_dev, n, passes, bits, hist);
     const uint32_t* kin = keys_in;
     const uint32_t* vin = vals_in;
     int in_b = 0;
     for (uint32_t p = 0; p < passes; ++p) {
-        const uint32_t shift = p * kRadixBits;
-        const uint32_t w = std::min<uint32_t>(bits - shift, kRadixBits);
+        const uint32_t shift = p * BITS;
+        const uint32_t w = std::min<uint32_t>(bits - shift, BITS);
         uint32_t* kout = (p % 2 == 0) ? keys_a : keys_b;
         uint32_t* vout = (p % 2 == 0) ? vals_a : vals_b;
         const bool wk = write_keys || (p + 1 < passes);
-        onesweep_pass_kernel<<<(uint32_t)parts, kThreads, 0, stream>>>(
-            kin, vin, kout, vout, n_dev, n, shift, (1u << w) - 1u, hist + p * kRadix,
-            lookback + (size_t)p * parts * kRadix, tickets + p, err, (vals_iota && p == 0) ? 1 : 0,
+        onesweep_pass_kernel<BITS><<<(uint32_t)parts, kThreads, 0, stream>>>(
+            kin, vin, kout, vout, n_dev, n, shift, (1u << w) - 1u, hist + p * R,
+            lookback + (size_t)p * parts * R, tickets + p, err, (vals_iota && p == 0) ? 1 : 0,
             wk ? 1 : 0, knobs);
         kin = kout;
         vin = vout;
@@ -472,6 +486,28 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
     *out_in_b = in_b;
     note_launches(1 + passes);
     return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_a,
+                             uint32_t* vals_a, uint32_t* keys_b, uint32_t* vals_b, uint32_t n,
+                             const uint32_t* n_dev, uint32_t max_n, uint32_t bits, bool write_keys,
+                             bool vals_iota, void* temp, uint32_t* err, int sm_count,
+                             cudaStream_t stream, int* out_in_b, LookbackKnobs knobs, uint32_t digit_bits) {
+    switch (digit_bits) {
+#define SF_RADIX_CASE(B)                                                                                      \
+    case B:                                                                                                   \
+        return radix_sort_bits<B>(keys_in, vals_in, keys_a, vals_a, keys_b, vals_b, n, n_dev, max_n, bits,   \
+                                  write_keys, vals_iota, temp, err, sm_count, stream, out_in_b, knobs);
+        SF_RADIX_CASE(4)
+        SF_RADIX_CASE(5)
+        SF_RADIX_CASE(6)
+        SF_RADIX_CASE(7)
+        SF_RADIX_CASE(8)
+#undef SF_RADIX_CASE
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 size_t scan_temp_bytes(uint32_t max_elems) {

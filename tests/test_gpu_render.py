@@ -20,6 +20,26 @@ KA = known_answers()
 BUILDS = [sf.ISECTS_BINNED, sf.ISECTS_DEPTH_SORTED]
 
 
+@pytest.mark.parametrize("radix_bits", [6, 8])
+def test_depth_sorted_build_at_other_digit_widths(ctx, oracle_mod, radix_bits):
+    """The depth-sorted build's sorts at 6- and 8-bit digits: the same
+    depth order, offsets, tile lists and image as the oracle."""
+    from splatfield_b200 import synth
+
+    O = oracle_mod
+    n, k, w, h = 30000, 4, 200, 150
+    attr, sh = synth.scene_uniform(n, k, 5)
+    cam_o = O.look_at((0.1, 0.0, -3.0), (0.0, 0.0, 0.0))
+    cam = sf.look_at((0.1, 0.0, -3.0), (0.0, 0.0, 0.0))
+    want = O.prepare(cam_o, w, h, attr, sh, k)
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    scratch.set_tuning(isect_build=sf.ISECTS_DEPTH_SORTED, radix_bits=radix_bits)
+    got = gpu_frame(splats, scratch, cam, w, h, n)
+    assert_frame_equal(got, want)
+    np.testing.assert_array_equal(got["bitmap"], O.rasterize(want, 0)["bitmap"])
+
+
 @pytest.mark.parametrize("build", BUILDS)
 @pytest.mark.parametrize("cull", [0, 1])
 @pytest.mark.parametrize("n,k,w,h,seed", [

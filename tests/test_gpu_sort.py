@@ -124,3 +124,21 @@ def test_scan_zero(ctx):
     offsets = sf.DeviceBuffer.from_array(np.array([0xDEADBEEF], np.uint32))
     sf.exclusive_scan_gather(gids, counts, offsets, 0, sf.ScanScratch(1))
     assert offsets.read()[0] == 0xDEADBEEF
+
+
+@pytest.mark.parametrize("digit_bits", [4, 5, 6, 7, 8])
+@pytest.mark.parametrize("bits", [5, 13, 32])
+def test_every_digit_width_sorts_stably(ctx, digit_bits, bits):
+    """sf_radix_set_digit_bits: 4..8-bit digits (the reference's is 6,
+    sort.rs:11-17) give numpy's stable argsort, at key widths that are and
+    are not multiples of the digit."""
+    rng = np.random.default_rng(0x5EED0100 + digit_bits * 64 + bits)
+    n = 300_001
+    keys = rng.integers(0, 2**bits, n, dtype=np.uint64).astype(np.uint32)
+    dk = sf.DeviceBuffer.from_array(keys)
+    scratch = sf.RadixScratch(n)
+    scratch.set_digit_bits(digit_bits)
+    ko, vo = scratch.argsort(dk, None, n, bits)
+    order = np.argsort(keys, kind="stable").astype(np.uint32)
+    np.testing.assert_array_equal(vo.read(), order)
+    np.testing.assert_array_equal(ko.read(), keys[order])
