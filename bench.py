@@ -659,6 +659,14 @@ def run_ours(args, rank, world):
     stream = torch.cuda.current_stream()
     size = (WIDTH, HEIGHT)
 
+    # The raster form (culling, CTAs per tile, list order, block schedule)
+    # picked by the frame autotuner on this rank's camera path (untimed; the
+    # images are the same in every form).
+    if args.tuning:
+        scratch.set_tuning(**json.loads(args.tuning))
+        frame_tuning = scratch.get_tuning()
+    else:
+        frame_tuning, _ = scratch.autotune(splats, my_cams[:N_CAMS], size, stream=stream)
     for i in range(max(args.warmup, 3)):
         splats.render_with(scratch, my_cams[i % N_CAMS], size, stream=stream)
     torch.cuda.synchronize()
@@ -668,6 +676,7 @@ def run_ours(args, rank, world):
             splats.render_with(scratch, my_cams[i % N_CAMS], size, stream=stream)
         torch.cuda.synchronize()
         if rank == 0:
+            print(json.dumps({"frame_tuning": frame_tuning}), flush=True)
             print(json.dumps({"frames_only": args.steps, "kernels_per_frame":
                               (_lib.lib().sf_kernel_launches()) / (args.steps + max(args.warmup, 3))}))
         return
@@ -710,14 +719,14 @@ def run_ours(args, rank, world):
     raster_ms = float(np.mean(rast_ms))
     pairs = stats["pairs_visited"] / n_split
     # Per-pair diagnostics from the counting form of the rasterizer (untimed).
-    scratch.set_tuning(raster_detail=1)
+    scratch.set_tuning(**{**frame_tuning, "raster_detail": 1})
     detail = None
     for i in range(n_split):
         isects = splats.prepare_isects(scratch, my_cams[i % N_CAMS], size, stream=stream)
         splats.finalize_rgb(scratch, isects, size, stream=stream)
         st = scratch.stats(stream)
         detail = st if detail is None else {k: detail[k] + st[k] for k in st}
-    scratch.set_tuning()
+    scratch.set_tuning(**frame_tuning)
     achieved = pairs * RASTER_FLOPS_PER_PAIR / (raster_ms / 1e3) / 1e12
 
     # ---- end to end through the host-facing calls: the camera path in
@@ -770,6 +779,7 @@ def run_ours(args, rank, world):
         "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(world),
+        "frame_tuning": frame_tuning,
         "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": 36,
                 "d2h_bytes_per_step": WIDTH * HEIGHT * 4,
                 "path": f"sf_render_frames_to_host ({N_CAMS}-camera path per call, camera by value, each RGBA8 "
@@ -813,6 +823,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames-only", action="store_true",
                     help="render warmup + steps frames and exit (for profilers)")
+    ap.add_argument("--tuning", default="",
+                    help="frame raster form as JSON (sf_tuning fields) instead of the frame autotuner's pick")
     ap.add_argument("--round-only", action="store_true",
                     help="run warmup + steps batched segmentation rounds (autotuned forms) and exit "
                          "(for profilers)")

@@ -200,6 +200,14 @@ typedef struct {
 #define SF_SCHEDULE_TILES 1u
 int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t);
 int sf_scratch_get_tuning(sf_scratch s, sf_tuning* t);
+/* Frame autotuner (no counterpart in the reference): times sf_render_frames
+ * over cams[count] at w x h for each raster form in a coordinate search (two
+ * sweeps over raster_cull {0,1}, raster_split {1,2,4}, raster_order {sorted,
+ * hybrid, in-raster} and raster_schedule {longest, tiles}; best of three
+ * paths after a warm-up path), keeps the fastest on the scratch and returns
+ * it with its time per frame. Images are the same in every form. */
+int sf_scratch_autotune(sf_splats s, sf_scratch scratch, const sf_camera* cams, uint32_t count, uint32_t w,
+                        uint32_t h, sf_stream stream, sf_tuning* best, double* best_ms);
 
 /* ---------------------------------------------------------------- render */
 /* Splats::render_with (src/render.rs:371-380): one RGBA8 frame. Syncs once

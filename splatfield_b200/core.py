@@ -582,6 +582,17 @@ class RenderScratch:
         t.radix_bits = int(radix_bits)
         check(lib().sf_scratch_set_tuning(self.handle, C.byref(t)))
 
+    def autotune(self, splats: "Splats", cameras, img_size, stream=None) -> tuple:
+        """Pick the raster form by measured time on a camera path (same images
+        in every form); returns (tuning, ms per frame)."""
+        w, h = img_size
+        arr = (Camera * len(cameras))(*cameras)
+        t = L.Tuning()
+        ms = C.c_double()
+        check(lib().sf_scratch_autotune(splats.handle, self.handle, arr, len(cameras), w, h, _stream(stream),
+                                        C.byref(t), C.byref(ms)))
+        return self.get_tuning(), float(ms.value)
+
     def get_tuning(self) -> dict:
         t = L.Tuning()
         check(lib().sf_scratch_get_tuning(self.handle, C.byref(t)))

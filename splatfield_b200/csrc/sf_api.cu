@@ -1320,6 +1320,76 @@ int sf_render_frames_to_host(sf_splats s, sf_scratch scratch, const sf_camera* c
     })
 }
 
+static int scratch_autotune(sf_splats s, sf_scratch scratch, const sf_camera* cams, uint32_t count, uint32_t w,
+                            uint32_t h, sf_stream stream, sf_tuning* best, double* best_ms) {
+    {
+        if (!s || !scratch || !cams || count == 0) return fail(SF_ERR_ARG, "null argument");
+        SF_CK(use_device(scratch->ctx->device));
+        cudaStream_t st = S(stream);
+        cudaEvent_t e0, e1;
+        SF_CK(cudaEventCreate(&e0));
+        SF_CK(cudaEventCreate(&e1));
+        // One warm-up path (captures the graph, settles the capacity), then
+        // the best of three timed paths.
+        auto time_of = [&](const sf_tuning& t, float* out_ms) -> int {
+            int rc = sf_scratch_set_tuning(scratch, &t);
+            if (rc != SF_OK) return rc;
+            rc = sf_render_frames(s, scratch, cams, count, w, h, stream);
+            if (rc != SF_OK) return rc;
+            float ms_best = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {
+                SF_CK(cudaEventRecord(e0, st));
+                rc = sf_render_frames(s, scratch, cams, count, w, h, stream);
+                if (rc != SF_OK) return rc;
+                SF_CK(cudaEventRecord(e1, st));
+                SF_CK(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                ms_best = std::min(ms_best, ms);
+            }
+            *out_ms = ms_best;
+            return SF_OK;
+        };
+        sf_tuning winner = scratch->tuning;
+        winner.raster_detail = 0;
+        if (winner.raster_split == 0) winner.raster_split = 1;
+        float winner_ms = 1e30f;
+        int rc = time_of(winner, &winner_ms);
+        if (rc != SF_OK) return rc;
+        const uint32_t vals[4][3] = {{0, 1, 0}, {1, 2, 4}, {SF_ORDER_SORTED, SF_ORDER_HYBRID, SF_ORDER_IN_RASTER},
+                                     {SF_SCHEDULE_LONGEST, SF_SCHEDULE_TILES, 0}};
+        const int nvals[4] = {2, 3, 3, 2};
+        for (int sweep = 0; sweep < 2; ++sweep)
+            for (int dim = 0; dim < 4; ++dim)
+                for (int k = 0; k < nvals[dim]; ++k) {
+                    sf_tuning t = winner;
+                    uint32_t* field = dim == 0 ? &t.raster_cull : dim == 1 ? &t.raster_split
+                                    : dim == 2 ? &t.raster_order : &t.raster_schedule;
+                    if (*field == vals[dim][k]) continue;
+                    *field = vals[dim][k];
+                    float ms = 0.f;
+                    rc = time_of(t, &ms);
+                    if (rc != SF_OK) return rc;
+                    if (ms < winner_ms) {
+                        winner_ms = ms;
+                        winner = t;
+                    }
+                }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        rc = sf_scratch_set_tuning(scratch, &winner);
+        if (rc != SF_OK) return rc;
+        if (best) *best = winner;
+        if (best_ms) *best_ms = winner_ms / count;
+        return SF_OK;
+    }
+}
+
+int sf_scratch_autotune(sf_splats s, sf_scratch scratch, const sf_camera* cams, uint32_t count, uint32_t w,
+                        uint32_t h, sf_stream stream, sf_tuning* best, double* best_ms) {
+    SF_TRY({ return scratch_autotune(s, scratch, cams, count, w, h, stream, best, best_ms); })
+}
+
 int sf_scratch_stats(sf_scratch s, uint64_t out[4], sf_stream stream) {
     if (!s || !out) return fail(SF_ERR_ARG, "null argument");
     SF_CK(use_device(s->ctx->device));

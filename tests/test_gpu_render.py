@@ -423,3 +423,25 @@ def test_split_rejects_other_values(ctx):
     scratch = sf.RenderScratch(10, (32, 32))
     with pytest.raises(sf.SplatfieldError):
         scratch.set_tuning(raster_split=3)
+
+
+def test_frame_autotune_picks_a_form_with_the_same_images(ctx, oracle_mod):
+    """sf_scratch_autotune times the raster forms on a camera path and keeps
+    the fastest; every form gives the oracle's images."""
+    from splatfield_b200 import synth
+
+    n, w, h = 30000, 240, 160
+    attr, sh = synth.scene_clustered(n, 4, seed=12, clusters=3, sigma=0.3, extent=1.0)
+    splats = sf.Splats(attr, sh)
+    scratch = sf.RenderScratch(n, (w, h))
+    cams = synth.orbit_cameras(4, 3.0, w, h, sf.look_at)
+    tuning, ms = scratch.autotune(splats, cams, (w, h))
+    assert ms > 0
+    assert tuning["raster_cull"] in (0, 1) and tuning["raster_split"] in (1, 2, 4)
+    assert tuning["raster_order"] in (sf.ORDER_SORTED, sf.ORDER_HYBRID, sf.ORDER_IN_RASTER)
+    assert scratch.get_tuning() == tuning
+    cams_o = synth.orbit_cameras(4, 3.0, w, h, oracle_mod.look_at)
+    for cam, cam_o in zip(cams, cams_o):
+        got = splats.render_with(scratch, cam, (w, h)).read()
+        prep = oracle_mod.prepare(cam_o, w, h, attr, sh, 4)
+        np.testing.assert_array_equal(got, oracle_mod.rasterize(prep, 0)["bitmap"])
