@@ -406,6 +406,48 @@ def time_uneven_round(sf, ctx, stream, args):
     return result
 
 
+def time_sharded_round(sf, splats, ctx, stream, rank, world, dist):
+    """The segmentation round sharded by view over the ranks (one GPU each):
+    rank r runs the batched evidence round (masked lift + LUT EIG) over views
+    r, r + world, ... and the ranks all-reduce the per-view EIG vector before
+    the argmax (replicas.sharded_round). Device-timed on every rank between
+    barriers, the job time is the slowest rank's."""
+    import torch
+
+    from splatfield_b200 import replicas, synth
+
+    size = (ROUND_SIDE, ROUND_SIDE)
+    a, b, cams, mask_bytes = synth.round_workload(N_SPLATS, sf.look_at)
+    views = replicas.owned_views(ROUND_VIEWS, rank, world)
+    beta = sf.BetaState.from_host(a, b, ctx)
+    masks = {v: sf.Mask.from_bytes(size, mask_bytes[v], ctx) for v in views}
+    rnd = sf.Round(N_SPLATS, [size] * len(views), ctx)
+    tuning, _ = rnd.autotune(splats, beta, [cams[v] for v in views], sf.EIG_LUT_F32, stream=stream,
+                             kind=sf.ROUND_EVIDENCE, masks=[masks[v] for v in views])
+
+    def score(vs):
+        return rnd.evidence(splats, beta, [cams[v] for v in vs], [masks[v] for v in vs], sf.EIG_LUT_F32,
+                            stream=stream)
+
+    for _ in range(2):
+        replicas.sharded_round(ROUND_VIEWS, score, dist)
+    times, best = [], None
+    for _ in range(5):
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, best = replicas.sharded_round(ROUND_VIEWS, score, dist)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(replicas.max_over_ranks(e0.elapsed_time(e1), dist))
+    ms = float(np.median(times))
+    return {"workload": f"round sharded by view: {ROUND_VIEWS} views {ROUND_SIDE}x{ROUND_SIDE}, evidence lift + "
+                        "LUT EIG, EIG vector all-reduced before the argmax",
+            "ranks": world, "views_per_rank": len(views), "tuning": tuning, "ms_per_round": ms,
+            "views_per_s": ROUND_VIEWS / (ms / 1e3), "best_view": int(best[0])}
+
+
 SORT_SIZES = (1_000, 10_000, 100_000, 500_000, 1_000_000, 5_000_000, 10_000_000)
 
 
@@ -760,6 +802,7 @@ def run_ours(args, rank, world):
     image0 = splats.render_float(scratch, cams[0], size, stream=stream).read(stream)
     bwd = time_backward(sf, splats, scratch, attr, sh, my_cams[0], stream, args)
     eig_round = time_eig_round(sf, splats, ctx, stream, args)
+    sharded = time_sharded_round(sf, splats, ctx, stream, rank, world, dist) if dist else None
     del scratch
     uneven = time_uneven_round(sf, ctx, stream, args)
     sort_scan = time_sort_scan(sf, ctx, stream)
@@ -807,6 +850,7 @@ def run_ours(args, rank, world):
         "sort_scan": sort_scan,
         "backward": bwd,
         "eig_round": eig_round,
+        "sharded_round": sharded,
         "uneven_round": uneven,
         "clocks": clk,
         "gpu_launches": int(launches),

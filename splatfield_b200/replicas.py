@@ -69,3 +69,17 @@ def best_view(scores: list[float]):
         if e > best_score:
             best, best_score = v, e
     return best, best_score
+
+
+def sharded_round(n_views: int, score_owned, dist=None):
+    """One view-sharded round: this rank scores its owned views with
+    ``score_owned(views) -> scores`` (a batched round over those views on
+    this rank's GPU), then the ranks exchange the scores and pick the best
+    view. Returns (all scores, (best view, its score)), equal on every rank.
+    Every rank takes the same collective steps: one all-reduce."""
+    rank = dist.get_rank() if dist is not None and dist.is_initialized() else 0
+    world = dist.get_world_size() if dist is not None and dist.is_initialized() else 1
+    views = owned_views(n_views, rank, world)
+    local = dict(zip(views, score_owned(views))) if views else {}
+    scores = gather_view_scores(local, n_views, dist)
+    return scores, best_view(scores)

@@ -33,7 +33,10 @@ def worker(rank, world, port, out):
         full = scores_for(n_views)
         local = {v: full[v] for v in replicas.owned_views(n_views, rank, world)}
         merged = replicas.gather_view_scores(local, n_views, dist)
-        out[rank] = (t, merged, replicas.best_view(merged))
+        calls = []
+        scores, best = replicas.sharded_round(n_views, lambda views: (calls.append(list(views)),
+                                                                      [full[v] for v in views])[1], dist)
+        out[rank] = (t, merged, replicas.best_view(merged), scores, best, calls)
     finally:
         dist.destroy_process_group()
 
@@ -45,10 +48,13 @@ def test_two_gloo_ranks_agree_on_time_and_best_view():
     mp.start_processes(worker, args=(world, free_port(), out), nprocs=world, join=True, start_method="spawn")
     want_scores = scores_for(13)
     for rank in range(world):
-        t, merged, best = out[rank]
+        t, merged, best, scores, best2, calls = out[rank]
         assert t == 2.5
         assert merged == want_scores
         assert best == (3, 5.0)
+        # The sharded round: each rank scored only its own views, once.
+        assert calls == [replicas.owned_views(13, rank, world)]
+        assert scores == want_scores and best2 == (3, 5.0)
 
 
 def test_replica_share_covers_the_orbit():
