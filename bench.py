@@ -661,7 +661,11 @@ def run_round_only(args):
     beta = sf.BetaState.from_host(a, b, ctx)
     rnd = sf.Round(N_SPLATS, [size] * ROUND_VIEWS, ctx)
     stream = torch.cuda.current_stream()
-    tuning, _ = rnd.autotune(splats, beta, cams, sf.EIG_LUT_F32, stream=stream)
+    if args.tuning:
+        rnd.set_tuning(**json.loads(args.tuning))
+        tuning = rnd.get_tuning()
+    else:
+        tuning, _ = rnd.autotune(splats, beta, cams, sf.EIG_LUT_F32, stream=stream)
     print(json.dumps({"round_only_tuning": tuning}), flush=True)
     for _ in range(args.warmup):
         rnd.eig(splats, beta, cams, sf.EIG_LUT_F32, stream=stream)
@@ -868,7 +872,8 @@ def main():
     ap.add_argument("--frames-only", action="store_true",
                     help="render warmup + steps frames and exit (for profilers)")
     ap.add_argument("--tuning", default="",
-                    help="frame raster form as JSON (sf_tuning fields) instead of the frame autotuner's pick")
+                    help="kernel forms as JSON (sf_tuning fields for --frames-only, sf_round_tuning fields for "
+                         "--round-only) instead of the autotuner's pick")
     ap.add_argument("--round-only", action="store_true",
                     help="run warmup + steps batched segmentation rounds (autotuned forms) and exit "
                          "(for profilers)")
