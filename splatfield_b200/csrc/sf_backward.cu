@@ -162,12 +162,25 @@ __global__ __launch_bounds__(256) void raster_bwd_kernel(BwdArgs a) {
 // forward state comes from the transmittance-only raster mode. Float sums
 // are reduced per warp, per tile in shared memory, then added to global
 // memory once per (tile, splat); their order of addition is not fixed.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Chunks of 256 entries walked from the last down to the first; the records
+// of chunk c - 1 are copied (cp.async, double-buffered) while chunk c is
+// replayed, and the ids of chunk c - 2 are loaded a chunk ahead.
 __global__ __launch_bounds__(256) void feature_bwd_kernel(FeatureBwdArgs a) {
-    __shared__ float4 s_g0[256];
-    __shared__ float4 s_g1[256];
-    __shared__ uint32_t s_gid[256];
-    __shared__ float s_fg[256];
-    __shared__ float s_bg[256];
+    __shared__ float4 s_g0[2][256];
+    __shared__ float4 s_g1[2][256];
+    __shared__ uint32_t s_gid[2][256];
+    __shared__ float s_fg[2][256];
+    __shared__ float s_bg[2][256];
     __shared__ uint32_t s_max_last;
 
     const uint32_t tile = blockIdx.x;
@@ -190,32 +203,63 @@ __global__ __launch_bounds__(256) void feature_bwd_kernel(FeatureBwdArgs a) {
         wb = 1.0f - wf;
     }
     if (tid == 0) s_max_last = 0;
-    s_fg[tid] = 0.0f;
-    s_bg[tid] = 0.0f;
+    s_fg[0][tid] = s_fg[1][tid] = 0.0f;
+    s_bg[0][tid] = s_bg[1][tid] = 0.0f;
     __syncthreads();
     const uint32_t wmax = __reduce_max_sync(0xffffffffu, last);
     if (lane == 0) atomicMax(&s_max_last, wmax);
     __syncthreads();
     const uint32_t max_last = s_max_last;
+    const uint32_t nch = (max_last + 255u) / 256u;
+    if (nch == 0) return;
     const float inv255 = 1.0f / 255.0f;
-
-    for (int64_t c0 = (int64_t)((max_last + 255u) / 256u) * 256 - 256; c0 >= 0; c0 -= 256) {
-        __syncthreads();
-        const uint32_t e_stage = (uint32_t)c0 + tid;
-        if (e_stage < max_last) {
-            const uint32_t gid = a.gaussian_ids[start + e_stage];
-            s_gid[tid] = gid;
-            s_g0[tid] = a.geo0[gid];
-            s_g1[tid] = a.geo1[gid];
+    uint32_t g_next = 0;
+    auto load_id = [&](uint32_t c) {
+        const uint32_t e = c * 256u + tid;
+        g_next = e < max_last ? a.gaussian_ids[start + e] : 0u;
+    };
+    auto issue = [&](uint32_t c, uint32_t b) {
+        if (c * 256u + tid < max_last) {
+            cp_async16(&s_g0[b][tid], a.geo0 + g_next);
+            cp_async16(&s_g1[b][tid], a.geo1 + g_next);
+            s_gid[b][tid] = g_next;
         }
+    };
+    auto flush = [&](uint32_t b, uint32_t cnt) {
+        if (tid < cnt) {
+            const uint32_t g = s_gid[b][tid];
+            const float f = s_fg[b][tid], bb = s_bg[b][tid];
+            if (f != 0.0f) atomicAdd(a.fg + g, f);
+            if (bb != 0.0f) atomicAdd(a.bg + g, bb);
+            s_fg[b][tid] = 0.0f;
+            s_bg[b][tid] = 0.0f;
+        }
+    };
+    load_id(nch - 1);
+    issue(nch - 1, 0);
+    cp_async_commit();
+    if (nch > 1) load_id(nch - 2);
+    for (uint32_t k = 0; k < nch; ++k) {
+        const uint32_t ci = nch - 1 - k, b = k & 1u;
+        // The replay of chunk ci + 1 is over: its buffer may be refilled
+        // and its sums are complete.
         __syncthreads();
-        const uint32_t cnt = min(256u, max_last - (uint32_t)c0);
+        if (k > 0) flush(b ^ 1u, min(256u, max_last - (ci + 1) * 256u));
+        if (ci > 0) {
+            issue(ci - 1, b ^ 1u);
+            if (ci > 1) load_id(ci - 2);
+        }
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        const uint32_t c0 = ci * 256u;
+        const uint32_t cnt = min(256u, max_last - c0);
         for (int j = (int)cnt - 1; j >= 0; --j) {
-            const uint32_t e = (uint32_t)c0 + (uint32_t)j;
+            const uint32_t e = c0 + (uint32_t)j;
             float w = 0.0f;
             if (e < last) {
-                const float4 g0 = s_g0[j];
-                const float4 g1 = s_g1[j];
+                const float4 g0 = s_g0[b][j];
+                const float4 g1 = s_g1[b][j];
                 const float dx = g0.x - fx, dy = g0.y - fy;
                 const float power = fma_(g0.z * dx, dx, fma_(g1.x * dy, dy, (g0.w * dx) * dy));
                 if (!(power > g1.z)) {
@@ -231,21 +275,14 @@ __global__ __launch_bounds__(256) void feature_bwd_kernel(FeatureBwdArgs a) {
                 const float sf = warp_sum(wf * w);
                 const float sb = warp_sum(wb * w);
                 if (lane == 0) {
-                    if (sf != 0.0f) atomicAdd(&s_fg[j], sf);
-                    if (sb != 0.0f) atomicAdd(&s_bg[j], sb);
+                    if (sf != 0.0f) atomicAdd(&s_fg[b][j], sf);
+                    if (sb != 0.0f) atomicAdd(&s_bg[b][j], sb);
                 }
             }
         }
-        __syncthreads();
-        if (tid < cnt) {
-            const uint32_t g = s_gid[tid];
-            const float f = s_fg[tid], b = s_bg[tid];
-            if (f != 0.0f) atomicAdd(a.fg + g, f);
-            if (b != 0.0f) atomicAdd(a.bg + g, b);
-            s_fg[tid] = 0.0f;
-            s_bg[tid] = 0.0f;
-        }
     }
+    __syncthreads();
+    flush((nch - 1) & 1u, min(256u, max_last));
 }
 
 struct V3 { float x, y, z; };
