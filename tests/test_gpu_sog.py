@@ -50,8 +50,14 @@ def test_loaded_scene_renders_as_the_oracle(ctx, oracle_mod):
     splats = sf.load_sog(data)
     attr, sh = splats.read_planes()
     w, h = 160, 120
-    cam = sf.look_at((0.3, 0.2, -4.0), (0.0, 0.0, 0.0))
+    # Looking at the loaded scene's centre from outside its extent.
+    means = attr.reshape(11, -1)[0:3].astype(np.float64)
+    centre = means.mean(axis=1)
+    extent = float(np.abs(means - centre[:, None]).max())
+    pos = tuple(float(c) for c in centre + np.array([0.3, 0.2, -2.0 * extent - 1.0]))
+    target = tuple(float(c) for c in centre)
+    cam = sf.look_at(pos, target)
     got = splats.render_with(sf.RenderScratch(splats.n, (w, h)), cam, (w, h)).read()
-    prep = oracle_mod.prepare(oracle_mod.look_at((0.3, 0.2, -4.0), (0.0, 0.0, 0.0)), w, h, attr, sh, 16)
+    prep = oracle_mod.prepare(oracle_mod.look_at(pos, target), w, h, attr, sh, 16)
     np.testing.assert_array_equal(got, oracle_mod.rasterize(prep, 0)["bitmap"])
     assert prep["num_isects"] > 0
