@@ -151,7 +151,7 @@ def test_adjoint_10k_subset_128_full_fp64_gradient(ctx, oracle_mod, frame_scene)
         report[name] = rel_l2(g, r)
         close = np.abs(g - r) <= 1e-3 * np.abs(r) + 1e-4 * np.abs(r).max()
         assert close.mean() > 0.98, (name, close.mean())
-    report["sh"] = rel_l2(d_sh, ref_sh)
+    report["sh"] = rel_l2(d_sh.reshape(3 * k, n), ref_sh)
     print("adjoint 10k subset, relative L2 error vs the FP64 adjoint:",
           {k_: f"{v:.2e}" for k_, v in report.items()})
     assert max(report.values()) < 5e-3, report
