@@ -644,6 +644,33 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_sort_only(args):
+    """Profiling mode: sf_radix_argsort of 1M random 32-bit keys (8-bit
+    digits), warmup + steps calls, device-timed."""
+    import torch
+
+    import splatfield_b200 as sf
+
+    torch.cuda.set_device(0)
+    ctx = sf.Context(0)
+    n = args.sort_n
+    rng = np.random.default_rng(0x5027)
+    keys = sf.DeviceBuffer.from_array(rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32), ctx)
+    scratch = sf.RadixScratch(n, ctx)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        scratch.argsort(keys, None, n, 32, True, stream=stream)
+    times = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        scratch.argsort(keys, None, n, 32, True, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    print(json.dumps({"sort_only": n, "ms": float(np.median(times))}))
+
+
 def run_round_only(args):
     """Profiling mode: the eig_round workload's batched round alone, with the
     tuning the autotuner picks for it fixed, timed on the host clock."""
@@ -874,6 +901,8 @@ def main():
     ap.add_argument("--tuning", default="",
                     help="kernel forms as JSON (sf_tuning fields for --frames-only, sf_round_tuning fields for "
                          "--round-only) instead of the autotuner's pick")
+    ap.add_argument("--sort-n", type=int, default=0,
+                    help="run warmup + steps radix argsorts of this many random 32-bit keys and exit (for profilers)")
     ap.add_argument("--round-only", action="store_true",
                     help="run warmup + steps batched segmentation rounds (autotuned forms) and exit "
                          "(for profilers)")
@@ -893,6 +922,8 @@ def main():
             run_reference(args, rank, world)
         elif args.round_only:
             run_round_only(args)
+        elif args.sort_n:
+            run_sort_only(args)
         else:
             run_ours(args, rank, world)
     finally:
