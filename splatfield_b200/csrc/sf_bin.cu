@@ -561,19 +561,60 @@ __global__ __launch_bounds__(THREADS) void tile_sort_kernel(const uint32_t* __re
     }
 }
 
-// Global form, lists longer than the largest shared class: the entries stay
-// in the tile's global ranges ((keys_tmp, ids) and the pair buffer as
-// scratch), only the buckets are in shared memory.
-template <uint32_t BINS, uint32_t THREADS>
+// Lists longer than the largest register-held class.
+// Up to SMAX entries (shared form): the bucket sort with the bucketed copy
+// (kb, vb) in shared memory; the entries are read from the tile's placed
+// pairs (L2-resident) in each of the three passes instead of being held in
+// registers, and SBINS buckets share the space. Longer lists, or bunched keys
+// (a bucket past kMaxBucket), go to the global form: the entries stay in the
+// tile's global ranges ((keys_tmp, ids) and the pair buffer as scratch), only
+// the BINS buckets are in shared memory.
+// Shared memory: [s_tmp: 128 words][buckets ...][kb: SMAX][vb: SMAX].
+template <uint32_t BINS, uint32_t SBINS, uint32_t SMAX, uint32_t THREADS>
 __device__ void sort_tile_global(uint32_t t, const uint32_t* __restrict__ tile_start, uint32_t capacity,
                                  uint2* pairs, uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp,
                                  uint32_t* sm) {
-    uint32_t* bins = sm;
-    uint32_t* s_tmp = bins + BINS;
+    static_assert(4 * (THREADS / 32) <= 128, "s_tmp size");
+    uint32_t* s_tmp = sm;
+    uint32_t* bins = sm + 128;
     const uint32_t tid = threadIdx.x;
     const uint32_t start = tile_start[t], end = tile_start[t + 1];
     const uint32_t n = end - start;
     if (end > capacity || end < start) return;
+    if (n <= SMAX) {
+        uint32_t* kb = bins + SBINS;
+        uint32_t* vb = kb + SMAX;
+        const uint2* pr = pairs + start;
+        uint32_t lo = 0xffffffffu, hi = 0;
+        for (uint32_t i = tid; i < n; i += THREADS) {
+            const uint32_t k = pr[i].x;
+            lo = min(lo, k);
+            hi = max(hi, k);
+        }
+        uint32_t mn, mx;
+        block_min_max<THREADS>(lo, hi, s_tmp, mn, mx);
+        const BucketPlan bp = bucket_plan(n, mn, mx, SBINS);
+        for (uint32_t b = tid; b < bp.nbins; b += THREADS) bins[b] = 0;
+        __syncthreads();
+        for (uint32_t i = tid; i < n; i += THREADS) atomicAdd(&bins[(pr[i].x - mn) >> bp.shift], 1u);
+        __syncthreads();
+        const uint32_t big = bucket_starts<THREADS>(bins, bp.nbins, s_tmp);
+        if (big <= kMaxBucket) {
+            for (uint32_t i = tid; i < n; i += THREADS) {
+                const uint2 q = pr[i];
+                const uint32_t pos = atomicAdd(&bins[(q.x - mn) >> bp.shift], 1u);
+                kb[pos] = q.x;
+                vb[pos] = q.y;
+            }
+            __syncthreads();
+            bucket_rank_store<THREADS>(kb, vb, bins, n, mn, bp.shift, ids + start,
+                                       tids_out ? tids_out + start : nullptr, t);
+            return;
+        }
+        // Bunched keys: the global form below (its first loop reads the
+        // pairs again).
+        __syncthreads();
+    }
     uint32_t* ka = keys_tmp + start;
     uint32_t* va = ids + start;
     uint32_t* kb = reinterpret_cast<uint32_t*>(pairs + start);
@@ -609,7 +650,7 @@ __device__ void sort_tile_global(uint32_t t, const uint32_t* __restrict__ tile_s
     bucket_rank_store<THREADS>(kb, vb, bins, n, mn, bp.shift, va, tids_out ? tids_out + start : nullptr, t);
 }
 
-template <uint32_t BINS, uint32_t THREADS>
+template <uint32_t BINS, uint32_t SBINS, uint32_t SMAX, uint32_t THREADS>
 __global__ __launch_bounds__(THREADS, 1) void tile_sort_global_kernel(const uint32_t* __restrict__ list,
                                                                    const uint32_t* list_n,
                                                                    const uint32_t* __restrict__ tile_start,
@@ -618,7 +659,8 @@ __global__ __launch_bounds__(THREADS, 1) void tile_sort_global_kernel(const uint
     extern __shared__ uint32_t sm[];
     const uint32_t count = *list_n;
     for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
-        sort_tile_global<BINS, THREADS>(list[idx], tile_start, capacity, pairs, ids, tids_out, keys_tmp, sm);
+        sort_tile_global<BINS, SBINS, SMAX, THREADS>(list[idx], tile_start, capacity, pairs, ids, tids_out,
+                                                     keys_tmp, sm);
         __syncthreads();
     }
 }
@@ -689,6 +731,12 @@ constexpr size_t sort_smem() {
 constexpr uint32_t kClassWarp = 64, kClassS = 512, kClass0 = 2048, kClassM = 4096, kClass1 = 6144,
                    kClass2 = kBinSharedMax;
 constexpr uint32_t kBinsS = 2304, kBins0 = 4096, kBinsM = 8192, kBins1 = 8192, kBins2 = 16384, kBinsGiant = 32768;
+// The longest lists: up to kGiantShared entries sorted in shared memory
+// (8448 buckets, two 24576-entry arrays), longer ones with 32768 buckets over
+// global scratch; 1024 threads, one CTA per SM.
+constexpr uint32_t kThreadsGiant = 1024, kBinsGiantShared = 8448, kGiantShared = 24576;
+constexpr size_t kGiantSmem = std::max<size_t>((128 + kBinsGiant) * 4, (128 + kBinsGiantShared + 2 * kGiantShared) * 4);
+static_assert(kGiantSmem <= 232448, "shared memory per block");
 constexpr uint32_t kThreadsS = 256, kThreads0 = 256, kThreadsM = 512, kThreads1 = 512, kThreads2 = 1024;
 static_assert(sort_smem<kClass2, kBins2, kThreads2>() <= 227 * 1024, "per-tile sort exceeds shared memory");
 static_assert(kSortClasses == 7, "class table");
@@ -853,7 +901,8 @@ cudaError_t launch_tile_sorts(const uint32_t grids[kSortClasses], const uint32_t
     }
     auto L = [&](int k) { return lists + (size_t)k * tiles; };
     auto N = [&](int k) { return words + 8 + k; };
-    e = launch_sort_kernel(tile_sort_global_kernel<kBinsGiant, 512>, 512, (kBinsGiant + 64) * 4, grids[6],
+    e = launch_sort_kernel(tile_sort_global_kernel<kBinsGiant, kBinsGiantShared, kGiantShared, kThreadsGiant>,
+                           kThreadsGiant, kGiantSmem, grids[6],
                            sm_count, L(6), N(6), tile_start, capacity, pairs, ids, tids_out, keys_tmp, s3);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClass1, kBins1, kThreads1>, kThreads1,

@@ -214,11 +214,14 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
     const uint32_t base = part * kTile;
     const uint32_t wbase = base + warp * (kItems * 32);
 
-    uint32_t k[kItems], rank[kItems];
+    // Keys and values are loaded together, before the ranking and the
+    // look-back, so no global load waits behind them.
+    uint32_t k[kItems], rank[kItems], vv[kItems];
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
         const uint32_t idx = wbase + i * 32 + lane;
         k[i] = idx < n ? keys_in[idx] : 0u;
+        vv[i] = idx < n ? (vals_iota ? idx : vals_in[idx]) : 0u;
     }
     // Stable warp ranking: items in index order, lanes in lane order.
     const uint32_t lt = lanemask_lt();
@@ -321,7 +324,7 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
             const uint32_t d = (k[i] >> shift) & digit_mask;
             const uint32_t pos = s_local_start[d] + s_warp_hist[warp][d] + rank[i];
             s_keys[pos] = k[i];
-            s_vals[pos] = vals_iota ? idx : vals_in[idx];
+            s_vals[pos] = vv[i];
         }
     }
     __syncthreads();

@@ -71,13 +71,14 @@ def test_binned_orders_exact_depth_ties_by_id(ctx, oracle_mod):
     check(got, want, img, want_img)
 
 
+@pytest.mark.parametrize("n", [20000, 40000])
 @pytest.mark.parametrize("quantised", [False, True])
-def test_binned_sorts_lists_beyond_shared_memory(ctx, oracle_mod, quantised):
-    """20,000 splats over one spot: the centre tiles' lists exceed the
-    largest shared-memory sort and are sorted in global memory. With depths
-    quantised to 5 values the buckets overflow and the global-memory radix
-    sort with its id passes runs."""
-    n = 20000
+def test_binned_sorts_lists_beyond_shared_memory(ctx, oracle_mod, quantised, n):
+    """n splats over one spot: the centre tiles' lists exceed the largest
+    register-held sort class. Up to 24576 entries they are bucket-sorted in
+    shared memory, longer ones in global memory. With depths quantised to 5
+    values the buckets overflow and the global-memory radix sort with its id
+    passes runs, from either form."""
     rng = np.random.default_rng(33)
     z = rng.uniform(0, 1, n)
     if quantised:
@@ -85,7 +86,7 @@ def test_binned_sorts_lists_beyond_shared_memory(ctx, oracle_mod, quantised):
     pos = np.stack([rng.normal(0, 0.002, n), rng.normal(0, 0.002, n), 1.0 + z], 1)
     attr = opaque(pos)
     got, want, img, want_img = build_both(oracle_mod, attr, zero_sh(n), 1, 64, 64)
-    assert np.diff(got["tile_start"]).max() > 12288
+    assert np.diff(got["tile_start"]).max() > (24576 if n > 24576 else 12288)
     check(got, want, img, want_img)
 
 
