@@ -511,6 +511,53 @@ def time_sort_scan(sf, ctx, stream):
                     "outside the events' device interval)"}
 
 
+def time_isect_build(sf, ctx, stream, splats_1m, scratch_1m, cams, tuning):
+    """The intersection build alone (projection, binning, per-tile sorts:
+    everything sf_prepare_isects runs before the rasterizer) at 1080p over
+    1M (the headline scene), 3M and 10M clustered splats, SH degree 0 for the
+    two larger scenes. Device time per frame from CUDA events around the call
+    (it returns after reading the intersection count), median of 5 cameras
+    after 2 warm-ups. Algorithmic bytes of the binning and sorts: 8 B read per
+    splat (count), 12 B read per splat and 8 B written per intersection
+    (place), 8 B read and 4 B written per intersection (sorts)."""
+    import torch
+
+    from splatfield_b200 import synth
+
+    def one(splats, scratch, n):
+        scratch.set_tuning(**tuning)
+        for i in range(2):
+            splats.prepare_isects(scratch, cams[i % len(cams)], (WIDTH, HEIGHT), stream=stream)
+        ms, isects = [], []
+        for i in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            t = splats.prepare_isects(scratch, cams[(2 + 5 * i) % len(cams)], (WIDTH, HEIGHT), stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            isects.append(t.raw.num_isects)
+        m = float(np.median(ms))
+        k = float(np.mean(isects))
+        binned = 20.0 * n + 32.0 * k
+        return {"splats": n, "isects": k, "ms": m, "misects_per_s": k / m / 1e3,
+                "bin_sort_gb_per_s_lower_bound": binned / m / 1e6}
+
+    out = [one(splats_1m, scratch_1m, N_SPLATS)]
+    for n in (3_000_000, 10_000_000):
+        attr, sh = synth.scene_clustered(n, 1, seed=0x15EC7 + n)
+        splats = sf.Splats(attr, sh, ctx)
+        scratch = sf.RenderScratch(n, (WIDTH, HEIGHT), ctx)
+        scratch.reserve(int(n * 12))
+        out.append(one(splats, scratch, n))
+        del scratch, splats
+    return {"sizes": out,
+            "note": "GB/s counts only the binning and sort bytes over the whole build's time (projection "
+                    "included), so it is a lower bound for those kernels; per-kernel times are in the "
+                    "launch lists"}
+
+
 def measure_fp32_peak(sf, ctx, stream):
     """FP32 FMA throughput of this GPU, measured: the best of a few 8192^3
     single-precision GEMMs with TF32 off (cuBLAS SGEMM runs on the FP32
@@ -642,6 +689,40 @@ def run_reference(args, rank, world):
                 "its kernels are timed as the C++/OpenMP restatement used as the parity oracle",
     }
     print(json.dumps(line), flush=True)
+
+
+def run_build_only(args):
+    """Profiling mode: the intersection build (sf_prepare_isects) of a 1080p
+    orbit camera over a clustered scene of --build-n splats (SH degree 0),
+    warmup + steps calls, device-timed, with the frame's default forms."""
+    import torch
+
+    import splatfield_b200 as sf
+    from splatfield_b200 import synth
+
+    torch.cuda.set_device(0)
+    ctx = sf.Context(0)
+    n = args.build_n
+    attr, sh = synth.scene_clustered(n, 1, seed=0x15EC7 + n)
+    splats = sf.Splats(attr, sh, ctx)
+    scratch = sf.RenderScratch(n, (WIDTH, HEIGHT), ctx)
+    scratch.reserve(int(n * 12))
+    if args.tuning:
+        scratch.set_tuning(**json.loads(args.tuning))
+    cams = orbit(sf.look_at)
+    stream = torch.cuda.current_stream()
+    for i in range(args.warmup):
+        splats.prepare_isects(scratch, cams[i % N_CAMS], (WIDTH, HEIGHT), stream=stream)
+    times, isects = [], []
+    for i in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t = splats.prepare_isects(scratch, cams[i % N_CAMS], (WIDTH, HEIGHT), stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        isects.append(t.raw.num_isects)
+    print(json.dumps({"build_only": n, "ms": float(np.median(times)), "isects": float(np.mean(isects))}))
 
 
 def run_sort_only(args):
@@ -831,6 +912,7 @@ def run_ours(args, rank, world):
     del batch_out, host_out
 
     image0 = splats.render_float(scratch, cams[0], size, stream=stream).read(stream)
+    isect_build = time_isect_build(sf, ctx, stream, splats, scratch, my_cams, frame_tuning)
     bwd = time_backward(sf, splats, scratch, attr, sh, my_cams[0], stream, args)
     eig_round = time_eig_round(sf, splats, ctx, stream, args)
     sharded = time_sharded_round(sf, splats, ctx, stream, rank, world, dist) if dist else None
@@ -879,6 +961,7 @@ def run_ours(args, rank, world):
                          "sample": f"{cpu_frames} full frame(s) of the workload, median"},
         "cpu_other_workloads": cpu_more,
         "sort_scan": sort_scan,
+        "isect_build": isect_build,
         "backward": bwd,
         "eig_round": eig_round,
         "sharded_round": sharded,
@@ -903,6 +986,9 @@ def main():
                          "--round-only) instead of the autotuner's pick")
     ap.add_argument("--sort-n", type=int, default=0,
                     help="run warmup + steps radix argsorts of this many random 32-bit keys and exit (for profilers)")
+    ap.add_argument("--build-n", type=int, default=0,
+                    help="run warmup + steps 1080p intersection builds of a clustered scene of this many splats "
+                         "and exit (for profilers)")
     ap.add_argument("--round-only", action="store_true",
                     help="run warmup + steps batched segmentation rounds (autotuned forms) and exit "
                          "(for profilers)")
@@ -924,6 +1010,8 @@ def main():
             run_round_only(args)
         elif args.sort_n:
             run_sort_only(args)
+        elif args.build_n:
+            run_build_only(args)
         else:
             run_ours(args, rank, world)
     finally:

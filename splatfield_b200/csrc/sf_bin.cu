@@ -43,8 +43,10 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 // their lanes (owner found by a shuffle search over the lanes' inclusive
 // ends), so a splat covering many tiles does not stall its warp. payload
 // (optional) is a per-splat word loaded once by the splat's lane with its box
-// and shuffled to the lanes that emit its pairs.
-template <typename F>
+// and shuffled to the lanes that emit its pairs. U rounds of 32 pairs are
+// handed out per step: their searches and f calls are independent, so their
+// shuffle and shared-memory latencies overlap.
+template <uint32_t U, typename F>
 __device__ __forceinline__ void for_each_pair(uint32_t begin, uint32_t end, const uint2* __restrict__ bbox,
                                               const uint32_t* __restrict__ payload, uint32_t tiles_x, F&& f) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -75,6 +77,8 @@ __device__ __forceinline__ void for_each_pair(uint32_t begin, uint32_t end, cons
             width = max_x - min_x;
             cnt = width * (max_y - min_y);
         }
+        // 1 / width, shuffled to the pair lanes with the box.
+        const float rw = __fdividef(1.0f, (float)width);
         uint32_t incl = cnt;
 #pragma unroll
         for (uint32_t d = 1; d < 32; d <<= 1) {
@@ -82,39 +86,53 @@ __device__ __forceinline__ void for_each_pair(uint32_t begin, uint32_t end, cons
             if (lane >= d) incl += v;
         }
         const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        for (uint32_t p0 = 0; p0 < total; p0 += 32) {
-            const uint32_t p = p0 + lane;
-            uint32_t o = 0;
+        for (uint32_t p0 = 0; p0 < total; p0 += 32u * U) {
+            uint32_t o[U];
+#pragma unroll
+            for (uint32_t u = 0; u < U; ++u) o[u] = 0;
 #pragma unroll
             for (uint32_t step = 16; step > 0; step >>= 1) {
-                const uint32_t v = __shfl_sync(0xffffffffu, incl, o + step - 1);
-                if (v <= p) o += step;
-            }
-            const uint32_t oend = __shfl_sync(0xffffffffu, incl, o);
-            const uint32_t ocnt = __shfl_sync(0xffffffffu, cnt, o);
-            const uint32_t ow = __shfl_sync(0xffffffffu, width, o);
-            const uint32_t ox = __shfl_sync(0xffffffffu, min_x, o);
-            const uint32_t oy = __shfl_sync(0xffffffffu, min_y, o);
-            const uint32_t opay = __shfl_sync(0xffffffffu, pay, o);
-            if (p < total) {
-                // Row and column of pair k in the owner's box: a float
-                // quotient (k < 2^16, so it is off by at most one) and an
-                // exact integer correction.
-                const uint32_t k = p - (oend - ocnt);
-                uint32_t row = (uint32_t)((float)k * __fdividef(1.0f, (float)ow));
-                int32_t col = (int32_t)(k - row * ow);
-                if (col < 0) {
-                    --row;
-                    col += (int32_t)ow;
-                } else if (col >= (int32_t)ow) {
-                    ++row;
-                    col -= (int32_t)ow;
+#pragma unroll
+                for (uint32_t u = 0; u < U; ++u) {
+                    const uint32_t v = __shfl_sync(0xffffffffu, incl, o[u] + step - 1);
+                    if (v <= p0 + 32u * u + lane) o[u] += step;
                 }
-                f(g0 + o, (ox + (uint32_t)col) + (oy + row) * tiles_x, opay);
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < U; ++u) {
+                const uint32_t p = p0 + 32u * u + lane;
+                const uint32_t oend = __shfl_sync(0xffffffffu, incl, o[u]);
+                const uint32_t ocnt = __shfl_sync(0xffffffffu, cnt, o[u]);
+                const uint32_t ow = __shfl_sync(0xffffffffu, width, o[u]);
+                const float orw = __shfl_sync(0xffffffffu, rw, o[u]);
+                const uint32_t ox = __shfl_sync(0xffffffffu, min_x, o[u]);
+                const uint32_t oy = __shfl_sync(0xffffffffu, min_y, o[u]);
+                const uint32_t opay = __shfl_sync(0xffffffffu, pay, o[u]);
+                if (p < total) {
+                    // Row and column of pair k in the owner's box: a float
+                    // quotient (k < 2^16, so it is off by at most one) and an
+                    // exact integer correction.
+                    const uint32_t k = p - (oend - ocnt);
+                    uint32_t row = (uint32_t)((float)k * orw);
+                    int32_t col = (int32_t)(k - row * ow);
+                    if (col < 0) {
+                        --row;
+                        col += (int32_t)ow;
+                    } else if (col >= (int32_t)ow) {
+                        ++row;
+                        col -= (int32_t)ow;
+                    }
+                    f(g0 + o[u], (ox + (uint32_t)col) + (oy + row) * tiles_x, opay);
+                }
             }
         }
     }
 }
+
+// Rounds of 32 pairs per step in the count and place walks. Two rounds in
+// place, and two place blocks per SM (32 registers), measured no faster.
+constexpr uint32_t kCountUnroll = 1;
+constexpr uint32_t kPlaceUnroll = 1;
 
 __global__ __launch_bounds__(kBinThreads) void bin_count_kernel(const uint2* __restrict__ bbox, uint32_t n,
                                                                 uint32_t chunk, uint32_t tiles_x,
@@ -126,8 +144,8 @@ __global__ __launch_bounds__(kBinThreads) void bin_count_kernel(const uint2* __r
     __syncthreads();
     const uint32_t begin = min(n, blockIdx.x * chunk);
     const uint32_t end = min(n, begin + chunk);
-    for_each_pair(begin, end, bbox, nullptr, tiles_x,
-                  [&](uint32_t, uint32_t t, uint32_t) { atomicAdd(&s_hist[t], 1u); });
+    for_each_pair<kCountUnroll>(begin, end, bbox, nullptr, tiles_x,
+                                [&](uint32_t, uint32_t t, uint32_t) { atomicAdd(&s_hist[t], 1u); });
     __syncthreads();
     uint32_t* row = hist + (size_t)blockIdx.x * tiles;
     for (uint32_t t = threadIdx.x; t < tiles; t += blockDim.x) row[t] = s_hist[t];
@@ -211,7 +229,7 @@ __global__ __launch_bounds__(kBinThreads) void bin_place_kernel(
     const uint32_t begin = min(n, blockIdx.x * chunk);
     const uint32_t end = min(n, begin + chunk);
     bool over = false;
-    for_each_pair(begin, end, bbox, depth_keys, tiles_x, [&](uint32_t s, uint32_t t, uint32_t key) {
+    for_each_pair<kPlaceUnroll>(begin, end, bbox, depth_keys, tiles_x, [&](uint32_t s, uint32_t t, uint32_t key) {
         const uint32_t slot = atomicAdd(&s_cur[t], 1u);
         if (slot < capacity) {
             pairs[slot] = make_uint2(key, s);

@@ -268,9 +268,15 @@ void build_entropy_table(float* table);  // host, f64 formulas
 double beta_entropy_host(double a, double b);
 // Per-block f64 partial sums of dH; then a single-block final sum into out.
 // resp2 (optional) is added word for word: eps = fg + bg of an evidence split.
+// h0 (optional): H(a_i, b_i) of every splat from launch_entropy (f32 for the
+// LUT mode, f64 for FP64), read instead of recomputed; the sums are the same.
 cudaError_t launch_eig(int mode, const float* a, const float* b, const uint32_t* resp, uint32_t n,
                        float scale, const float* table, double* partials, uint32_t max_blocks,
-                       double* out, cudaStream_t stream, const uint32_t* resp2 = nullptr);
+                       double* out, cudaStream_t stream, const uint32_t* resp2 = nullptr,
+                       const void* h0 = nullptr);
+// out[i] = H(a_i, b_i) (mode SF_EIG_LUT_F32: f32 table values; SF_EIG_FP64: f64).
+cudaError_t launch_entropy(int mode, const float* a, const float* b, uint32_t n, const float* table, void* out,
+                           cudaStream_t stream);
 uint32_t eig_blocks(uint32_t n, int sm_count);
 // Posterior heatmap colours and foreground tint (src/seg/paint.rs).
 cudaError_t launch_paint_posterior(const float* a, const float* b, uint32_t n, float4* color,
@@ -287,7 +293,7 @@ cudaError_t launch_beta_update(float scale, const uint32_t* fg, const uint32_t* 
 // may be null for the EIG).
 cudaError_t launch_eig_real(int mode, const float* a, const float* b, const float* fg, const float* bg,
                             uint32_t n, const float* table, double* partials, uint32_t blocks, double* out,
-                            cudaStream_t stream);
+                            cudaStream_t stream, const void* h0 = nullptr);
 cudaError_t launch_beta_update_real(const float* fg, const float* bg, float* a, float* b, uint32_t n,
                                     cudaStream_t stream);
 cudaError_t launch_table_probe(const float* a, const float* b, uint32_t n, const float* table,

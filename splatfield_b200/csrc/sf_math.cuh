@@ -84,11 +84,17 @@ SF_HD float exp_(float x) {
     return (p * u2f((uint32_t)(k1 + 127) << 23)) * u2f((uint32_t)(k2 + 127) << 23);
 }
 
-// exp for arguments known to lie in [-87, 0]: the same arithmetic as exp_
-// without the range guards (k in [-126, 0], so 2^k needs one multiply's worth
-// of split only when k < -125 — kept as the two-step scale for bit equality).
+// exp for arguments known to lie in [-86, 0] (the raster's -power, which the
+// power_max test bounds far tighter): the value of exp_ bit for bit, in fewer
+// instructions.
+//  * k = rint(x*log2e) by the round-to-integer shift: t + 1.5*2^23 rounds t
+//    to an integer with ties to even (the rounding rint uses) for
+//    |t| < 2^22, and that sum's low mantissa bits hold k in two's complement.
+//  * The two-step 2^k scale equals one add of k to p's exponent field: for
+//    k >= -125 and p in [0.7, 1.42] every step is exact and p*2^k is normal.
 SF_HD float exp_neg_(float x) {
-    const float kf = rint_(x * 1.44269502f);
+    const float kr = x * 1.44269502f + 12582912.0f;
+    const float kf = kr - 12582912.0f;
     float r = fma_(kf, -0.693145751953125f, x);
     r = fma_(kf, -1.42860677e-06f, r);
     float p = 1.98412701e-04f;
@@ -99,10 +105,7 @@ SF_HD float exp_neg_(float x) {
     p = fma_(p, r, 0.5f);
     p = fma_(p, r, 1.0f);
     p = fma_(p, r, 1.0f);
-    const int k = (int)kf;
-    const int k1 = k / 2;
-    const int k2 = k - k1;
-    return (p * u2f((uint32_t)(k1 + 127) << 23)) * u2f((uint32_t)(k2 + 127) << 23);
+    return u2f(f2u(p) + (f2u(kr) << 23));
 }
 
 SF_HD float log_(float x) {

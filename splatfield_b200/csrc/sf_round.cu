@@ -106,6 +106,9 @@ struct sf_round_t {
     uint32_t* words_host = nullptr; // pinned
     double* eig_dev = nullptr;
     double* eig_host = nullptr;     // pinned
+    // H(a_i, b_i) of every splat, computed once per round by the graph's
+    // first kernel and read by every view's EIG (f32 or f64 by mode).
+    double* h0 = nullptr;
     uint32_t* resp = nullptr;       // [views][n]: total responsibility, or fg under masks
     uint32_t* bg = nullptr;         // [views][n]: bg under masks (allocated on first use)
     std::vector<const sf_mask_t*> masks;  // this round's per-view masks (empty: responsibility)
@@ -272,7 +275,7 @@ cudaError_t raster_and_eig(sf_round_t* r, RoundLane& L, uint32_t v, uint32_t tx,
     if (beta_a) {
         // Under masks the EIG sees eps = fg + bg, the same words mode 1 sums.
         if ((e = launch_eig(mode, beta_a, beta_b, resp, n, a.scale, lut, L.partials, r->eig_blocks,
-                            r->eig_dev + v, st, bg)) != cudaSuccess)
+                            r->eig_dev + v, st, bg, r->h0)) != cudaSuccess)
             return e;
     }
     return cudaSuccess;
@@ -323,7 +326,8 @@ cudaError_t adjoint_and_eig(sf_round_t* r, RoundLane& L, uint32_t v, uint32_t tx
     f.bg = bg;
     if ((e = launch_feature_bwd(f, st)) != cudaSuccess) return e;
     if (beta_a)
-        return launch_eig_real(mode, beta_a, beta_b, fg, bg, n, lut, L.partials, r->eig_blocks, r->eig_dev + v, st);
+        return launch_eig_real(mode, beta_a, beta_b, fg, bg, n, lut, L.partials, r->eig_blocks, r->eig_dev + v, st,
+                               r->h0);
     return cudaSuccess;
 }
 
@@ -406,6 +410,7 @@ int build_graph(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, int
     RF_CK(cudaStreamBeginCapture(r->main, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaMemcpyAsync(r->views_dev, r->views_host, sizeof(sf_view) * r->views,
                                     cudaMemcpyHostToDevice, r->main);
+    if (e == cudaSuccess && beta) e = launch_entropy(mode, beta->a, beta->b, r->n, beta->ctx->lut, r->h0, r->main);
     if (e == cudaSuccess) e = cudaEventRecord(r->fork, r->main);
     for (auto& L : r->lanes)
         if (e == cudaSuccess) e = cudaStreamWaitEvent(L.stream, r->fork, 0);
@@ -552,6 +557,7 @@ int sf_round_create(sf_ctx ctx, uint32_t total, uint32_t n_views, const uint32_t
     if (e == cudaSuccess) e = dalloc(&r->eig_dev, n_views);
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&r->eig_host), 8 * (size_t)n_views);
     if (e == cudaSuccess) e = dalloc(&r->resp, (size_t)n_views * total);
+    if (e == cudaSuccess) e = dalloc(&r->h0, total);
     if (e != cudaSuccess) {
         sf_round_destroy(r);
         return rfail(e == cudaErrorMemoryAllocation ? SF_ERR_NOMEM : SF_ERR_CUDA, cudaGetErrorString(e));
@@ -566,7 +572,7 @@ int sf_round_destroy(sf_round r) {
     graph_drop(r);
     for (auto& L : r->lanes) lane_free(L);
     dfree(r->views_dev); dfree(r->words); dfree(r->eig_dev); dfree(r->resp); dfree(r->bg);
-    dfree(r->afg); dfree(r->abg);
+    dfree(r->afg); dfree(r->abg); dfree(r->h0);
     if (r->views_host) cudaFreeHost(r->views_host);
     if (r->words_host) cudaFreeHost(r->words_host);
     if (r->eig_host) cudaFreeHost(r->eig_host);

@@ -125,7 +125,8 @@ __global__ __launch_bounds__(kEigThreads) void eig_kernel(const float* __restric
                                                           const uint32_t* __restrict__ resp2,
                                                           uint32_t n, float scale,
                                                           const float* __restrict__ table,
-                                                          double* __restrict__ partials) {
+                                                          double* __restrict__ partials,
+                                                          const void* __restrict__ h0) {
     __shared__ double s_warp[kEigThreads / 32];
     double acc = 0.0;
     const uint32_t stride = gridDim.x * kEigThreads;
@@ -137,13 +138,15 @@ __global__ __launch_bounds__(kEigThreads) void eig_kernel(const float* __restric
         if (MODE == SF_EIG_LUT_F32) {
             const float eps = (float)bits / scale;
             const float k = 1.0f + eps / (ai + bi);
-            const float d = max_(table_entropy_d(ai, bi, table) - table_entropy_d(ai * k, bi * k, table), 0.0f);
+            const float hab = h0 ? static_cast<const float*>(h0)[i] : table_entropy_d(ai, bi, table);
+            const float d = max_(hab - table_entropy_d(ai * k, bi * k, table), 0.0f);
             acc += (double)d;
         } else {
             const double eps = (double)bits / (double)scale;
             const double ad = ai, bd = bi;
             const double k = 1.0 + eps / (ad + bd);
-            const double d = beta_entropy_d(ad, bd) - beta_entropy_d(ad * k, bd * k);
+            const double hab = h0 ? static_cast<const double*>(h0)[i] : beta_entropy_d(ad, bd);
+            const double d = hab - beta_entropy_d(ad * k, bd * k);
             acc += d > 0.0 ? d : 0.0;
         }
     }
@@ -160,7 +163,8 @@ __global__ __launch_bounds__(kEigThreads) void eig_real_kernel(const float* __re
                                                                const float* __restrict__ fg,
                                                                const float* __restrict__ bg, uint32_t n,
                                                                const float* __restrict__ table,
-                                                               double* __restrict__ partials) {
+                                                               double* __restrict__ partials,
+                                                               const void* __restrict__ h0) {
     __shared__ double s_warp[kEigThreads / 32];
     double acc = 0.0;
     const uint32_t stride = gridDim.x * kEigThreads;
@@ -170,18 +174,33 @@ __global__ __launch_bounds__(kEigThreads) void eig_real_kernel(const float* __re
         const float ai = a[i], bi = b[i];
         if (MODE == SF_EIG_LUT_F32) {
             const float k = 1.0f + (f + g) / (ai + bi);
-            const float d = max_(table_entropy_d(ai, bi, table) - table_entropy_d(ai * k, bi * k, table), 0.0f);
+            const float hab = h0 ? static_cast<const float*>(h0)[i] : table_entropy_d(ai, bi, table);
+            const float d = max_(hab - table_entropy_d(ai * k, bi * k, table), 0.0f);
             acc += (double)d;
         } else {
             const double eps = (double)f + (double)g;
             const double ad = ai, bd = bi;
             const double k = 1.0 + eps / (ad + bd);
-            const double d = beta_entropy_d(ad, bd) - beta_entropy_d(ad * k, bd * k);
+            const double hab = h0 ? static_cast<const double*>(h0)[i] : beta_entropy_d(ad, bd);
+            const double d = hab - beta_entropy_d(ad * k, bd * k);
             acc += d > 0.0 ? d : 0.0;
         }
     }
     const double total = block_sum(acc, s_warp);
     if (threadIdx.x == 0) partials[blockIdx.x] = total;
+}
+
+// H(a_i, b_i) of every splat, once per batched round: every view's EIG term
+// is H(a, b) - H(k a, k b) over the same posterior, so the views read the
+// first half instead of each recomputing it (the same value, bit for bit, as
+// the per-view kernel computes). LUT: f32 values; FP64: f64 values.
+template <int MODE>
+__global__ void entropy_kernel(const float* __restrict__ a, const float* __restrict__ b, uint32_t n,
+                               const float* __restrict__ table, void* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (MODE == SF_EIG_LUT_F32) static_cast<float*>(out)[i] = table_entropy_d(a[i], b[i], table);
+    else static_cast<double*>(out)[i] = beta_entropy_d((double)a[i], (double)b[i]);
 }
 
 __global__ __launch_bounds__(kEigThreads) void eig_final_kernel(const double* __restrict__ partials,
@@ -336,23 +355,33 @@ uint32_t eig_blocks(uint32_t n, int sm_count) {
 
 cudaError_t launch_eig(int mode, const float* a, const float* b, const uint32_t* resp, uint32_t n,
                        float scale, const float* table, double* partials, uint32_t blocks,
-                       double* out, cudaStream_t stream, const uint32_t* resp2) {
+                       double* out, cudaStream_t stream, const uint32_t* resp2, const void* h0) {
     if (mode == SF_EIG_LUT_F32)
-        eig_kernel<SF_EIG_LUT_F32><<<blocks, kEigThreads, 0, stream>>>(a, b, resp, resp2, n, scale, table, partials);
+        eig_kernel<SF_EIG_LUT_F32><<<blocks, kEigThreads, 0, stream>>>(a, b, resp, resp2, n, scale, table, partials,
+                                                                      h0);
     else
-        eig_kernel<SF_EIG_FP64><<<blocks, kEigThreads, 0, stream>>>(a, b, resp, resp2, n, scale, table, partials);
+        eig_kernel<SF_EIG_FP64><<<blocks, kEigThreads, 0, stream>>>(a, b, resp, resp2, n, scale, table, partials, h0);
     eig_final_kernel<<<1, kEigThreads, 0, stream>>>(partials, blocks, out);
     note_launches(2);
     return cudaGetLastError();
 }
 
+cudaError_t launch_entropy(int mode, const float* a, const float* b, uint32_t n, const float* table, void* out,
+                           cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    if (mode == SF_EIG_LUT_F32) entropy_kernel<SF_EIG_LUT_F32><<<(n + 255) / 256, 256, 0, stream>>>(a, b, n, table, out);
+    else entropy_kernel<SF_EIG_FP64><<<(n + 255) / 256, 256, 0, stream>>>(a, b, n, table, out);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_eig_real(int mode, const float* a, const float* b, const float* fg, const float* bg,
                             uint32_t n, const float* table, double* partials, uint32_t blocks, double* out,
-                            cudaStream_t stream) {
+                            cudaStream_t stream, const void* h0) {
     if (mode == SF_EIG_LUT_F32)
-        eig_real_kernel<SF_EIG_LUT_F32><<<blocks, kEigThreads, 0, stream>>>(a, b, fg, bg, n, table, partials);
+        eig_real_kernel<SF_EIG_LUT_F32><<<blocks, kEigThreads, 0, stream>>>(a, b, fg, bg, n, table, partials, h0);
     else
-        eig_real_kernel<SF_EIG_FP64><<<blocks, kEigThreads, 0, stream>>>(a, b, fg, bg, n, table, partials);
+        eig_real_kernel<SF_EIG_FP64><<<blocks, kEigThreads, 0, stream>>>(a, b, fg, bg, n, table, partials, h0);
     eig_final_kernel<<<1, kEigThreads, 0, stream>>>(partials, blocks, out);
     note_launches(2);
     return cudaGetLastError();
