@@ -565,6 +565,14 @@ int sf_exclusive_scan_gather_noalloc(const uint32_t* gids, const uint32_t* count
  * frame, round and backward paths never see them. */
 int sf_debug_lookback(uint32_t spin_limit, int withhold);
 
+/* No counterpart in the reference. The binned build sorts each list longer
+ * than 12288 entries by cutting it into key-contiguous segments over many
+ * CTAs, for up to 4096 such lists per frame; the later ones of a frame are
+ * sorted by one CTA each. Scratches and rounds created after this call cut
+ * at most `lists` lists (0: none), so tests can reach the one-CTA form;
+ * 4096 restores the default. Both forms give the same order. */
+int sf_debug_giant_lists(uint32_t lists);
+
 #ifdef __cplusplus
 }
 #endif

@@ -173,6 +173,7 @@ SIGNATURES = {
         "sf_exclusive_scan": (i32, [P, P, u32, P]),
         "sf_exclusive_scan_gather_noalloc": (i32, [P, P, P, u32, P]),
         "sf_debug_lookback": (i32, [u32, i32]),
+        "sf_debug_giant_lists": (i32, [u32]),
         "sf_scratch_autotune": (i32, [P, P, P, u32, u32, u32, P, P, P]),
         "sf_sog_inspect": (i32, [P, sz, P, P]),
         "sf_sog_load": (i32, [P, P, sz, PP]),

@@ -131,6 +131,8 @@ struct sf_scratch_t {
     uint32_t* bin_hist = nullptr;
     uint32_t* bin_cnt = nullptr;
     uint32_t* bin_lists = nullptr;
+    GiantState giant;  // segmented sort of the longest lists
+    uint32_t longest = 0;  // longest tile list of the last binned frame
     bool binned = false;
     // The last prepare left the binned build's placed pairs unsorted: the
     // rasterizer orders each tile's list itself (no gaussian_ids).
@@ -151,6 +153,7 @@ struct sf_scratch_t {
         uint32_t K = 0, n = 0, w = 0, h = 0;
         uint64_t cap = 0;
         sf_tuning tuning{};
+        bool giant = false;  // the graph includes the segmented sort
         // Frames to host memory in a batch: each image is copied out of the
         // bitmap into one of two staging images, whose device-to-host copy
         // (copy stream) runs while the next frame renders.
@@ -222,6 +225,9 @@ void scratch_free_frame(sf_scratch s) {
     dfree(s->color); dfree(s->ext); dfree(s->keys_a); dfree(s->keys_b); dfree(s->order_a); dfree(s->order_b);
     dfree(s->offsets); dfree(s->scan_tmp); dfree(s->tile_start); dfree(s->bitmap);
     dfree(s->bin_hist); dfree(s->bin_cnt); dfree(s->bin_lists);
+    dfree(s->giant.ctrl); dfree(s->giant.sel); dfree(s->giant.mm); dfree(s->giant.hist);
+    dfree(s->giant.taken); dfree(s->giant.segs);
+    s->giant.lists = s->giant.seg_cap = 0;
     dfree(s->rgba); dfree(s->final_t); dfree(s->n_contrib); dfree(s->d2d);
     s->order = nullptr;
     s->prepared = false;
@@ -295,6 +301,14 @@ cudaError_t scratch_build(sf_scratch s, uint32_t total, uint32_t w, uint32_t h) 
         SF_AL(s->bin_hist, (size_t)s->bin_chunks * tiles);
         SF_AL(s->bin_cnt, tiles + 1);
         SF_AL(s->bin_lists, (size_t)(kSortClasses + 1) * tiles);
+        s->giant.lists = giant_lists((uint32_t)tiles);
+        s->giant.seg_cap = giant_seg_cap(s->giant.lists);
+        SF_AL(s->giant.ctrl, 4);
+        SF_AL(s->giant.sel, s->giant.lists);
+        SF_AL(s->giant.mm, 2 * (size_t)s->giant.lists);
+        SF_AL(s->giant.hist, (size_t)s->giant.lists * kGiantBins);
+        SF_AL(s->giant.taken, tiles);
+        SF_AL(s->giant.segs, s->giant.seg_cap);
     }
     SF_AL(s->bitmap, (size_t)h * s->row_stride);
 #undef SF_AL
@@ -335,6 +349,7 @@ int prepare_binned(sf_scratch s, uint32_t n, uint32_t tiles, cudaStream_t st, bo
     std::memcpy(&total, hw + 4, 8);
     s->num_visible = hw[0];
     s->last_isects_raw = total;
+    s->longest = hw[6];
     if (total > kMaxIsects) return fail(SF_ERR_CAPACITY, "intersection count exceeds 2^30-1");
     if (total > s->cap) {
         std::fprintf(stderr, "splatfield_b200: intersection capacity %llu reached (%llu needed); growing\n",
@@ -352,8 +367,11 @@ int prepare_binned(sf_scratch s, uint32_t n, uint32_t tiles, cudaStream_t st, bo
         uint32_t grids[kSortClasses];
         for (int k = 0; k < kSortClasses; ++k) grids[k] = hw[8 + k];
         if (order == SF_ORDER_HYBRID) grids[kSortClasses - 1] = 0;
+        // The longest list is known here: the segmented sort runs only when
+        // some list is long enough to gain from it.
         SF_CK(launch_tile_sorts(grids, s->bin_lists, words, tiles, s->tile_start, (uint32_t)s->cap, pairs,
-                                s->gid_e, want_tile_ids ? s->tid_e : nullptr, s->tid_e, s->ctx->sm_count, st));
+                                s->gid_e, want_tile_ids ? s->tid_e : nullptr, s->tid_e, s->ctx->sm_count, st,
+                                nullptr, hw[6] > kGiantMinList ? &s->giant : nullptr));
         s->tids = want_tile_ids ? s->tid_e : nullptr;
         s->gids = s->gid_e;
     }
@@ -553,6 +571,7 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
     const uint32_t tiles = s->tiles_x * s->tiles_y;
     const uint32_t cap = (uint32_t)s->cap;
     const uint32_t order = s->tuning.raster_order;
+    const bool giant = giant_wanted(s->longest, g.giant);
     uint32_t* words = s->words;
     auto* total = reinterpret_cast<unsigned long long*>(words + 4);
     cudaStream_t st = g.stream;
@@ -582,7 +601,7 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
         for (int k = 0; k < kSortClasses; ++k) grids[k] = tiles;
         if (order == SF_ORDER_HYBRID) grids[kSortClasses - 1] = 0;
         e = launch_tile_sorts(grids, s->bin_lists, words, tiles, s->tile_start, cap, pairs, s->gid_e, nullptr,
-                              s->tid_e, s->ctx->sm_count, st, &s->sort_streams);
+                              s->tid_e, s->ctx->sm_count, st, &s->sort_streams, giant ? &s->giant : nullptr);
     }
     if (e == cudaSuccess) {
         RasterArgs a{};
@@ -635,6 +654,7 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
     g.h = s->h;
     g.cap = s->cap;
     g.tuning = s->tuning;
+    g.giant = giant;
     return SF_OK;
 }
 
@@ -643,7 +663,8 @@ int frame_graph_capture(sf_splats sp, sf_scratch s) {
 int frame_graph_ready(sf_splats sp, sf_scratch s, uint32_t w, uint32_t h) {
     auto& g = s->fg;
     if (!g.exec || g.splats != sp || g.attr != sp->attr || g.sh != sp->sh || g.K != sp->K || g.n != sp->n ||
-        g.w != w || g.h != h || g.cap != s->cap || std::memcmp(&g.tuning, &s->tuning, sizeof(sf_tuning)) != 0)
+        g.w != w || g.h != h || g.cap != s->cap || std::memcmp(&g.tuning, &s->tuning, sizeof(sf_tuning)) != 0 ||
+        giant_wanted(s->longest, g.giant) != g.giant)
         return frame_graph_capture(sp, s);
     return SF_OK;
 }
@@ -655,6 +676,7 @@ void frame_graph_settle(sf_scratch s, const uint32_t* hw, uint64_t total) {
     s->num_visible = hw[0];
     s->last_isects_raw = total;
     s->num_isects = (uint32_t)total;
+    s->longest = hw[6];
     s->binned = true;
     s->lazy = order != SF_ORDER_SORTED;
     s->lazy_min = order == SF_ORDER_HYBRID ? kBinSharedMax : 0u;
@@ -787,6 +809,7 @@ int frames_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cams, uint3
                          cudaMemcpyDeviceToHost));
     }
     uint64_t need = 0;
+    uint32_t longest = 0;
     for (uint32_t i = 0; i < count; ++i) {
         const uint32_t* hw = g.frame_words + 16 * (size_t)i;
         if (hw[1] & SF_DEV_ERR_TIMEOUT) return fail(SF_ERR_TIMEOUT, "device look-back wait timed out");
@@ -794,6 +817,7 @@ int frames_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cams, uint3
         std::memcpy(&total, hw + 4, 8);
         if (total > kMaxIsects) return fail(SF_ERR_CAPACITY, "intersection count exceeds 2^30-1");
         if (total > need) need = total;
+        longest = std::max(longest, hw[6]);
     }
     if (need > s->cap) {
         // Frames past the capacity (their images were drawn from clamped
@@ -819,6 +843,7 @@ int frames_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cams, uint3
     uint64_t total = 0;
     std::memcpy(&total, last + 4, 8);
     frame_graph_settle(s, last, total);
+    s->longest = longest;  // the batch's longest list picks the next graph's sort form
     return SF_OK;
 }
 

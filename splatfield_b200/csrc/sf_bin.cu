@@ -484,13 +484,15 @@ __device__ void bucket_rank_store(const uint32_t* kb, const uint32_t* vb, const 
     }
 }
 
-// Shared form: lists of up to MAXN entries, held in registers (ITEMS per
-// thread, all loads in flight together); shared memory holds the bucketed
-// copy (kb, vb) and the buckets.
-template <uint32_t MAXN, uint32_t BINS, uint32_t THREADS>
-__device__ void sort_tile_shared(uint32_t t, const uint32_t* __restrict__ tile_start, uint32_t capacity,
-                                 uint2* pairs, uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp,
-                                 uint32_t* sm) {
+// Shared form: the n <= MAXN entries of slots [start, start + n) of tile t,
+// held in registers (ITEMS per thread, all loads in flight together); shared
+// memory holds the bucketed copy (kb, vb) and the buckets. load(i) gives
+// entry i as (depth key, splat id); the sorted splat ids go to
+// ids[start, start + n) (and t to tids_out there). Every load completes
+// before the first write, so the input may be (keys_tmp, ids) themselves.
+template <uint32_t MAXN, uint32_t BINS, uint32_t THREADS, typename Load>
+__device__ void sort_range_shared(uint32_t t, uint32_t start, uint32_t n, Load load, uint2* pairs, uint32_t* ids,
+                                  uint32_t* tids_out, uint32_t* keys_tmp, uint32_t* sm) {
     constexpr uint32_t ITEMS = MAXN / THREADS;
     constexpr uint32_t WARPS = THREADS / 32;
     static_assert(MAXN % THREADS == 0 && BINS >= 256 + WARPS * 256, "sort shape");
@@ -499,11 +501,6 @@ __device__ void sort_tile_shared(uint32_t t, const uint32_t* __restrict__ tile_s
     uint32_t* bins = vb + MAXN;
     uint32_t* s_tmp = bins + BINS;
     const uint32_t tid = threadIdx.x;
-    const uint32_t start = tile_start[t], end = tile_start[t + 1];
-    const uint32_t n = end - start;
-    // The size class and the capacity check before this launch keep both
-    // conditions false; they guard the shared and global bounds regardless.
-    if (n > MAXN || end > capacity || end < start) return;
     uint32_t k[ITEMS], v[ITEMS];
     uint32_t lo = 0xffffffffu, hi = 0;
 #pragma unroll
@@ -512,7 +509,7 @@ __device__ void sort_tile_shared(uint32_t t, const uint32_t* __restrict__ tile_s
         k[j] = 0;
         v[j] = 0;
         if (i < n) {
-            const uint2 p = pairs[start + i];
+            const uint2 p = load(i);
             k[j] = p.x;
             v[j] = p.y;
         }
@@ -564,6 +561,21 @@ __device__ void sort_tile_shared(uint32_t t, const uint32_t* __restrict__ tile_s
                                t);
 }
 
+// One tile's whole list from the placed pairs.
+template <uint32_t MAXN, uint32_t BINS, uint32_t THREADS>
+__device__ void sort_tile_shared(uint32_t t, const uint32_t* __restrict__ tile_start, uint32_t capacity,
+                                 uint2* pairs, uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp,
+                                 uint32_t* sm) {
+    const uint32_t start = tile_start[t], end = tile_start[t + 1];
+    const uint32_t n = end - start;
+    // The size class and the capacity check before this launch keep both
+    // conditions false; they guard the shared and global bounds regardless.
+    if (n > MAXN || end > capacity || end < start) return;
+    const uint2* pr = pairs + start;
+    sort_range_shared<MAXN, BINS, THREADS>(t, start, n, [pr](uint32_t i) { return pr[i]; }, pairs, ids, tids_out,
+                                           keys_tmp, sm);
+}
+
 // Persistent: each CTA takes the class's tiles in turn.
 template <uint32_t MAXN, uint32_t BINS, uint32_t THREADS>
 __global__ __launch_bounds__(THREADS) void tile_sort_kernel(const uint32_t* __restrict__ list,
@@ -588,24 +600,23 @@ __global__ __launch_bounds__(THREADS) void tile_sort_kernel(const uint32_t* __re
 // tile's global ranges ((keys_tmp, ids) and the pair buffer as scratch), only
 // the BINS buckets are in shared memory.
 // Shared memory: [s_tmp: 128 words][buckets ...][kb: SMAX][vb: SMAX].
-template <uint32_t BINS, uint32_t SBINS, uint32_t SMAX, uint32_t THREADS>
-__device__ void sort_tile_global(uint32_t t, const uint32_t* __restrict__ tile_start, uint32_t capacity,
-                                 uint2* pairs, uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp,
-                                 uint32_t* sm) {
+// The same for slots [start, start + n) of tile t with entry i given by
+// load(i) (the placed pairs, or (keys_tmp, ids) themselves: the global form
+// copies its input into (keys_tmp, ids) before it uses the pair slots
+// [start, start + n) as scratch).
+template <uint32_t BINS, uint32_t SBINS, uint32_t SMAX, uint32_t THREADS, typename Load>
+__device__ void sort_range_global(uint32_t t, uint32_t start, uint32_t n, Load load, uint2* pairs, uint32_t* ids,
+                                  uint32_t* tids_out, uint32_t* keys_tmp, uint32_t* sm) {
     static_assert(4 * (THREADS / 32) <= 128, "s_tmp size");
     uint32_t* s_tmp = sm;
     uint32_t* bins = sm + 128;
     const uint32_t tid = threadIdx.x;
-    const uint32_t start = tile_start[t], end = tile_start[t + 1];
-    const uint32_t n = end - start;
-    if (end > capacity || end < start) return;
     if (n <= SMAX) {
         uint32_t* kb = bins + SBINS;
         uint32_t* vb = kb + SMAX;
-        const uint2* pr = pairs + start;
         uint32_t lo = 0xffffffffu, hi = 0;
         for (uint32_t i = tid; i < n; i += THREADS) {
-            const uint32_t k = pr[i].x;
+            const uint32_t k = load(i).x;
             lo = min(lo, k);
             hi = max(hi, k);
         }
@@ -614,12 +625,12 @@ __device__ void sort_tile_global(uint32_t t, const uint32_t* __restrict__ tile_s
         const BucketPlan bp = bucket_plan(n, mn, mx, SBINS);
         for (uint32_t b = tid; b < bp.nbins; b += THREADS) bins[b] = 0;
         __syncthreads();
-        for (uint32_t i = tid; i < n; i += THREADS) atomicAdd(&bins[(pr[i].x - mn) >> bp.shift], 1u);
+        for (uint32_t i = tid; i < n; i += THREADS) atomicAdd(&bins[(load(i).x - mn) >> bp.shift], 1u);
         __syncthreads();
         const uint32_t big = bucket_starts<THREADS>(bins, bp.nbins, s_tmp);
         if (big <= kMaxBucket) {
             for (uint32_t i = tid; i < n; i += THREADS) {
-                const uint2 q = pr[i];
+                const uint2 q = load(i);
                 const uint32_t pos = atomicAdd(&bins[(q.x - mn) >> bp.shift], 1u);
                 kb[pos] = q.x;
                 vb[pos] = q.y;
@@ -639,7 +650,7 @@ __device__ void sort_tile_global(uint32_t t, const uint32_t* __restrict__ tile_s
     uint32_t* vb = kb + n;
     uint32_t lo = 0xffffffffu, hi = 0;
     for (uint32_t i = tid; i < n; i += THREADS) {
-        const uint2 p = pairs[start + i];
+        const uint2 p = load(i);
         ka[i] = p.x;
         va[i] = p.y;
         lo = min(lo, p.x);
@@ -669,14 +680,28 @@ __device__ void sort_tile_global(uint32_t t, const uint32_t* __restrict__ tile_s
 }
 
 template <uint32_t BINS, uint32_t SBINS, uint32_t SMAX, uint32_t THREADS>
+__device__ void sort_tile_global(uint32_t t, const uint32_t* __restrict__ tile_start, uint32_t capacity,
+                                 uint2* pairs, uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp,
+                                 uint32_t* sm) {
+    const uint32_t start = tile_start[t], end = tile_start[t + 1];
+    if (end > capacity || end < start) return;
+    const uint2* pr = pairs + start;
+    sort_range_global<BINS, SBINS, SMAX, THREADS>(t, start, end - start, [pr](uint32_t i) { return pr[i]; }, pairs,
+                                                  ids, tids_out, keys_tmp, sm);
+}
+
+// taken (may be null): entries of the class list the segmented sort took.
+template <uint32_t BINS, uint32_t SBINS, uint32_t SMAX, uint32_t THREADS>
 __global__ __launch_bounds__(THREADS, 1) void tile_sort_global_kernel(const uint32_t* __restrict__ list,
                                                                    const uint32_t* list_n,
                                                                    const uint32_t* __restrict__ tile_start,
                                                                    uint32_t capacity, uint2* pairs, uint32_t* ids,
-                                                                   uint32_t* tids_out, uint32_t* keys_tmp) {
+                                                                   uint32_t* tids_out, uint32_t* keys_tmp,
+                                                                   const uint32_t* taken) {
     extern __shared__ uint32_t sm[];
     const uint32_t count = *list_n;
     for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
+        if (taken && taken[idx]) continue;  // uniform
         sort_tile_global<BINS, SBINS, SMAX, THREADS>(list[idx], tile_start, capacity, pairs, ids, tids_out,
                                                      keys_tmp, sm);
         __syncthreads();
@@ -759,6 +784,330 @@ constexpr uint32_t kThreadsS = 256, kThreads0 = 256, kThreadsM = 512, kThreads1 
 static_assert(sort_smem<kClass2, kBins2, kThreads2>() <= 227 * 1024, "per-tile sort exceeds shared memory");
 static_assert(kSortClasses == 7, "class table");
 
+// ---- segmented sort of the longest lists
+//
+// One CTA sorting a list of 10^5 entries takes milliseconds. Lists of the
+// longest class past kGiantMinList entries (the first GiantState::lists of
+// them) are instead sorted over all SMs:
+//   0. giant_select (one CTA): picks those lists, gives each its first chunk
+//      of kGiantChunk entries in one numbering over the picked lists, resets
+//      their key ranges and marks them taken for the one-CTA form.
+//   1. giant_minmax: the key range of each picked list (CTAs take chunks
+//      round-robin; each finds its list in a shared copy of the chunk bases);
+//      the lists' bucket counts are cleared on the way.
+//   2. giant_hist: a kGiantBins-bucket histogram of (key - min) >> shift per
+//      list (monotone in the key).
+//   3. giant_plan (a CTA per list): the buckets' exclusive prefix (their
+//      first slots) and the segments: runs of buckets whose first slot has
+//      the same quotient by kGiantSegTarget. Segments are contiguous in key,
+//      so the list sorted is its segments sorted, one after the other.
+//   4. giant_scatter: each entry to its bucket's slots in (keys_tmp, ids).
+//   5. giant_seg_sort: each segment of up to kClass1 entries sorted by one
+//      CTA in shared memory (entries in registers); giant_seg_big: longer
+//      ones (bunched keys) by the global form; ids and tile ids in place.
+// Every list comes out in the same total (key, id) order as a sort of the
+// whole list, so the result is bit-identical whichever form sorted it.
+
+constexpr uint32_t kGiantThreads = 256, kGiantItems = 8, kGiantChunk = kGiantThreads * kGiantItems;
+constexpr uint32_t kGiantPlanThreads = 1024;
+static_assert(kGiantBins == 2 * kGiantPlanThreads, "two buckets per plan thread");
+static_assert(kGiantMinList >= kClass2, "the segmented lists belong to the longest class");
+
+__device__ __forceinline__ uint32_t giant_shift(uint32_t mn, uint32_t mx) {
+    const uint32_t range = mx - mn;
+    const uint32_t rbits = range == 0 ? 0u : 32u - __clz(range);
+    constexpr uint32_t lbits = 11;  // log2(kGiantBins)
+    static_assert((1u << lbits) == kGiantBins, "bucket bits");
+    return rbits > lbits ? rbits - lbits : 0u;
+}
+
+__device__ __forceinline__ uint32_t giant_bucket(uint32_t k, uint32_t mn, uint32_t shift) {
+    return min((k - mn) >> shift, kGiantBins - 1);
+}
+
+// Block-wide exclusive scan of one value per thread; s32 holds 32 words.
+// Returns the exclusive prefix; total gets the sum (uniform).
+template <uint32_t THREADS>
+__device__ __forceinline__ uint32_t block_scan(uint32_t x, uint32_t* s32, uint32_t& total) {
+    constexpr uint32_t WARPS = THREADS / 32;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t incl = x;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += v;
+    }
+    __syncthreads();
+    if (lane == 31) s32[warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0, tot = 0;
+    for (uint32_t w = 0; w < WARPS; ++w) {
+        const uint32_t v = s32[w];
+        if (w < warp) wbase += v;
+        tot += v;
+    }
+    total = tot;
+    return wbase + incl - x;
+}
+
+__global__ __launch_bounds__(1024) void giant_select_kernel(const uint32_t* __restrict__ list, const uint32_t* list_n,
+                                                            const uint32_t* __restrict__ tile_start,
+                                                            uint32_t capacity, GiantState gs) {
+    __shared__ uint32_t s32[32];
+    const uint32_t count = *list_n;
+    const uint32_t tid = threadIdx.x;
+    uint32_t picked = 0, chunks = 0;
+    for (uint32_t i0 = 0; i0 < count; i0 += 1024) {
+        const uint32_t idx = i0 + tid;
+        uint32_t t = 0, start = 0, n = 0;
+        bool big = false;
+        if (idx < count) {
+            t = list[idx];
+            start = tile_start[t];
+            const uint32_t end = tile_start[t + 1];
+            n = end - start;
+            big = end <= capacity && end >= start && n > kGiantMinList;
+        }
+        uint32_t nbig;
+        const uint32_t r = picked + block_scan<1024>(big ? 1u : 0u, s32, nbig);
+        const bool take = big && r < gs.lists;
+        const uint32_t nch = take ? (n + kGiantChunk - 1) / kGiantChunk : 0u;
+        uint32_t tch;
+        const uint32_t cb = chunks + block_scan<1024>(nch, s32, tch);
+        if (idx < count) gs.taken[idx] = take ? 1u : 0u;
+        if (take) {
+            gs.sel[r] = make_uint4(t, start, n, cb);
+            gs.mm[2 * r] = 0xffffffffu;
+            gs.mm[2 * r + 1] = 0u;
+        }
+        picked += nbig;
+        chunks += tch;
+    }
+    if (tid == 0) {
+        gs.ctrl[0] = min(picked, gs.lists);
+        gs.ctrl[1] = chunks;
+        gs.ctrl[2] = 0;
+        gs.ctrl[3] = 0;
+    }
+}
+
+// The picked lists' first chunks, in shared memory (s_cb[lists] = chunks);
+// returns the picked list count. s_cb holds kGiantMaxLists + 1 words.
+__device__ __forceinline__ uint32_t giant_load_bases(const GiantState& gs, uint32_t* s_cb, uint32_t& chunks) {
+    const uint32_t m = min(gs.ctrl[0], gs.lists);
+    chunks = gs.ctrl[1];
+    for (uint32_t r = threadIdx.x; r < m; r += blockDim.x) s_cb[r] = gs.sel[r].w;
+    if (threadIdx.x == 0) s_cb[m] = chunks;
+    __syncthreads();
+    return m;
+}
+
+// The picked list holding global chunk g, searching forward from r (the
+// chunks a CTA takes rise, so its search only moves forward).
+__device__ __forceinline__ uint32_t giant_list_of(const uint32_t* s_cb, uint32_t m, uint32_t r, uint32_t g) {
+    while (r + 1 < m && s_cb[r + 1] <= g) ++r;
+    return r;
+}
+
+__global__ __launch_bounds__(kGiantThreads) void giant_minmax_kernel(const uint2* __restrict__ pairs, GiantState gs) {
+    __shared__ uint32_t s_cb[kGiantMaxLists + 1];
+    __shared__ uint32_t s_tmp[2 * (kGiantThreads / 32)];
+    uint32_t chunks;
+    const uint32_t m = giant_load_bases(gs, s_cb, chunks);
+    const uint32_t tid = threadIdx.x;
+    // Clear the picked lists' bucket counts.
+    const size_t words = (size_t)m * kGiantBins;
+    for (size_t b = (size_t)blockIdx.x * kGiantThreads + tid; b < words; b += (size_t)gridDim.x * kGiantThreads)
+        gs.hist[b] = 0;
+    uint32_t r = 0;
+    for (uint32_t g = blockIdx.x; g < chunks; g += gridDim.x) {
+        r = giant_list_of(s_cb, m, r, g);
+        const uint4 sl = gs.sel[r];
+        const uint32_t c = g - sl.w;
+        uint32_t lo = 0xffffffffu, hi = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < kGiantItems; ++j) {
+            const uint32_t i = c * kGiantChunk + j * kGiantThreads + tid;
+            if (i < sl.z) {
+                const uint32_t k = pairs[sl.y + i].x;
+                lo = min(lo, k);
+                hi = max(hi, k);
+            }
+        }
+        uint32_t mn, mx;
+        block_min_max<kGiantThreads>(lo, hi, s_tmp, mn, mx);
+        if (tid == 0) {
+            atomicMin(gs.mm + 2 * r, mn);
+            atomicMax(gs.mm + 2 * r + 1, mx);
+        }
+    }
+}
+
+__global__ __launch_bounds__(kGiantThreads) void giant_hist_kernel(const uint2* __restrict__ pairs, GiantState gs) {
+    __shared__ uint32_t s_cb[kGiantMaxLists + 1];
+    __shared__ uint32_t s_h[kGiantBins];
+    uint32_t chunks;
+    const uint32_t m = giant_load_bases(gs, s_cb, chunks);
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t b = tid; b < kGiantBins; b += kGiantThreads) s_h[b] = 0;
+    __syncthreads();
+    uint32_t r = 0;
+    for (uint32_t g = blockIdx.x; g < chunks; g += gridDim.x) {
+        r = giant_list_of(s_cb, m, r, g);
+        const uint4 sl = gs.sel[r];
+        const uint32_t c = g - sl.w;
+        const uint32_t mn = gs.mm[2 * r], shift = giant_shift(mn, gs.mm[2 * r + 1]);
+#pragma unroll
+        for (uint32_t j = 0; j < kGiantItems; ++j) {
+            const uint32_t i = c * kGiantChunk + j * kGiantThreads + tid;
+            if (i < sl.z) atomicAdd(&s_h[giant_bucket(pairs[sl.y + i].x, mn, shift)], 1u);
+        }
+        __syncthreads();
+        uint32_t* row = gs.hist + (size_t)r * kGiantBins;
+        for (uint32_t b = tid; b < kGiantBins; b += kGiantThreads) {
+            const uint32_t v = s_h[b];
+            if (v) {
+                atomicAdd(row + b, v);
+                s_h[b] = 0;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// A CTA per picked list (persistent). ctrl[2] counts the segments of up to
+// kClass1 entries (filed from the front of gs.segs), ctrl[3] the longer ones
+// (filed from the back).
+__global__ __launch_bounds__(kGiantPlanThreads) void giant_plan_kernel(GiantState gs) {
+    __shared__ uint32_t s_ex[kGiantBins + 1];
+    __shared__ uint32_t s_off[kGiantBins], s_end[kGiantBins];
+    __shared__ uint32_t s32[32];
+    const uint32_t m = min(gs.ctrl[0], gs.lists);
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t r = blockIdx.x; r < m; r += gridDim.x) {
+        const uint4 sl = gs.sel[r];
+        uint32_t* row = gs.hist + (size_t)r * kGiantBins;
+        const uint32_t b0 = 2 * tid, b1 = b0 + 1;
+        const uint32_t c0 = row[b0], c1 = row[b1];
+        uint32_t total;
+        const uint32_t e0 = block_scan<kGiantPlanThreads>(c0 + c1, s32, total);
+        const uint32_t e1 = e0 + c0;
+        row[b0] = e0;
+        row[b1] = e1;
+        s_ex[b0] = e0;
+        s_ex[b1] = e1;
+        if (tid == 0) s_ex[kGiantBins] = total;
+        __syncthreads();
+        const uint32_t T = kGiantSegTarget;
+        // Bucket b starts a run when its first slot's quotient differs from
+        // the previous bucket's.
+        const bool f0 = b0 == 0 || e0 / T != s_ex[b0 - 1] / T;
+        const bool f1 = e1 / T != e0 / T;
+        uint32_t nruns;
+        const uint32_t r0 = block_scan<kGiantPlanThreads>((uint32_t)f0 + (uint32_t)f1, s32, nruns);
+        // Run of each bucket: the starts up to and including it, minus one.
+        const uint32_t ri0 = r0 + (uint32_t)f0 - 1u, ri1 = ri0 + (uint32_t)f1;
+        if (f0) s_off[ri0] = e0;
+        if (f1) s_off[ri1] = e1;
+        // Bucket b ends its run when it is the last bucket or b + 1 starts one.
+        const bool l1 = b1 == kGiantBins - 1 || s_ex[b1 + 1] / T != e1 / T;
+        if (f1) s_end[ri0] = e1;
+        if (l1) s_end[ri1] = s_ex[b1 + 1];
+        __syncthreads();
+        // total == entries always (every chunk was counted); the test guards
+        // the scatter's slots regardless.
+        if (total == sl.z)
+            for (uint32_t q = tid; q < nruns; q += kGiantPlanThreads) {
+                const uint32_t off = s_off[q], len = s_end[q] - off;
+                if (len == 0) continue;
+                const uint32_t slot = len <= kClass1 ? atomicAdd(gs.ctrl + 2, 1u)
+                                                     : gs.seg_cap - 1u - atomicAdd(gs.ctrl + 3, 1u);
+                if (slot < gs.seg_cap) gs.segs[slot] = make_uint4(sl.x, sl.y + off, len, 0u);
+            }
+        __syncthreads();
+    }
+}
+
+__global__ __launch_bounds__(kGiantThreads) void giant_scatter_kernel(const uint2* __restrict__ pairs, GiantState gs,
+                                                                      uint32_t* keys_tmp, uint32_t* ids) {
+    __shared__ uint32_t s_cb[kGiantMaxLists + 1];
+    __shared__ uint32_t s_cnt[kGiantBins], s_base[kGiantBins];
+    uint32_t chunks;
+    const uint32_t m = giant_load_bases(gs, s_cb, chunks);
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t b = tid; b < kGiantBins; b += kGiantThreads) s_cnt[b] = 0;
+    __syncthreads();
+    uint32_t r = 0;
+    for (uint32_t g = blockIdx.x; g < chunks; g += gridDim.x) {
+        r = giant_list_of(s_cb, m, r, g);
+        const uint4 sl = gs.sel[r];
+        const uint32_t c = g - sl.w;
+        const uint32_t mn = gs.mm[2 * r], shift = giant_shift(mn, gs.mm[2 * r + 1]);
+        uint32_t* row = gs.hist + (size_t)r * kGiantBins;
+        uint32_t k[kGiantItems], v[kGiantItems], q[kGiantItems];
+#pragma unroll
+        for (uint32_t j = 0; j < kGiantItems; ++j) {
+            const uint32_t i = c * kGiantChunk + j * kGiantThreads + tid;
+            q[j] = 0xffffffffu;
+            if (i < sl.z) {
+                const uint2 p = pairs[sl.y + i];
+                k[j] = p.x;
+                v[j] = p.y;
+                q[j] = atomicAdd(&s_cnt[giant_bucket(p.x, mn, shift)], 1u);
+            }
+        }
+        __syncthreads();
+        for (uint32_t b = tid; b < kGiantBins; b += kGiantThreads) {
+            const uint32_t cnt = s_cnt[b];
+            if (cnt) {
+                s_base[b] = atomicAdd(row + b, cnt);
+                s_cnt[b] = 0;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (uint32_t j = 0; j < kGiantItems; ++j)
+            if (q[j] != 0xffffffffu) {
+                const uint32_t pos = s_base[giant_bucket(k[j], mn, shift)] + q[j];
+                if (pos < sl.z) {
+                    keys_tmp[sl.y + pos] = k[j];
+                    ids[sl.y + pos] = v[j];
+                }
+            }
+    }
+}
+
+__global__ __launch_bounds__(kThreads1) void giant_seg_sort_kernel(GiantState gs, uint2* pairs, uint32_t* ids,
+                                                                   uint32_t* tids_out, uint32_t* keys_tmp) {
+    extern __shared__ uint32_t sm[];
+    const uint32_t count = min(gs.ctrl[2], gs.seg_cap);
+    for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {
+        const uint4 sg = gs.segs[i];
+        if (sg.z > kClass1) continue;
+        const uint32_t* kk = keys_tmp + sg.y;
+        const uint32_t* vv = ids + sg.y;
+        sort_range_shared<kClass1, kBins1, kThreads1>(
+            sg.x, sg.y, sg.z, [kk, vv](uint32_t j) { return make_uint2(kk[j], vv[j]); }, pairs, ids, tids_out,
+            keys_tmp, sm);
+        __syncthreads();
+    }
+}
+
+__global__ __launch_bounds__(kThreadsGiant, 1) void giant_seg_big_kernel(GiantState gs, uint2* pairs, uint32_t* ids,
+                                                                         uint32_t* tids_out, uint32_t* keys_tmp) {
+    extern __shared__ uint32_t sm[];
+    const uint32_t count = min(gs.ctrl[3], gs.seg_cap);
+    for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {
+        const uint4 sg = gs.segs[gs.seg_cap - 1u - i];
+        const uint32_t* kk = keys_tmp + sg.y;
+        const uint32_t* vv = ids + sg.y;
+        sort_range_global<kBinsGiant, kBinsGiantShared, kGiantShared, kThreadsGiant>(
+            sg.x, sg.y, sg.z, [kk, vv](uint32_t j) { return make_uint2(kk[j], vv[j]); }, pairs, ids, tids_out,
+            keys_tmp, sm);
+        __syncthreads();
+    }
+}
+
 // grid: the class's tile count when the host knows it, else an upper bound;
 // capped at the CTAs resident at once (the kernels loop over their tiles).
 template <typename K>
@@ -792,6 +1141,16 @@ uint32_t bin_chunks(uint32_t n, int sm_count) {
 }
 
 uint32_t bin_chunk_size(uint32_t n, uint32_t chunks) { return ((n + chunks - 1) / chunks + 31) / 32 * 32; }
+
+namespace {
+uint32_t g_giant_max_lists = kGiantMaxLists;  // lowered only by sf_debug_giant_lists
+}  // namespace
+
+uint32_t giant_lists(uint32_t tiles) { return std::min(tiles, g_giant_max_lists); }
+
+void set_giant_max_lists(uint32_t lists) { g_giant_max_lists = std::min(lists, kGiantMaxLists); }
+
+uint32_t giant_seg_cap(uint32_t lists) { return (1u << 30) / kGiantSegTarget + lists + 1u; }
 
 uint32_t bin_class_limit(int k) {
     const uint32_t lim[kSortClasses - 1] = {kClassWarp, kClassS, kClass0, kClassM, kClass1, kClass2};
@@ -900,10 +1259,58 @@ void sort_streams_destroy(SortStreams* ss) {
     }
 }
 
+namespace {
+
+template <typename K>
+cudaError_t smem_attr(K kernel, size_t smem) {
+    if (smem <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+// The longest class: the segmented sort for its lists past kGiantMinList
+// entries (the first gs->lists of them), the one-CTA global form for the
+// rest. grid: the class's tile count (or an upper bound); 0 leaves the class
+// unsorted.
+cudaError_t launch_giant_sorts(uint32_t grid, const uint32_t* list, const uint32_t* words,
+                               const uint32_t* tile_start, uint32_t capacity, uint2* pairs, uint32_t* ids,
+                               uint32_t* tids_out, uint32_t* keys_tmp, int sm_count, cudaStream_t st,
+                               const GiantState* gs) {
+    if (grid == 0) return cudaSuccess;
+    const uint32_t* n = words + 8 + (kSortClasses - 1);
+    const uint32_t sms = (uint32_t)std::max(sm_count, 1);
+    auto global_form = tile_sort_global_kernel<kBinsGiant, kBinsGiantShared, kGiantShared, kThreadsGiant>;
+    cudaError_t e = smem_attr(global_form, kGiantSmem);
+    if (e != cudaSuccess) return e;
+    const bool seg = gs && gs->sel && gs->lists > 0;
+    if (seg) {
+        const GiantState g = *gs;
+        const uint32_t wide = 4 * sms;
+        giant_select_kernel<<<1, 1024, 0, st>>>(list, n, tile_start, capacity, g);
+        giant_minmax_kernel<<<wide, kGiantThreads, 0, st>>>(pairs, g);
+        giant_hist_kernel<<<wide, kGiantThreads, 0, st>>>(pairs, g);
+        giant_plan_kernel<<<std::min(std::min(grid, g.lists), 2 * sms), kGiantPlanThreads, 0, st>>>(g);
+        giant_scatter_kernel<<<wide, kGiantThreads, 0, st>>>(pairs, g, keys_tmp, ids);
+        constexpr size_t seg_smem = sort_smem<kClass1, kBins1, kThreads1>();
+        if ((e = smem_attr(giant_seg_sort_kernel, seg_smem)) != cudaSuccess) return e;
+        giant_seg_sort_kernel<<<2 * sms, kThreads1, seg_smem, st>>>(g, pairs, ids, tids_out, keys_tmp);
+        if ((e = smem_attr(giant_seg_big_kernel, kGiantSmem)) != cudaSuccess) return e;
+        giant_seg_big_kernel<<<sms, kThreadsGiant, kGiantSmem, st>>>(g, pairs, ids, tids_out, keys_tmp);
+        note_launches(7);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    global_form<<<std::min(grid, sms), kThreadsGiant, kGiantSmem, st>>>(list, n, tile_start, capacity, pairs, ids,
+                                                                         tids_out, keys_tmp,
+                                                                         seg ? gs->taken : nullptr);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
 cudaError_t launch_tile_sorts(const uint32_t grids[kSortClasses], const uint32_t* lists, const uint32_t* words,
                               uint32_t tiles, const uint32_t* tile_start, uint32_t capacity, uint2* pairs,
                               uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, int sm_count,
-                              cudaStream_t st, const SortStreams* side) {
+                              cudaStream_t st, const SortStreams* side, const GiantState* gs) {
     cudaError_t e;
     // Each form reads and overwrites only its own tiles' ranges, so the
     // classes may run concurrently.
@@ -919,9 +1326,8 @@ cudaError_t launch_tile_sorts(const uint32_t grids[kSortClasses], const uint32_t
     }
     auto L = [&](int k) { return lists + (size_t)k * tiles; };
     auto N = [&](int k) { return words + 8 + k; };
-    e = launch_sort_kernel(tile_sort_global_kernel<kBinsGiant, kBinsGiantShared, kGiantShared, kThreadsGiant>,
-                           kThreadsGiant, kGiantSmem, grids[6],
-                           sm_count, L(6), N(6), tile_start, capacity, pairs, ids, tids_out, keys_tmp, s3);
+    e = launch_giant_sorts(grids[6], L(6), words, tile_start, capacity, pairs, ids, tids_out, keys_tmp, sm_count,
+                           s3, gs);
     if (e != cudaSuccess) return e;
     e = launch_sort_kernel(tile_sort_kernel<kClass1, kBins1, kThreads1>, kThreads1,
                            sort_smem<kClass1, kBins1, kThreads1>(), grids[4], sm_count, L(4), N(4), tile_start,

@@ -219,8 +219,41 @@ constexpr uint32_t kBinSharedMax = 12288;
 // (all zero on entry).
 cudaError_t launch_bin_count(const uint2* bbox, uint32_t n, uint32_t tiles_x, uint32_t tiles, uint32_t chunks,
                              uint32_t* hist, cudaStream_t st);
+// Segmented sort of the longest lists (sf_bin.cu): each list past 24576
+// entries (up to `lists` of them per frame) gets a key histogram of
+// kGiantBins buckets, cut into segments of about kGiantSegTarget entries that
+// are sorted on separate CTAs; shorter lists of the longest class, and any
+// past `lists`, are sorted by one CTA each.
+constexpr uint32_t kGiantBins = 2048, kGiantSegTarget = 4096, kGiantMaxLists = 4096;
+constexpr uint32_t kGiantMinList = 24576;
+struct GiantState {
+    uint32_t* ctrl = nullptr;  // [4]: lists taken, chunks, short segments, long segments
+    uint4* sel = nullptr;      // [lists]: (tile, first slot, entries, first chunk)
+    uint32_t* mm = nullptr;    // [2 * lists]: key min, max of each taken list
+    uint32_t* hist = nullptr;  // [lists][kGiantBins]
+    uint32_t* taken = nullptr; // [tiles]: 1 where the longest class's entry i was taken
+    uint4* segs = nullptr;     // [seg_cap]: (tile, first slot, entries, 0)
+    uint32_t lists = 0;
+    uint32_t seg_cap = 0;
+};
+// Whether a captured graph includes the segmented sort, from the longest
+// list of the frames seen so far (`on`: the last graph had it): on past
+// kGiantMinList entries, off again below half of that. Either way the lists
+// come out in the same order; the choice is only about speed (the segmented
+// chain's seven launches cost more than they save when no list is that long).
+inline bool giant_wanted(uint32_t longest, bool on) {
+    return on ? longest > kGiantMinList / 2 : longest > kGiantMinList;
+}
+// lists = min(tiles, kGiantMaxLists); seg_cap bounds the segments of lists
+// holding up to 2^30 slots in all (each list has at most n / target + 1).
+uint32_t giant_lists(uint32_t tiles);
+uint32_t giant_seg_cap(uint32_t lists);
+// Test hook: scratches built afterwards segment at most `lists` lists (0:
+// none), so the one-CTA form takes the rest.
+void set_giant_max_lists(uint32_t lists);
 cudaError_t launch_bin_colscan(uint32_t* hist, uint32_t chunks, uint32_t tiles, uint32_t* cnt, uint32_t* lists,
                                uint32_t* words, cudaStream_t st);
+
 cudaError_t launch_bin_place(const uint2* bbox, const uint32_t* depth_keys, uint32_t n, uint32_t tiles_x,
                              uint32_t tiles, uint32_t chunks, const uint32_t* hist, const uint32_t* tile_start,
                              uint32_t capacity, uint2* pairs, uint32_t* err, cudaStream_t st);
@@ -256,10 +289,12 @@ void sort_streams_destroy(SortStreams* ss);
 // (tids_out may be null); keys_tmp: capacity u32 of scratch (may alias
 // tids_out). grids[k]: the tile count of size class k, or an upper bound
 // when the counts are on the device (0 skips the class).
+// gs (may be null: every longest list on the one-CTA form): the segmented
+// sort's buffers, sized for `tiles` tiles.
 cudaError_t launch_tile_sorts(const uint32_t grids[kSortClasses], const uint32_t* lists, const uint32_t* words,
                               uint32_t tiles, const uint32_t* tile_start, uint32_t capacity, uint2* pairs,
                               uint32_t* ids, uint32_t* tids_out, uint32_t* keys_tmp, int sm_count,
-                              cudaStream_t st, const SortStreams* side = nullptr);
+                              cudaStream_t st, const SortStreams* side = nullptr, const GiantState* gs = nullptr);
 
 // ---- segmentation (sf_seg.cu)
 constexpr int kGridPts = 445;

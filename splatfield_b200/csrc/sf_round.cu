@@ -84,6 +84,7 @@ struct RoundLane {
     uint32_t* hist = nullptr;
     uint32_t* cnt = nullptr;
     uint32_t* lists = nullptr;
+    GiantState giant;  // segmented sort of the longest lists
     SortStreams sort_streams;
 };
 
@@ -130,6 +131,10 @@ struct sf_round_t {
     int g_mode = -1;
     int g_adjoint = -1;
     uint32_t g_lanes = 0, g_cull = 0, g_build = 0, g_order = 0, g_split = 0, g_radix = 0;
+    // Per view: the longest tile list of the last round, and whether the
+    // graph includes the segmented sort of the longest lists for the view.
+    std::vector<uint32_t> longest;
+    std::vector<uint8_t> g_giant;
     uint32_t chunks = 1;
     std::vector<const sf_mask_t*> g_masks;
 };
@@ -146,6 +151,9 @@ void lane_free(RoundLane& L) {
     L.gid_a = nullptr;
     dfree(L.tile_start); dfree(L.partials); dfree(L.final_t); dfree(L.n_contrib);
     dfree(L.hist); dfree(L.cnt); dfree(L.lists);
+    dfree(L.giant.ctrl); dfree(L.giant.sel); dfree(L.giant.mm); dfree(L.giant.hist);
+    dfree(L.giant.taken); dfree(L.giant.segs);
+    L.giant.lists = L.giant.seg_cap = 0;
     sort_streams_destroy(&L.sort_streams);
     if (L.stream) cudaStreamDestroy(L.stream);
     if (L.join) cudaEventDestroy(L.join);
@@ -170,6 +178,14 @@ cudaError_t lane_alloc(sf_round_t* r, RoundLane& L, uint64_t cap) {
         RA(L.hist, (size_t)r->chunks * r->max_tiles);
         RA(L.cnt, (size_t)r->max_tiles + 1);
         RA(L.lists, (size_t)(kSortClasses + 1) * r->max_tiles);
+        L.giant.lists = giant_lists(r->max_tiles);
+        L.giant.seg_cap = giant_seg_cap(L.giant.lists);
+        RA(L.giant.ctrl, 4);
+        RA(L.giant.sel, L.giant.lists);
+        RA(L.giant.mm, 2 * (size_t)L.giant.lists);
+        RA(L.giant.hist, (size_t)L.giant.lists * kGiantBins);
+        RA(L.giant.taken, r->max_tiles);
+        RA(L.giant.segs, L.giant.seg_cap);
     }
 #undef RA
     if ((e = cudaMalloc(&L.scan_tmp, scan_temp_bytes(std::max(n, r->max_tiles + 1)))) != cudaSuccess) return e;
@@ -370,7 +386,9 @@ cudaError_t enqueue_view(sf_round_t* r, RoundLane& L, uint32_t v, const sf_splat
             for (int k = 0; k < kSortClasses; ++k) grids[k] = tiles;
             if (order == SF_ORDER_HYBRID) grids[kSortClasses - 1] = 0;
             if ((e = launch_tile_sorts(grids, L.lists, words, tiles, L.tile_start, (uint32_t)L.cap, pairs, L.gid_e,
-                                       nullptr, L.tid_e, r->sm_count, st, &L.sort_streams)) != cudaSuccess)
+                                       nullptr, L.tid_e, r->sm_count, st, &L.sort_streams,
+                                       giant_wanted(r->longest[v], r->g_giant[v]) ? &L.giant : nullptr)) !=
+                cudaSuccess)
                 return e;
             gids = L.gid_e;
         }
@@ -454,7 +472,15 @@ int build_graph(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, int
     r->g_split = r->tuning.raster_split;
     r->g_radix = r->tuning.radix_bits;
     r->g_masks = r->masks;
+    for (uint32_t v = 0; v < r->views; ++v) r->g_giant[v] = giant_wanted(r->longest[v], r->g_giant[v]);
     return SF_OK;
+}
+
+// Whether some view's choice of the segmented sort differs from the graph's.
+bool giant_changed(const sf_round_t* r) {
+    for (uint32_t v = 0; v < r->views; ++v)
+        if (giant_wanted(r->longest[v], r->g_giant[v]) != (r->g_giant[v] != 0)) return true;
+    return false;
 }
 
 // Launch the round (rebuilding buffers/graph when needed), wait, check.
@@ -470,8 +496,8 @@ int run_round(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, const
             r->g_adjoint != (int)r->adjoint ||
             r->g_cull != r->tuning.raster_cull || r->g_build != r->tuning.isect_build ||
             r->g_order != r->tuning.raster_order || r->g_split != r->tuning.raster_split ||
-            r->g_radix != r->tuning.radix_bits ||
-            r->g_masks != r->masks) {
+            r->g_radix != r->tuning.radix_bits || r->g_masks != r->masks ||
+            giant_changed(r)) {
             const int rc = build_graph(r, sp, beta, mode);
             if (rc != SF_OK) return rc;
         }
@@ -492,6 +518,7 @@ int run_round(sf_round_t* r, const sf_splats_t* sp, const sf_beta_t* beta, const
             uint64_t total;
             std::memcpy(&total, w + 4, 8);
             worst = std::max(worst, total);
+            r->longest[v] = w[6];
             if (w[1] & SF_DEV_ERR_CAPACITY) over = true;
         }
         if (!over) return SF_OK;
@@ -540,6 +567,8 @@ int sf_round_create(sf_ctx ctx, uint32_t total, uint32_t n_views, const uint32_t
     r->views = n_views;
     r->w.assign(widths, widths + n_views);
     r->h.assign(heights, heights + n_views);
+    r->longest.assign(n_views, 0u);
+    r->g_giant.assign(n_views, 0u);
     for (uint32_t v = 0; v < n_views; ++v) {
         r->max_tiles = std::max(r->max_tiles, ((widths[v] + 15) / 16) * ((heights[v] + 15) / 16));
         r->max_pixels = std::max<uint64_t>(r->max_pixels, (uint64_t)widths[v] * heights[v]);

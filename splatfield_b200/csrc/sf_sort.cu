@@ -545,3 +545,8 @@ extern "C" int sf_debug_lookback(uint32_t spin_limit, int withhold) {
     sfk::g_test_knobs = sfk::LookbackKnobs{spin_limit, withhold ? 1u : 0u};
     return SF_OK;
 }
+
+extern "C" int sf_debug_giant_lists(uint32_t lists) {
+    sfk::set_giant_max_lists(lists);
+    return SF_OK;
+}

@@ -71,14 +71,31 @@ def test_binned_orders_exact_depth_ties_by_id(ctx, oracle_mod):
     check(got, want, img, want_img)
 
 
-@pytest.mark.parametrize("n", [20000, 40000])
+@pytest.fixture
+def giant_lists():
+    """Sets how many of a frame's longest lists the segmented sort takes
+    (for scratches created afterwards); restores the default after."""
+    def set_(k):
+        assert L.lib().sf_debug_giant_lists(k) == 0
+
+    yield set_
+    set_(4096)
+
+
+@pytest.mark.parametrize("segmented", [4096, 1, 0])
+@pytest.mark.parametrize("n", [20000, 40000, 150000])
 @pytest.mark.parametrize("quantised", [False, True])
-def test_binned_sorts_lists_beyond_shared_memory(ctx, oracle_mod, quantised, n):
+def test_binned_sorts_lists_beyond_shared_memory(ctx, oracle_mod, giant_lists, quantised, n, segmented):
     """n splats over one spot: the centre tiles' lists exceed the largest
-    register-held sort class. Up to 24576 entries they are bucket-sorted in
-    shared memory, longer ones in global memory. With depths quantised to 5
-    values the buckets overflow and the global-memory radix sort with its id
-    passes runs, from either form."""
+    register-held sort class (12288 entries). Up to 24576 entries one CTA
+    sorts each list in shared memory. Longer lists are by default cut into
+    key-contiguous segments sorted on separate CTAs (segments of up to 6144
+    entries in registers, longer ones, from bunched keys, by the shared- or
+    global-memory form); `segmented` 1 cuts only the first such list and
+    sorts the others on one CTA each in global memory, 0 sorts all of them
+    that way. With depths quantised to 5 values the buckets overflow and the
+    radix sort with its id passes runs, in every form."""
+    giant_lists(segmented)
     rng = np.random.default_rng(33)
     z = rng.uniform(0, 1, n)
     if quantised:
@@ -86,8 +103,52 @@ def test_binned_sorts_lists_beyond_shared_memory(ctx, oracle_mod, quantised, n):
     pos = np.stack([rng.normal(0, 0.002, n), rng.normal(0, 0.002, n), 1.0 + z], 1)
     attr = opaque(pos)
     got, want, img, want_img = build_both(oracle_mod, attr, zero_sh(n), 1, 64, 64)
-    assert np.diff(got["tile_start"]).max() > (24576 if n > 24576 else 12288)
+    lens = np.diff(got["tile_start"])
+    assert lens.max() > (24576 if n > 24576 else 12288)
+    if n > 24576:
+        assert (lens > 24576).sum() > 1
     check(got, want, img, want_img)
+
+
+def test_segmented_sort_in_frame_graph_and_round(ctx, oracle_mod):
+    """Lists of up to ~100k entries through the frame graph (device-side
+    counts, sort classes on side streams) and the batched round: the same
+    image as the oracle, and round responsibility words equal to the plain
+    per-view path's. The first frame batch and the first round are captured
+    before any list length is known (one-CTA sorts); the second ones include
+    the segmented sort, chosen from the lists the first ones saw."""
+    rng = np.random.default_rng(35)
+    n, w, h = 150000, 96, 80
+    pos = np.stack([rng.normal(0, 0.01, n), rng.normal(0, 0.01, n), 1.0 + rng.uniform(0, 1, n)], 1)
+    attr, sh = opaque(pos), zero_sh(n)
+    splats = sf.Splats(attr, sh)
+    cam = sf.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    cam.fov[0], cam.fov[1] = synth.fov_for(w, h)
+    scratch = sf.RenderScratch(n, (w, h))
+    cam_o = oracle_mod.look_at((0.0, 0.0, -3.0), (0.0, 0.0, 0.0))
+    cam_o.fov[0], cam_o.fov[1] = synth.fov_for(w, h)
+    want = oracle_mod.prepare(cam_o, w, h, attr, sh, 1)
+    assert np.diff(want["ranges"], axis=1).max() > 50000
+    want_img = oracle_mod.rasterize(want, 0)["bitmap"]
+    for _ in range(2):
+        got = splats.render_frames(scratch, [cam, cam], (w, h)).read()
+        np.testing.assert_array_equal(got, want_img)
+    rnd = sf.Round(n, [(w, h)] * 3)
+    cams = [cam, sf.look_at((0.2, 0.1, -3.0), (0.0, 0.0, 0.0)), sf.look_at((-0.1, 0.2, -3.0), (0.0, 0.0, 0.0))]
+    for c in cams:
+        c.fov[0], c.fov[1] = synth.fov_for(w, h)
+    rnd.set_tuning(lanes=2)
+    plain = []
+    for c in cams:
+        acc = sf.Accumulators(n)
+        splats.render_responsibility(scratch, acc, c, (w, h))
+        plain.append((acc.bits.read(), acc.scale))
+    for _ in range(2):
+        rnd.eig(splats, None, cams)
+        for v in range(len(cams)):
+            words, scale, _, _ = rnd.responsibility(v)
+            np.testing.assert_array_equal(words.read(), plain[v][0])
+            assert scale == plain[v][1]
 
 
 def scene_for(kind):
