@@ -189,7 +189,14 @@ typedef struct {
      * pass (0: 8). Same order either way; narrower digits take more passes
      * with fewer bins each. */
     uint32_t radix_bits;
-    uint32_t reserved[1];
+    /* Frame pipes of the camera-path calls (sf_render_frames / _to_host):
+     * 0 or 2 (default): frames alternate between the scratch and a second,
+     * internal copy of its frame buffers, each with its own frame graph and
+     * stream, so one frame's projection and build run while the other's
+     * raster finishes (the copy is allocated on the first path of two or
+     * more frames and holds the scratch's capacity); 1: one pipe. Same
+     * images either way. */
+    uint32_t frame_pipes;
 } sf_tuning;
 #define SF_ISECTS_BINNED 0u
 #define SF_ISECTS_DEPTH_SORTED 1u
@@ -203,7 +210,8 @@ int sf_scratch_get_tuning(sf_scratch s, sf_tuning* t);
 /* Frame autotuner (no counterpart in the reference): times sf_render_frames
  * over cams[count] at w x h for each raster form in a coordinate search (two
  * sweeps over raster_cull {0,1}, raster_split {1,2,4}, raster_order {sorted,
- * hybrid, in-raster} and raster_schedule {longest, tiles}; best of three
+ * hybrid, in-raster}, raster_schedule {longest, tiles} and frame_pipes
+ * {2, 1}; best of three
  * paths after a warm-up path), keeps the fastest on the scratch and returns
  * it with its time per frame. Images are the same in every form. */
 int sf_scratch_autotune(sf_splats s, sf_scratch scratch, const sf_camera* cams, uint32_t count, uint32_t w,

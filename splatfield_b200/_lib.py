@@ -57,7 +57,7 @@ class Tuning(C.Structure):
 
     _fields_ = [("raster_cull", C.c_uint32), ("isect_build", C.c_uint32), ("raster_detail", C.c_uint32),
                 ("raster_order", C.c_uint32), ("raster_schedule", C.c_uint32), ("raster_split", C.c_uint32),
-                ("radix_bits", C.c_uint32), ("reserved", C.c_uint32 * 1)]
+                ("radix_bits", C.c_uint32), ("frame_pipes", C.c_uint32)]
 
 
 class RoundTuning(C.Structure):

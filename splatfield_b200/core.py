@@ -564,14 +564,15 @@ class RenderScratch:
 
     def set_tuning(self, raster_cull: int = 0, isect_build: int = L.ISECTS_BINNED, raster_detail: int = 0,
                    raster_order: int = L.ORDER_SORTED, raster_schedule: int = L.SCHEDULE_LONGEST,
-                   raster_split: int = 1, radix_bits: int = 8) -> None:
+                   raster_split: int = 1, radix_bits: int = 8, frame_pipes: int = 2) -> None:
         """Kernel forms (results are identical across forms): raster_cull 0/1,
         isect_build ISECTS_BINNED (default) or ISECTS_DEPTH_SORTED,
         raster_detail 1 to count the per-pair diagnostics of ``stats``,
         raster_order ORDER_SORTED (default), ORDER_IN_RASTER or ORDER_HYBRID,
         raster_schedule SCHEDULE_LONGEST (default) or SCHEDULE_TILES,
         raster_split 1 (default), 2 or 4 rasterizer CTAs per tile,
-        radix_bits 4..8 (default 8) digit width of the depth-sorted build."""
+        radix_bits 4..8 (default 8) digit width of the depth-sorted build,
+        frame_pipes 2 (default) or 1 frame pipes of the camera-path calls."""
         t = L.Tuning()
         t.raster_cull = int(raster_cull)
         t.isect_build = int(isect_build)
@@ -580,6 +581,7 @@ class RenderScratch:
         t.raster_schedule = int(raster_schedule)
         t.raster_split = int(raster_split)
         t.radix_bits = int(radix_bits)
+        t.frame_pipes = int(frame_pipes)
         check(lib().sf_scratch_set_tuning(self.handle, C.byref(t)))
 
     def autotune(self, splats: "Splats", cameras, img_size, stream=None) -> tuple:
@@ -599,7 +601,7 @@ class RenderScratch:
         return {"raster_cull": int(t.raster_cull), "isect_build": int(t.isect_build),
                 "raster_detail": int(t.raster_detail), "raster_order": int(t.raster_order),
                 "raster_schedule": int(t.raster_schedule), "raster_split": int(t.raster_split) or 1,
-                "radix_bits": int(t.radix_bits) or 8}
+                "radix_bits": int(t.radix_bits) or 8, "frame_pipes": int(t.frame_pipes) or 2}
 
     def read(self, what: int, count: int, dtype=np.uint32, stream=None) -> np.ndarray:
         out = np.empty(count, dtype)

@@ -188,6 +188,13 @@ struct sf_scratch_t {
     bool has_forward = false;
     sf_camera fwd_cam{};
     float* d2d = nullptr;
+    // Second frame pipe of the camera-path calls (tuning.frame_pipes): an
+    // internal scratch with its own frame buffers, frame graph and launch
+    // stream; frames alternate between it and this scratch. fork / join
+    // order its stream after the caller's and the caller's after it.
+    sf_scratch_t* twin = nullptr;
+    cudaStream_t twin_stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 struct sf_radix_t {
@@ -758,58 +765,120 @@ cudaError_t frames_batch_resources(sf_scratch s, uint32_t count, size_t image_wo
     return cudaSuccess;
 }
 
+// The second frame pipe of s at w x h (allocated on first use): the twin
+// scratch holds at least s's capacity and s's tuning and list statistics,
+// so both pipes capture the same kernels.
+int twin_ready(sf_splats sp, sf_scratch s, uint32_t w, uint32_t h) {
+    if (!s->twin) {
+        s->twin = new sf_scratch_t();
+        s->twin->ctx = s->ctx;
+    }
+    sf_scratch t = s->twin;
+    if (t->total != sp->n || t->w != w || t->h != h || !t->bitmap) SF_CK(scratch_build(t, sp->n, w, h));
+    if (t->cap < s->cap) SF_CK(grow_isects(t, s->cap));
+    t->tuning = s->tuning;
+    t->longest = s->longest;
+    if (!s->twin_stream) SF_CK(cudaStreamCreateWithFlags(&s->twin_stream, cudaStreamNonBlocking));
+    if (!s->fork) SF_CK(cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming));
+    if (!s->join) SF_CK(cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming));
+    return frame_graph_ready(sp, t, w, h);
+}
+
+// Copies the status words that run [first, end) of a camera path saved to
+// its pipes' device rings into frame_words[16 * i] (frame i on pipe
+// pipe_of(i); each pipe's ring holds its frames of the run in launch order).
+template <typename PipeOf>
+cudaError_t read_rings(sf_scratch const pipes[2], PipeOf pipe_of, uint32_t first, uint32_t end,
+                       uint32_t* frame_words) {
+    uint32_t on[2] = {0, 0};
+    for (uint32_t i = first; i < end; ++i) ++on[pipe_of(i)];
+    std::vector<uint32_t> ring[2];
+    for (int p = 0; p < 2; ++p) {
+        if (!on[p]) continue;
+        ring[p].resize(16 * (size_t)on[p]);
+        const cudaError_t e =
+            cudaMemcpy(ring[p].data(), pipes[p]->fg.ring, 64 * (size_t)on[p], cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return e;
+    }
+    uint32_t k[2] = {0, 0};
+    for (uint32_t i = first; i < end; ++i) {
+        const int p = pipe_of(i);
+        std::memcpy(frame_words + 16 * (size_t)i, ring[p].data() + 16 * (size_t)k[p]++, 64);
+    }
+    return cudaSuccess;
+}
+
 // `count` frames through the frame graph, frame i's image to
 // host_out + i * w * h (host_out null: the images stay on the device, the
 // last one in the scratch). The device-to-host copy of frame i (copy stream,
-// from a staging image) overlaps frame i + 1 on st. Frames whose
-// intersections passed the capacity are rendered again, one by one, after
-// the capacity has grown. Syncs at the end.
+// from a staging image) overlaps the next frames. With two frame pipes the
+// frames alternate between s (on st) and its twin (on the twin's stream),
+// the last frame on s, so one frame's projection and intersection build
+// overlap the other's raster. Frames whose intersections passed their
+// pipe's capacity are rendered again, one by one, after the capacity has
+// grown. Syncs at the end.
 int frames_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cams, uint32_t count, uint32_t w,
                         uint32_t h, cudaStream_t st, uint32_t* host_out) {
     auto& g = s->fg;
     const size_t img = (size_t)w * h;
+    const bool two = count >= 2 && s->tuning.frame_pipes != 1;
     int rc = frame_graph_ready(sp, s, w, h);
     if (rc != SF_OK) return rc;
+    if (two && (rc = twin_ready(sp, s, w, h)) != SF_OK) return rc;
+    sf_scratch const pipes[2] = {s, two ? s->twin : s};
+    cudaStream_t const streams[2] = {st, two ? s->twin_stream : st};
+    auto pipe_of = [&](uint32_t i) { return two ? (int)((count - 1 - i) & 1u) : 0; };
     SF_CK(frames_batch_resources(s, count, host_out ? img : 0));
     for (uint32_t i = 0; i < count; ++i) view_for_camera(cams[i], w, h, g.views + i);
     // The copy stream may still hold another batch's copies of the staging
     // images: the first two frames of this one wait for them.
     SF_CK(cudaEventRecord(g.ready[0], g.copy));
     SF_CK(cudaStreamWaitEvent(st, g.ready[0], 0));
+    if (two) {
+        SF_CK(cudaEventRecord(s->fork, st));
+        SF_CK(cudaStreamWaitEvent(streams[1], s->fork, 0));
+    }
     for (uint32_t i = 0; i < count; ++i) {
         const int slot = (int)(i & 1u);
-        // Each run of up to kFrameRing frames saves its words to the device
-        // ring, read back once after the run has finished (a read-back after
-        // every frame cost 2% of the frame rate).
+        const int p = pipe_of(i);
+        sf_scratch P = pipes[p];
+        cudaStream_t ps = streams[p];
+        // Each run of up to kFrameRing frames saves its words to the pipes'
+        // device rings, read back once after the run has finished (a
+        // read-back after every frame cost 2% of the frame rate).
         if (i % kFrameRing == 0) {
             if (i > 0) {
-                SF_CK(cudaStreamSynchronize(st));
-                SF_CK(cudaMemcpy(g.frame_words + 16 * (size_t)(i - kFrameRing), g.ring, 64 * (size_t)kFrameRing,
-                                 cudaMemcpyDeviceToHost));
+                SF_CK(cudaStreamSynchronize(streams[0]));
+                SF_CK(cudaStreamSynchronize(streams[1]));
+                SF_CK(read_rings(pipes, pipe_of, i - kFrameRing, i, g.frame_words));
             }
-            SF_CK(cudaMemsetAsync(g.ring_counter, 0, 4, st));
+            SF_CK(cudaMemsetAsync(pipes[0]->fg.ring_counter, 0, 4, streams[0]));
+            if (two) SF_CK(cudaMemsetAsync(pipes[1]->fg.ring_counter, 0, 4, streams[1]));
         }
-        SF_CK(cudaMemcpyAsync(g.view_dev, g.views + i, sizeof(sf_view), cudaMemcpyHostToDevice, st));
-        SF_CK(cudaGraphLaunch(g.exec, st));
-        note_launches(g.kernels);
+        SF_CK(cudaMemcpyAsync(P->fg.view_dev, g.views + i, sizeof(sf_view), cudaMemcpyHostToDevice, ps));
+        SF_CK(cudaGraphLaunch(P->fg.exec, ps));
+        note_launches(P->fg.kernels);
         if (!host_out) continue;
-        if (i >= 2) SF_CK(cudaStreamWaitEvent(st, g.copied[slot], 0));
-        SF_CK(cudaMemcpy2DAsync(g.stage[slot], (size_t)w * 4, s->bitmap, (size_t)s->row_stride * 4,
-                                (size_t)w * 4, h, cudaMemcpyDeviceToDevice, st));
-        SF_CK(cudaEventRecord(g.ready[slot], st));
+        // Frames i and i + 2 share a staging image (and, with two pipes, a
+        // pipe).
+        if (i >= 2) SF_CK(cudaStreamWaitEvent(ps, g.copied[slot], 0));
+        SF_CK(cudaMemcpy2DAsync(g.stage[slot], (size_t)w * 4, P->bitmap, (size_t)P->row_stride * 4,
+                                (size_t)w * 4, h, cudaMemcpyDeviceToDevice, ps));
+        SF_CK(cudaEventRecord(g.ready[slot], ps));
         SF_CK(cudaStreamWaitEvent(g.copy, g.ready[slot], 0));
         SF_CK(cudaMemcpyAsync(host_out + i * img, g.stage[slot], img * 4, cudaMemcpyDeviceToHost, g.copy));
         SF_CK(cudaEventRecord(g.copied[slot], g.copy));
     }
+    if (two) {
+        SF_CK(cudaEventRecord(s->join, streams[1]));
+        SF_CK(cudaStreamWaitEvent(st, s->join, 0));
+    }
     SF_CK(cudaStreamSynchronize(g.copy));
     SF_CK(cudaStreamSynchronize(st));
-    {
-        const uint32_t first = (count - 1) / kFrameRing * kFrameRing;
-        SF_CK(cudaMemcpy(g.frame_words + 16 * (size_t)first, g.ring, 64 * (size_t)(count - first),
-                         cudaMemcpyDeviceToHost));
-    }
+    SF_CK(read_rings(pipes, pipe_of, (count - 1) / kFrameRing * kFrameRing, count, g.frame_words));
     uint64_t need = 0;
     uint32_t longest = 0;
+    bool over = false;
     for (uint32_t i = 0; i < count; ++i) {
         const uint32_t* hw = g.frame_words + 16 * (size_t)i;
         if (hw[1] & SF_DEV_ERR_TIMEOUT) return fail(SF_ERR_TIMEOUT, "device look-back wait timed out");
@@ -817,20 +886,23 @@ int frames_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cams, uint3
         std::memcpy(&total, hw + 4, 8);
         if (total > kMaxIsects) return fail(SF_ERR_CAPACITY, "intersection count exceeds 2^30-1");
         if (total > need) need = total;
+        if (total > pipes[pipe_of(i)]->cap) over = true;
         longest = std::max(longest, hw[6]);
     }
-    if (need > s->cap) {
-        // Frames past the capacity (their images were drawn from clamped
-        // lists) are rendered again after one growth.
+    if (two) s->twin->longest = longest;
+    if (over) {
+        // Frames past their pipe's capacity (their images were drawn from
+        // clamped lists) are rendered again on s after one growth.
         std::vector<uint32_t> redo;
         for (uint32_t i = 0; i < count; ++i) {
             uint64_t total = 0;
             std::memcpy(&total, g.frame_words + 16 * (size_t)i + 4, 8);
-            if (total > s->cap) redo.push_back(i);
+            if (total > pipes[pipe_of(i)]->cap) redo.push_back(i);
         }
         std::fprintf(stderr, "splatfield_b200: intersection capacity %llu reached (%llu needed); growing\n",
                      (unsigned long long)s->cap, (unsigned long long)need);
         SF_CK(grow_isects(s, need));
+        if (two) SF_CK(grow_isects(s->twin, need));
         for (uint32_t i : redo) {
             rc = frame_graph_render(sp, s, cams + i, w, h, st, host_out ? host_out + i * img : nullptr);
             if (rc != SF_OK) return rc;
@@ -1043,6 +1115,13 @@ int sf_scratch_create(sf_ctx ctx, uint32_t total, uint32_t w, uint32_t h, sf_scr
 int sf_scratch_destroy(sf_scratch s) {
     if (!s) return SF_OK;
     use_device(s->ctx->device);
+    if (s->twin_stream) {
+        cudaStreamSynchronize(s->twin_stream);
+        cudaStreamDestroy(s->twin_stream);
+    }
+    if (s->fork) cudaEventDestroy(s->fork);
+    if (s->join) cudaEventDestroy(s->join);
+    sf_scratch_destroy(s->twin);
     scratch_free_frame(s);
     scratch_free_isects(s);
     dfree(s->words);
@@ -1080,6 +1159,7 @@ int sf_scratch_set_tuning(sf_scratch s, const sf_tuning* t) {
         return fail(SF_ERR_ARG, "raster_split must be 1, 2 or 4");
     if (t->radix_bits != 0 && (t->radix_bits < 4 || t->radix_bits > 8))
         return fail(SF_ERR_ARG, "radix_bits must be 4..8 (0: 8)");
+    if (t->frame_pipes > 2) return fail(SF_ERR_ARG, "frame_pipes must be 1 or 2 (0: 2)");
     s->tuning = *t;
     return SF_OK;
 }
@@ -1102,6 +1182,7 @@ int sf_scratch_reserve(sf_scratch s, uint64_t isects) {
         if (isects > kMaxIsects) return fail(SF_ERR_CAPACITY, "intersection count exceeds 2^30-1");
         SF_CK(use_device(s->ctx->device));
         SF_CK(grow_isects(s, isects));
+        if (s->twin && s->twin->bitmap) SF_CK(grow_isects(s->twin, isects));
         return SF_OK;
     })
 }
@@ -1378,18 +1459,20 @@ static int scratch_autotune(sf_splats s, sf_scratch scratch, const sf_camera* ca
         sf_tuning winner = scratch->tuning;
         winner.raster_detail = 0;
         if (winner.raster_split == 0) winner.raster_split = 1;
+        if (winner.frame_pipes == 0) winner.frame_pipes = 2;
         float winner_ms = 1e30f;
         int rc = time_of(winner, &winner_ms);
         if (rc != SF_OK) return rc;
-        const uint32_t vals[4][3] = {{0, 1, 0}, {1, 2, 4}, {SF_ORDER_SORTED, SF_ORDER_HYBRID, SF_ORDER_IN_RASTER},
-                                     {SF_SCHEDULE_LONGEST, SF_SCHEDULE_TILES, 0}};
-        const int nvals[4] = {2, 3, 3, 2};
+        const uint32_t vals[5][3] = {{0, 1, 0}, {1, 2, 4}, {SF_ORDER_SORTED, SF_ORDER_HYBRID, SF_ORDER_IN_RASTER},
+                                     {SF_SCHEDULE_LONGEST, SF_SCHEDULE_TILES, 0}, {2, 1, 0}};
+        const int nvals[5] = {2, 3, 3, 2, 2};
         for (int sweep = 0; sweep < 2; ++sweep)
-            for (int dim = 0; dim < 4; ++dim)
+            for (int dim = 0; dim < 5; ++dim)
                 for (int k = 0; k < nvals[dim]; ++k) {
                     sf_tuning t = winner;
                     uint32_t* field = dim == 0 ? &t.raster_cull : dim == 1 ? &t.raster_split
-                                    : dim == 2 ? &t.raster_order : &t.raster_schedule;
+                                    : dim == 2 ? &t.raster_order : dim == 3 ? &t.raster_schedule
+                                                                            : &t.frame_pipes;
                     if (*field == vals[dim][k]) continue;
                     *field = vals[dim][k];
                     float ms = 0.f;

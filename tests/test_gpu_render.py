@@ -384,6 +384,49 @@ def test_render_frames_equals_render_with_and_counts_replays(ctx, oracle_mod):
     np.testing.assert_array_equal(last, oracle_mod.rasterize(prep, 0)["bitmap"])
 
 
+@pytest.mark.parametrize("count", [2, 3, 6])
+def test_two_frame_pipes_equal_one_pipe_and_oracle(ctx, oracle_mod, count):
+    """frame_pipes 2 (frames alternating between the scratch and its internal
+    second pipe, on two streams) and frame_pipes 1 give the same images frame
+    for frame, through sf_render_frames_to_host and sf_render_frames, for odd
+    and even path lengths. The first path starts below the capacity its
+    frames need, on both pipes, so frames of either pipe are rendered again
+    after the growth; the scratch is left holding the last frame."""
+    from splatfield_b200 import synth
+
+    n, w, h = 50000, 288, 200
+    attr, sh = synth.scene_uniform(n, 1, 31)
+    attr = attr.reshape(11, n)
+    attr[7:10] += 3.0  # about 5M intersections per frame, past the first capacity (2^22)
+    attr = attr.reshape(-1)
+    splats = sf.Splats(attr, sh)
+    poses = [(0.0, 0.0, -3.0), (0.4, 0.2, -3.2), (-0.5, 0.1, -2.6), (0.0, 0.6, -3.5), (0.2, -0.3, -2.9),
+             (-0.3, -0.4, -3.1)][:count]
+    cams = [sf.look_at(p, (0.0, 0.0, 0.0)) for p in poses]
+    two = sf.RenderScratch(n, (w, h))
+    assert two.get_tuning()["frame_pipes"] == 2
+    got = sf.pinned_empty((count, h, w), np.uint32)
+    splats.render_frames_to_host(two, cams, (w, h), out=got)
+    assert two.capacity() > (1 << 22)
+    for i, p in enumerate(poses):
+        prep = oracle_mod.prepare(oracle_mod.look_at(p, (0.0, 0.0, 0.0)), w, h, attr, sh, 1)
+        np.testing.assert_array_equal(got[i], oracle_mod.rasterize(prep, 0)["bitmap"][:, :w])
+    one = sf.RenderScratch(n, (w, h))
+    one.set_tuning(frame_pipes=1)
+    want = sf.pinned_empty((count, h, w), np.uint32)
+    splats.render_frames_to_host(one, cams[::-1], (w, h), out=want)
+    again = sf.pinned_empty((count, h, w), np.uint32)
+    splats.render_frames_to_host(two, cams[::-1], (w, h), out=again)
+    np.testing.assert_array_equal(again, want)
+    np.testing.assert_array_equal(again[::-1], got)
+    last = splats.render_frames(two, cams, (w, h)).read()
+    np.testing.assert_array_equal(last, splats.render_frames(one, cams, (w, h)).read())
+    np.testing.assert_array_equal(last[:, :w], got[-1])
+    two.reserve(1 << 24)
+    splats.render_frames_to_host(two, cams, (w, h), out=again)
+    np.testing.assert_array_equal(again, got)
+
+
 @pytest.mark.parametrize("split", [2, 4])
 @pytest.mark.parametrize("cull", [0, 1])
 @pytest.mark.parametrize("order", [sf.ORDER_SORTED, sf.ORDER_HYBRID, sf.ORDER_IN_RASTER])
