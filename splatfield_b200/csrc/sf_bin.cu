@@ -428,18 +428,32 @@ __device__ __forceinline__ BucketPlan bucket_plan(uint32_t n, uint32_t mn, uint3
     return {shift, (range >> shift) + 1u};  // nbins <= 2^lbits <= max_bins
 }
 
+// Clears the counts of buckets [0, nbins) in 16-byte words (bins is 16-byte
+// aligned and holds a whole number of them past nbins).
+template <uint32_t THREADS>
+__device__ __forceinline__ void bucket_clear(uint32_t* bins, uint32_t nbins) {
+    uint4* b4 = reinterpret_cast<uint4*>(bins);
+    for (uint32_t q = threadIdx.x; q < (nbins + 3u) / 4u; q += THREADS) b4[q] = make_uint4(0u, 0u, 0u, 0u);
+}
+
 // Turns bucket counts into bucket starts (exclusive scan, each thread a
-// consecutive run); returns the largest bucket (uniform).
+// consecutive run of 16-byte words, cleared by bucket_clear); returns the
+// largest bucket (uniform). The counts of a word's buckets past nbins are
+// zero, so their starts (never read) do not disturb the others.
 template <uint32_t THREADS>
 __device__ uint32_t bucket_starts(uint32_t* bins, uint32_t nbins, uint32_t* s_tmp) {
     constexpr uint32_t WARPS = THREADS / 32;
+    static_assert(WARPS <= 32, "one total per lane");
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    const uint32_t per = (nbins + THREADS - 1) / THREADS;
-    const uint32_t b0 = min(nbins, tid * per), b1 = min(nbins, b0 + per);
+    uint4* b4 = reinterpret_cast<uint4*>(bins);
+    const uint32_t nq = (nbins + 3u) / 4u;
+    const uint32_t per = (nq + THREADS - 1) / THREADS;
+    const uint32_t q0 = min(nq, tid * per), q1 = min(nq, q0 + per);
     uint32_t run = 0, big = 0;
-    for (uint32_t b = b0; b < b1; ++b) {
-        run += bins[b];
-        big = max(big, bins[b]);
+    for (uint32_t q = q0; q < q1; ++q) {
+        const uint4 c = b4[q];
+        run += (c.x + c.y) + (c.z + c.w);
+        big = max(big, max(max(c.x, c.y), max(c.z, c.w)));
     }
     uint32_t incl = run;
 #pragma unroll
@@ -451,14 +465,25 @@ __device__ uint32_t bucket_starts(uint32_t* bins, uint32_t nbins, uint32_t* s_tm
     if (lane == 31) s_tmp[2 * WARPS + warp] = incl;
     if (lane == 0) s_tmp[3 * WARPS + warp] = big;
     __syncthreads();
-    uint32_t base = incl - run;
-    for (uint32_t w = 0; w < warp; ++w) base += s_tmp[2 * WARPS + w];
-    for (uint32_t w = 0; w < WARPS; ++w) big = max(big, s_tmp[3 * WARPS + w]);
+    // Lane w holds warp w's total and largest bucket: the warps before this
+    // one add up to its base.
+    const uint32_t tot = lane < warp ? s_tmp[2 * WARPS + lane] : 0u;
+    const uint32_t wb = lane < WARPS ? s_tmp[3 * WARPS + lane] : 0u;
+    uint32_t base = incl - run + __reduce_add_sync(0xffffffffu, tot);
+    big = __reduce_max_sync(0xffffffffu, wb);
     if (big <= kMaxBucket) {
-        for (uint32_t b = b0; b < b1; ++b) {
-            const uint32_t c = bins[b];
-            bins[b] = base;
-            base += c;
+        for (uint32_t q = q0; q < q1; ++q) {
+            const uint4 c = b4[q];
+            uint4 st;
+            st.x = base;
+            base += c.x;
+            st.y = base;
+            base += c.y;
+            st.z = base;
+            base += c.z;
+            st.w = base;
+            base += c.w;
+            b4[q] = st;
         }
     }
     __syncthreads();
@@ -523,7 +548,7 @@ __device__ void sort_range_shared(uint32_t t, uint32_t start, uint32_t n, Load l
     uint32_t mn, mx;
     block_min_max<THREADS>(lo, hi, s_tmp, mn, mx);
     const BucketPlan bp = bucket_plan(n, mn, mx, BINS);
-    for (uint32_t b = tid; b < bp.nbins; b += THREADS) bins[b] = 0;
+    bucket_clear<THREADS>(bins, bp.nbins);
     __syncthreads();
 #pragma unroll
     for (uint32_t j = 0; j < ITEMS; ++j)
@@ -583,7 +608,7 @@ __global__ __launch_bounds__(THREADS) void tile_sort_kernel(const uint32_t* __re
                                                             const uint32_t* __restrict__ tile_start,
                                                             uint32_t capacity, uint2* pairs, uint32_t* ids,
                                                             uint32_t* tids_out, uint32_t* keys_tmp) {
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     const uint32_t count = *list_n;
     for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
         sort_tile_shared<MAXN, BINS, THREADS>(list[idx], tile_start, capacity, pairs, ids, tids_out, keys_tmp, sm);
@@ -623,7 +648,7 @@ __device__ void sort_range_global(uint32_t t, uint32_t start, uint32_t n, Load l
         uint32_t mn, mx;
         block_min_max<THREADS>(lo, hi, s_tmp, mn, mx);
         const BucketPlan bp = bucket_plan(n, mn, mx, SBINS);
-        for (uint32_t b = tid; b < bp.nbins; b += THREADS) bins[b] = 0;
+        bucket_clear<THREADS>(bins, bp.nbins);
         __syncthreads();
         for (uint32_t i = tid; i < n; i += THREADS) atomicAdd(&bins[(load(i).x - mn) >> bp.shift], 1u);
         __syncthreads();
@@ -659,7 +684,7 @@ __device__ void sort_range_global(uint32_t t, uint32_t start, uint32_t n, Load l
     uint32_t mn, mx;
     block_min_max<THREADS>(lo, hi, s_tmp, mn, mx);  // its barriers also order the copies above
     const BucketPlan bp = bucket_plan(n, mn, mx, BINS);
-    for (uint32_t b = tid; b < bp.nbins; b += THREADS) bins[b] = 0;
+    bucket_clear<THREADS>(bins, bp.nbins);
     __syncthreads();
     for (uint32_t i = tid; i < n; i += THREADS) atomicAdd(&bins[(ka[i] - mn) >> bp.shift], 1u);
     __syncthreads();
@@ -698,7 +723,7 @@ __global__ __launch_bounds__(THREADS, 1) void tile_sort_global_kernel(const uint
                                                                    uint32_t capacity, uint2* pairs, uint32_t* ids,
                                                                    uint32_t* tids_out, uint32_t* keys_tmp,
                                                                    const uint32_t* taken) {
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     const uint32_t count = *list_n;
     for (uint32_t idx = blockIdx.x; idx < count; idx += gridDim.x) {
         if (taken && taken[idx]) continue;  // uniform
@@ -1079,7 +1104,7 @@ __global__ __launch_bounds__(kGiantThreads) void giant_scatter_kernel(const uint
 
 __global__ __launch_bounds__(kThreads1) void giant_seg_sort_kernel(GiantState gs, uint2* pairs, uint32_t* ids,
                                                                    uint32_t* tids_out, uint32_t* keys_tmp) {
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     const uint32_t count = min(gs.ctrl[2], gs.seg_cap);
     for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {
         const uint4 sg = gs.segs[i];
@@ -1095,7 +1120,7 @@ __global__ __launch_bounds__(kThreads1) void giant_seg_sort_kernel(GiantState gs
 
 __global__ __launch_bounds__(kThreadsGiant, 1) void giant_seg_big_kernel(GiantState gs, uint2* pairs, uint32_t* ids,
                                                                          uint32_t* tids_out, uint32_t* keys_tmp) {
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];
     const uint32_t count = min(gs.ctrl[3], gs.seg_cap);
     for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {
         const uint4 sg = gs.segs[gs.seg_cap - 1u - i];
