@@ -71,6 +71,38 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// CULL's second test, for an entry whose power_max box reaches the warp's
+// 8x4 block: whether the splat's quadratic form q(dx, dy) = hx dx^2 +
+// cy dx dy + hz dy^2 stays above power_max at every pixel of the block. The
+// pixel offsets (splat centre minus pixel centre) lie in [X0 - 7, X0] x
+// [Y0 - 3, Y0], widened by 1e-3 for the rounding of X0 and Y0. The form is
+// convex, so its minimum over that rectangle is 0 with the centre inside it,
+// else the least of its minima along the four edges (each a 1-D quadratic,
+// minimised at a clamped point; an approximate minimiser only raises q by
+// the square of its error). The entry is skipped only when that minimum
+// exceeds power_max by 1e-5 of the largest sum of |terms| over the block
+// plus 1e-5: both this minimum and the per-pixel power are a few roundings
+// of such terms (error below 1e-6 of their sum), so every pixel's computed
+// power is then above power_max and the pixel would skip the pair itself.
+// A form that is not positive definite has no box (ext infinite) and is
+// never skipped.
+__device__ __forceinline__ bool block_misses(const float4 g0, const float4 g1, const float2 e, float wxf,
+                                             float wyf) {
+    if (!(e.x < INFINITY)) return false;
+    const float hx = g0.z, cy = g0.w, hz = g1.x, pmax = g1.z;
+    const float x0 = g0.x - wxf, y0 = g0.y - wyf;
+    const float xlo = x0 - 7.001f, xhi = x0 + 0.001f, ylo = y0 - 3.001f, yhi = y0 + 0.001f;
+    if (xlo <= 0.0f && xhi >= 0.0f && ylo <= 0.0f && yhi >= 0.0f) return false;
+    const float ky = __fdividef(-0.5f * cy, hz), kx = __fdividef(-0.5f * cy, hx);
+    auto q = [&](float x, float y) { return fmaf(hx * x, x, fmaf(hz * y, y, (cy * x) * y)); };
+    const float y1 = fminf(fmaxf(ky * xlo, ylo), yhi), y2 = fminf(fmaxf(ky * xhi, ylo), yhi);
+    const float x1 = fminf(fmaxf(kx * ylo, xlo), xhi), x2 = fminf(fmaxf(kx * yhi, xlo), xhi);
+    const float qmin = fminf(fminf(q(xlo, y1), q(xhi, y2)), fminf(q(x1, ylo), q(x2, yhi)));
+    const float dx = fmaxf(fabsf(xlo), fabsf(xhi)), dy = fmaxf(fabsf(ylo), fabsf(yhi));
+    const float smax = fmaf(hx * dx, dx, fmaf(hz * dy, dy, (fabsf(cy) * dx) * dy));
+    return qmin > fmaf(1e-5f, smax, pmax + 1e-5f);
+}
+
 // Modes: 0 RGB, 1 total responsibility words, 2 evidence (fg / bg) words,
 // 3 transmittance only (final T and last contributor per pixel).
 template <int MODE>
@@ -245,6 +277,7 @@ __device__ bool composite_list(const RasterArgs& a, Stage<MODE, CULL>& sm, IdOf 
                     const float lx = (g0.x - e.x) - wxf, hx = (g0.x + e.x) - wxf;
                     const float ly = (g0.y - e.y) - wyf, hy = (g0.y + e.y) - wyf;
                     hit = lx <= 7.0f && hx >= 0.0f && ly <= 3.0f && hy >= 0.0f;
+                    if (hit) hit = !block_misses(g0, sm.g1[b][j], e, wxf, wyf);
                 }
                 uint32_t word = __ballot_sync(0xffffffffu, hit);
                 while (word) {
