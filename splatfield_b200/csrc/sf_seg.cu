@@ -69,9 +69,9 @@ using namespace sfm;
 // psi keeps its recurrence (no division for x >= 6, most arguments).
 // Arguments past 2^32 take the per-term forms (the fractions' products of
 // eight factors stay below 2^260 under that bound). Measured on the
-// 20-view FP64 round: 3.68 -> 3.50 ms, with the EIG kernels held to four
+// 20-view FP64 round: 3.68 -> 3.48 ms, with the EIG kernels held to five
 // blocks per SM (the fractions raise register use; at two blocks per SM
-// the round took 3.71 ms).
+// the round took 3.71 ms, at three 3.54, at four 3.52).
 __device__ __forceinline__ double lgamma_terms(double x) {
     const double z = x - 1.0;
     double series = 0.9999999999998099;
@@ -162,7 +162,7 @@ __device__ __forceinline__ double block_sum(double v, double* s_warp) {
 // entropy_delta_kernel (beta.rs:152-201): per splat with eps > 0,
 // dH = max(0, H(a,b) - H(k a, k b)), k = 1 + eps/(a+b).
 template <int MODE>
-__global__ __launch_bounds__(kEigThreads, 4) void eig_kernel(const float* __restrict__ a,
+__global__ __launch_bounds__(kEigThreads, 5) void eig_kernel(const float* __restrict__ a,
                                                           const float* __restrict__ b,
                                                           const uint32_t* __restrict__ resp,
                                                           const uint32_t* __restrict__ resp2,
@@ -201,7 +201,7 @@ __global__ __launch_bounds__(kEigThreads, 4) void eig_kernel(const float* __rest
 // per-splat scalar feature, sf_backward.cu): eps = fg + bg directly, with no
 // fixed-point scale; the LUT form adds in f32, the FP64 form in f64.
 template <int MODE>
-__global__ __launch_bounds__(kEigThreads, 4) void eig_real_kernel(const float* __restrict__ a,
+__global__ __launch_bounds__(kEigThreads, 5) void eig_real_kernel(const float* __restrict__ a,
                                                                const float* __restrict__ b,
                                                                const float* __restrict__ fg,
                                                                const float* __restrict__ bg, uint32_t n,
