@@ -194,8 +194,9 @@ typedef struct {
      * internal copy of its frame buffers, each with its own frame graph and
      * stream, so one frame's projection and build run while the other's
      * raster finishes (the copy is allocated on the first path of two or
-     * more frames and holds the scratch's capacity); 1: one pipe. Same
-     * images either way. */
+     * more frames and holds the scratch's capacity; when the device has no
+     * room for it, the path runs on one pipe); 1: one pipe. Same images
+     * either way. */
     uint32_t frame_pipes;
 } sf_tuning;
 #define SF_ISECTS_BINNED 0u

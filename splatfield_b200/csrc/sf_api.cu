@@ -821,10 +821,18 @@ int frames_graph_render(sf_splats sp, sf_scratch s, const sf_camera* cams, uint3
                         uint32_t h, cudaStream_t st, uint32_t* host_out) {
     auto& g = s->fg;
     const size_t img = (size_t)w * h;
-    const bool two = count >= 2 && s->tuning.frame_pipes != 1;
+    bool two = count >= 2 && s->tuning.frame_pipes != 1;
     int rc = frame_graph_ready(sp, s, w, h);
     if (rc != SF_OK) return rc;
-    if (two && (rc = twin_ready(sp, s, w, h)) != SF_OK) return rc;
+    if (two && (rc = twin_ready(sp, s, w, h)) != SF_OK) {
+        if (rc != SF_ERR_NOMEM) return rc;
+        // No room for the second pipe: release what it took and render the
+        // path on one pipe.
+        cudaGetLastError();
+        sf_scratch_destroy(s->twin);
+        s->twin = nullptr;
+        two = false;
+    }
     sf_scratch const pipes[2] = {s, two ? s->twin : s};
     cudaStream_t const streams[2] = {st, two ? s->twin_stream : st};
     auto pipe_of = [&](uint32_t i) { return two ? (int)((count - 1 - i) & 1u) : 0; };
