@@ -150,7 +150,9 @@ int sf_scratch_reserve(sf_scratch s, uint64_t isects);
  * autotuner picks by measured time). */
 typedef struct {
     uint32_t raster_cull; /* 0: every warp walks every staged entry;
-                             1: per-warp culling by each splat's power_max box */
+                             1: per-warp culling by each splat's power_max box,
+                             then by the minimum of its quadratic form over
+                             the warp's 8x4 pixel block */
     /* Intersection build, same lists either way:
      *   SF_ISECTS_BINNED (default, frames up to 49152 tiles): per-tile
      *     counts in shared memory, place, then a sort of each tile's list by
