@@ -533,6 +533,17 @@ int sf_radix_destroy(sf_radix r);
 int sf_radix_argsort(sf_radix r, const uint32_t* keys, const uint32_t* vals, uint32_t n,
                      uint32_t bits, int write_keys, sf_stream stream, const uint32_t** keys_out,
                      const uint32_t** vals_out);
+/* No counterpart in the reference (its sorts block on their own read-backs).
+ * sf_radix_argsort without the wait: the sort is only enqueued, so a caller
+ * can run several sorts (or other work) back to back on the stream; a
+ * look-back wait that ran out is kept in the scratch's error word until
+ * sf_radix_status, which waits for the stream and returns SF_ERR_TIMEOUT if
+ * any sort on the scratch since the last status (or synchronous sort) timed
+ * out, then clears the word. */
+int sf_radix_argsort_async(sf_radix r, const uint32_t* keys, const uint32_t* vals, uint32_t n,
+                           uint32_t bits, int write_keys, sf_stream stream, const uint32_t** keys_out,
+                           const uint32_t** vals_out);
+int sf_radix_status(sf_radix r, sf_stream stream);
 /* Digit width of the scratch's passes, 4..8 bits (default 8; the
  * reference's RADIX_BITS is 6, crates/sort/src/sort.rs:11-17). The order is
  * the same at every width. */
@@ -546,6 +557,12 @@ int sf_scan_destroy(sf_scan s);
  * and returns SF_ERR_TIMEOUT if a look-back wait ran out. */
 int sf_exclusive_scan_gather(sf_scan s, const uint32_t* gids, const uint32_t* counts,
                              uint32_t* offsets, uint32_t n, sf_stream stream);
+/* No counterpart in the reference. sf_exclusive_scan_gather without the
+ * wait; sf_scan_status reports and clears a timed-out wait, as
+ * sf_radix_status does for sorts. */
+int sf_exclusive_scan_gather_async(sf_scan s, const uint32_t* gids, const uint32_t* counts,
+                                   uint32_t* offsets, uint32_t n, sf_stream stream);
+int sf_scan_status(sf_scan s, sf_stream stream);
 /* exclusive_scan_buf (crates/sort/src/scan.rs:185-213): in place. */
 int sf_exclusive_scan(sf_scan s, uint32_t* buf, uint32_t n, sf_stream stream);
 /* No counterpart in the reference. sf_exclusive_scan_gather for callers that

@@ -166,10 +166,14 @@ SIGNATURES = {
         "sf_radix_create": (i32, [P, u32, PP]),
         "sf_radix_destroy": (i32, [P]),
         "sf_radix_argsort": (i32, [P, P, P, u32, u32, i32, P, PP, PP]),
+        "sf_radix_argsort_async": (i32, [P, P, P, u32, u32, i32, P, PP, PP]),
+        "sf_radix_status": (i32, [P, P]),
         "sf_radix_set_digit_bits": (i32, [P, u32]),
         "sf_scan_create": (i32, [P, u32, PP]),
         "sf_scan_destroy": (i32, [P]),
         "sf_exclusive_scan_gather": (i32, [P, P, P, P, u32, P]),
+        "sf_exclusive_scan_gather_async": (i32, [P, P, P, P, u32, P]),
+        "sf_scan_status": (i32, [P, P]),
         "sf_exclusive_scan": (i32, [P, P, u32, P]),
         "sf_exclusive_scan_gather_noalloc": (i32, [P, P, P, u32, P]),
         "sf_debug_lookback": (i32, [u32, i32]),

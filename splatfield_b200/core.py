@@ -999,11 +999,19 @@ class RadixScratch:
         """Digit width of the passes, 4..8 bits (default 8)."""
         check(lib().sf_radix_set_digit_bits(self.handle, int(digit_bits)))
 
-    def argsort(self, keys, vals, n: int, bits: int, write_keys: bool = True, stream=None):
+    def argsort(self, keys, vals, n: int, bits: int, write_keys: bool = True, stream=None, sync: bool = True):
+        """Sorted (keys, values) views into the scratch. sync=False only
+        enqueues the sort (sf_radix_argsort_async); ``status`` then reports a
+        timed-out look-back wait of any sort since the last check."""
         ko, vo = C.c_void_p(), C.c_void_p()
-        check(lib().sf_radix_argsort(self.handle, _vp(keys), _vp(vals), n, bits, 1 if write_keys else 0,
-                                     _stream(stream), C.byref(ko), C.byref(vo)))
+        fn = lib().sf_radix_argsort if sync else lib().sf_radix_argsort_async
+        check(fn(self.handle, _vp(keys), _vp(vals), n, bits, 1 if write_keys else 0, _stream(stream),
+                 C.byref(ko), C.byref(vo)))
         return DeviceView(ko.value, np.uint32, (n,), self), DeviceView(vo.value, np.uint32, (n,), self)
+
+    def status(self, stream=None) -> None:
+        """Waits for the stream; raises if a sort since the last check timed out."""
+        check(lib().sf_radix_status(self.handle, _stream(stream)))
 
     def close(self):
         if getattr(self, "handle", None):
@@ -1026,6 +1034,10 @@ class ScanScratch:
         check(lib().sf_scan_create(self.ctx.handle, max_elems, C.byref(h)))
         self.handle = h
 
+    def status(self, stream=None) -> None:
+        """Waits for the stream; raises if a scan since the last check timed out."""
+        check(lib().sf_scan_status(self.handle, _stream(stream)))
+
     def close(self):
         if getattr(self, "handle", None):
             lib().sf_scan_destroy(self.handle)
@@ -1038,10 +1050,12 @@ class ScanScratch:
             pass
 
 
-def exclusive_scan_gather(gids, counts, offsets, n: int, scratch: ScanScratch, stream=None) -> None:
-    """offsets[i] = sum_{j<i} counts[gids[j]] (crates/sort/src/scan.rs:219-255)."""
-    check(lib().sf_exclusive_scan_gather(scratch.handle, _vp(gids), _vp(counts), _vp(offsets), n,
-                                         _stream(stream)))
+def exclusive_scan_gather(gids, counts, offsets, n: int, scratch: ScanScratch, stream=None,
+                          sync: bool = True) -> None:
+    """offsets[i] = sum_{j<i} counts[gids[j]] (crates/sort/src/scan.rs:219-255).
+    sync=False only enqueues the scan (``scratch.status`` checks it later)."""
+    fn = lib().sf_exclusive_scan_gather if sync else lib().sf_exclusive_scan_gather_async
+    check(fn(scratch.handle, _vp(gids), _vp(counts), _vp(offsets), n, _stream(stream)))
 
 
 def exclusive_scan_buf(buf, n: int, scratch: ScanScratch, stream=None) -> None:

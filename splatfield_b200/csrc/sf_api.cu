@@ -1938,28 +1938,60 @@ int sf_radix_destroy(sf_radix r) {
     return SF_OK;
 }
 
+// The sort of sf_radix_argsort enqueued on st; a timed-out look-back wait
+// is left in r->err.
+static int radix_argsort_enqueue(sf_radix r, const uint32_t* keys, const uint32_t* vals, uint32_t n,
+                                 uint32_t bits, int write_keys, cudaStream_t st, const uint32_t** keys_out,
+                                 const uint32_t** vals_out, bool* launched) {
+    *launched = false;
+    if (!r || !keys_out || !vals_out) return fail(SF_ERR_ARG, "null argument");
+    if (bits > 32) return fail(SF_ERR_ARG, "bits > 32");
+    if (n <= 1 || bits == 0) {
+        *keys_out = keys;
+        *vals_out = vals;
+        return SF_OK;
+    }
+    if (!keys) return fail(SF_ERR_ARG, "null keys");
+    if (n > r->max)
+        return fail(SF_ERR_SHAPE, "radix scratch undersized: sorted " + std::to_string(n) + " elements, capacity " +
+                                      std::to_string(r->max));
+    SF_CK(use_device(r->ctx->device));
+    int in_b = 0;
+    SF_CK(radix_sort_pairs(keys, vals, r->ka, r->va, r->kb, r->vb, n, nullptr, n, bits, write_keys != 0,
+                           vals == nullptr, r->tmp, r->err, r->ctx->sm_count, st, &in_b, lookback_test_knobs(),
+                           r->digit_bits));
+    *keys_out = in_b ? r->kb : r->ka;
+    *vals_out = in_b ? r->vb : r->va;
+    *launched = true;
+    return SF_OK;
+}
+
 int sf_radix_argsort(sf_radix r, const uint32_t* keys, const uint32_t* vals, uint32_t n, uint32_t bits,
                      int write_keys, sf_stream stream, const uint32_t** keys_out,
                      const uint32_t** vals_out) {
     SF_TRY({
-        if (!r || !keys_out || !vals_out) return fail(SF_ERR_ARG, "null argument");
-        if (bits > 32) return fail(SF_ERR_ARG, "bits > 32");
-        if (n <= 1 || bits == 0) {
-            *keys_out = keys;
-            *vals_out = vals;
-            return SF_OK;
-        }
-        if (!keys) return fail(SF_ERR_ARG, "null keys");
-        if (n > r->max)
-            return fail(SF_ERR_SHAPE, "radix scratch undersized: sorted " + std::to_string(n) +
-                                          " elements, capacity " + std::to_string(r->max));
+        bool launched = false;
+        const int rc = radix_argsort_enqueue(r, keys, vals, n, bits, write_keys, S(stream), keys_out, vals_out,
+                                             &launched);
+        if (rc != SF_OK || !launched) return rc;
+        return read_timeout_word(r->err, S(stream));
+    })
+}
+
+int sf_radix_argsort_async(sf_radix r, const uint32_t* keys, const uint32_t* vals, uint32_t n, uint32_t bits,
+                           int write_keys, sf_stream stream, const uint32_t** keys_out,
+                           const uint32_t** vals_out) {
+    SF_TRY({
+        bool launched = false;
+        return radix_argsort_enqueue(r, keys, vals, n, bits, write_keys, S(stream), keys_out, vals_out,
+                                     &launched);
+    })
+}
+
+int sf_radix_status(sf_radix r, sf_stream stream) {
+    SF_TRY({
+        if (!r) return fail(SF_ERR_ARG, "null radix scratch");
         SF_CK(use_device(r->ctx->device));
-        int in_b = 0;
-        SF_CK(radix_sort_pairs(keys, vals, r->ka, r->va, r->kb, r->vb, n, nullptr, n, bits,
-                               write_keys != 0, vals == nullptr, r->tmp, r->err, r->ctx->sm_count,
-                               S(stream), &in_b, lookback_test_knobs(), r->digit_bits));
-        *keys_out = in_b ? r->kb : r->ka;
-        *vals_out = in_b ? r->vb : r->va;
         return read_timeout_word(r->err, S(stream));
     })
 }
@@ -2003,18 +2035,46 @@ int sf_scan_destroy(sf_scan s) {
     return SF_OK;
 }
 
+// The scan of sf_exclusive_scan_gather enqueued on st; a timed-out
+// look-back wait is left in s->err.
+static int scan_gather_enqueue(sf_scan s, const uint32_t* gids, const uint32_t* counts, uint32_t* offsets,
+                               uint32_t n, cudaStream_t st, bool* launched) {
+    *launched = false;
+    if (!s) return fail(SF_ERR_ARG, "null scan scratch");
+    if (n == 0) return SF_OK;
+    if (!counts || !offsets) return fail(SF_ERR_ARG, "null buffer");
+    if (n > s->max)
+        return fail(SF_ERR_SHAPE, "offsets undersized: scanned " + std::to_string(n) + " elements, capacity " +
+                                      std::to_string(s->max));
+    SF_CK(use_device(s->ctx->device));
+    SF_CK(exclusive_scan(gids, counts, offsets, n, nullptr, n, s->tmp, s->total, s->err, st,
+                         lookback_test_knobs()));
+    *launched = true;
+    return SF_OK;
+}
+
 int sf_exclusive_scan_gather(sf_scan s, const uint32_t* gids, const uint32_t* counts, uint32_t* offsets,
                              uint32_t n, sf_stream stream) {
     SF_TRY({
+        bool launched = false;
+        const int rc = scan_gather_enqueue(s, gids, counts, offsets, n, S(stream), &launched);
+        if (rc != SF_OK || !launched) return rc;
+        return read_timeout_word(s->err, S(stream));
+    })
+}
+
+int sf_exclusive_scan_gather_async(sf_scan s, const uint32_t* gids, const uint32_t* counts, uint32_t* offsets,
+                                   uint32_t n, sf_stream stream) {
+    SF_TRY({
+        bool launched = false;
+        return scan_gather_enqueue(s, gids, counts, offsets, n, S(stream), &launched);
+    })
+}
+
+int sf_scan_status(sf_scan s, sf_stream stream) {
+    SF_TRY({
         if (!s) return fail(SF_ERR_ARG, "null scan scratch");
-        if (n == 0) return SF_OK;
-        if (!counts || !offsets) return fail(SF_ERR_ARG, "null buffer");
-        if (n > s->max)
-            return fail(SF_ERR_SHAPE, "offsets undersized: scanned " + std::to_string(n) +
-                                          " elements, capacity " + std::to_string(s->max));
         SF_CK(use_device(s->ctx->device));
-        SF_CK(exclusive_scan(gids, counts, offsets, n, nullptr, n, s->tmp, s->total, s->err, S(stream),
-                             lookback_test_knobs()));
         return read_timeout_word(s->err, S(stream));
     })
 }

@@ -142,3 +142,32 @@ def test_every_digit_width_sorts_stably(ctx, digit_bits, bits):
     order = np.argsort(keys, kind="stable").astype(np.uint32)
     np.testing.assert_array_equal(vo.read(), order)
     np.testing.assert_array_equal(ko.read(), keys[order])
+
+
+def test_async_sorts_and_scans_back_to_back_equal_sync(ctx):
+    """Sorts enqueued with sync=False and checked by status, and three scans
+    enqueued back to back on one stream with one status after them: the same
+    arrays as the synchronous calls (stable order, exact offsets)."""
+    rng = np.random.default_rng(0x5EED0009)
+    n = 1_000_003
+    radix = sf.RadixScratch(n)
+    scan = sf.ScanScratch(n)
+    results = []
+    for bits in (32, 20, 8):
+        keys = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32) & np.uint32((1 << bits) - 1 if bits < 32 else 0xFFFFFFFF)
+        dk = sf.DeviceBuffer.from_array(keys)
+        _, vo = radix.argsort(dk, None, n, bits, sync=False)
+        radix.status()
+        results.append((keys, vo.read()))
+    for keys, got in results:
+        np.testing.assert_array_equal(got, np.argsort(keys, kind="stable").astype(np.uint32))
+    counts = rng.integers(0, 20, n).astype(np.uint32)
+    gids = rng.permutation(n).astype(np.uint32)
+    dg, dc = sf.DeviceBuffer.from_array(gids), sf.DeviceBuffer.from_array(counts)
+    outs = [sf.DeviceBuffer.empty(n) for _ in range(3)]
+    for o in outs:
+        sf.exclusive_scan_gather(dg, dc, o, n, scan, sync=False)
+    scan.status()
+    want = np.concatenate([[0], np.cumsum(counts[gids].astype(np.uint64))[:-1]]).astype(np.uint32)
+    for o in outs:
+        np.testing.assert_array_equal(o.read(), want)

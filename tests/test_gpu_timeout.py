@@ -60,3 +60,39 @@ def test_look_back_timeouts_are_reported_then_cleared(ctx):
     np.testing.assert_array_equal(out.read(), _cpu_scan(counts))
     ko, vo = radix.argsort(dk, None, N, 32)
     np.testing.assert_array_equal(vo.read(), np.argsort(keys, kind="stable").astype(np.uint32))
+
+
+def test_async_sort_and_scan_report_timeouts_at_status(ctx):
+    """sf_radix_argsort_async / sf_exclusive_scan_gather_async only enqueue;
+    a wait that ran out in any of several calls is reported once by the
+    scratch's status call, which clears it, so the next status is clean."""
+    rng = np.random.default_rng(0x5EED0072)
+    counts = rng.integers(0, 50, N).astype(np.uint32)
+    keys = rng.integers(0, 2**32, N, dtype=np.uint64).astype(np.uint32)
+    dc = sf.DeviceBuffer.from_array(counts)
+    dk = sf.DeviceBuffer.from_array(keys)
+    out = sf.DeviceBuffer.empty(N)
+    scan = sf.ScanScratch(N)
+    radix = sf.RadixScratch(N)
+    L = lib()
+    assert L.sf_debug_lookback(16, 1) == SF_OK
+    try:
+        for _ in range(2):
+            sf.exclusive_scan_gather(None, dc, out, N, scan, sync=False)
+            radix.argsort(dk, None, N, 32, sync=False)
+        with pytest.raises(sf.SplatfieldError) as e:
+            scan.status()
+        assert e.value.code == SF_ERR_TIMEOUT
+        with pytest.raises(sf.SplatfieldError) as e:
+            radix.status()
+        assert e.value.code == SF_ERR_TIMEOUT
+    finally:
+        assert L.sf_debug_lookback(0, 0) == SF_OK
+    scan.status()
+    radix.status()
+    sf.exclusive_scan_gather(None, dc, out, N, scan, sync=False)
+    scan.status()
+    np.testing.assert_array_equal(out.read(), _cpu_scan(counts))
+    ko, vo = radix.argsort(dk, None, N, 32, sync=False)
+    radix.status()
+    np.testing.assert_array_equal(vo.read(), np.argsort(keys, kind="stable").astype(np.uint32))
