@@ -731,8 +731,9 @@ def run_build_only(args):
 
 
 def run_sort_only(args):
-    """Profiling mode: sf_radix_argsort of 1M random 32-bit keys (8-bit
-    digits), warmup + steps calls, device-timed."""
+    """Profiling mode: sf_radix_argsort of --sort-n random 32-bit keys (8-bit
+    digits), warmup + steps calls, device-timed through the asynchronous
+    form (the error word is checked after each call's timing)."""
     import torch
 
     import splatfield_b200 as sf
@@ -750,11 +751,41 @@ def run_sort_only(args):
     for _ in range(args.steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        scratch.argsort(keys, None, n, 32, True, stream=stream)
+        scratch.argsort(keys, None, n, 32, True, stream=stream, sync=False)
         e1.record(stream)
-        torch.cuda.synchronize()
+        scratch.status(stream)
         times.append(e0.elapsed_time(e1))
     print(json.dumps({"sort_only": n, "ms": float(np.median(times))}))
+
+
+def run_scan_only(args):
+    """Profiling mode: sf_exclusive_scan_gather over --scan-n elements (a
+    random permutation gathering counts in [0, 16)), warmup + steps calls,
+    device-timed through the asynchronous form."""
+    import torch
+
+    import splatfield_b200 as sf
+
+    torch.cuda.set_device(0)
+    ctx = sf.Context(0)
+    n = args.scan_n
+    rng = np.random.default_rng(0x5027)
+    counts = sf.DeviceBuffer.from_array(rng.integers(0, 16, n).astype(np.uint32), ctx)
+    gids = sf.DeviceBuffer.from_array(rng.permutation(n).astype(np.uint32), ctx)
+    out = sf.DeviceBuffer.empty(n, np.uint32, ctx)
+    scratch = sf.ScanScratch(n, ctx)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        sf.exclusive_scan_gather(gids, counts, out, n, scratch, stream=stream)
+    times = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sf.exclusive_scan_gather(gids, counts, out, n, scratch, stream=stream, sync=False)
+        e1.record(stream)
+        scratch.status(stream)
+        times.append(e0.elapsed_time(e1))
+    print(json.dumps({"scan_only": n, "ms": float(np.median(times))}))
 
 
 def run_round_only(args):
@@ -991,6 +1022,8 @@ def main():
                          "--round-only) instead of the autotuner's pick")
     ap.add_argument("--sort-n", type=int, default=0,
                     help="run warmup + steps radix argsorts of this many random 32-bit keys and exit (for profilers)")
+    ap.add_argument("--scan-n", type=int, default=0,
+                    help="run warmup + steps gather scans over this many elements and exit (for profilers)")
     ap.add_argument("--build-n", type=int, default=0,
                     help="run warmup + steps 1080p intersection builds of a clustered scene of this many splats "
                          "and exit (for profilers)")
@@ -1015,6 +1048,8 @@ def main():
             run_round_only(args)
         elif args.sort_n:
             run_sort_only(args)
+        elif args.scan_n:
+            run_scan_only(args)
         elif args.build_n:
             run_build_only(args)
         else:
