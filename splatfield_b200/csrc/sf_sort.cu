@@ -346,6 +346,50 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
     }
 }
 
+// The scan's look-back done by one whole warp: lane l reads the status of
+// partition p - l (p the newest predecessor not yet summed), so one L2 round
+// trip covers 32 predecessors. If some lane finds an inclusive prefix and
+// every lane before it an aggregate, the warp sums those lanes and stops;
+// otherwise it sums the aggregates before the first lane whose partition
+// has published nothing and reads again from there, with the same backoff
+// and bound as lookback_window. Lanes past partition 0 read a zero prefix.
+// Returns the exclusive prefix in every lane.
+__device__ unsigned long long lookback_warp64(const unsigned long long* stat, uint32_t part, uint32_t* err,
+                                              uint32_t spin_limit, unsigned long long flag_prefix,
+                                              unsigned long long value_mask) {
+    const uint32_t lane = threadIdx.x & 31u;
+    unsigned long long excl = 0;
+    int64_t p = (int64_t)part - 1;
+    uint32_t spins = 0, nap = 32;
+    const uint32_t limit = spin_limit ? spin_limit : kSpinLimit;
+    while (p >= 0) {
+        const int64_t q = p - (int64_t)lane;
+        const unsigned long long st = q >= 0 ? ld_relaxed64(stat + q) : flag_prefix;
+        const unsigned long long flag = st & ~value_mask;
+        const uint32_t not_ready = __ballot_sync(0xffffffffu, flag == 0);
+        const uint32_t prefix = __ballot_sync(0xffffffffu, flag == flag_prefix);
+        const uint32_t first_nr = not_ready ? (uint32_t)(__ffs(not_ready) - 1) : 32u;
+        const uint32_t first_pf = prefix ? (uint32_t)(__ffs(prefix) - 1) : 32u;
+        const bool done = first_pf < first_nr;
+        const uint32_t take = done ? first_pf + 1 : first_nr;
+        unsigned long long v = lane < take ? (st & value_mask) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        excl += v;
+        if (done) break;
+        if (take == 0) {
+            if (++spins > limit) {
+                if (lane == 0) atomicOr(err, SF_DEV_ERR_TIMEOUT);
+                break;
+            }
+            __nanosleep(nap);
+            nap = min(nap * 2u, 256u);
+        }
+        p -= take;
+    }
+    return excl;
+}
+
 // Single-pass exclusive scan with optional gather:
 // out[i] = sum_{j<i} counts[gids ? gids[j] : j], 64-bit running sums, the
 // u32 low word stored; *total_out = the 64-bit total.
@@ -412,18 +456,19 @@ __global__ __launch_bounds__(kThreads) void scan_kernel(
         if ((uint32_t)w < warp) warp_prefix += s_warp[w];
         block_total += s_warp[w];
     }
-    if (tid == 0) {
+    if (warp == 0) {
         unsigned long long excl = 0;
         if (part == 0) {
-            if (!knobs.withhold) st_relaxed64(&lookback[0], kScanFlagPrefix | block_total);
+            if (lane == 0 && !knobs.withhold) st_relaxed64(&lookback[0], kScanFlagPrefix | block_total);
         } else {
-            st_relaxed64(&lookback[part], kScanFlagAgg | block_total);
-            excl = lookback_window<unsigned long long>(lookback, 1, part, kScanFlagPrefix, kScanValMask, err,
-                                                      knobs.spin_limit);
-            st_relaxed64(&lookback[part], kScanFlagPrefix | (excl + block_total));
+            if (lane == 0) st_relaxed64(&lookback[part], kScanFlagAgg | block_total);
+            excl = lookback_warp64(lookback, part, err, knobs.spin_limit, kScanFlagPrefix, kScanValMask);
+            if (lane == 0) st_relaxed64(&lookback[part], kScanFlagPrefix | (excl + block_total));
         }
-        s_prefix = excl;
-        if (part == num_parts - 1 && total_out) *total_out = excl + block_total;
+        if (lane == 0) {
+            s_prefix = excl;
+            if (part == num_parts - 1 && total_out) *total_out = excl + block_total;
+        }
     }
     __syncthreads();
     unsigned long long running = s_prefix + warp_prefix + (incl - local);
