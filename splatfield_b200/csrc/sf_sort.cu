@@ -6,7 +6,7 @@
 // "Onesweep: A Faster Least Significant Digit Radix Sort for GPUs", 2022):
 //  * one upfront kernel reads the keys once and builds the 256-bin histogram
 //    of every 8-bit digit position;
-//  * one kernel per digit: a partition of 4096 keys is ranked in registers and
+//  * one kernel per digit: a partition of 8192 keys is ranked in registers and
 //    shared memory (warp match-any ranking, stable), publishes its digit
 //    counts, resolves its global digit offsets by decoupled look-back over the
 //    preceding partitions, and scatters through shared memory so each digit's
@@ -17,6 +17,7 @@
 // SF_DEV_ERR_TIMEOUT in the error word and carries on, so a lost predecessor
 // can corrupt the result but never hang the GPU.
 #include <cstdint>
+#include <type_traits>
 #include <string>
 #include "sf_handles.h"
 
@@ -31,8 +32,18 @@ constexpr int kRadix = 1 << kRadixBits;
 constexpr int kHistWords = 1024;  // passes x bins <= 1024 for every width
 constexpr int kThreads = 256;
 constexpr int kItems = 16;
-constexpr int kTile = kThreads * kItems;  // 4096 keys per partition
 constexpr int kWarps = kThreads / 32;
+// Digit passes: partitions of THREADS x 16 keys. The look-back chain across
+// partitions bounds a large pass (a partition publishes its inclusive prefix
+// only after its own look-back), so from kWidePassN keys on the partitions
+// are 8192 keys of 512 threads (half the chain: 10M keys 0.47 -> 0.44 ms);
+// smaller sorts keep 4096-key partitions of 256 threads, whose single
+// partitions finish sooner (1k-500k keys 12-17% faster than the wide form).
+// The keys and values staged for the scatter are dynamic shared memory.
+constexpr uint32_t kWidePassN = 1u << 21;
+constexpr int kMinPassTile = 256 * kItems;  // look-back space is sized for it
+template <int THREADS>
+constexpr size_t pass_smem() { return 2 * (size_t)THREADS * kItems * 4; }
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kCountMask = (1u << 30) - 1u;
@@ -195,30 +206,32 @@ __global__ __launch_bounds__(kThreads) void radix_histogram_kernel(
 }
 
 // One BITS-bit digit pass. `vals_iota` substitutes vals_in[i] = i.
-template <int BITS>
-__global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
+template <int BITS, int THREADS>
+__global__ __launch_bounds__(THREADS, THREADS >= 512 ? 2 : 4) void onesweep_pass_kernel(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, const uint32_t* n_dev,
     uint32_t n_static, uint32_t shift, uint32_t digit_mask, const uint32_t* __restrict__ pass_hist,
     uint32_t* lookback, uint32_t* ticket, uint32_t* err, int vals_iota, int write_keys, LookbackKnobs knobs) {
     constexpr uint32_t R = 1u << BITS;
+    constexpr int kPassThreads = THREADS, kPassWarps = THREADS / 32, kPassTile = THREADS * kItems;
     __shared__ uint32_t s_part;
-    __shared__ uint32_t s_warp_hist[kWarps][R];
+    __shared__ uint32_t s_warp_hist[kPassWarps][R];
     __shared__ uint32_t s_local_start[R];
     __shared__ uint32_t s_global_base[R];
-    __shared__ uint32_t s_scan[kWarps];
-    __shared__ uint32_t s_keys[kTile];
-    __shared__ uint32_t s_vals[kTile];
+    __shared__ uint32_t s_scan[kPassWarps];
+    extern __shared__ __align__(16) uint32_t s_stage[];
+    uint32_t* s_keys = s_stage;
+    uint32_t* s_vals = s_stage + kPassTile;
 
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t n = load_n(n_dev, n_static);
-    const uint32_t num_parts = (n + kTile - 1) / kTile;
+    const uint32_t num_parts = (n + kPassTile - 1) / kPassTile;
     if (tid == 0) s_part = atomicAdd(ticket, 1u);
-    for (uint32_t i = tid; i < kWarps * R; i += kThreads) (&s_warp_hist[0][0])[i] = 0;
+    for (uint32_t i = tid; i < kPassWarps * R; i += kPassThreads) (&s_warp_hist[0][0])[i] = 0;
     __syncthreads();
     const uint32_t part = s_part;
     if (part >= num_parts) return;
-    const uint32_t base = part * kTile;
+    const uint32_t base = part * kPassTile;
     const uint32_t wbase = base + warp * (kItems * 32);
 
     // Keys and values are loaded together, before the ranking and the
@@ -255,7 +268,7 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
     if (tid < R) {
         uint32_t sum = 0;
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
+        for (int w = 0; w < kPassWarps; ++w) {
             const uint32_t c = s_warp_hist[w][tid];
             s_warp_hist[w][tid] = sum;
             sum += c;
@@ -275,13 +288,13 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
         if (lane == 31) s_scan[warp] = v;
         __syncthreads();
         if (tid < 32) {
-            uint32_t w = tid < (uint32_t)kWarps ? s_scan[tid] : 0u;
+            uint32_t w = tid < (uint32_t)kPassWarps ? s_scan[tid] : 0u;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
                 if (lane >= (uint32_t)o) w += t;
             }
-            if (tid < (uint32_t)kWarps) s_scan[tid] = w;
+            if (tid < (uint32_t)kPassWarps) s_scan[tid] = w;
         }
         __syncthreads();
         if (tid < R) s_local_start[tid] = v - digit_total + (warp ? s_scan[warp - 1] : 0u);
@@ -300,13 +313,13 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
         if (lane == 31) s_scan[warp] = v;
         __syncthreads();
         if (tid < 32) {
-            uint32_t w = tid < (uint32_t)kWarps ? s_scan[tid] : 0u;
+            uint32_t w = tid < (uint32_t)kPassWarps ? s_scan[tid] : 0u;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
                 if (lane >= (uint32_t)o) w += t;
             }
-            if (tid < (uint32_t)kWarps) s_scan[tid] = w;
+            if (tid < (uint32_t)kPassWarps) s_scan[tid] = w;
         }
         __syncthreads();
         gstart = v - h + (warp ? s_scan[warp - 1] : 0u);
@@ -335,8 +348,8 @@ __global__ __launch_bounds__(kThreads, 4) void onesweep_pass_kernel(
         }
     }
     __syncthreads();
-    const uint32_t cnt = min((uint32_t)kTile, n - base);
-    for (uint32_t j = tid; j < cnt; j += kThreads) {
+    const uint32_t cnt = min((uint32_t)kPassTile, n - base);
+    for (uint32_t j = tid; j < cnt; j += kPassThreads) {
         const uint32_t key = s_keys[j];
         const uint32_t d = (key >> shift) & digit_mask;
         const uint32_t out = s_global_base[d] + j;
@@ -492,7 +505,7 @@ __global__ __launch_bounds__(kThreads) void scan_kernel(
 uint32_t radix_passes(uint32_t bits, uint32_t digit_bits) { return (bits + digit_bits - 1) / digit_bits; }
 
 size_t radix_temp_bytes(uint32_t max_elems, uint32_t max_passes) {
-    const size_t parts = (max_elems + kTile - 1) / kTile;
+    const size_t parts = (max_elems + kMinPassTile - 1) / kMinPassTile;
     // hist [1024] + tickets [16] + lookback [passes][parts][256]: 32-bit keys
     // at 8-bit digits (4 passes x 256 bins) need the most, and every narrower
     // digit (passes x bins <= 1024) fits the same space.
@@ -513,7 +526,9 @@ cudaError_t radix_sort_bits(const uint32_t* keys_in, const uint32_t* vals_in, ui
     uint32_t* hist = reinterpret_cast<uint32_t*>(t);
     uint32_t* tickets = reinterpret_cast<uint32_t*>(t + kHistWords * 4);
     uint32_t* lookback = reinterpret_cast<uint32_t*>(t + kHistWords * 4 + 64);
-    const size_t parts = (grid_n + kTile - 1) / kTile;
+    const bool wide = grid_n >= kWidePassN;
+    const uint32_t tile = (wide ? 512u : 256u) * kItems;
+    const size_t parts = (grid_n + tile - 1) / tile;
     cudaError_t e = cudaMemsetAsync(temp, 0, kHistWords * 4 + 64 + passes * parts * R * 4, stream);
     if (e != cudaSuccess) return e;
     if (parts == 0) { *out_in_b = 0; return cudaSuccess; }
@@ -521,23 +536,32 @@ cudaError_t radix_sort_bits(const uint32_t* keys_in, const uint32_t* vals_in, ui
                                                              (size_t)sm_count * 4);
     radix_histogram_kernel<BITS><<<std::max(hist_blocks, 1u), kThreads, 0, stream>>>(
         keys_in, n_dev, n, passes, bits, hist);
-    const uint32_t* kin = keys_in;
-    const uint32_t* vin = vals_in;
     int in_b = 0;
-    for (uint32_t p = 0; p < passes; ++p) {
-        const uint32_t shift = p * BITS;
-        const uint32_t w = std::min<uint32_t>(bits - shift, BITS);
-        uint32_t* kout = (p % 2 == 0) ? keys_a : keys_b;
-        uint32_t* vout = (p % 2 == 0) ? vals_a : vals_b;
-        const bool wk = write_keys || (p + 1 < passes);
-        onesweep_pass_kernel<BITS><<<(uint32_t)parts, kThreads, 0, stream>>>(
-            kin, vin, kout, vout, n_dev, n, shift, (1u << w) - 1u, hist + p * R,
-            lookback + (size_t)p * parts * R, tickets + p, err, (vals_iota && p == 0) ? 1 : 0,
-            wk ? 1 : 0, knobs);
-        kin = kout;
-        vin = vout;
-        in_b = (p % 2 == 1);
-    }
+    auto run_passes = [&](auto threads) -> cudaError_t {
+        constexpr int TH = decltype(threads)::value;
+        cudaError_t e2 = cudaFuncSetAttribute(onesweep_pass_kernel<BITS, TH>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_smem<TH>());
+        if (e2 != cudaSuccess) return e2;
+        const uint32_t* kin = keys_in;
+        const uint32_t* vin = vals_in;
+        for (uint32_t p = 0; p < passes; ++p) {
+            const uint32_t shift = p * BITS;
+            const uint32_t w = std::min<uint32_t>(bits - shift, BITS);
+            uint32_t* kout = (p % 2 == 0) ? keys_a : keys_b;
+            uint32_t* vout = (p % 2 == 0) ? vals_a : vals_b;
+            const bool wk = write_keys || (p + 1 < passes);
+            onesweep_pass_kernel<BITS, TH><<<(uint32_t)parts, TH, pass_smem<TH>(), stream>>>(
+                kin, vin, kout, vout, n_dev, n, shift, (1u << w) - 1u, hist + p * R,
+                lookback + (size_t)p * parts * R, tickets + p, err, (vals_iota && p == 0) ? 1 : 0,
+                wk ? 1 : 0, knobs);
+            kin = kout;
+            vin = vout;
+            in_b = (p % 2 == 1);
+        }
+        return cudaSuccess;
+    };
+    e = wide ? run_passes(std::integral_constant<int, 512>{}) : run_passes(std::integral_constant<int, 256>{});
+    if (e != cudaSuccess) return e;
     *out_in_b = in_b;
     note_launches(1 + passes);
     return cudaGetLastError();
