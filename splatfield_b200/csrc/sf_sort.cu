@@ -6,8 +6,9 @@
 // "Onesweep: A Faster Least Significant Digit Radix Sort for GPUs", 2022):
 //  * one upfront kernel reads the keys once and builds the 256-bin histogram
 //    of every 8-bit digit position;
-//  * one kernel per digit: a partition of 8192 keys is ranked in registers and
-//    shared memory (warp match-any ranking, stable), publishes its digit
+//  * one kernel per digit: a partition of 4096 keys (8192 from 2M keys on)
+//    is ranked in registers and shared memory (stable warp ranking by one
+//    ballot per digit bit), publishes its digit
 //    counts, resolves its global digit offsets by decoupled look-back over the
 //    preceding partitions, and scatters through shared memory so each digit's
 //    run is written contiguously.
